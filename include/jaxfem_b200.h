@@ -1,0 +1,212 @@
+/*
+ * jaxfem_b200.h -- C ABI of the B200 (sm_100a) HEX8 assemble-and-solve library.
+ *
+ * The reference (JAX-FEM) is pure Python: its hot path is a chain of Python
+ * functions with no foreign-function boundary.  Each entry point below
+ * replaces one of those functions; the comment above it cites the reference
+ * interface (file:line inside the reference project) whose role it takes.
+ *
+ * Conventions
+ *  - Plain pointers and sizes only.  Pointers named d_* are device pointers,
+ *    h_* are host pointers.  `stream` is a cudaStream_t passed as void*
+ *    (NULL = legacy default stream).
+ *  - Every function returns an int status: FEM_OK (0) or a negative code.
+ *    No exception crosses the ABI.  fem_last_error() returns a message for
+ *    the last failure on the calling thread.
+ *  - The caller owns every buffer.  Workspaces are passed in with their size
+ *    (query with the *_workspace_bytes functions).  A workspace must not be
+ *    shared by two calls that may run concurrently.
+ *  - Layouts: points (num_nodes,3) f64 row-major; cells (num_cells,8) int32
+ *    in VTK/meshio HEX8 order; dof = node*vec + component; block-CSR (BSR)
+ *    matrices with vec x vec row-major blocks, sorted columns per block row.
+ *  - Per-quadrature-point data is (num_cells, 8, ...) with the quadrature
+ *    points in basix order (2x2x2 Gauss-Legendre on [0,1]^3, x slowest).
+ */
+#ifndef JAXFEM_B200_H
+#define JAXFEM_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define FEM_API __attribute__((visibility("default")))
+#else
+#define FEM_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------ */
+#define FEM_OK 0
+#define FEM_ERR_ARG (-1)           /* invalid argument / unsupported combination */
+#define FEM_ERR_CUDA (-2)          /* a CUDA runtime call failed */
+#define FEM_ERR_NOT_CONVERGED (-3) /* Krylov hit maxiter before the tolerance */
+#define FEM_ERR_BREAKDOWN (-4)     /* Krylov breakdown (p.Ap <= 0, rho == 0, ...) */
+#define FEM_ERR_NONFINITE (-5)     /* NaN/Inf met in a reduction */
+#define FEM_ERR_CAPACITY (-6)      /* output buffer too small */
+
+/* ---- constitutive laws (the registered replacements for get_tensor_map) --
+ * Each law maps the displacement gradient at a quadrature point to the
+ * stress of the weak form, with its exact (consistent) tangent.
+ *   FEM_LAW_LAPLACE     P = grad u                       params: -
+ *   FEM_LAW_LINEAR      sigma = lmbda tr(eps) I + 2 mu eps    params: E, nu
+ *   FEM_LAW_SIMP        as LINEAR with E = Emin + (E0-Emin) theta^penal
+ *                       params: E0, Emin, nu, penal; ivar0 = theta (C,8)
+ *   FEM_LAW_NEO_HOOKEAN P = dpsi/dF, psi = mu/2 (J^-2/3 I1 - 3) + kappa/2 (J-1)^2
+ *                       params: E, nu; ivar0 = optional psi scale (C,8) or NULL
+ *   FEM_LAW_J2          small-strain radial return, linear isotropic hardening
+ *                       params: E, nu, sigma_y, H;
+ *                       ivar0 = sigma_old (C,8,3,3), ivar1 = eps_old (C,8,3,3),
+ *                       ivar2 = alpha_old (C,8)
+ * ------------------------------------------------------------------------ */
+#define FEM_LAW_LAPLACE 0
+#define FEM_LAW_LINEAR 1
+#define FEM_LAW_SIMP 2
+#define FEM_LAW_NEO_HOOKEAN 3
+#define FEM_LAW_J2 4
+
+/* Krylov methods and preconditioners. */
+#define FEM_KRYLOV_CG 0
+#define FEM_KRYLOV_BICGSTAB 1
+#define FEM_PRECOND_NONE 0
+#define FEM_PRECOND_JACOBI 1
+#define FEM_PRECOND_BLOCK_JACOBI 2
+
+/* Library version string and a message for the last failure on this thread. */
+FEM_API const char* fem_version(void);
+FEM_API const char* fem_last_error(void);
+/* Number of kernels this library has launched since load (all threads). */
+FEM_API int64_t fem_launch_count(void);
+
+/* ---- sparsity pattern (host, one-off setup) -----------------------------
+ * Replaces the COO pattern of Problem.__post_init__ (problem.py:86-107) and
+ * PETSc's setPreallocationCOO (solver.py:469-475): instead of num_cells*576
+ * duplicated (I, J) pairs it builds the node-adjacency block-CSR pattern and a
+ * cell -> block scatter map, so assembly never sorts.
+ *   pass 1: h_col_idx == NULL  -> fills h_row_ptr (num_nodes+1), *h_nnzb
+ *   pass 2: h_col_idx != NULL  -> fills h_col_idx (capacity >= nnzb),
+ *           h_scatter (num_cells*64: block index of local pair (a,b) at
+ *           [c*64 + a*8 + b]) and h_diag (num_nodes: index of block (n,n)).
+ * ------------------------------------------------------------------------ */
+FEM_API int fem_bsr_pattern(const int32_t* h_cells, int64_t num_cells, int64_t num_nodes,
+                    int32_t* h_row_ptr, int64_t* h_nnzb, int32_t* h_col_idx,
+                    int64_t col_capacity, int32_t* h_scatter, int32_t* h_diag);
+
+/* ---- cell assembly ------------------------------------------------------
+ * Replaces Problem.newton_update / compute_residual (problem.py:439-491): the
+ * per-cell weak-form kernel and its jacfwd (problem.py:189-214, 262-266,
+ * 299-301), the residual scatter (problem.py:426-437) and the PETSc COO value
+ * insertion + zeroRows of get_A (solver.py:485-491).
+ *
+ * Residual:   d_res[dof] = sum_cells int P(grad u) : grad v   (zeroed first)
+ * Tangent:    d_vals (BSR, value type per suffix) = dR/du with Dirichlet rows
+ *             AND columns eliminated (unit diagonal), zeroed first.
+ * Lift:       d_lift = K_full * d_dvec restricted to free rows, where d_dvec
+ *             holds the prescribed Dirichlet increment (zero at free dofs);
+ *             the eliminated system A x = b with b_free = -(R_free + lift),
+ *             b_bc = dvec has the solution of the reference's row-zeroed
+ *             system (solver.py:390-421) while staying symmetric for CG.
+ * Any of d_res / d_lift / d_vals may be NULL to skip that output.  d_bc_mask
+ * (uint8 per dof, 1 = Dirichlet) may be NULL (no elimination).
+ * d_params: host array of law parameters (see FEM_LAW_*), n_params entries.
+ * d_ivar0..2: per-law internal variables (device, f64) or NULL.
+ * ------------------------------------------------------------------------ */
+FEM_API int fem_assemble_f64(int law, const double* h_params, int n_params, int vec,
+                     int64_t num_cells, int64_t num_nodes, const int32_t* d_cells,
+                     const double* d_points, const double* d_u,
+                     const double* d_ivar0, const double* d_ivar1, const double* d_ivar2,
+                     const int32_t* d_scatter, const int32_t* d_diag, int64_t nnzb,
+                     const uint8_t* d_bc_mask, const double* d_dvec,
+                     double* d_res, double* d_lift, double* d_vals, void* stream);
+/* Same with the tangent computed and stored in FP32 (mixed-precision path).
+ * d_res / d_lift stay FP64 but are computed in FP32 arithmetic here; the
+ * mixed path takes its Newton residual from a residual-only f64 call. */
+FEM_API int fem_assemble_f32(int law, const double* h_params, int n_params, int vec,
+                     int64_t num_cells, int64_t num_nodes, const int32_t* d_cells,
+                     const double* d_points, const double* d_u,
+                     const double* d_ivar0, const double* d_ivar1, const double* d_ivar2,
+                     const int32_t* d_scatter, const int32_t* d_diag, int64_t nnzb,
+                     const uint8_t* d_bc_mask, const double* d_dvec,
+                     double* d_res, double* d_lift, float* d_vals, void* stream);
+
+/* ---- J2 state commit ----------------------------------------------------
+ * Replaces the reference plasticity update (test_plasticity.py:67-78 with
+ * fe.py:366-382): at every quadrature point run the return map at the
+ * converged u and write sigma_new, eps_new = sym grad u, alpha_new. */
+FEM_API int fem_j2_commit(const double* h_params, int n_params, int64_t num_cells,
+                  const int32_t* d_cells, const double* d_points, const double* d_u,
+                  const double* d_sigma_old, const double* d_eps_old, const double* d_alpha_old,
+                  double* d_sigma_new, double* d_eps_new, double* d_alpha_new, void* stream);
+
+/* ---- adjoint parameter VJP ----------------------------------------------
+ * Replaces jax.vjp of the BC-applied residual w.r.t. internal variables in
+ * implicit_vjp (solver.py:1340-1356, 1376-1378):
+ *   d_grad[c,q] = - (dR/dtheta_{c,q})^T lambda
+ * for the law's per-quad scalar parameter (SIMP: theta; NEO_HOOKEAN: psi
+ * scale).  lambda must be zero at Dirichlet dofs (their residual rows do not
+ * depend on theta).  d_grad is (num_cells, 8) f64, overwritten. */
+FEM_API int fem_param_vjp_f64(int law, const double* h_params, int n_params, int64_t num_cells,
+                      const int32_t* d_cells, const double* d_points, const double* d_u,
+                      const double* d_ivar0, const double* d_lambda, double* d_grad,
+                      void* stream);
+
+/* ---- block-CSR operators ------------------------------------------------
+ * Replace the BCOO mat-vec inside jax.scipy bicgstab (solver.py:63-92). */
+FEM_API int fem_bsr_spmv_f64(int vec, int64_t n_brows, const int32_t* d_row_ptr, const int32_t* d_col_idx,
+                     const double* d_vals, const double* d_x, double* d_y, void* stream);
+FEM_API int fem_bsr_spmv_f32(int vec, int64_t n_brows, const int32_t* d_row_ptr, const int32_t* d_col_idx,
+                     const float* d_vals, const float* d_x, float* d_y, void* stream);
+/* r = b - A x with FP32 matrix values, FP64 vectors and FP64 accumulation
+ * (the refinement residual of the mixed path). */
+FEM_API int fem_bsr_residual_mixed(int vec, int64_t n_brows, const int32_t* d_row_ptr,
+                           const int32_t* d_col_idx, const float* d_vals, const double* d_x,
+                           const double* d_b, double* d_r, void* stream);
+
+/* ---- Krylov solvers -----------------------------------------------------
+ * Replace linear_solver / jax_solve (solver.py:63-92, 261-284): solve
+ * A x = b to ||b - A x|| <= max(rtol ||b||, atol) with the true (unpreconditioned)
+ * residual, starting from the x passed in.  The iteration runs on the device;
+ * the host polls a status word every `check_every` iterations.
+ * *h_iters and *h_relres receive the iteration count and ||r||/||b||.
+ * Returns FEM_ERR_NOT_CONVERGED / FEM_ERR_BREAKDOWN / FEM_ERR_NONFINITE with
+ * x holding the last iterate.
+ * _f64: values/vectors f64.  _f32: values/vectors f32, dot products and
+ * their reductions in f64.  d_work must hold fem_krylov_workspace_bytes(). */
+FEM_API size_t fem_krylov_workspace_bytes(int method, int precond, int vec, int64_t n_brows, int fp32);
+FEM_API int fem_krylov_solve_f64(int method, int precond, int vec, int64_t n_brows,
+                         const int32_t* d_row_ptr, const int32_t* d_col_idx,
+                         const int32_t* d_diag, const double* d_vals, const double* d_b,
+                         double* d_x, double rtol, double atol, int maxiter, int check_every,
+                         void* d_work, size_t work_bytes, int* h_iters, double* h_relres,
+                         void* stream);
+FEM_API int fem_krylov_solve_f32(int method, int precond, int vec, int64_t n_brows,
+                         const int32_t* d_row_ptr, const int32_t* d_col_idx,
+                         const int32_t* d_diag, const float* d_vals, const float* d_b,
+                         float* d_x, double rtol, double atol, int maxiter, int check_every,
+                         void* d_work, size_t work_bytes, int* h_iters, double* h_relres,
+                         void* stream);
+
+/* ---- vector helpers of the Newton loop ----------------------------------
+ * fem_newton_rhs: the BC handling of newton_update_helper + newton_step
+ * (solver.py:290-304, 390-409).  With R = res + f_ext:
+ *   d_rbc[dof] = R[dof] at free dofs, u[dof] - ubc[dof] at Dirichlet dofs
+ *               (the reference's BC-applied residual vector, whose norm is the
+ *               Newton criterion)
+ *   d_rhs[dof] = -(R + lift) at free dofs, ubc - u at Dirichlet dofs
+ * and *h_norm2 (optional, synchronous) = ||d_rbc||^2 in f64. */
+FEM_API int fem_newton_rhs(int64_t ndofs, const double* d_res, const double* d_fext,
+                   const double* d_lift, const uint8_t* d_bc_mask, const double* d_u,
+                   const double* d_ubc, double* d_rbc, double* d_rhs, double* h_norm2,
+                   void* d_work, size_t work_bytes, void* stream);
+/* Deterministic f64 dot product: *h_out = x . y (synchronous). d_work needs
+ * fem_dot_workspace_bytes(n) bytes (per-block partial sums). */
+FEM_API size_t fem_dot_workspace_bytes(int64_t n);
+FEM_API int fem_dot_f64(int64_t n, const double* d_x, const double* d_y, double* h_out,
+                void* d_work, size_t work_bytes, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* JAXFEM_B200_H */

@@ -1,0 +1,20 @@
+"""jax_fem_b200: JAX-FEM's HEX8 assemble-and-solve path on B200 (sm_100a).
+
+Drop-in for the reference's ``Problem`` / ``solver`` / ``ad_wrapper``
+(jax_fem/problem.py, jax_fem/solver.py): Python host code on PyTorch calls
+hand-written CUDA kernels in ``lib/libjaxfem_b200.so`` through a C ABI
+(include/jaxfem_b200.h).  There is no CPU fallback.
+
+The package directory is ``jax-fem_b200/``; it is imported under the module
+name ``jax_fem_b200`` by ``load_package()`` in the repository root's
+``__graft_entry__.py`` (a hyphen cannot appear in an import statement).
+"""
+from . import _native
+from .generate_mesh import Mesh, box_mesh, get_meshio_cell_type
+from .laws import J2Plasticity, Laplace, LinearElastic, NeoHookean, SIMPElastic
+from .problem import BSRMatrix, Problem, compliance
+from .solver import ad_wrapper, get_A, solver
+
+__all__ = ["Mesh", "box_mesh", "get_meshio_cell_type", "Problem", "solver", "ad_wrapper", "get_A",
+           "BSRMatrix", "compliance", "Laplace", "LinearElastic", "SIMPElastic", "NeoHookean",
+           "J2Plasticity", "_native"]

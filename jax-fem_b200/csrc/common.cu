@@ -1,0 +1,34 @@
+// Error reporting, launch accounting and version of the jaxfem_b200 library.
+#include <cstdarg>
+
+#include "common.cuh"
+
+namespace fem {
+
+static thread_local char g_err[1024] = "";
+
+void set_error(const char* fmt, ...) {
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(g_err, sizeof(g_err), fmt, ap);
+  va_end(ap);
+}
+
+std::atomic<int64_t>& launch_counter() {
+  static std::atomic<int64_t> n{0};
+  return n;
+}
+
+double* host_mailbox() {
+  static double* p = nullptr;
+  if (p == nullptr) {
+    if (cudaMallocHost(&p, 64 * sizeof(double)) != cudaSuccess) p = nullptr;
+  }
+  return p;
+}
+
+}  // namespace fem
+
+extern "C" const char* fem_version(void) { return "jaxfem_b200 0.1 (sm_100a)"; }
+extern "C" const char* fem_last_error(void) { return fem::g_err; }
+extern "C" int64_t fem_launch_count(void) { return fem::launch_counter().load(); }

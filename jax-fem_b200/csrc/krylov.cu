@@ -1,0 +1,562 @@
+// Preconditioned CG and BiCGSTAB on block-CSR matrices, iterating on the
+// device.  Replaces jax_solve / linear_solver (solver.py:63-92, 261-284).
+//
+// Every scalar of the recurrences (alpha, beta, rho, omega, norms) lives in a
+// device-side state record; each reduction finishes in the last block of the
+// kernel that produced it (fixed summation order, so results are bitwise
+// reproducible) and that block also updates the scalars and the status word.
+// Kernels see a non-zero status and return at once, so the host only polls
+// the status every `check_every` iterations and never stalls the pipeline.
+//
+// CG uses 2 kernels per iteration: the search direction p = z + beta p_old is
+// formed on the fly inside the SpMV (ping-pong buffers avoid read/write races
+// between neighbouring rows), and the update kernel applies the Jacobi /
+// 3x3 block-Jacobi preconditioner while it reduces r.z and r.r.
+#include "sparse.cuh"
+
+namespace fem {
+namespace {
+
+enum : int { ST_RUNNING = 0, ST_CONVERGED = 1 };
+
+struct KState {
+  double rz, rr, pq, alpha, beta, tol2, bnorm2;
+  double rho, omega;
+  int iter, status, maxiter, pad;
+};
+
+template <typename T>
+struct KVecs {
+  T *r, *z, *p0, *p1, *q;                 // CG
+  T *rhat, *p, *phat, *v, *s, *shat, *t;  // BiCGSTAB (p/q/r reused where possible)
+  T* minv;                                // preconditioner (n or n*VEC values)
+};
+
+__device__ __forceinline__ bool finite_d(double x) { return isfinite(x); }
+
+// ---- preconditioner setup -------------------------------------------------
+template <int VEC, typename T>
+__global__ void precond_setup_kernel(int precond, int64_t n_brows, const int32_t* diag,
+                                     const T* vals, T* minv) {
+  const int64_t nd = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (nd >= n_brows) return;
+  const T* B = vals + int64_t(diag[nd]) * VEC * VEC;
+  if (precond == FEM_PRECOND_JACOBI || VEC == 1) {
+#pragma unroll
+    for (int i = 0; i < VEC; ++i) {
+      const double d = double(B[i * VEC + i]);
+      minv[nd * VEC + i] = T(d != 0.0 ? 1.0 / d : 1.0);
+    }
+  } else {
+    // 3x3 inverse in f64
+    double a[3][3];
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+      for (int j = 0; j < 3; ++j) a[i][j] = double(B[i * 3 + j]);
+    const double c00 = a[1][1] * a[2][2] - a[1][2] * a[2][1];
+    const double c01 = a[1][2] * a[2][0] - a[1][0] * a[2][2];
+    const double c02 = a[1][0] * a[2][1] - a[1][1] * a[2][0];
+    const double det = a[0][0] * c00 + a[0][1] * c01 + a[0][2] * c02;
+    const double id = 1.0 / det;
+    T* o = minv + nd * 9;
+    o[0] = T(c00 * id);
+    o[3] = T(c01 * id);
+    o[6] = T(c02 * id);
+    o[1] = T((a[0][2] * a[2][1] - a[0][1] * a[2][2]) * id);
+    o[4] = T((a[0][0] * a[2][2] - a[0][2] * a[2][0]) * id);
+    o[7] = T((a[0][1] * a[2][0] - a[0][0] * a[2][1]) * id);
+    o[2] = T((a[0][1] * a[1][2] - a[0][2] * a[1][1]) * id);
+    o[5] = T((a[0][2] * a[1][0] - a[0][0] * a[1][2]) * id);
+    o[8] = T((a[0][0] * a[1][1] - a[0][1] * a[1][0]) * id);
+  }
+}
+
+// z_node = M^{-1} r_node
+template <int VEC, typename T>
+__device__ __forceinline__ void apply_precond(int precond, int64_t nd, const T* minv, const T r[VEC],
+                                              T z[VEC]) {
+  if (precond == FEM_PRECOND_NONE) {
+#pragma unroll
+    for (int i = 0; i < VEC; ++i) z[i] = r[i];
+  } else if (precond == FEM_PRECOND_JACOBI || VEC == 1) {
+#pragma unroll
+    for (int i = 0; i < VEC; ++i) z[i] = minv[nd * VEC + i] * r[i];
+  } else {
+    const T* m = minv + nd * 9;
+#pragma unroll
+    for (int i = 0; i < 3; ++i) z[i] = m[i * 3] * r[0] + m[i * 3 + 1] * r[1] + m[i * 3 + 2] * r[2];
+  }
+}
+
+// r = b - A x
+template <int VEC, typename T>
+__global__ void __launch_bounds__(kRowThreads) kr_residual_kernel(int64_t n_brows, const int32_t* rp,
+                                                                 const int32_t* ci, const T* vals,
+                                                                 const T* __restrict__ x,
+                                                                 const T* b, T* r) {
+  const int lane = threadIdx.x & 31;
+  const int64_t w0 = int64_t(blockIdx.x) * (kRowThreads / 32) + (threadIdx.x >> 5);
+  const int64_t ws = int64_t(gridDim.x) * (kRowThreads / 32);
+  for (int64_t row = w0; row < n_brows; row += ws) {
+    double out[VEC];
+    bsr_row<VEC, T, double>(row, lane, rp, ci, vals, [&](int64_t i) { return x[i]; }, out);
+    if (lane < VEC) {
+      double o = out[0];
+#pragma unroll
+      for (int k = 1; k < VEC; ++k)
+        if (lane == k) o = out[k];
+      r[row * VEC + lane] = T(double(b[row * VEC + lane]) - o);
+    }
+  }
+}
+
+// z = M r; rz = r.z, rr = r.r, bb = b.b; initial status.
+template <int VEC, typename T>
+__global__ void cg_init_kernel(int precond, int64_t n_brows, const T* minv, const T* r, T* z,
+                               const T* b, double* partials, unsigned int* counter, KState* S,
+                               double rtol, double atol) {
+  double v[3] = {0.0, 0.0, 0.0};
+  for (int64_t nd = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; nd < n_brows;
+       nd += int64_t(gridDim.x) * blockDim.x) {
+    T rn[VEC], zn[VEC];
+#pragma unroll
+    for (int i = 0; i < VEC; ++i) rn[i] = r[nd * VEC + i];
+    apply_precond<VEC, T>(precond, nd, minv, rn, zn);
+#pragma unroll
+    for (int i = 0; i < VEC; ++i) {
+      if (z != r) z[nd * VEC + i] = zn[i];
+      const double bi = double(b[nd * VEC + i]);
+      v[0] = fma(double(rn[i]), double(zn[i]), v[0]);
+      v[1] = fma(double(rn[i]), double(rn[i]), v[1]);
+      v[2] = fma(bi, bi, v[2]);
+    }
+  }
+  double tot[3];
+  if (last_block_reduce<3>(v, partials, counter, tot)) {
+    S->rz = tot[0];
+    S->rr = tot[1];
+    S->bnorm2 = tot[2];
+    const double t1 = rtol * rtol * tot[2], t2 = atol * atol;
+    S->tol2 = t1 > t2 ? t1 : t2;
+    S->beta = 0.0;
+    S->rho = tot[0];
+    S->omega = 1.0;
+    S->alpha = 1.0;
+    S->iter = 0;
+    if (!finite_d(tot[0]) || !finite_d(tot[1]) || !finite_d(tot[2]))
+      S->status = FEM_ERR_NONFINITE;
+    else if (tot[1] <= S->tol2)
+      S->status = ST_CONVERGED;
+    else if (S->maxiter <= 0)
+      S->status = FEM_ERR_NOT_CONVERGED;
+    else
+      S->status = ST_RUNNING;
+  }
+}
+
+// CG step 1: p_new = z + beta p_old (own rows), q = A p_new, pq = p_new . q
+template <int VEC, typename T>
+__global__ void __launch_bounds__(kRowThreads) cg_spmv_kernel(int64_t n_brows, const int32_t* rp,
+                                                             const int32_t* ci, const T* vals,
+                                                             const T* __restrict__ z,
+                                                             const T* __restrict__ p_old, T* p_new,
+                                                             T* q, double* partials,
+                                                             unsigned int* counter, KState* S) {
+  if (S->status != ST_RUNNING) return;
+  const T beta = T(S->beta);
+  const int lane = threadIdx.x & 31;
+  const int64_t w0 = int64_t(blockIdx.x) * (kRowThreads / 32) + (threadIdx.x >> 5);
+  const int64_t ws = int64_t(gridDim.x) * (kRowThreads / 32);
+  double v[1] = {0.0};
+  for (int64_t row = w0; row < n_brows; row += ws) {
+    double out[VEC];
+    bsr_row<VEC, T, double>(row, lane, rp, ci, vals,
+                            [&](int64_t i) { return z[i] + beta * p_old[i]; }, out);
+    if (lane < VEC) {
+      double o = out[0];
+#pragma unroll
+      for (int k = 1; k < VEC; ++k)
+        if (lane == k) o = out[k];
+      const int64_t i = row * VEC + lane;
+      const T pn = z[i] + beta * p_old[i];
+      p_new[i] = pn;
+      const T qo = T(o);
+      q[i] = qo;
+      v[0] = fma(double(pn), double(qo), v[0]);
+    }
+  }
+  double tot[1];
+  if (last_block_reduce<1>(v, partials, counter, tot)) {
+    S->pq = tot[0];
+    if (!finite_d(tot[0]))
+      S->status = FEM_ERR_NONFINITE;
+    else if (!(tot[0] > 0.0))
+      S->status = FEM_ERR_BREAKDOWN;
+    else
+      S->alpha = S->rz / tot[0];
+  }
+}
+
+// CG step 2: x += alpha p, r -= alpha q, z = M r; rz, rr; scalar update.
+template <int VEC, typename T>
+__global__ void cg_update_kernel(int precond, int64_t n_brows, const T* minv, T* x, T* r, T* z,
+                                 const T* p, const T* q, double* partials, unsigned int* counter,
+                                 KState* S) {
+  if (S->status != ST_RUNNING) return;
+  const T alpha = T(S->alpha);
+  double v[2] = {0.0, 0.0};
+  for (int64_t nd = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; nd < n_brows;
+       nd += int64_t(gridDim.x) * blockDim.x) {
+    T rn[VEC], zn[VEC];
+#pragma unroll
+    for (int i = 0; i < VEC; ++i) {
+      const int64_t k = nd * VEC + i;
+      x[k] += alpha * p[k];
+      rn[i] = r[k] - alpha * q[k];
+      r[k] = rn[i];
+    }
+    apply_precond<VEC, T>(precond, nd, minv, rn, zn);
+#pragma unroll
+    for (int i = 0; i < VEC; ++i) {
+      if (z != r) z[nd * VEC + i] = zn[i];
+      v[0] = fma(double(rn[i]), double(zn[i]), v[0]);
+      v[1] = fma(double(rn[i]), double(rn[i]), v[1]);
+    }
+  }
+  double tot[2];
+  if (last_block_reduce<2>(v, partials, counter, tot)) {
+    S->iter += 1;
+    S->rr = tot[1];
+    if (!finite_d(tot[0]) || !finite_d(tot[1])) {
+      S->status = FEM_ERR_NONFINITE;
+    } else if (tot[1] <= S->tol2) {
+      S->status = ST_CONVERGED;
+    } else if (S->iter >= S->maxiter) {
+      S->status = FEM_ERR_NOT_CONVERGED;
+    } else if (S->rz == 0.0) {
+      S->status = FEM_ERR_BREAKDOWN;
+    } else {
+      S->beta = tot[0] / S->rz;
+      S->rz = tot[0];
+    }
+  }
+}
+
+// ---- BiCGSTAB (right-looking, as scipy/JAX bicgstab) ----------------------
+// B1: p = r + beta (p - omega v); phat = M p
+template <int VEC, typename T>
+__global__ void bicg_p_kernel(int precond, int64_t n_brows, const T* minv, const T* r, T* p,
+                              const T* v, T* phat, KState* S) {
+  if (S->status != ST_RUNNING) return;
+  const T beta = T(S->beta), omega = T(S->omega);
+  for (int64_t nd = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; nd < n_brows;
+       nd += int64_t(gridDim.x) * blockDim.x) {
+    T pn[VEC], ph[VEC];
+#pragma unroll
+    for (int i = 0; i < VEC; ++i) {
+      const int64_t k = nd * VEC + i;
+      pn[i] = r[k] + beta * (p[k] - omega * v[k]);
+      p[k] = pn[i];
+    }
+    apply_precond<VEC, T>(precond, nd, minv, pn, ph);
+#pragma unroll
+    for (int i = 0; i < VEC; ++i) phat[nd * VEC + i] = ph[i];
+  }
+}
+
+// y = A x with partial dot products of y against up to two vectors.
+// mode 0: (rhat . v) -> alpha; mode 1: (t . s, t . t) -> omega
+template <int VEC, typename T>
+__global__ void __launch_bounds__(kRowThreads) bicg_spmv_kernel(int mode, int64_t n_brows, const int32_t* rp,
+                                                               const int32_t* ci, const T* vals,
+                                                               const T* __restrict__ x, T* y,
+                                                               const T* w, double* partials,
+                                                               unsigned int* counter, KState* S) {
+  if (S->status != ST_RUNNING) return;
+  const int lane = threadIdx.x & 31;
+  const int64_t w0 = int64_t(blockIdx.x) * (kRowThreads / 32) + (threadIdx.x >> 5);
+  const int64_t wsd = int64_t(gridDim.x) * (kRowThreads / 32);
+  double v[2] = {0.0, 0.0};
+  for (int64_t row = w0; row < n_brows; row += wsd) {
+    double out[VEC];
+    bsr_row<VEC, T, double>(row, lane, rp, ci, vals, [&](int64_t i) { return x[i]; }, out);
+    if (lane < VEC) {
+      double o = out[0];
+#pragma unroll
+      for (int k = 1; k < VEC; ++k)
+        if (lane == k) o = out[k];
+      const int64_t i = row * VEC + lane;
+      const T yo = T(o);
+      y[i] = yo;
+      v[0] = fma(double(w[i]), double(yo), v[0]);
+      v[1] = fma(double(yo), double(yo), v[1]);
+    }
+  }
+  double tot[2];
+  if (last_block_reduce<2>(v, partials, counter, tot)) {
+    if (mode == 0) {
+      if (!finite_d(tot[0]))
+        S->status = FEM_ERR_NONFINITE;
+      else if (tot[0] == 0.0)
+        S->status = FEM_ERR_BREAKDOWN;
+      else
+        S->alpha = S->rho / tot[0];
+    } else {
+      if (!finite_d(tot[0]) || !finite_d(tot[1]))
+        S->status = FEM_ERR_NONFINITE;
+      else
+        S->omega = tot[1] > 0.0 ? tot[0] / tot[1] : 0.0;
+    }
+  }
+}
+
+// B3: s = r - alpha v; shat = M s
+template <int VEC, typename T>
+__global__ void bicg_s_kernel(int precond, int64_t n_brows, const T* minv, const T* r, const T* v,
+                              T* s, T* shat, KState* S) {
+  if (S->status != ST_RUNNING) return;
+  const T alpha = T(S->alpha);
+  for (int64_t nd = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; nd < n_brows;
+       nd += int64_t(gridDim.x) * blockDim.x) {
+    T sn[VEC], sh[VEC];
+#pragma unroll
+    for (int i = 0; i < VEC; ++i) {
+      const int64_t k = nd * VEC + i;
+      sn[i] = r[k] - alpha * v[k];
+      s[k] = sn[i];
+    }
+    apply_precond<VEC, T>(precond, nd, minv, sn, sh);
+#pragma unroll
+    for (int i = 0; i < VEC; ++i) shat[nd * VEC + i] = sh[i];
+  }
+}
+
+// B5: x += alpha phat + omega shat; r = s - omega t; rho_new = rhat.r, rr
+template <int VEC, typename T>
+__global__ void bicg_x_kernel(int64_t n, T* x, T* r, const T* rhat, const T* phat, const T* shat,
+                              const T* s, const T* t, double* partials, unsigned int* counter,
+                              KState* S) {
+  if (S->status != ST_RUNNING) return;
+  const T alpha = T(S->alpha), omega = T(S->omega);
+  double v[2] = {0.0, 0.0};
+  for (int64_t k = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; k < n;
+       k += int64_t(gridDim.x) * blockDim.x) {
+    x[k] += alpha * phat[k] + omega * shat[k];
+    const T rn = s[k] - omega * t[k];
+    r[k] = rn;
+    v[0] = fma(double(rhat[k]), double(rn), v[0]);
+    v[1] = fma(double(rn), double(rn), v[1]);
+  }
+  double tot[2];
+  if (last_block_reduce<2>(v, partials, counter, tot)) {
+    S->iter += 1;
+    S->rr = tot[1];
+    if (!finite_d(tot[0]) || !finite_d(tot[1])) {
+      S->status = FEM_ERR_NONFINITE;
+    } else if (tot[1] <= S->tol2) {
+      S->status = ST_CONVERGED;
+    } else if (S->iter >= S->maxiter) {
+      S->status = FEM_ERR_NOT_CONVERGED;
+    } else if (S->omega == 0.0 || S->rho == 0.0) {
+      S->status = FEM_ERR_BREAKDOWN;
+    } else {
+      S->beta = (tot[0] / S->rho) * (S->alpha / S->omega);
+      S->rho = tot[0];
+    }
+  }
+}
+
+template <typename T>
+__global__ void copy_kernel(int64_t n, const T* a, T* b) {
+  for (int64_t k = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; k < n;
+       k += int64_t(gridDim.x) * blockDim.x)
+    b[k] = a[k];
+}
+
+// ---- workspace ----------------------------------------------------------------
+inline size_t al256(size_t x) { return (x + 255) & ~size_t(255); }
+
+size_t workspace_bytes(int method, int precond, int vec, int64_t n_brows, size_t elem) {
+  const size_t n = size_t(n_brows) * vec;
+  const size_t nvec = (method == FEM_KRYLOV_CG) ? 5 : 8;
+  size_t bytes = 256 /*state*/ + 256 /*counter*/ + al256(size_t(num_sms()) * 8 * 4 * sizeof(double));
+  bytes += nvec * al256(n * elem);
+  const size_t pre = (precond == FEM_PRECOND_BLOCK_JACOBI && vec == 3) ? size_t(n_brows) * 9 : n;
+  bytes += al256(pre * elem);
+  return bytes;
+}
+
+template <int VEC, typename T>
+int solve_impl(int method, int precond, int64_t n_brows, const int32_t* rp, const int32_t* ci,
+               const int32_t* diag, const T* vals, const T* b, T* x, double rtol, double atol,
+               int maxiter, int check_every, void* work, size_t work_bytes, int* h_iters,
+               double* h_relres, cudaStream_t st) {
+  const size_t need = workspace_bytes(method, precond, VEC, n_brows, sizeof(T));
+  FEM_CHECK_ARG(work != nullptr && work_bytes >= need, "krylov workspace too small (%zu < %zu)",
+                work_bytes, need);
+  FEM_CHECK_ARG(precond == FEM_PRECOND_NONE || diag != nullptr, "preconditioner needs diag");
+  if (check_every <= 0) check_every = 16;
+  const int64_t n = n_brows * VEC;
+  char* p = static_cast<char*>(work);
+  KState* S = reinterpret_cast<KState*>(p);
+  unsigned int* counter = reinterpret_cast<unsigned int*>(p + 256);
+  double* partials = reinterpret_cast<double*>(p + 512);
+  p += 512 + al256(size_t(num_sms()) * 8 * 4 * sizeof(double));
+  auto take = [&](size_t cnt) {
+    T* q = reinterpret_cast<T*>(p);
+    p += al256(cnt * sizeof(T));
+    return q;
+  };
+  const int nvec = (method == FEM_KRYLOV_CG) ? 5 : 8;
+  T* V[8];
+  for (int i = 0; i < nvec; ++i) V[i] = take(size_t(n));
+  T* minv = take((precond == FEM_PRECOND_BLOCK_JACOBI && VEC == 3) ? size_t(n_brows) * 9 : size_t(n));
+
+  FEM_CUDA_TRY(cudaMemsetAsync(work, 0, 512, st));
+  KState init{};
+  init.maxiter = maxiter;
+  FEM_CUDA_TRY(cudaMemcpyAsync(S, &init, sizeof(KState), cudaMemcpyHostToDevice, st));
+  // cudaMemcpyAsync from pageable memory is synchronous w.r.t. the host copy,
+  // so `init` may go out of scope after this point.
+  if (precond != FEM_PRECOND_NONE) {
+    precond_setup_kernel<VEC, T><<<unsigned((n_brows + 255) / 256), 256, 0, st>>>(precond, n_brows,
+                                                                                diag, vals, minv);
+    FEM_LAUNCH_CHECK();
+  }
+  const unsigned rg = row_grid(n_brows), vg = vec_grid(n_brows), vgn = vec_grid(n);
+  T* r = V[0];
+  kr_residual_kernel<VEC, T><<<rg, kRowThreads, 0, st>>>(n_brows, rp, ci, vals, x, b, r);
+  FEM_LAUNCH_CHECK();
+
+  T *z = nullptr, *p0 = nullptr, *p1 = nullptr, *q = nullptr;
+  T *rhat = nullptr, *pp = nullptr, *phat = nullptr, *vv = nullptr, *s = nullptr, *shat = nullptr,
+    *t = nullptr;
+  if (method == FEM_KRYLOV_CG) {
+    z = (precond == FEM_PRECOND_NONE) ? r : V[1];
+    p0 = V[2];
+    p1 = V[3];
+    q = V[4];
+    FEM_CUDA_TRY(cudaMemsetAsync(p0, 0, sizeof(T) * n, st));
+    cg_init_kernel<VEC, T><<<vg, 256, 0, st>>>(precond, n_brows, minv, r, z, b, partials, counter, S,
+                                               rtol, atol);
+    FEM_LAUNCH_CHECK();
+  } else {
+    rhat = V[1];
+    pp = V[2];
+    phat = V[3];
+    vv = V[4];
+    s = V[5];
+    shat = V[6];
+    t = V[7];
+    FEM_CUDA_TRY(cudaMemsetAsync(pp, 0, sizeof(T) * n, st));
+    FEM_CUDA_TRY(cudaMemsetAsync(vv, 0, sizeof(T) * n, st));
+    copy_kernel<T><<<vgn, 256, 0, st>>>(n, r, rhat);
+    FEM_LAUNCH_CHECK();
+    // init reduces r.r and b.b; rho = rhat.r = r.r for precond NONE path
+    cg_init_kernel<VEC, T><<<vg, 256, 0, st>>>(FEM_PRECOND_NONE, n_brows, minv, r, r, b, partials,
+                                               counter, S, rtol, atol);
+    FEM_LAUNCH_CHECK();
+  }
+
+  double* mb = host_mailbox();
+  FEM_CHECK_ARG(mb != nullptr, "pinned mailbox allocation failed");
+  int status = ST_RUNNING, iters = 0;
+  double rr = 0.0, bb = 0.0;
+  int launched = 0;
+  while (true) {
+    FEM_CUDA_TRY(cudaMemcpyAsync(mb, S, sizeof(KState), cudaMemcpyDeviceToHost, st));
+    FEM_CUDA_TRY(cudaStreamSynchronize(st));
+    const KState* hs = reinterpret_cast<const KState*>(mb);
+    status = hs->status;
+    iters = hs->iter;
+    rr = hs->rr;
+    bb = hs->bnorm2;
+    if (status != ST_RUNNING || launched >= maxiter) break;
+    const int chunk = check_every < (maxiter - launched) ? check_every : (maxiter - launched);
+    for (int k = 0; k < chunk; ++k) {
+      if (method == FEM_KRYLOV_CG) {
+        cg_spmv_kernel<VEC, T><<<rg, kRowThreads, 0, st>>>(n_brows, rp, ci, vals, z, p0, p1, q,
+                                                           partials, counter, S);
+        FEM_LAUNCH_CHECK();
+        cg_update_kernel<VEC, T><<<vg, 256, 0, st>>>(precond, n_brows, minv, x, r, z, p1, q, partials,
+                                                     counter, S);
+        FEM_LAUNCH_CHECK();
+        T* tmp = p0;
+        p0 = p1;
+        p1 = tmp;
+      } else {
+        bicg_p_kernel<VEC, T><<<vg, 256, 0, st>>>(precond, n_brows, minv, r, pp, vv, phat, S);
+        FEM_LAUNCH_CHECK();
+        bicg_spmv_kernel<VEC, T><<<rg, kRowThreads, 0, st>>>(0, n_brows, rp, ci, vals, phat, vv,
+                                                             rhat, partials, counter, S);
+        FEM_LAUNCH_CHECK();
+        bicg_s_kernel<VEC, T><<<vg, 256, 0, st>>>(precond, n_brows, minv, r, vv, s, shat, S);
+        FEM_LAUNCH_CHECK();
+        bicg_spmv_kernel<VEC, T><<<rg, kRowThreads, 0, st>>>(1, n_brows, rp, ci, vals, shat, t, s,
+                                                             partials, counter, S);
+        FEM_LAUNCH_CHECK();
+        bicg_x_kernel<VEC, T><<<vgn, 256, 0, st>>>(n, x, r, rhat, phat, shat, s, t, partials,
+                                                   counter, S);
+        FEM_LAUNCH_CHECK();
+      }
+    }
+    launched += chunk;
+  }
+  if (h_iters) *h_iters = iters;
+  if (h_relres) *h_relres = bb > 0 ? sqrt(rr / bb) : sqrt(rr);
+  if (status == ST_CONVERGED) return FEM_OK;
+  if (status == ST_RUNNING) status = FEM_ERR_NOT_CONVERGED;
+  set_error("krylov: status %d after %d iterations (relres %.3e)", status, iters,
+            bb > 0 ? sqrt(rr / bb) : sqrt(rr));
+  return status;
+}
+
+template <typename T>
+int solve_dispatch(int method, int precond, int vec, int64_t n_brows, const int32_t* rp,
+                   const int32_t* ci, const int32_t* diag, const T* vals, const T* b, T* x,
+                   double rtol, double atol, int maxiter, int check_every, void* work,
+                   size_t work_bytes, int* h_iters, double* h_relres, void* stream) {
+  FEM_CHECK_ARG(vec == 1 || vec == 3, "vec must be 1 or 3");
+  FEM_CHECK_ARG(method == FEM_KRYLOV_CG || method == FEM_KRYLOV_BICGSTAB, "unknown method %d", method);
+  FEM_CHECK_ARG(precond >= FEM_PRECOND_NONE && precond <= FEM_PRECOND_BLOCK_JACOBI,
+                "unknown preconditioner %d", precond);
+  FEM_CHECK_ARG(n_brows > 0, "empty system");
+  FEM_CHECK_ARG(rtol >= 0 && atol >= 0, "negative tolerance");
+  auto st = as_stream(stream);
+  if (vec == 3)
+    return solve_impl<3, T>(method, precond, n_brows, rp, ci, diag, vals, b, x, rtol, atol, maxiter,
+                            check_every, work, work_bytes, h_iters, h_relres, st);
+  return solve_impl<1, T>(method, precond, n_brows, rp, ci, diag, vals, b, x, rtol, atol, maxiter,
+                          check_every, work, work_bytes, h_iters, h_relres, st);
+}
+
+}  // namespace
+}  // namespace fem
+
+extern "C" size_t fem_krylov_workspace_bytes(int method, int precond, int vec, int64_t n_brows,
+                                             int fp32) {
+  return fem::workspace_bytes(method, precond, vec, n_brows, fp32 ? 4 : 8);
+}
+
+extern "C" int fem_krylov_solve_f64(int method, int precond, int vec, int64_t n_brows,
+                                    const int32_t* d_row_ptr, const int32_t* d_col_idx,
+                                    const int32_t* d_diag, const double* d_vals, const double* d_b,
+                                    double* d_x, double rtol, double atol, int maxiter,
+                                    int check_every, void* d_work, size_t work_bytes, int* h_iters,
+                                    double* h_relres, void* stream) {
+  return fem::solve_dispatch<double>(method, precond, vec, n_brows, d_row_ptr, d_col_idx, d_diag,
+                                     d_vals, d_b, d_x, rtol, atol, maxiter, check_every, d_work,
+                                     work_bytes, h_iters, h_relres, stream);
+}
+
+extern "C" int fem_krylov_solve_f32(int method, int precond, int vec, int64_t n_brows,
+                                    const int32_t* d_row_ptr, const int32_t* d_col_idx,
+                                    const int32_t* d_diag, const float* d_vals, const float* d_b,
+                                    float* d_x, double rtol, double atol, int maxiter,
+                                    int check_every, void* d_work, size_t work_bytes, int* h_iters,
+                                    double* h_relres, void* stream) {
+  return fem::solve_dispatch<float>(method, precond, vec, n_brows, d_row_ptr, d_col_idx, d_diag,
+                                    d_vals, d_b, d_x, rtol, atol, maxiter, check_every, d_work,
+                                    work_bytes, h_iters, h_relres, stream);
+}

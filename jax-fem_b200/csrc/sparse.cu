@@ -1,0 +1,216 @@
+// Block-CSR SpMV, mixed-precision refinement residual, dot product and the
+// Newton right-hand side.  All HBM-streaming kernels.
+#include "sparse.cuh"
+
+namespace fem {
+namespace {
+
+template <int VEC, typename VT, typename XT, typename YT>
+__global__ void __launch_bounds__(kRowThreads) spmv_kernel(int64_t n_brows, const int32_t* rp,
+                                                          const int32_t* ci, const VT* vals,
+                                                          const XT* __restrict__ x, YT* y) {
+  const int lane = threadIdx.x & 31;
+  const int64_t w0 = int64_t(blockIdx.x) * (kRowThreads / 32) + (threadIdx.x >> 5);
+  const int64_t ws = int64_t(gridDim.x) * (kRowThreads / 32);
+  using AT = typename std::conditional<(sizeof(VT) == 8 || sizeof(XT) == 8), double, float>::type;
+  for (int64_t row = w0; row < n_brows; row += ws) {
+    AT out[VEC];
+    bsr_row<VEC, VT, AT>(row, lane, rp, ci, vals, [&](int64_t i) { return x[i]; }, out);
+    if (lane < VEC) {
+      AT o = out[0];
+#pragma unroll
+      for (int r = 1; r < VEC; ++r)
+        if (lane == r) o = out[r];
+      y[row * VEC + lane] = YT(o);
+    }
+  }
+}
+
+// r = b - A x (A f32, x/b/r f64, f64 accumulation)
+template <int VEC>
+__global__ void __launch_bounds__(kRowThreads) residual_mixed_kernel(int64_t n_brows, const int32_t* rp,
+                                                                    const int32_t* ci, const float* vals,
+                                                                    const double* __restrict__ x,
+                                                                    const double* b, double* r) {
+  const int lane = threadIdx.x & 31;
+  const int64_t w0 = int64_t(blockIdx.x) * (kRowThreads / 32) + (threadIdx.x >> 5);
+  const int64_t ws = int64_t(gridDim.x) * (kRowThreads / 32);
+  for (int64_t row = w0; row < n_brows; row += ws) {
+    double out[VEC];
+    bsr_row<VEC, float, double>(row, lane, rp, ci, vals, [&](int64_t i) { return x[i]; }, out);
+    if (lane < VEC) {
+      double o = out[0];
+#pragma unroll
+      for (int rr = 1; rr < VEC; ++rr)
+        if (lane == rr) o = out[rr];
+      r[row * VEC + lane] = b[row * VEC + lane] - o;
+    }
+  }
+}
+
+__global__ void dot_kernel(int64_t n, const double* x, const double* y, double* partials,
+                           unsigned int* counter, double* out) {
+  double v[1] = {0.0};
+  for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+       i += int64_t(gridDim.x) * blockDim.x)
+    v[0] = fma(x[i], y[i], v[0]);
+  double tot[1];
+  if (last_block_reduce<1>(v, partials, counter, tot)) *out = tot[0];
+}
+
+__global__ void newton_rhs_kernel(int64_t n, const double* res, const double* fext,
+                                  const double* lift, const uint8_t* bc, const double* u,
+                                  const double* ubc, double* rbc, double* rhs, double* partials,
+                                  unsigned int* counter, double* out) {
+  double v[1] = {0.0};
+  for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+       i += int64_t(gridDim.x) * blockDim.x) {
+    const double R = res[i] + (fext ? fext[i] : 0.0);
+    double rb, rh;
+    if (bc != nullptr && bc[i]) {
+      rb = u[i] - ubc[i];
+      rh = -rb;
+    } else {
+      rb = R;
+      rh = -(R + (lift ? lift[i] : 0.0));
+    }
+    if (rbc) rbc[i] = rb;
+    if (rhs) rhs[i] = rh;
+    v[0] = fma(rb, rb, v[0]);
+  }
+  double tot[1];
+  if (out != nullptr) {
+    if (last_block_reduce<1>(v, partials, counter, tot)) *out = tot[0];
+  }
+}
+
+}  // namespace
+}  // namespace fem
+
+using namespace fem;
+
+extern "C" int fem_bsr_spmv_f64(int vec, int64_t n_brows, const int32_t* d_row_ptr,
+                                const int32_t* d_col_idx, const double* d_vals, const double* d_x,
+                                double* d_y, void* stream) {
+  FEM_CHECK_ARG(vec == 1 || vec == 3, "vec must be 1 or 3");
+  FEM_CHECK_ARG(n_brows >= 0, "negative size");
+  if (n_brows == 0) return FEM_OK;
+  auto st = as_stream(stream);
+  if (vec == 3)
+    spmv_kernel<3, double, double, double><<<row_grid(n_brows), kRowThreads, 0, st>>>(
+        n_brows, d_row_ptr, d_col_idx, d_vals, d_x, d_y);
+  else
+    spmv_kernel<1, double, double, double><<<row_grid(n_brows), kRowThreads, 0, st>>>(
+        n_brows, d_row_ptr, d_col_idx, d_vals, d_x, d_y);
+  FEM_LAUNCH_CHECK();
+  return FEM_OK;
+}
+
+extern "C" int fem_bsr_spmv_f32(int vec, int64_t n_brows, const int32_t* d_row_ptr,
+                                const int32_t* d_col_idx, const float* d_vals, const float* d_x,
+                                float* d_y, void* stream) {
+  FEM_CHECK_ARG(vec == 1 || vec == 3, "vec must be 1 or 3");
+  FEM_CHECK_ARG(n_brows >= 0, "negative size");
+  if (n_brows == 0) return FEM_OK;
+  auto st = as_stream(stream);
+  if (vec == 3)
+    spmv_kernel<3, float, float, float><<<row_grid(n_brows), kRowThreads, 0, st>>>(
+        n_brows, d_row_ptr, d_col_idx, d_vals, d_x, d_y);
+  else
+    spmv_kernel<1, float, float, float><<<row_grid(n_brows), kRowThreads, 0, st>>>(
+        n_brows, d_row_ptr, d_col_idx, d_vals, d_x, d_y);
+  FEM_LAUNCH_CHECK();
+  return FEM_OK;
+}
+
+extern "C" int fem_bsr_residual_mixed(int vec, int64_t n_brows, const int32_t* d_row_ptr,
+                                      const int32_t* d_col_idx, const float* d_vals,
+                                      const double* d_x, const double* d_b, double* d_r,
+                                      void* stream) {
+  FEM_CHECK_ARG(vec == 1 || vec == 3, "vec must be 1 or 3");
+  FEM_CHECK_ARG(n_brows >= 0, "negative size");
+  if (n_brows == 0) return FEM_OK;
+  auto st = as_stream(stream);
+  if (vec == 3)
+    residual_mixed_kernel<3><<<row_grid(n_brows), kRowThreads, 0, st>>>(
+        n_brows, d_row_ptr, d_col_idx, d_vals, d_x, d_b, d_r);
+  else
+    residual_mixed_kernel<1><<<row_grid(n_brows), kRowThreads, 0, st>>>(
+        n_brows, d_row_ptr, d_col_idx, d_vals, d_x, d_b, d_r);
+  FEM_LAUNCH_CHECK();
+  return FEM_OK;
+}
+
+extern "C" size_t fem_dot_workspace_bytes(int64_t n) {
+  // partials for vec_grid(n) blocks + counter + result slot, 256-B aligned pieces
+  (void)n;
+  return size_t(num_sms()) * 8 * sizeof(double) + 512;
+}
+
+namespace {
+struct RedWork {
+  double* partials;
+  unsigned int* counter;
+  double* result;
+};
+int carve_red(void* d_work, size_t work_bytes, RedWork* w) {
+  const size_t need = fem_dot_workspace_bytes(0);
+  FEM_CHECK_ARG(d_work != nullptr && work_bytes >= need, "workspace too small (%zu < %zu)",
+                work_bytes, need);
+  char* p = static_cast<char*>(d_work);
+  w->counter = reinterpret_cast<unsigned int*>(p);
+  w->result = reinterpret_cast<double*>(p + 256);
+  w->partials = reinterpret_cast<double*>(p + 512);
+  return FEM_OK;
+}
+}  // namespace
+
+extern "C" int fem_dot_f64(int64_t n, const double* d_x, const double* d_y, double* h_out,
+                           void* d_work, size_t work_bytes, void* stream) {
+  FEM_CHECK_ARG(n >= 0 && h_out != nullptr, "bad arguments");
+  RedWork w;
+  int rc = carve_red(d_work, work_bytes, &w);
+  if (rc) return rc;
+  auto st = as_stream(stream);
+  FEM_CUDA_TRY(cudaMemsetAsync(w.counter, 0, 256, st));
+  FEM_CUDA_TRY(cudaMemsetAsync(w.result, 0, sizeof(double), st));
+  dot_kernel<<<vec_grid(n), 256, 0, st>>>(n, d_x, d_y, w.partials, w.counter, w.result);
+  FEM_LAUNCH_CHECK();
+  double* mb = host_mailbox();
+  FEM_CHECK_ARG(mb != nullptr, "pinned mailbox allocation failed");
+  FEM_CUDA_TRY(cudaMemcpyAsync(mb, w.result, sizeof(double), cudaMemcpyDeviceToHost, st));
+  FEM_CUDA_TRY(cudaStreamSynchronize(st));
+  *h_out = mb[0];
+  return FEM_OK;
+}
+
+extern "C" int fem_newton_rhs(int64_t ndofs, const double* d_res, const double* d_fext,
+                              const double* d_lift, const uint8_t* d_bc_mask, const double* d_u,
+                              const double* d_ubc, double* d_rbc, double* d_rhs, double* h_norm2,
+                              void* d_work, size_t work_bytes, void* stream) {
+  FEM_CHECK_ARG(ndofs >= 0 && d_res != nullptr, "bad arguments");
+  FEM_CHECK_ARG(d_bc_mask == nullptr || (d_u != nullptr && d_ubc != nullptr),
+                "BC mask needs u and ubc");
+  auto st = as_stream(stream);
+  RedWork w{nullptr, nullptr, nullptr};
+  if (h_norm2 != nullptr) {
+    int rc = carve_red(d_work, work_bytes, &w);
+    if (rc) return rc;
+    FEM_CUDA_TRY(cudaMemsetAsync(w.counter, 0, 256, st));
+    FEM_CUDA_TRY(cudaMemsetAsync(w.result, 0, sizeof(double), st));
+  }
+  if (ndofs > 0) {
+    newton_rhs_kernel<<<vec_grid(ndofs), 256, 0, st>>>(ndofs, d_res, d_fext, d_lift, d_bc_mask, d_u,
+                                                       d_ubc, d_rbc, d_rhs, w.partials, w.counter,
+                                                       w.result);
+    FEM_LAUNCH_CHECK();
+  }
+  if (h_norm2 != nullptr) {
+    double* mb = host_mailbox();
+    FEM_CHECK_ARG(mb != nullptr, "pinned mailbox allocation failed");
+    FEM_CUDA_TRY(cudaMemcpyAsync(mb, w.result, sizeof(double), cudaMemcpyDeviceToHost, st));
+    FEM_CUDA_TRY(cudaStreamSynchronize(st));
+    *h_norm2 = mb[0];
+  }
+  return FEM_OK;
+}

@@ -1,0 +1,244 @@
+"""Host-side HEX8 finite-element setup: Dirichlet and boundary-face discovery,
+face geometry and the (u-independent) body/surface load vectors.
+
+Mirrors ``FiniteElement`` (fe.py:20-322 in the reference) for what runs once
+per problem or per load step.  Nothing here is on the per-iteration path:
+cell kernels, assembly and solves run in libjaxfem_b200.
+
+User location/value/mass/surface functions are evaluated the way the
+reference's ``jax.vmap`` does -- one point at a time semantically -- but
+batched: a function is first called once with the coordinate axes as arrays
+(``point[0]`` is the vector of all x coordinates) and the batched answer is
+kept only if it agrees with point-by-point calls on a sample; otherwise it is
+called point by point.
+"""
+import numpy as np
+
+# basix hexahedron facets (vertex lists in basix numbering) and outward normals,
+# in the order the reference's face tables use (basis.py:215-240).
+_BASIX_FACETS = np.array([[0, 1, 2, 3], [0, 1, 4, 5], [0, 2, 4, 6],
+                          [1, 3, 5, 7], [2, 3, 6, 7], [4, 5, 6, 7]])
+_FACET_NORMALS = np.array([[0, 0, -1], [0, -1, 0], [-1, 0, 0],
+                           [1, 0, 0], [0, 1, 0], [0, 0, 1]], dtype=np.float64)
+# VTK <-> basix HEX8 node permutation (basis.py:53); it is its own inverse.
+_REORDER = np.array([0, 1, 3, 2, 4, 5, 7, 6])
+# basix vertex coordinates of the unit hexahedron (x fastest)
+_BASIX_VERTS = np.array([[(v >> 0) & 1, (v >> 1) & 1, (v >> 2) & 1] for v in range(8)], dtype=np.float64)
+VTK_NODE_XI = _BASIX_VERTS[_REORDER]  # reference coordinates of VTK node a
+FACE_INDS = _REORDER[_BASIX_FACETS]   # (6,4) VTK node numbers of each face
+
+_G = 0.5 / np.sqrt(3.0)
+_GAUSS = np.array([0.5 - _G, 0.5 + _G])
+
+
+def hex8_eval(xi):
+    """Shape values (n,8) and reference gradients (n,8,3) at points xi (n,3)."""
+    xi = np.atleast_2d(np.asarray(xi, dtype=np.float64))
+    X = VTK_NODE_XI
+    f = np.where(X[None] > 0.5, xi[:, None, :], 1.0 - xi[:, None, :])  # (n,8,3)
+    s = np.where(X > 0.5, 1.0, -1.0)[None]
+    vals = f.prod(axis=2)
+    grads = np.stack([s[..., 0] * f[..., 1] * f[..., 2],
+                      f[..., 0] * s[..., 1] * f[..., 2],
+                      f[..., 0] * f[..., 1] * s[..., 2]], axis=2)
+    return vals, grads
+
+
+def volume_quadrature():
+    """2x2x2 Gauss points (x slowest) and weights on [0,1]^3."""
+    pts = np.array([[a, b, c] for a in _GAUSS for b in _GAUSS for c in _GAUSS])
+    return pts, np.full(8, 0.125)
+
+
+def face_quadrature(face):
+    """2x2 Gauss points of one face (reference coords, basix facet map) and weights."""
+    v = _BASIX_VERTS[_BASIX_FACETS[face]]
+    pts = np.array([v[0] + s * (v[1] - v[0]) + t * (v[2] - v[0]) for s in _GAUSS for t in _GAUSS])
+    return pts, np.full(4, 0.25)
+
+
+def _batched_or_pointwise(fn, args, out_tail, sample=8):
+    """Evaluate fn over leading axis of each array in ``args`` (see module doc)."""
+    n = len(args[0])
+    if n == 0:
+        return np.zeros((0,) + out_tail)
+
+    def pointwise(idx):
+        out = [np.asarray(fn(*[a[i] for a in args]), dtype=np.float64) for i in idx]
+        return np.array(out).reshape((len(idx),) + out_tail)
+
+    batched = None
+    try:
+        r = np.asarray(fn(*[a.T for a in args]), dtype=np.float64)
+        if r.shape == out_tail:  # constant answer
+            batched = np.broadcast_to(r, (n,) + out_tail)
+        elif r.shape == out_tail + (n,):  # one answer per point, point axis last
+            batched = np.moveaxis(r, -1, 0)
+    except Exception:  # noqa: BLE001 - fall back to point-by-point
+        batched = None
+    rng = np.random.default_rng(0)
+    idx = np.unique(np.concatenate([[0, n - 1], rng.integers(0, n, size=min(sample, n))]))
+    ref = pointwise(idx)
+    if batched is not None and np.array_equal(np.asarray(batched[idx], dtype=np.float64), ref):
+        return np.array(batched)
+    return pointwise(np.arange(n))
+
+
+def _location_flags(fn, points):
+    nargs = getattr(getattr(fn, "__code__", None), "co_argcount", 1)
+    if nargs == 1:
+        args = (points,)
+        f = fn
+    elif nargs == 2:
+        args = (points, np.arange(len(points)))
+        f = fn
+    else:
+        raise ValueError(f"Wrong number of arguments for location_fn: must be 1 or 2, get {nargs}")
+    return _batched_or_pointwise(f, args, ()).astype(bool)
+
+
+class FiniteElement:
+    """One HEX8 field (fe.py:20-110).  Holds Dirichlet data as host arrays."""
+
+    def __init__(self, mesh, vec, dim, ele_type="HEX8", quadrature_rule=None, quadrature_order=None,
+                 dirichlet_bc_info=None):
+        if ele_type != "HEX8":
+            raise NotImplementedError(f"element {ele_type}: only HEX8 is on this path")
+        if dim != 3:
+            raise NotImplementedError("only dim=3 is supported")
+        if quadrature_order not in (None, 2) or quadrature_rule not in (None, "default"):
+            raise NotImplementedError("only the default 2x2x2 Gauss rule is supported")
+        self.mesh = mesh
+        self.points = mesh.points
+        self.cells = mesh.cells
+        self.vec, self.dim, self.ele_type = vec, dim, ele_type
+        self.num_cells = len(self.cells)
+        self.num_total_nodes = len(self.points)
+        self.num_total_dofs = self.num_total_nodes * vec
+        self.num_nodes, self.num_quads, self.num_faces, self.num_face_quads = 8, 8, 6, 4
+        self.face_inds = FACE_INDS
+        qp, self.quad_weights = volume_quadrature()
+        self.shape_vals, self.shape_grads_ref = hex8_eval(qp)
+        self.dirichlet_bc_info = dirichlet_bc_info
+        self.bc_version = 0
+        self.node_inds_list, self.vec_inds_list, self.vals_list = self.Dirichlet_boundary_conditions(
+            dirichlet_bc_info)
+
+    # -- Dirichlet (fe.py:220-269) -------------------------------------------
+    def Dirichlet_boundary_conditions(self, dirichlet_bc_info):
+        node_inds_list, vec_inds_list, vals_list = [], [], []
+        if dirichlet_bc_info is not None:
+            location_fns, vecs, value_fns = dirichlet_bc_info
+            assert len(location_fns) == len(value_fns) and len(value_fns) == len(vecs)
+            for lf, v, vf in zip(location_fns, vecs, value_fns):
+                flags = _location_flags(lf, self.points)
+                node_inds = np.argwhere(flags).reshape(-1)
+                vals = _batched_or_pointwise(vf, (self.points[node_inds],), ())
+                node_inds_list.append(node_inds)
+                vec_inds_list.append(np.full(len(node_inds), int(v), dtype=np.int32))
+                vals_list.append(np.asarray(vals, dtype=np.float64).reshape(-1))
+        return node_inds_list, vec_inds_list, vals_list
+
+    def update_Dirichlet_boundary_conditions(self, dirichlet_bc_info):
+        self.dirichlet_bc_info = dirichlet_bc_info
+        self.node_inds_list, self.vec_inds_list, self.vals_list = self.Dirichlet_boundary_conditions(
+            dirichlet_bc_info)
+        self.bc_version += 1
+
+    def dirichlet_arrays(self):
+        """(mask uint8 (ndofs,), values (ndofs,)); later conditions win on overlap
+        (the reference applies them in order, solver.py:297-300)."""
+        mask = np.zeros(self.num_total_dofs, dtype=np.uint8)
+        vals = np.zeros(self.num_total_dofs, dtype=np.float64)
+        for n, v, val in zip(self.node_inds_list, self.vec_inds_list, self.vals_list):
+            d = n * self.vec + v
+            mask[d] = 1
+            vals[d] = val
+        return mask, vals
+
+    # -- boundary faces (fe.py:271-322) ---------------------------------------
+    def get_boundary_conditions_inds(self, location_fns):
+        out = []
+        if location_fns is None:
+            return out
+        for lf in location_fns:
+            flags = _location_flags(lf, self.points)
+            cf = flags[self.cells[:, FACE_INDS]]  # (C,6,4)
+            out.append(np.argwhere(cf.all(axis=2)))
+        return out
+
+    def get_face_shape_grads(self, boundary_inds):
+        """Physical face shape gradients (F,4,8,3) and Nanson scale (F,4) (fe.py:143-183)."""
+        binds = np.asarray(boundary_inds).reshape(-1, 2)
+        F = len(binds)
+        grads = np.zeros((F, 4, 8, 3))
+        scale = np.zeros((F, 4))
+        X = self.points[self.cells[binds[:, 0]]] if F else np.zeros((0, 8, 3))
+        for face in range(6):
+            sel = np.nonzero(binds[:, 1] == face)[0]
+            if len(sel) == 0:
+                continue
+            pts, w = face_quadrature(face)
+            _, gref = hex8_eval(pts)  # (4,8,3)
+            J = np.einsum("fai,qaj->fqij", X[sel], gref)
+            Jinv = np.linalg.inv(J)
+            grads[sel] = np.einsum("qaj,fqjk->fqak", gref, Jinv)
+            nJ = np.einsum("i,fqij->fqj", _FACET_NORMALS[face], Jinv)
+            scale[sel] = np.linalg.norm(nJ, axis=-1) * np.linalg.det(J) * w[None]
+        return grads, scale
+
+    def face_shape_vals_at(self, faces):
+        out = np.zeros((len(faces), 4, 8))
+        for face in range(6):
+            sel = np.nonzero(np.asarray(faces) == face)[0]
+            if len(sel):
+                out[sel] = hex8_eval(face_quadrature(face)[0])[0][None]
+        return out
+
+    # -- load vectors of u-independent maps (problem.py:216-259) ---------------
+    def _check_u_independent(self, fn, x):
+        rng = np.random.default_rng(7)
+        k = min(4, len(x))
+        for i in range(k):
+            a = np.asarray(fn(np.zeros(self.vec), x[i]), dtype=np.float64)
+            b = np.asarray(fn(rng.standard_normal(self.vec), x[i]), dtype=np.float64)
+            if not np.array_equal(a, b):
+                raise NotImplementedError(
+                    "mass/surface maps that depend on u are not supported on this path; "
+                    "only u-independent loads (evaluated once into a load vector) are")
+
+    def body_load(self, mass_map):
+        """int mass_map(u, x) . v dx as a (ndofs,) vector."""
+        X = self.points[self.cells]  # (C,8,3)
+        J = np.einsum("cai,qaj->cqij", X, self.shape_grads_ref)
+        jxw = np.linalg.det(J) * self.quad_weights[None]
+        xq = np.einsum("qa,cai->cqi", self.shape_vals, X).reshape(-1, 3)
+        self._check_u_independent(mass_map, xq)
+        u0 = np.zeros((len(xq), self.vec))
+        val = _batched_or_pointwise(mass_map, (u0, xq), (self.vec,)).reshape(self.num_cells, 8, self.vec)
+        r = np.einsum("cqi,qa,cq->cai", val, self.shape_vals, jxw)
+        f = np.zeros((self.num_total_nodes, self.vec))
+        np.add.at(f, self.cells.reshape(-1), r.reshape(-1, self.vec))
+        return f.reshape(-1)
+
+    def surface_load(self, surface_map, boundary_inds):
+        """int surface_map(u, x) . v ds over the selected faces as a (ndofs,) vector."""
+        f = np.zeros((self.num_total_nodes, self.vec))
+        binds = np.asarray(boundary_inds).reshape(-1, 2)
+        if len(binds) == 0:
+            return f.reshape(-1)
+        _, scale = self.get_face_shape_grads(binds)
+        fv = self.face_shape_vals_at(binds[:, 1])  # (F,4,8)
+        X = self.points[self.cells[binds[:, 0]]]
+        xq = np.einsum("fqa,fai->fqi", fv, X).reshape(-1, 3)
+        self._check_u_independent(surface_map, xq)
+        u0 = np.zeros((len(xq), self.vec))
+        val = _batched_or_pointwise(surface_map, (u0, xq), (self.vec,)).reshape(len(binds), 4, self.vec)
+        r = np.einsum("fqi,fqa,fq->fai", val, fv, scale)
+        np.add.at(f, self.cells[binds[:, 0]].reshape(-1), r.reshape(-1, self.vec))
+        return f.reshape(-1)
+
+    def JxW(self):
+        X = self.points[self.cells]
+        J = np.einsum("cai,qaj->cqij", X, self.shape_grads_ref)
+        return np.linalg.det(J) * self.quad_weights[None]

@@ -1,0 +1,135 @@
+"""Registered constitutive laws: what ``get_tensor_map`` returns here.
+
+The reference's ``get_tensor_map`` returns a JAX-traceable callable that the
+framework differentiates with jacfwd (problem.py:262-266, 283-285).  This
+implementation has no tracer and no CPU fallback, so each supported law is a
+descriptor naming a hand-written CUDA kernel with its exact tangent:
+
+================  ==========================================  ===================
+descriptor        stress                                     internal_vars
+================  ==========================================  ===================
+Laplace()         P = grad u                                 -
+LinearElastic     sigma = lmbda tr(eps) I + 2 mu eps          -
+SIMPElastic       LinearElastic with E = Emin+(E0-Emin)t^p    [theta (C,Q[,1])]
+NeoHookean        P = dpsi/dF (compressible Neo-Hookean)      [] or [scale (C,Q)]
+J2Plasticity      radial return + linear iso. hardening       [sigma_old, eps_old(, alpha_old)]
+================  ==========================================  ===================
+
+``as_law`` also accepts a plain callable when it is recognisably the
+identity (the Poisson test's ``lambda x: x``) or a linear isotropic elastic
+stress; anything else raises ``NotImplementedError``.
+"""
+import numpy as np
+
+from . import _native as nat
+
+
+class Law:
+    law_id = None
+    vec = 3
+
+    def params(self):
+        return []
+
+
+class Laplace(Law):
+    """Tensor map P = grad u (the linear Poisson test, test_linear_poisson.py:15-17)."""
+    law_id = nat.LAW_LAPLACE
+    vec = None  # any vec
+
+
+class LinearElastic(Law):
+    """Isotropic linear elasticity (test_linear_elasticity_cube.py:16-25)."""
+    law_id = nat.LAW_LINEAR
+
+    def __init__(self, E, nu):
+        self.E, self.nu = float(E), float(nu)
+
+    def params(self):
+        return [self.E, self.nu]
+
+
+class SIMPElastic(Law):
+    """SIMP-penalised linear elasticity (top_opt/fem_model.py:67-80 in the reference)."""
+    law_id = nat.LAW_SIMP
+
+    def __init__(self, E0=70e3, Emin=70.0, nu=0.3, penal=3.0):
+        self.E0, self.Emin, self.nu, self.penal = float(E0), float(Emin), float(nu), float(penal)
+
+    def params(self):
+        return [self.E0, self.Emin, self.nu, self.penal]
+
+
+class NeoHookean(Law):
+    """psi = mu/2 (J^-2/3 I1 - 3) + kappa/2 (J-1)^2, P = dpsi/dF
+    (test_hyper_elasticity.py:17-33; scalability/hyperelastic3d_common.py:152-202)."""
+    law_id = nat.LAW_NEO_HOOKEAN
+
+    def __init__(self, E, nu):
+        self.E, self.nu = float(E), float(nu)
+
+    def params(self):
+        return [self.E, self.nu]
+
+
+class J2Plasticity(Law):
+    """Small-strain J2 radial return (test_plasticity.py:42-64) with linear
+    isotropic hardening modulus H (H=0 is the reference's perfect plasticity)."""
+    law_id = nat.LAW_J2
+
+    def __init__(self, E, nu, sigma_y, H=0.0):
+        self.E, self.nu, self.sigma_y, self.H = float(E), float(nu), float(sigma_y), float(H)
+
+    def params(self):
+        return [self.E, self.nu, self.sigma_y, self.H]
+
+
+def _probe(fn, vec, dim, rng):
+    x = rng.standard_normal((vec, dim))
+    return x, np.asarray(fn(x), dtype=np.float64)
+
+
+def as_law(obj, vec, dim=3):
+    """Turn what ``get_tensor_map`` returned into a registered law."""
+    if isinstance(obj, Law):
+        if obj.vec is not None and obj.vec != vec:
+            raise NotImplementedError(f"{type(obj).__name__} needs vec={obj.vec}, problem has vec={vec}")
+        return obj
+    if not callable(obj):
+        raise NotImplementedError(f"get_tensor_map returned {type(obj)}; expected a law descriptor")
+    try:
+        nargs = obj.__code__.co_argcount
+    except AttributeError:
+        nargs = 1
+    if nargs != 1:
+        raise NotImplementedError(
+            "tensor maps with internal variables must be registered laws "
+            "(SIMPElastic, NeoHookean, J2Plasticity)")
+    rng = np.random.default_rng(1234)
+    try:
+        samples = [_probe(obj, vec, dim, rng) for _ in range(4)]
+    except Exception as e:  # noqa: BLE001 - any failure means "not recognisable"
+        raise NotImplementedError(f"cannot evaluate tensor map on numpy input: {e}") from e
+    if all(y.shape == x.shape and np.allclose(y, x, rtol=1e-13, atol=1e-13) for x, y in samples):
+        return Laplace()
+    if vec == 3 and dim == 3:
+        # linear isotropic elasticity: sigma(eps) = lmbda tr I + 2 mu eps
+        e11 = np.zeros((3, 3))
+        e11[0, 0] = 1.0
+        s = np.asarray(obj(e11), dtype=np.float64)
+        lmbda = s[1, 1]
+        mu = 0.5 * (s[0, 0] - lmbda)
+        if mu > 0:
+            E = mu * (3 * lmbda + 2 * mu) / (lmbda + mu)
+            nu = lmbda / (2 * (lmbda + mu))
+            cand = LinearElastic(E, nu)
+            ok = True
+            for x, y in samples:
+                eps = 0.5 * (x + x.T)
+                ref = lmbda * np.trace(eps) * np.eye(3) + 2 * mu * eps
+                ok &= y.shape == (3, 3) and np.allclose(y, ref, rtol=1e-11, atol=1e-9 * abs(mu))
+            if ok:
+                return cand
+    raise NotImplementedError(
+        "unrecognised tensor map: return a registered law (Laplace, LinearElastic, "
+        "SIMPElastic, NeoHookean, J2Plasticity) from get_tensor_map")

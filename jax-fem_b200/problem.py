@@ -1,0 +1,306 @@
+"""``Problem``: the reference's plugin API over the B200 kernels.
+
+Same class name, constructor fields and hooks as the reference
+(problem.py:15-128, 184-187, 462-556): subclass it, override
+``get_tensor_map`` (returning a registered law, see ``laws``),
+optionally ``get_mass_map`` / ``get_surface_maps`` (u-independent loads),
+``custom_init`` and ``set_params``, and pass ``dirichlet_bc_info`` /
+``location_fns`` exactly as for the reference.
+
+What changes underneath: per-cell kernels, assembly, Dirichlet elimination
+and solves run in libjaxfem_b200 on the current CUDA device; solutions,
+residuals and internal variables are torch CUDA tensors (float64).
+"""
+from dataclasses import dataclass
+from typing import Any
+
+import numpy as np
+import torch
+
+from . import _native as nat
+from .fe import FiniteElement
+from .generate_mesh import Mesh
+from .laws import J2Plasticity, NeoHookean, SIMPElastic, as_law
+
+
+class BSRMatrix:
+    """Block-CSR matrix on the device (vec x vec blocks, sorted columns)."""
+
+    def __init__(self, vec, row_ptr, col_idx, diag, vals):
+        self.vec, self.row_ptr, self.col_idx, self.diag, self.vals = vec, row_ptr, col_idx, diag, vals
+        self.n_brows = row_ptr.numel() - 1
+        self.shape = (self.n_brows * vec, self.n_brows * vec)
+
+    @property
+    def dtype(self):
+        return self.vals.dtype
+
+    def matvec(self, x, out=None):
+        x = x.to(self.vals.dtype).contiguous()
+        out = torch.empty_like(x) if out is None else out
+        fn = nat.lib().fem_bsr_spmv_f64 if self.vals.dtype == torch.float64 else nat.lib().fem_bsr_spmv_f32
+        nat.check(fn(self.vec, self.n_brows, nat.ptr(self.row_ptr), nat.ptr(self.col_idx),
+                     nat.ptr(self.vals), nat.ptr(x), nat.ptr(out), nat.stream_ptr()), "bsr_spmv")
+        return out
+
+    def __matmul__(self, x):
+        return self.matvec(x)
+
+    def to_scipy(self):
+        """Host copy as scipy CSR (tests / debugging)."""
+        import scipy.sparse as sp
+        v = self.vec
+        rp = self.row_ptr.cpu().numpy()
+        ci = self.col_idx.cpu().numpy()
+        vals = self.vals.double().cpu().numpy().reshape(-1, v, v)
+        return sp.bsr_matrix((vals, ci, rp), shape=self.shape).tocsr()
+
+
+class DeviceMesh:
+    """Mesh arrays, block-CSR pattern and cell->block scatter map on the device."""
+
+    def __init__(self, mesh, vec, device):
+        cells = np.ascontiguousarray(mesh.cells, dtype=np.int32)
+        C, N = cells.shape[0], mesh.points.shape[0]
+        lib = nat.lib()
+        row_ptr = np.zeros(N + 1, dtype=np.int32)
+        nnzb = nat.I64(0)
+        nat.check(lib.fem_bsr_pattern(cells.ctypes.data, C, N, row_ptr.ctypes.data, nnzb, None, 0,
+                                      None, None), "bsr_pattern(count)")
+        col = np.zeros(max(1, nnzb.value), dtype=np.int32)
+        scatter = np.zeros((max(1, C), 64), dtype=np.int32)
+        diag = np.zeros(max(1, N), dtype=np.int32)
+        nat.check(lib.fem_bsr_pattern(cells.ctypes.data, C, N, row_ptr.ctypes.data, nnzb,
+                                      col.ctypes.data, col.size, scatter.ctypes.data, diag.ctypes.data),
+                  "bsr_pattern(fill)")
+        self.vec, self.num_cells, self.num_nodes, self.nnzb = vec, C, N, int(nnzb.value)
+        self.ndofs = N * vec
+        self.device = device
+        self.points = torch.from_numpy(np.ascontiguousarray(mesh.points, dtype=np.float64)).to(device)
+        self.cells = torch.from_numpy(cells).to(device)
+        self.row_ptr = torch.from_numpy(row_ptr).to(device)
+        self.col_idx = torch.from_numpy(col[: self.nnzb]).to(device)
+        self.scatter = torch.from_numpy(scatter[:C]).to(device).contiguous()
+        self.diag = torch.from_numpy(diag[:N]).to(device)
+
+    def new_matrix(self, dtype):
+        vals = torch.zeros(self.nnzb * self.vec * self.vec, dtype=dtype, device=self.device)
+        return BSRMatrix(self.vec, self.row_ptr, self.col_idx, self.diag, vals)
+
+
+def _to_dev(x, device, dtype=torch.float64):
+    if isinstance(x, torch.Tensor):
+        return x.detach().to(device=device, dtype=dtype).contiguous()
+    return torch.as_tensor(np.asarray(x), dtype=dtype, device=device).contiguous()
+
+
+@dataclass
+class Problem:
+    """One HEX8 field; see the module docstring.  Fields as the reference's."""
+    mesh: Mesh
+    vec: int
+    dim: int
+    ele_type: str = "HEX8"
+    quadrature_rule: Any = None
+    quadrature_order: int = None
+    dirichlet_bc_info: list = None
+    location_fns: list = None
+    additional_info: tuple = ()
+
+    def __post_init__(self):
+        if isinstance(self.mesh, list):
+            if len(self.mesh) != 1:
+                raise NotImplementedError("multi-variable problems are not on this path")
+            self.mesh = self.mesh[0]
+            self.vec = self.vec[0] if isinstance(self.vec, list) else self.vec
+            self.ele_type = self.ele_type[0] if isinstance(self.ele_type, list) else self.ele_type
+            if isinstance(self.dirichlet_bc_info, list) and len(self.dirichlet_bc_info) == 1 and (
+                    self.dirichlet_bc_info[0] is None or isinstance(self.dirichlet_bc_info[0], list)
+                    and len(self.dirichlet_bc_info[0]) == 3 and isinstance(self.dirichlet_bc_info[0][0], list)):
+                self.dirichlet_bc_info = self.dirichlet_bc_info[0]
+        if not isinstance(self.mesh, Mesh):
+            self.mesh = Mesh(self.mesh.points, self.mesh.cells)
+        self.fes = [FiniteElement(mesh=self.mesh, vec=self.vec, dim=self.dim, ele_type=self.ele_type,
+                                  quadrature_rule=self.quadrature_rule,
+                                  quadrature_order=self.quadrature_order,
+                                  dirichlet_bc_info=self.dirichlet_bc_info)]
+        self.num_vars = 1
+        self.cells_list = [self.fes[0].cells]
+        self.num_cells = self.fes[0].num_cells
+        self.boundary_inds_list = self.fes[0].get_boundary_conditions_inds(self.location_fns)
+        self.offset = [0]
+        self.num_total_dofs_all_vars = self.fes[0].num_total_dofs
+        self.internal_vars = ()
+        self.internal_vars_surfaces = [() for _ in range(len(self.boundary_inds_list))]
+        self._dev = None
+        self._bc_cache = None
+        self._fext = None
+        self._law = None
+        self.custom_init(*self.additional_info)
+        if hasattr(self, "get_surface_maps"):
+            assert len(self.boundary_inds_list) == len(self.get_surface_maps())
+        else:
+            assert len(self.boundary_inds_list) == 0, "Missing definitions for surface integral"
+
+    # ---- hooks (problem.py:184-187, 493-556) ---------------------------------
+    def custom_init(self, *args):
+        pass
+
+    def set_params(self, params):
+        raise NotImplementedError("Child class must implement this function!")
+
+    # ---- helpers ---------------------------------------------------------------
+    @property
+    def law(self):
+        if self._law is None:
+            if not hasattr(self, "get_tensor_map"):
+                raise NotImplementedError("a Problem on this path needs get_tensor_map")
+            self._law = as_law(self.get_tensor_map(), self.vec, self.dim)
+        return self._law
+
+    def device(self):
+        return torch.device("cuda", torch.cuda.current_device())
+
+    def dev(self):
+        """Device mesh + pattern, built on first use."""
+        if self._dev is None:
+            if not torch.cuda.is_available():
+                raise nat.FEMNativeError(nat.FEM_ERR_CUDA, "no CUDA device: this path has no CPU fallback")
+            nat.load()
+            self._dev = DeviceMesh(self.mesh, self.vec, self.device())
+        return self._dev
+
+    def unflatten_fn_sol_list(self, dofs):
+        return [dofs.reshape(-1, self.vec)]
+
+    def dirichlet_device(self):
+        """(mask uint8, values f64) on the device, refreshed after BC updates."""
+        fe = self.fes[0]
+        key = fe.bc_version
+        if self._bc_cache is None or self._bc_cache[0] != key:
+            mask, vals = fe.dirichlet_arrays()
+            d = self.dev().device
+            self._bc_cache = (key, torch.from_numpy(mask).to(d), torch.from_numpy(vals).to(d))
+        return self._bc_cache[1], self._bc_cache[2]
+
+    def surface_load_vectors(self):
+        """Per-surface load vectors int surface_map . v ds (device f64)."""
+        if not hasattr(self, "_surface_loads"):
+            loads = []
+            if hasattr(self, "get_surface_maps"):
+                for binds, smap in zip(self.boundary_inds_list, self.get_surface_maps()):
+                    loads.append(self.fes[0].surface_load(smap, binds))
+            d = self.dev().device
+            self._surface_loads = [torch.from_numpy(np.ascontiguousarray(f)).to(d) for f in loads]
+        return self._surface_loads
+
+    def external_load(self):
+        """f_ext = int mass_map . v dx + sum_surfaces int surface_map . v ds (device f64)."""
+        if self._fext is None:
+            d = self.dev().device
+            f = torch.zeros(self.num_total_dofs_all_vars, dtype=torch.float64, device=d)
+            if hasattr(self, "get_mass_map"):
+                f += torch.from_numpy(self.fes[0].body_load(self.get_mass_map())).to(d)
+            for fs in self.surface_load_vectors():
+                f += fs
+            self._fext = f
+        return self._fext
+
+    def law_ivars(self, ivars=None):
+        """Device pointers (iv0, iv1, iv2) of the law's internal variables."""
+        ivars = self.internal_vars if ivars is None else ivars
+        law = self.law
+        d = self.dev().device
+        C = self.num_cells
+        if isinstance(law, SIMPElastic):
+            if len(ivars) < 1:
+                raise ValueError("SIMPElastic needs internal_vars = [theta] (set_params)")
+            th = _to_dev(ivars[0], d)
+            if th.numel() == C:
+                th = th.reshape(C, 1).expand(C, 8).contiguous()
+            return (th.reshape(C, 8), None, None)
+        if isinstance(law, NeoHookean):
+            if len(ivars) == 0:
+                return (None, None, None)
+            sc = _to_dev(ivars[0], d)
+            if sc.numel() == C:
+                sc = sc.reshape(C, 1).expand(C, 8).contiguous()
+            return (sc.reshape(C, 8), None, None)
+        if isinstance(law, J2Plasticity):
+            if len(ivars) < 2:
+                raise ValueError("J2Plasticity needs internal_vars = [sigma_old, eps_old(, alpha_old)]")
+            so = _to_dev(ivars[0], d).reshape(C, 8, 9)
+            eo = _to_dev(ivars[1], d).reshape(C, 8, 9)
+            ao = _to_dev(ivars[2], d).reshape(C, 8) if len(ivars) > 2 else torch.zeros(
+                C, 8, dtype=torch.float64, device=d)
+            return (so, eo, ao)
+        return (None, None, None)
+
+    # ---- assembly (problem.py:439-491) -----------------------------------------
+    def assemble(self, dofs, res=None, vals=None, lift=None, dvec=None, bc=True, fp32=False,
+                 ivars=None):
+        """One fused pass of the cell kernel: residual, tangent, Dirichlet lift."""
+        dv = self.dev()
+        law = self.law
+        mask, _ = self.dirichlet_device() if bc else (None, None)
+        iv = self.law_ivars(ivars)
+        pr, n = nat.params_array(law.params())
+        fn = nat.lib().fem_assemble_f32 if fp32 else nat.lib().fem_assemble_f64
+        nat.check(fn(law.law_id, pr, n, self.vec, dv.num_cells, dv.num_nodes, nat.ptr(dv.cells),
+                     nat.ptr(dv.points), nat.ptr(dofs), nat.ptr(iv[0]), nat.ptr(iv[1]), nat.ptr(iv[2]),
+                     nat.ptr(dv.scatter), nat.ptr(dv.diag), dv.nnzb,
+                     nat.ptr(mask) if bc else None, nat.ptr(dvec), nat.ptr(res), nat.ptr(lift),
+                     nat.ptr(vals), nat.stream_ptr()), "assemble")
+
+    def _flat_dofs(self, sol_list):
+        s = sol_list[0] if isinstance(sol_list, (list, tuple)) else sol_list
+        return _to_dev(s, self.dev().device).reshape(-1)
+
+    def compute_residual(self, sol_list):
+        """Residual list (without Dirichlet rows applied), as the reference's."""
+        dofs = self._flat_dofs(sol_list)
+        res = torch.empty_like(dofs)
+        self.assemble(dofs, res=res, bc=False)
+        return [(res + self.external_load()).reshape(-1, self.vec)]
+
+    def newton_update(self, sol_list):
+        """Residual list; also assembles the BC-eliminated tangent into ``self.A``."""
+        dofs = self._flat_dofs(sol_list)
+        res = torch.empty_like(dofs)
+        if getattr(self, "A", None) is None or self.A.vals.dtype != torch.float64:
+            self.A = self.dev().new_matrix(torch.float64)
+        self.assemble(dofs, res=res, vals=self.A.vals)
+        return [(res + self.external_load()).reshape(-1, self.vec)]
+
+    # ---- J2 state commit (test_plasticity.py:67-78) -----------------------------
+    def update_j2_state(self, sol):
+        """Commit the return map at the converged ``sol``: internal_vars <- new state."""
+        law = self.law
+        if not isinstance(law, J2Plasticity):
+            raise TypeError("update_j2_state needs a J2Plasticity law")
+        dv = self.dev()
+        so, eo, ao = self.law_ivars()
+        sn, en, an = torch.empty_like(so), torch.empty_like(eo), torch.empty_like(ao)
+        dofs = self._flat_dofs(sol)
+        pr, n = nat.params_array(law.params())
+        nat.check(nat.lib().fem_j2_commit(pr, n, dv.num_cells, nat.ptr(dv.cells), nat.ptr(dv.points),
+                                          nat.ptr(dofs), nat.ptr(so), nat.ptr(eo), nat.ptr(ao),
+                                          nat.ptr(sn), nat.ptr(en), nat.ptr(an), nat.stream_ptr()),
+                  "j2_commit")
+        C = self.num_cells
+        self.internal_vars = [sn.reshape(C, 8, 3, 3), en.reshape(C, 8, 3, 3), an]
+        return self.internal_vars
+
+    def JxW(self):
+        if not hasattr(self, "_jxw"):
+            self._jxw = torch.from_numpy(self.fes[0].JxW()).to(self.dev().device)
+        return self._jxw
+
+
+def compliance(problem, sol, surface_index=0):
+    """C = int t . u ds with t = -surface_map on one surface set
+    (compute_compliance of the reference's topology-optimisation example).
+    Differentiable in ``sol`` (a torch expression)."""
+    f = problem.surface_load_vectors()[surface_index]
+    u = sol[0] if isinstance(sol, (list, tuple)) else sol
+    return -(f * u.reshape(-1)).sum()

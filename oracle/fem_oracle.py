@@ -1,0 +1,613 @@
+"""FP64 numpy restatement of the reference's HEX8 assemble-and-solve path.
+
+TEST INFRASTRUCTURE ONLY: the parity checker and the CPU baseline.  The
+product (``jax-fem_b200``) never imports this module.
+
+Every function cites the reference file:line it restates (paths inside the
+reference project).  Arithmetic is float64 (the reference forces x64 when
+``jax_fem.solver`` is imported, solver.py:10-11).  The per-cell Jacobian is
+computed the way the reference does it -- forward-mode derivatives of the
+weak-form kernel along the 24 cell dofs (problem.py:262-266, ``jax.jvp``
+over an identity basis) -- here by complex-step differentiation, which gives
+the same directional derivatives to round-off for these analytic kernels.
+The GPU path uses closed-form tangents instead and is checked against this.
+
+Third-party arithmetic restated here (absent from the reference tree):
+basix 0.10.0 (HEX8 Lagrange tabulation, Gauss-Jacobi quadrature; see
+``hex8_tables``) and PETSc 3.25.1 COO summation / ``zeroRows`` (see
+``assemble_global``).
+"""
+import numpy as np
+import scipy.sparse as sp
+import scipy.sparse.linalg as spla
+
+# --------------------------------------------------------------------------
+# Basis and quadrature (basis.py:19-57, 117-124, 141-250)
+# --------------------------------------------------------------------------
+
+# basix hexahedron vertices on [0,1]^3, x fastest (basix cell geometry).
+BASIX_HEX_VERTICES = np.array(
+    [[0, 0, 0], [1, 0, 0], [0, 1, 0], [1, 1, 0],
+     [0, 0, 1], [1, 0, 1], [0, 1, 1], [1, 1, 1]], dtype=np.float64)
+# VTK/meshio -> basix node permutation for HEX8 (basis.py:53).
+HEX8_REORDER = np.array([0, 1, 3, 2, 4, 5, 7, 6])
+# basix hexahedron facets (sub-entity connectivity, dim 2) and outward normals.
+BASIX_HEX_FACETS = np.array(
+    [[0, 1, 2, 3], [0, 1, 4, 5], [0, 2, 4, 6], [1, 3, 5, 7], [2, 3, 6, 7], [4, 5, 6, 7]])
+BASIX_HEX_NORMALS = np.array(
+    [[0, 0, -1], [0, -1, 0], [-1, 0, 0], [1, 0, 0], [0, 1, 0], [0, 0, 1]], dtype=np.float64)
+
+
+def gauss_jacobi_01(m):
+    """m-point Gauss-Legendre rule on [0,1], points ascending (basix GJ rule)."""
+    x, w = np.polynomial.legendre.leggauss(m)
+    return 0.5 + 0.5 * x, 0.5 * w
+
+
+def hex8_shape(xi):
+    """Trilinear shape values/gradients at points xi (n,3), VTK node order.
+
+    Returns vals (n,8), grads (n,8,3).  Equivalent to basix P1 hexahedron
+    tabulation followed by ``[:, :, re_order]`` (basis.py:170-173).
+    """
+    X = BASIX_HEX_VERTICES[HEX8_REORDER]  # VTK node positions
+    xi = np.atleast_2d(xi)
+    f = X[None, :, :] * xi[:, None, :] + (1 - X[None, :, :]) * (1 - xi[:, None, :])  # (n,8,3)
+    df = (2 * X - 1)[None, :, :] * np.ones_like(f)
+    vals = f.prod(axis=2)
+    grads = np.stack([df[:, :, 0] * f[:, :, 1] * f[:, :, 2],
+                      f[:, :, 0] * df[:, :, 1] * f[:, :, 2],
+                      f[:, :, 0] * f[:, :, 1] * df[:, :, 2]], axis=2)
+    return vals, grads
+
+
+def hex8_tables(quadrature_order=2):
+    """shape_vals (Q,8), shape_grads_ref (Q,8,3), weights (Q,) (basis.py:141-175).
+
+    basix ``make_quadrature(hexahedron, order)`` with the default Gauss-Jacobi
+    rule uses m = (order+2)//2 points per axis, tensor product with the x
+    coordinate slowest and z fastest.
+    """
+    m = (quadrature_order + 2) // 2
+    p, w = gauss_jacobi_01(m)
+    pts = np.array([[a, b, c] for a in p for b in p for c in p])
+    wts = np.array([wa * wb * wc for wa in w for wb in w for wc in w])
+    vals, grads = hex8_shape(pts)
+    return vals, grads, wts
+
+
+def hex8_face_tables(quadrature_order=2):
+    """Face tables (basis.py:178-250): vals (6,F,8), grads (6,F,8,3),
+    weights (6,F), normals (6,3), face_inds (6,4) in VTK node numbering."""
+    m = (quadrature_order + 2) // 2
+    p, w = gauss_jacobi_01(m)
+    qpts = np.array([[a, b] for a in p for b in p])
+    qw = np.array([wa * wb for wa in w for wb in w])
+    s, t = qpts[:, 0], qpts[:, 1]
+    lag = np.stack([(1 - s) * (1 - t), s * (1 - t), (1 - s) * t, s * t], axis=1)  # P1 quad map
+    fpts, fw, finds = [], [], []
+    for facet in BASIX_HEX_FACETS:
+        v = BASIX_HEX_VERTICES[facet]
+        fpts.append(lag @ v)
+        jac = np.stack([v[1] - v[0], v[2] - v[0]], axis=1)
+        fw.append(qw * np.linalg.norm(np.cross(jac[:, 0], jac[:, 1])))
+        finds.append([int(np.argwhere(HEX8_REORDER == i)[0, 0]) for i in facet])
+    fpts = np.stack(fpts)
+    vals, grads = hex8_shape(fpts.reshape(-1, 3))
+    nf, nq = fpts.shape[:2]
+    return (vals.reshape(nf, nq, 8), grads.reshape(nf, nq, 8, 3), np.stack(fw),
+            BASIX_HEX_NORMALS.copy(), np.array(finds))
+
+
+# --------------------------------------------------------------------------
+# Mesh (generate_mesh.py:151-189)
+# --------------------------------------------------------------------------
+
+def box_mesh(Nx, Ny, Nz, Lx, Ly, Lz):
+    x = np.linspace(0, Lx, Nx + 1)
+    y = np.linspace(0, Ly, Ny + 1)
+    z = np.linspace(0, Lz, Nz + 1)
+    xv, yv, zv = np.meshgrid(x, y, z, indexing="ij")
+    points = np.stack((xv, yv, zv), axis=3).reshape(-1, 3)
+    ind = np.arange(len(points)).reshape(Nx + 1, Ny + 1, Nz + 1)
+    cells = np.stack((ind[:-1, :-1, :-1], ind[1:, :-1, :-1], ind[1:, 1:, :-1], ind[:-1, 1:, :-1],
+                      ind[:-1, :-1, 1:], ind[1:, :-1, 1:], ind[1:, 1:, 1:], ind[:-1, 1:, 1:]),
+                     axis=3).reshape(-1, 8)
+    return points, cells.astype(np.int32)
+
+
+# --------------------------------------------------------------------------
+# Geometry (fe.py:112-218)
+# --------------------------------------------------------------------------
+
+def shape_grads(points, cells, grads_ref, weights):
+    """Physical shape gradients (C,Q,8,3) and JxW (C,Q) (fe.py:112-141)."""
+    X = points[cells]  # (C,8,3)
+    J = np.einsum("cai,qaj->cqij", X, grads_ref)
+    det = np.linalg.det(J)
+    Jinv = np.linalg.inv(J)
+    g = np.einsum("qaj,cqjk->cqak", grads_ref, Jinv)
+    return g, det * weights[None, :]
+
+
+def physical_quad_points(points, cells, vals):
+    return np.einsum("qa,cai->cqi", vals, points[cells])
+
+
+def eval_pointwise(fn, *args):
+    """Evaluate a per-point user function over leading axes of ``args``.
+
+    The reference evaluates location/value/mass/surface functions one point
+    at a time under ``jax.vmap`` (fe.py:252-254, problem.py:230,253).  Here a
+    Python loop plays the role of vmap.
+    """
+    n = len(args[0])
+    out = [np.asarray(fn(*[a[i] for a in args])) for i in range(n)]
+    return np.array(out)
+
+
+def dirichlet_bcs(points, bc_info):
+    """node_inds, vec_inds, vals lists (fe.py:220-258)."""
+    nodes, vecs, vals = [], [], []
+    if bc_info is None:
+        return nodes, vecs, vals
+    loc_fns, vec_list, val_fns = bc_info
+    for lf, v, vf in zip(loc_fns, vec_list, val_fns):
+        nargs = lf.__code__.co_argcount
+        if nargs == 1:
+            flags = np.array([bool(lf(p)) for p in points])
+        else:
+            flags = np.array([bool(lf(p, i)) for i, p in enumerate(points)])
+        ni = np.argwhere(flags).reshape(-1)
+        nodes.append(ni)
+        vecs.append(np.full(len(ni), v, dtype=np.int64))
+        vals.append(np.array([float(vf(points[i])) for i in ni], dtype=np.float64).reshape(-1))
+    return nodes, vecs, vals
+
+
+def boundary_faces(points, cells, location_fns, face_inds):
+    """(num_selected_faces, 2) [cell, local face] per location fn (fe.py:271-322)."""
+    out = []
+    if location_fns is None:
+        return out
+    for lf in location_fns:
+        nargs = lf.__code__.co_argcount
+        if nargs == 1:
+            flag = np.array([bool(lf(p)) for p in points])
+        else:
+            flag = np.array([bool(lf(p, i)) for i, p in enumerate(points)])
+        cf = flag[cells[:, face_inds]]  # (C,6,4)
+        out.append(np.argwhere(cf.all(axis=2)))
+    return out
+
+
+def face_geometry(points, cells, binds, fgrads_ref, fweights, normals):
+    """face shape grads and Nanson scale (fe.py:143-183)."""
+    X = points[cells][binds[:, 0]]
+    gr = fgrads_ref[binds[:, 1]]  # (F,q,8,3)
+    J = np.einsum("fai,fqaj->fqij", X, gr)
+    det = np.linalg.det(J)
+    Jinv = np.linalg.inv(J)
+    n = normals[binds[:, 1]]
+    nJ = np.einsum("fi,fqij->fqj", n, Jinv)
+    scale = np.linalg.norm(nJ, axis=-1) * det * fweights[binds[:, 1]]
+    return scale
+
+
+# --------------------------------------------------------------------------
+# Constitutive laws (complex-step safe)
+# --------------------------------------------------------------------------
+
+def _eye(shape):
+    return np.broadcast_to(np.eye(3), shape + (3, 3))
+
+
+def lame(E, nu):
+    mu = E / (2.0 * (1.0 + nu))
+    lmbda = E * nu / ((1 + nu) * (1 - 2 * nu))
+    return lmbda, mu
+
+
+def stress_linear(u_grad, E, nu):
+    """Isotropic linear elasticity (test_linear_elasticity_cube.py:16-25)."""
+    lmbda, mu = lame(E, nu)
+    eps = 0.5 * (u_grad + np.swapaxes(u_grad, -1, -2))
+    tr = np.trace(eps, axis1=-2, axis2=-1)
+    return lmbda * tr[..., None, None] * _eye(tr.shape) + 2 * mu * eps
+
+
+def simp_modulus(theta, E0, Emin, penal):
+    """E = Emin + (E0-Emin) theta^p (top_opt/fem_model.py:67-80)."""
+    return Emin + (E0 - Emin) * theta ** penal
+
+
+def stress_simp(u_grad, theta, E0, Emin, nu, penal):
+    E = simp_modulus(theta, E0, Emin, penal)
+    lmbda, mu = lame(E, nu)
+    eps = 0.5 * (u_grad + np.swapaxes(u_grad, -1, -2))
+    tr = np.trace(eps, axis1=-2, axis2=-1)
+    return (lmbda * tr)[..., None, None] * _eye(tr.shape) + (2 * mu)[..., None, None] * eps
+
+
+def _det3(F):
+    return (F[..., 0, 0] * (F[..., 1, 1] * F[..., 2, 2] - F[..., 1, 2] * F[..., 2, 1])
+            - F[..., 0, 1] * (F[..., 1, 0] * F[..., 2, 2] - F[..., 1, 2] * F[..., 2, 0])
+            + F[..., 0, 2] * (F[..., 1, 0] * F[..., 2, 1] - F[..., 1, 1] * F[..., 2, 0]))
+
+
+def _cof3(F):
+    """Cofactor matrix (det(F) F^{-T}), complex-safe."""
+    c = np.empty(F.shape, dtype=F.dtype)
+    c[..., 0, 0] = F[..., 1, 1] * F[..., 2, 2] - F[..., 1, 2] * F[..., 2, 1]
+    c[..., 0, 1] = F[..., 1, 2] * F[..., 2, 0] - F[..., 1, 0] * F[..., 2, 2]
+    c[..., 0, 2] = F[..., 1, 0] * F[..., 2, 1] - F[..., 1, 1] * F[..., 2, 0]
+    c[..., 1, 0] = F[..., 0, 2] * F[..., 2, 1] - F[..., 0, 1] * F[..., 2, 2]
+    c[..., 1, 1] = F[..., 0, 0] * F[..., 2, 2] - F[..., 0, 2] * F[..., 2, 0]
+    c[..., 1, 2] = F[..., 0, 1] * F[..., 2, 0] - F[..., 0, 0] * F[..., 2, 1]
+    c[..., 2, 0] = F[..., 0, 1] * F[..., 1, 2] - F[..., 0, 2] * F[..., 1, 1]
+    c[..., 2, 1] = F[..., 0, 2] * F[..., 1, 0] - F[..., 0, 0] * F[..., 1, 2]
+    c[..., 2, 2] = F[..., 0, 0] * F[..., 1, 1] - F[..., 0, 1] * F[..., 1, 0]
+    return c
+
+
+def psi_neo_hookean(F, E, nu):
+    """Strain energy (test_hyper_elasticity.py:17-27; scalability/hyperelastic3d_common.py:152-169)."""
+    mu = E / (2.0 * (1.0 + nu))
+    kappa = E / (3.0 * (1.0 - 2.0 * nu))
+    J = _det3(F)
+    I1 = np.einsum("...ij,...ij->...", F, F)
+    return (mu / 2.0) * (J ** (-2.0 / 3.0) * I1 - 3.0) + (kappa / 2.0) * (J - 1.0) ** 2
+
+
+def stress_neo_hookean(u_grad, E, nu, scale=None):
+    """First Piola stress P = dpsi/dF, F = I + grad u (jax.grad of psi in the reference).
+
+    ``scale`` multiplies psi (the density-scaled variant,
+    scalability/hyperelastic3d_common.py:186-202).
+    """
+    mu = E / (2.0 * (1.0 + nu))
+    kappa = E / (3.0 * (1.0 - 2.0 * nu))
+    F = u_grad + _eye(u_grad.shape[:-2])
+    J = _det3(F)
+    H = _cof3(F) / J[..., None, None]  # F^{-T}
+    I1 = np.einsum("...ij,...ij->...", F, F)
+    m = mu * J ** (-2.0 / 3.0)
+    P = m[..., None, None] * (F - (I1 / 3.0)[..., None, None] * H) \
+        + (kappa * J * (J - 1.0))[..., None, None] * H
+    if scale is not None:
+        P = scale[..., None, None] * P
+    return P
+
+
+def safe_sqrt(x):
+    return np.where(np.real(x) > 0.0, np.sqrt(np.where(np.real(x) > 0.0, x, 1.0)), 0.0)
+
+
+def safe_divide(x, y):
+    return np.where(np.real(y) == 0.0, 0.0, x / np.where(np.real(y) == 0.0, 1.0, y))
+
+
+def j2_return_map(u_grad, sigma_old, eps_old, alpha_old, E, nu, sig0, H):
+    """Small-strain J2 radial return (test_plasticity.py:42-64).
+
+    The reference's map has no hardening; with linear isotropic hardening
+    modulus H and equivalent plastic strain alpha the yield stress is
+    sig0 + H*alpha_old and the plastic multiplier is f/(3 mu + H) (radial
+    return, Simo & Hughes, Computational Inelasticity, Box 3.1).  With H=0
+    this is exactly the reference's map.  Returns (sigma, alpha_new).
+    """
+    lmbda, mu = lame(E, nu)
+    eps = 0.5 * (u_grad + np.swapaxes(u_grad, -1, -2))
+    deps = eps - eps_old
+    tr = np.trace(deps, axis1=-2, axis2=-1)
+    sig_tr = lmbda * tr[..., None, None] * _eye(tr.shape) + 2 * mu * deps + sigma_old
+    trs = np.trace(sig_tr, axis1=-2, axis2=-1)
+    s = sig_tr - (trs / 3.0)[..., None, None] * _eye(trs.shape)
+    q = safe_sqrt(1.5 * np.einsum("...ij,...ij->...", s, s))
+    f = q - (sig0 + H * alpha_old)
+    fp = np.where(np.real(f) > 0.0, f, 0.0)
+    dgam = fp / (3.0 * mu + H)
+    sigma = sig_tr - safe_divide((3.0 * mu * dgam)[..., None, None] * s, q[..., None, None])
+    return sigma, alpha_old + dgam
+
+
+class Law:
+    """A tensor map P(u_grad, *ivars) over (..., vec, 3) arrays (problem.py:203-210)."""
+
+    def __init__(self, kind, vec=3, **params):
+        self.kind, self.vec, self.params = kind, vec, params
+
+    def __call__(self, u_grad, ivars):
+        p = self.params
+        if self.kind == "laplace":
+            return u_grad
+        if self.kind == "linear":
+            return stress_linear(u_grad, p["E"], p["nu"])
+        if self.kind == "simp":
+            return stress_simp(u_grad, ivars[0], p["E0"], p["Emin"], p["nu"], p["penal"])
+        if self.kind == "neo_hookean":
+            return stress_neo_hookean(u_grad, p["E"], p["nu"], ivars[0] if ivars else None)
+        if self.kind == "j2":
+            sig, _ = j2_return_map(u_grad, ivars[0], ivars[1], ivars[2],
+                                   p["E"], p["nu"], p["sig0"], p["H"])
+            return sig
+        raise ValueError(self.kind)
+
+
+# --------------------------------------------------------------------------
+# Problem (problem.py) -- cell kernels, assembly, residual
+# --------------------------------------------------------------------------
+
+class OracleProblem:
+    """Single-variable HEX8 problem mirroring ``Problem`` (problem.py:15-128).
+
+    ``mass_map(u, x)`` and ``surface_maps[i](u, x)`` follow the reference's
+    per-quad-point signatures (problem.py:216-259); ``law`` replaces the
+    traced ``get_tensor_map`` callable.
+    """
+
+    def __init__(self, points, cells, vec, law, dirichlet_bc_info=None, location_fns=None,
+                 mass_map=None, surface_maps=None, internal_vars=()):
+        self.points = np.asarray(points, dtype=np.float64)
+        self.cells = np.asarray(cells, dtype=np.int64)
+        self.vec, self.law = vec, law
+        self.num_cells, self.num_nodes = len(self.cells), len(self.points)
+        self.ndofs = self.num_nodes * vec
+        self.vals, self.grads_ref, self.weights = hex8_tables()
+        (self.fvals, self.fgrads_ref, self.fweights, self.normals,
+         self.face_inds) = hex8_face_tables()
+        self.shape_grads, self.JxW = shape_grads(self.points, self.cells, self.grads_ref, self.weights)
+        self.quad_points = physical_quad_points(self.points, self.cells, self.vals)
+        self.bc_info = dirichlet_bc_info
+        self.node_inds, self.vec_inds, self.bc_vals = dirichlet_bcs(self.points, dirichlet_bc_info)
+        self.location_fns = location_fns
+        self.boundary_inds = boundary_faces(self.points, self.cells, location_fns, self.face_inds)
+        self.mass_map, self.surface_maps = mass_map, surface_maps or []
+        self.internal_vars = list(internal_vars)
+        # dof index table (problem.py:86-97)
+        self.cell_dofs = (vec * self.cells[:, :, None] + np.arange(vec)[None, None, :]).reshape(
+            self.num_cells, -1)
+
+    def update_dirichlet(self, bc_info):
+        """fe.py:260-269."""
+        self.bc_info = bc_info
+        self.node_inds, self.vec_inds, self.bc_vals = dirichlet_bcs(self.points, bc_info)
+
+    def bc_rows(self):
+        return np.concatenate([n * self.vec + v for n, v in zip(self.node_inds, self.vec_inds)]
+                              ) if self.node_inds else np.zeros(0, dtype=np.int64)
+
+    # -- kernels ---------------------------------------------------------
+    def cell_residual(self, cell_u, ivars):
+        """Laplace-kernel residual (problem.py:189-214) for all cells.
+
+        cell_u (C,8,vec) -> (C,8,vec).
+        """
+        u_grad = np.einsum("cai,cqaj->cqij", cell_u, self.shape_grads)
+        P = self.law(u_grad, ivars)
+        return np.einsum("cqij,cqaj,cq->cai", P, self.shape_grads, self.JxW)
+
+    def cell_residual_and_jacobian(self, cell_u, ivars, h=1e-30):
+        """Residual (C,8*vec) and Jacobian (C,8*vec,8*vec) via forward
+        directional derivatives along each cell dof (problem.py:262-266,299-301)."""
+        C, n = self.num_cells, 8 * self.vec
+        r = self.cell_residual(cell_u, ivars).reshape(C, n)
+        jac = np.empty((C, n, n))
+        base = cell_u.reshape(C, n).astype(np.complex128)
+        civars = [np.asarray(v, dtype=np.complex128) for v in ivars]
+        for d in range(n):
+            up = base.copy()
+            up[:, d] += 1j * h
+            jac[:, :, d] = np.imag(self.cell_residual(up.reshape(C, 8, self.vec), civars).reshape(C, n)) / h
+        return r, jac
+
+    def body_load(self):
+        """Mass-kernel vector (problem.py:216-236) for u-independent maps."""
+        f = np.zeros((self.num_nodes, self.vec))
+        if self.mass_map is None:
+            return f.reshape(-1)
+        x = self.quad_points.reshape(-1, 3)
+        u0 = np.zeros((len(x), self.vec))
+        val = eval_pointwise(self.mass_map, u0, x).reshape(self.num_cells, 8, self.vec)
+        r = np.einsum("cqi,qa,cq->cai", val, self.vals, self.JxW)
+        np.add.at(f, self.cells.reshape(-1), r.reshape(-1, self.vec))
+        return f.reshape(-1)
+
+    def surface_load(self):
+        """Surface-kernel vector (problem.py:238-259, 398-424) for u-independent maps."""
+        f = np.zeros((self.num_nodes, self.vec))
+        for binds, smap in zip(self.boundary_inds, self.surface_maps):
+            if len(binds) == 0:
+                continue
+            scale = face_geometry(self.points, self.cells, binds, self.fgrads_ref,
+                                  self.fweights, self.normals)
+            fv = self.fvals[binds[:, 1]]  # (F,q,8)
+            xq = np.einsum("fqa,fai->fqi", fv, self.points[self.cells[binds[:, 0]]])
+            u0 = np.zeros((xq.shape[0] * xq.shape[1], self.vec))
+            val = eval_pointwise(smap, u0, xq.reshape(-1, 3)).reshape(xq.shape[0], xq.shape[1], self.vec)
+            r = np.einsum("fqi,fqa,fq->fai", val, fv, scale)
+            np.add.at(f, self.cells[binds[:, 0]].reshape(-1), r.reshape(-1, self.vec))
+        return f.reshape(-1)
+
+    def external_load(self):
+        if not hasattr(self, "_fext"):
+            self._fext = self.body_load() + self.surface_load()
+        return self._fext
+
+    def residual(self, dofs):
+        """compute_residual (problem.py:426-445,462-475), flattened."""
+        cell_u = dofs.reshape(self.num_nodes, self.vec)[self.cells]
+        r = self.cell_residual(cell_u, self.internal_vars)
+        R = np.zeros((self.num_nodes, self.vec))
+        np.add.at(R, self.cells.reshape(-1), r.reshape(-1, self.vec))
+        return R.reshape(-1) + self.external_load()
+
+    def newton_update(self, dofs):
+        """compute_newton_vars (problem.py:447-460): residual + COO values V."""
+        cell_u = dofs.reshape(self.num_nodes, self.vec)[self.cells]
+        r, jac = self.cell_residual_and_jacobian(cell_u, self.internal_vars)
+        R = np.zeros(self.ndofs)
+        np.add.at(R, self.cell_dofs.reshape(-1), r.reshape(-1))
+        self.V = jac
+        return R + self.external_load()
+
+    def assemble_global(self, jac=None):
+        """PETSc COO -> AIJ with duplicate summation (solver.py:466-491, problem.py:94-107)."""
+        jac = self.V if jac is None else jac
+        n = jac.shape[1]
+        I = np.repeat(self.cell_dofs[:, :, None], n, axis=2).reshape(-1)
+        J = np.repeat(self.cell_dofs[:, None, :], n, axis=1).reshape(-1)
+        return sp.csr_matrix((jac.reshape(-1), (I, J)), shape=(self.ndofs, self.ndofs))
+
+    def get_A(self):
+        """Tangent with BC rows zeroed and unit diagonal, columns kept (solver.py:485-491)."""
+        A = self.assemble_global()
+        keep = np.ones(self.ndofs)
+        rows = self.bc_rows()
+        keep[rows] = 0.0
+        unit = np.zeros(self.ndofs)
+        unit[rows] = 1.0
+        A = sp.diags(keep) @ A + sp.diags(unit)
+        return A.tocsr()
+
+    # -- BCs (solver.py:290-363) ------------------------------------------
+    def apply_bc_vec(self, res, dofs, scale=1.0):
+        res = res.copy()
+        for n, v, val in zip(self.node_inds, self.vec_inds, self.bc_vals):
+            rows = n * self.vec + v
+            res[rows] = dofs[rows] - val * scale
+        return res
+
+    def assign_bc(self, dofs):
+        dofs = dofs.copy()
+        for n, v, val in zip(self.node_inds, self.vec_inds, self.bc_vals):
+            dofs[n * self.vec + v] = val
+        return dofs
+
+    def copy_bc(self, dofs):
+        out = np.zeros_like(dofs)
+        rows = self.bc_rows()
+        out[rows] = dofs[rows]
+        return out
+
+
+def newton_solve(problem, initial_guess=None, rel_tol=1e-8, tol=1e-6, linear="spsolve",
+                 max_iter=50, return_info=False):
+    """Newton loop of ``solver`` (solver.py:1232-1318) with the step of
+    ``newton_step`` (solver.py:390-421).  ``linear='spsolve'`` is the
+    reference's ``spsolve_solver`` (solver.py:94-107)."""
+    dofs = np.zeros(problem.ndofs) if initial_guess is None else np.asarray(initial_guess, dtype=np.float64).reshape(-1).copy()
+
+    def update(d):
+        res = problem.newton_update(d)
+        res = problem.apply_bc_vec(res, d)
+        return res, problem.get_A()
+
+    res, A = update(dofs)
+    r0 = np.linalg.norm(res)
+    rel = 1.0 if r0 > 0 else 0.0
+    hist = [r0]
+    it = 0
+    while rel > rel_tol and np.linalg.norm(res) > tol and it < max_iter:
+        it += 1
+        b = -res
+        x0 = problem.assign_bc(np.zeros(problem.ndofs)) - problem.copy_bc(dofs)
+        if linear == "spsolve":
+            inc = spla.spsolve(A.tocsc(), b)
+        else:
+            inc, _ = spla.bicgstab(A, b, x0=x0, rtol=1e-12, atol=1e-14, maxiter=20000)
+        dofs = dofs + inc
+        res, A = update(dofs)
+        hist.append(np.linalg.norm(res))
+        rel = hist[-1] / r0
+    assert np.all(np.isfinite(dofs))
+    if return_info:
+        return dofs, dict(iters=it, res_hist=hist)
+    return dofs
+
+
+# --------------------------------------------------------------------------
+# Plasticity state commit (test_plasticity.py:67-78, fe.py:366-382)
+# --------------------------------------------------------------------------
+
+def sol_to_grad(problem, dofs):
+    cell_u = dofs.reshape(problem.num_nodes, problem.vec)[problem.cells]
+    return np.einsum("cai,cqaj->cqij", cell_u, problem.shape_grads)
+
+
+def j2_commit(problem, dofs):
+    p = problem.law.params
+    sig_old, eps_old, alpha_old = problem.internal_vars
+    ug = sol_to_grad(problem, dofs)
+    sig, alpha = j2_return_map(ug, sig_old, eps_old, alpha_old, p["E"], p["nu"], p["sig0"], p["H"])
+    eps = 0.5 * (ug + np.swapaxes(ug, -1, -2))
+    problem.internal_vars = [sig, eps, alpha]
+
+
+def avg_stress(problem):
+    sig = problem.internal_vars[0]
+    return np.einsum("cqij,cq->ij", sig, problem.JxW) / problem.JxW.sum()
+
+
+# --------------------------------------------------------------------------
+# Adjoint (solver.py:1324-1380)
+# --------------------------------------------------------------------------
+
+def implicit_vjp_cellwise(problem, dofs, v, h=1e-30):
+    """-(dc/dtheta)^T lambda for a per-cell scalar internal variable theta
+    stored per quad in ``internal_vars[0]`` (shape (C,Q)).
+
+    A^T lambda = v with the BC-row-zeroed tangent at the solution
+    (solver.py:1358-1371); the parameter VJP is taken through the residual
+    with BC rows replaced (BC rows do not depend on theta).  Each cell's
+    residual depends only on its own theta, so one complex-step evaluation
+    with every theta perturbed gives all per-cell partials at once.
+    Returns dJ/dtheta per (cell, quad).
+    """
+    problem.newton_update(dofs)
+    A = problem.get_A()
+    lam = spla.spsolve(A.T.tocsc(), v)
+    lam[problem.bc_rows()] = 0.0  # BC rows of dc/dtheta vanish
+    cell_u = dofs.reshape(problem.num_nodes, problem.vec)[problem.cells]
+    cell_lam = lam.reshape(problem.num_nodes, problem.vec)[problem.cells]
+    theta = np.asarray(problem.internal_vars[0], dtype=np.float64)
+    Q = theta.shape[1]
+    grads = np.zeros_like(theta)
+    others = [np.asarray(x, dtype=np.complex128) for x in problem.internal_vars[1:]]
+    for q in range(Q):
+        tp = theta.astype(np.complex128)
+        tp[:, q] += 1j * h
+        dr = np.imag(problem.cell_residual(cell_u.astype(np.complex128), [tp] + others)) / h
+        grads[:, q] = -np.einsum("cai,cai->c", dr, cell_lam)
+    return grads
+
+
+def compliance(problem, dofs, surface_index=0):
+    """C = int t . u ds with t = -surface_map (topology_optimization cell 9)."""
+    binds = problem.boundary_inds[surface_index]
+    smap = problem.surface_maps[surface_index]
+    scale = face_geometry(problem.points, problem.cells, binds, problem.fgrads_ref,
+                          problem.fweights, problem.normals)
+    fv = problem.fvals[binds[:, 1]]
+    cu = dofs.reshape(problem.num_nodes, problem.vec)[problem.cells[binds[:, 0]]]
+    uq = np.einsum("fqa,fai->fqi", fv, cu)
+    xq = np.einsum("fqa,fai->fqi", fv, problem.points[problem.cells[binds[:, 0]]])
+    t = -eval_pointwise(smap, uq.reshape(-1, problem.vec), xq.reshape(-1, 3)).reshape(uq.shape)
+    return float(np.sum(t * uq * scale[:, :, None]))
+
+
+def surface_integral(problem, location_fn, surface_fn, dofs):
+    """Post-processing face integral of f(u_grad) used by the reference tests
+    (test_hyper_elasticity.py:36-45, test_linear_elasticity_cylinder.py:40-66)."""
+    binds = boundary_faces(problem.points, problem.cells.astype(np.int64), [location_fn], problem.face_inds)[0]
+    X = problem.points[problem.cells[binds[:, 0]]]
+    gr = problem.fgrads_ref[binds[:, 1]]
+    J = np.einsum("fai,fqaj->fqij", X, gr)
+    Jinv = np.linalg.inv(J)
+    g = np.einsum("fqaj,fqjk->fqak", gr, Jinv)
+    scale = face_geometry(problem.points, problem.cells, binds, problem.fgrads_ref,
+                          problem.fweights, problem.normals)
+    cu = dofs.reshape(problem.num_nodes, problem.vec)[problem.cells[binds[:, 0]]]
+    ug = np.einsum("fai,fqaj->fqij", cu, g)
+    val = surface_fn(ug)
+    return np.sum(val * scale[:, :, None], axis=(0, 1))

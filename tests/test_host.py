@@ -1,0 +1,174 @@
+"""Host-side logic without a GPU: the C ABI loads and exports every declared
+symbol, the pattern builder, mesh numbering, Dirichlet/face discovery, load
+vectors, law recognition and solver-option resolution."""
+import ctypes
+import os
+import re
+
+import numpy as np
+import pytest
+import scipy.sparse as sp
+
+from helpers import golden
+from oracle import fem_oracle as fo
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def test_library_exports_every_declared_symbol(pkg):
+    lib = pkg._native.load()
+    header = open(os.path.join(ROOT, "include", "jaxfem_b200.h")).read()
+    declared = set(re.findall(r"FEM_API\s+[\w\s\*]+?\b(fem_\w+)\s*\(", header))
+    assert declared, "no declarations parsed"
+    for name in declared:
+        assert hasattr(lib, name), name
+    assert declared == set(pkg._native.exported_symbols())
+    assert pkg._native.version().startswith("jaxfem_b200")
+
+
+def _pattern(pkg, cells, N):
+    lib = pkg._native.load()
+    C = len(cells)
+    cells = np.ascontiguousarray(cells, dtype=np.int32)
+    rp = np.zeros(N + 1, dtype=np.int32)
+    nnzb = ctypes.c_int64(0)
+    assert lib.fem_bsr_pattern(cells.ctypes.data, C, N, rp.ctypes.data, nnzb, None, 0, None, None) == 0
+    col = np.zeros(nnzb.value, dtype=np.int32)
+    sc = np.zeros((C, 64), dtype=np.int32)
+    dg = np.zeros(N, dtype=np.int32)
+    assert lib.fem_bsr_pattern(cells.ctypes.data, C, N, rp.ctypes.data, nnzb, col.ctypes.data, col.size,
+                               sc.ctypes.data, dg.ctypes.data) == 0
+    return rp, col, sc, dg, nnzb.value
+
+
+@pytest.mark.parametrize("shape", [(1, 1, 1), (3, 2, 4), (20, 20, 20)])
+def test_pattern_matches_node_adjacency(pkg, shape):
+    pts, cells = fo.box_mesh(*shape, 1.0, 1.0, 1.0)
+    N = len(pts)
+    rp, col, sc, dg, nnzb = _pattern(pkg, cells, N)
+    rows = np.repeat(cells[:, :, None], 8, axis=2).reshape(-1)
+    cols = np.repeat(cells[:, None, :], 8, axis=1).reshape(-1)
+    A = sp.csr_matrix((np.ones(len(rows)), (rows, cols)), shape=(N, N))
+    A.sum_duplicates()
+    A.sort_indices()
+    np.testing.assert_array_equal(rp, A.indptr)
+    np.testing.assert_array_equal(col, A.indices)
+    # scatter map points at the (cells[c,a], cells[c,b]) block
+    c = np.arange(len(cells))[:, None, None]
+    a = np.arange(8)[None, :, None]
+    b = np.arange(8)[None, None, :]
+    blk = sc.reshape(-1, 8, 8)
+    np.testing.assert_array_equal(col[blk], np.broadcast_to(cells[c, b], blk.shape))
+    row_of_blk = np.searchsorted(rp, blk, side="right") - 1
+    np.testing.assert_array_equal(row_of_blk, np.broadcast_to(cells[c, a], blk.shape))
+    np.testing.assert_array_equal(col[dg], np.arange(N))
+    Nx, Ny, Nz = shape
+    assert nnzb == (3 * Nx + 1) * (3 * Ny + 1) * (3 * Nz + 1)  # prod(3 n_i - 2) over node counts
+
+
+def test_pattern_rejects_bad_node(pkg):
+    lib = pkg._native.load()
+    cells = np.arange(8, dtype=np.int32).reshape(1, 8)
+    cells[0, 3] = 99
+    rp = np.zeros(9, dtype=np.int32)
+    n = ctypes.c_int64(0)
+    assert lib.fem_bsr_pattern(cells.ctypes.data, 1, 8, rp.ctypes.data, n, None, 0, None, None) == -1
+    assert b"outside" in lib.fem_last_error()
+
+
+def test_box_mesh_numbering_matches_reference(pkg):
+    m = pkg.box_mesh(3, 4, 5, 3.0, 2.0, 1.0)
+    p, c = fo.box_mesh(3, 4, 5, 3.0, 2.0, 1.0)
+    np.testing.assert_array_equal(m.points, p)
+    np.testing.assert_array_equal(m.cells_dict["hexahedron"], c)
+
+
+def test_dirichlet_discovery_batched_and_pointwise(pkg):
+    d = golden("hyperelasticity")
+    mesh = pkg.Mesh(d["points"], d["cells"])
+    top = lambda p: np.isclose(p[2], 10.0, atol=1e-5)  # noqa: E731
+    # a function that cannot be batched (uses Python control flow per point)
+    def ring(p):
+        return bool(p[0] ** 2 + p[1] ** 2 > 16.0) and bool(np.isclose(p[2], 0.0, atol=1e-5))
+    val = lambda p: 0.1 * p[0]  # noqa: E731
+    fe = pkg.fe.FiniteElement(mesh, 3, 3, dirichlet_bc_info=[[top, ring], [2, 0], [val, val]])
+    n_ref, v_ref, val_ref = fo.dirichlet_bcs(d["points"], [[top, ring], [2, 0], [val, val]])
+    for a, b in zip(fe.node_inds_list, n_ref):
+        np.testing.assert_array_equal(a, b)
+    for a, b in zip(fe.vals_list, val_ref):
+        np.testing.assert_allclose(a, b, rtol=0, atol=0)
+
+
+def test_load_vectors_match_oracle(pkg):
+    d = golden("linear_elasticity_cylinder")
+    mesh = pkg.Mesh(d["points"], d["cells"])
+    top = lambda p: np.isclose(p[2], 10.0, atol=1e-5)  # noqa: E731
+    mass = lambda u, x: -np.array([1e3 * x[0], 2e3 * x[1], 3e3 * x[2]])  # noqa: E731
+    surf = lambda u, x: -np.array([1e3 * x[0] ** 2 + 1e3 * x[1] ** 2, 0.0, 0.0])  # noqa: E731
+    fe = pkg.fe.FiniteElement(mesh, 3, 3)
+    binds = fe.get_boundary_conditions_inds([top])
+    op = fo.OracleProblem(d["points"], d["cells"], 3, fo.Law("linear", E=1.0, nu=0.3), location_fns=[top],
+                          mass_map=mass, surface_maps=[surf])
+    np.testing.assert_array_equal(binds[0], op.boundary_inds[0])
+    fb = fe.body_load(mass)
+    fs = fe.surface_load(surf, binds[0])
+    np.testing.assert_allclose(fb, op.body_load(), rtol=1e-12, atol=1e-9)
+    np.testing.assert_allclose(fs, op.surface_load(), rtol=1e-12, atol=1e-9)
+
+
+def test_u_dependent_maps_are_rejected(pkg):
+    m = pkg.box_mesh(2, 2, 2, 1.0, 1.0, 1.0)
+    fe = pkg.fe.FiniteElement(pkg.Mesh(m.points, m.cells_dict["hexahedron"]), 3, 3)
+    with pytest.raises(NotImplementedError):
+        fe.body_load(lambda u, x: -u)
+
+
+def test_law_recognition(pkg):
+    assert isinstance(pkg.laws.as_law(lambda x: x, 1), pkg.Laplace)
+
+    def stress(u_grad):
+        E, nu = 70e3, 0.3
+        mu = E / (2.0 * (1.0 + nu))
+        lmbda = E * nu / ((1 + nu) * (1 - 2 * nu))
+        eps = 0.5 * (u_grad + u_grad.T)
+        return lmbda * np.trace(eps) * np.eye(3) + 2 * mu * eps
+
+    law = pkg.laws.as_law(stress, 3)
+    assert isinstance(law, pkg.LinearElastic)
+    assert abs(law.E - 70e3) < 1e-6 and abs(law.nu - 0.3) < 1e-12
+    with pytest.raises(NotImplementedError):
+        pkg.laws.as_law(lambda F: F @ F.T, 3)  # nonlinear: must be a registered law
+    with pytest.raises(NotImplementedError):
+        pkg.laws.as_law(lambda u, th: u, 3)   # internal variables: must be registered
+
+
+def test_solver_option_resolution(pkg):
+    import importlib
+    s = importlib.import_module("jax_fem_b200.solver")
+    assert s._resolve_solver_options({}) == ("newton", {})
+    m, cfg = s._resolve_solver_options({"petsc_solver": {}, "tol": 1e-5})
+    assert m == "newton" and cfg["tol"] == 1e-5 and "petsc_solver" in cfg["linear"]
+    lc = s.resolve_linear({})
+    assert lc.method == pkg._native.KRYLOV_BICGSTAB and lc.precond == pkg._native.PRECOND_JACOBI
+    assert lc.rtol == 1e-10 and lc.atol == 1e-10 and lc.maxiter == 10000
+    lc = s.resolve_linear({"petsc_solver": {"ksp_type": "cg", "pc_type": "jacobi"}})
+    assert lc.method == pkg._native.KRYLOV_CG and lc.precond == pkg._native.PRECOND_JACOBI
+    with pytest.raises(ValueError):
+        s._resolve_solver_options({"newton": {}, "arc_length": {}})
+    with pytest.raises(NotImplementedError):
+        s.resolve_linear({"amgx_solver": {}})
+
+
+def test_no_gpu_means_loud_failure(pkg):
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    m = pkg.box_mesh(1, 1, 1, 1.0, 1.0, 1.0)
+
+    class P(pkg.Problem):
+        def get_tensor_map(self):
+            return pkg.LinearElastic(1.0, 0.3)
+
+    p = P(pkg.Mesh(m.points, m.cells_dict["hexahedron"]), vec=3, dim=3)
+    with pytest.raises(pkg._native.FEMNativeError):
+        pkg.solver(p)
