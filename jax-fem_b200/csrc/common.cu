@@ -1,7 +1,10 @@
 // Error reporting, launch accounting and version of the jaxfem_b200 library.
 #include <cstdarg>
+#include <mutex>
+#include <set>
+#include <utility>
 
-#include "common.cuh"
+#include "sparse.cuh"
 
 namespace fem {
 
@@ -25,6 +28,23 @@ double* host_mailbox() {
     if (cudaMallocHost(&p, 64 * sizeof(double)) != cudaSuccess) p = nullptr;
   }
   return p;
+}
+
+int ensure_smem_attr_ptr(const void* kernel) {
+  static std::mutex mu;
+  static std::set<std::pair<const void*, int>> done;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  std::lock_guard<std::mutex> lock(mu);
+  if (done.count({kernel, dev})) return FEM_OK;
+  cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       int(bsr_rows_smem()));
+  if (e != cudaSuccess) {
+    set_error("cudaFuncSetAttribute(bsr smem) -> %s", cudaGetErrorString(e));
+    return FEM_ERR_CUDA;
+  }
+  done.insert({kernel, dev});
+  return FEM_OK;
 }
 
 }  // namespace fem

@@ -8,10 +8,11 @@
 // Kernels see a non-zero status and return at once, so the host only polls
 // the status every `check_every` iterations and never stalls the pipeline.
 //
-// CG uses 2 kernels per iteration: the search direction p = z + beta p_old is
-// formed on the fly inside the SpMV (ping-pong buffers avoid read/write races
-// between neighbouring rows), and the update kernel applies the Jacobi /
-// 3x3 block-Jacobi preconditioner while it reduces r.z and r.r.
+// CG is the Chronopoulos-Gear formulation (one reduction phase per
+// iteration): a vector kernel updates p, s = A p, x, r and applies the Jacobi
+// / 3x3 block-Jacobi preconditioner u = M r while it reduces gamma = r.u and
+// r.r; a pure SpMV w = A u reduces delta = w.u, and its last block forms
+// alpha and beta for the next iteration.  Two kernels per iteration.
 #include "sparse.cuh"
 
 namespace fem {
@@ -21,8 +22,8 @@ enum : int { ST_RUNNING = 0, ST_CONVERGED = 1 };
 
 struct KState {
   double rz, rr, pq, alpha, beta, tol2, bnorm2;
-  double rho, omega;
-  int iter, status, maxiter, pad;
+  double rho, omega, rz_prev;
+  int iter, status, maxiter, first;
 };
 
 template <typename T>
@@ -95,20 +96,11 @@ __global__ void __launch_bounds__(kRowThreads) kr_residual_kernel(int64_t n_brow
                                                                  const int32_t* ci, const T* vals,
                                                                  const T* __restrict__ x,
                                                                  const T* b, T* r) {
-  const int lane = threadIdx.x & 31;
-  const int64_t w0 = int64_t(blockIdx.x) * (kRowThreads / 32) + (threadIdx.x >> 5);
-  const int64_t ws = int64_t(gridDim.x) * (kRowThreads / 32);
-  for (int64_t row = w0; row < n_brows; row += ws) {
-    double out[VEC];
-    bsr_row<VEC, T, double>(row, lane, rp, ci, vals, [&](int64_t i) { return x[i]; }, out);
-    if (lane < VEC) {
-      double o = out[0];
-#pragma unroll
-      for (int k = 1; k < VEC; ++k)
-        if (lane == k) o = out[k];
-      r[row * VEC + lane] = T(double(b[row * VEC + lane]) - o);
-    }
-  }
+  bsr_rows<VEC, T, double>(
+      n_brows, rp, ci, vals, [&](int64_t i) { return x[i]; },
+      [&](int64_t row, const double (&out)[VEC], int lane) {
+        if (lane < VEC) r[row * VEC + lane] = T(double(b[row * VEC + lane]) - lane_pick<VEC, double>(out, lane));
+      });
 }
 
 // z = M r; rz = r.z, rr = r.r, bb = b.b; initial status.
@@ -155,72 +147,75 @@ __global__ void cg_init_kernel(int precond, int64_t n_brows, const T* minv, cons
   }
 }
 
-// CG step 1: p_new = z + beta p_old (own rows), q = A p_new, pq = p_new . q
+// CG SpMV: w = A u, delta = w . u; last block forms alpha, beta.
 template <int VEC, typename T>
 __global__ void __launch_bounds__(kRowThreads) cg_spmv_kernel(int64_t n_brows, const int32_t* rp,
                                                              const int32_t* ci, const T* vals,
-                                                             const T* __restrict__ z,
-                                                             const T* __restrict__ p_old, T* p_new,
-                                                             T* q, double* partials,
-                                                             unsigned int* counter, KState* S) {
+                                                             const T* __restrict__ u, T* w,
+                                                             double* partials, unsigned int* counter,
+                                                             KState* S) {
   if (S->status != ST_RUNNING) return;
-  const T beta = T(S->beta);
-  const int lane = threadIdx.x & 31;
-  const int64_t w0 = int64_t(blockIdx.x) * (kRowThreads / 32) + (threadIdx.x >> 5);
-  const int64_t ws = int64_t(gridDim.x) * (kRowThreads / 32);
   double v[1] = {0.0};
-  for (int64_t row = w0; row < n_brows; row += ws) {
-    double out[VEC];
-    bsr_row<VEC, T, double>(row, lane, rp, ci, vals,
-                            [&](int64_t i) { return z[i] + beta * p_old[i]; }, out);
-    if (lane < VEC) {
-      double o = out[0];
-#pragma unroll
-      for (int k = 1; k < VEC; ++k)
-        if (lane == k) o = out[k];
-      const int64_t i = row * VEC + lane;
-      const T pn = z[i] + beta * p_old[i];
-      p_new[i] = pn;
-      const T qo = T(o);
-      q[i] = qo;
-      v[0] = fma(double(pn), double(qo), v[0]);
-    }
-  }
+  bsr_rows<VEC, T, T>(
+      n_brows, rp, ci, vals, [&](int64_t i) { return u[i]; },
+      [&](int64_t row, const T (&out)[VEC], int lane) {
+        if (lane < VEC) {
+          const int64_t i = row * VEC + lane;
+          const T wo = lane_pick<VEC, T>(out, lane);
+          w[i] = wo;
+          v[0] = fma(double(u[i]), double(wo), v[0]);
+        }
+      });
   double tot[1];
   if (last_block_reduce<1>(v, partials, counter, tot)) {
-    S->pq = tot[0];
-    if (!finite_d(tot[0]))
+    const double delta = tot[0], gamma = S->rz;
+    S->pq = delta;
+    double denom;
+    if (S->first) {
+      S->beta = 0.0;
+      denom = delta;
+      S->first = 0;
+    } else {
+      S->beta = gamma / S->rz_prev;
+      denom = delta - S->beta * gamma / S->alpha;
+    }
+    S->rz_prev = gamma;
+    if (!finite_d(delta))
       S->status = FEM_ERR_NONFINITE;
-    else if (!(tot[0] > 0.0))
+    else if (!(denom > 0.0))
       S->status = FEM_ERR_BREAKDOWN;
     else
-      S->alpha = S->rz / tot[0];
+      S->alpha = gamma / denom;
   }
 }
 
-// CG step 2: x += alpha p, r -= alpha q, z = M r; rz, rr; scalar update.
+// CG vector step: p = u + beta p; s = w + beta s; x += alpha p; r -= alpha s;
+// u = M r; gamma = r.u, rr = r.r; convergence / iteration bookkeeping.
 template <int VEC, typename T>
-__global__ void cg_update_kernel(int precond, int64_t n_brows, const T* minv, T* x, T* r, T* z,
-                                 const T* p, const T* q, double* partials, unsigned int* counter,
-                                 KState* S) {
+__global__ void cg_vec_kernel(int precond, int64_t n_brows, const T* minv, T* x, T* r, T* u, T* p,
+                              T* sv, const T* w, double* partials, unsigned int* counter, KState* S) {
   if (S->status != ST_RUNNING) return;
-  const T alpha = T(S->alpha);
+  const T alpha = T(S->alpha), beta = T(S->beta);
   double v[2] = {0.0, 0.0};
   for (int64_t nd = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; nd < n_brows;
        nd += int64_t(gridDim.x) * blockDim.x) {
-    T rn[VEC], zn[VEC];
+    T rn[VEC], un[VEC];
 #pragma unroll
     for (int i = 0; i < VEC; ++i) {
       const int64_t k = nd * VEC + i;
-      x[k] += alpha * p[k];
-      rn[i] = r[k] - alpha * q[k];
+      const T pk = u[k] + beta * p[k];
+      const T sk = w[k] + beta * sv[k];
+      p[k] = pk;
+      sv[k] = sk;
+      x[k] += alpha * pk;
+      rn[i] = r[k] - alpha * sk;
       r[k] = rn[i];
     }
-    apply_precond<VEC, T>(precond, nd, minv, rn, zn);
+    apply_precond<VEC, T>(precond, nd, minv, rn, un);
 #pragma unroll
     for (int i = 0; i < VEC; ++i) {
-      if (z != r) z[nd * VEC + i] = zn[i];
-      v[0] = fma(double(rn[i]), double(zn[i]), v[0]);
+      if (u != r) u[nd * VEC + i] = un[i];
+      v[0] = fma(double(rn[i]), double(un[i]), v[0]);
       v[1] = fma(double(rn[i]), double(rn[i]), v[1]);
     }
   }
@@ -228,17 +223,15 @@ __global__ void cg_update_kernel(int precond, int64_t n_brows, const T* minv, T*
   if (last_block_reduce<2>(v, partials, counter, tot)) {
     S->iter += 1;
     S->rr = tot[1];
+    S->rz = tot[0];
     if (!finite_d(tot[0]) || !finite_d(tot[1])) {
       S->status = FEM_ERR_NONFINITE;
     } else if (tot[1] <= S->tol2) {
       S->status = ST_CONVERGED;
     } else if (S->iter >= S->maxiter) {
       S->status = FEM_ERR_NOT_CONVERGED;
-    } else if (S->rz == 0.0) {
+    } else if (tot[0] == 0.0) {
       S->status = FEM_ERR_BREAKDOWN;
-    } else {
-      S->beta = tot[0] / S->rz;
-      S->rz = tot[0];
     }
   }
 }
@@ -274,25 +267,18 @@ __global__ void __launch_bounds__(kRowThreads) bicg_spmv_kernel(int mode, int64_
                                                                const T* w, double* partials,
                                                                unsigned int* counter, KState* S) {
   if (S->status != ST_RUNNING) return;
-  const int lane = threadIdx.x & 31;
-  const int64_t w0 = int64_t(blockIdx.x) * (kRowThreads / 32) + (threadIdx.x >> 5);
-  const int64_t wsd = int64_t(gridDim.x) * (kRowThreads / 32);
   double v[2] = {0.0, 0.0};
-  for (int64_t row = w0; row < n_brows; row += wsd) {
-    double out[VEC];
-    bsr_row<VEC, T, double>(row, lane, rp, ci, vals, [&](int64_t i) { return x[i]; }, out);
-    if (lane < VEC) {
-      double o = out[0];
-#pragma unroll
-      for (int k = 1; k < VEC; ++k)
-        if (lane == k) o = out[k];
-      const int64_t i = row * VEC + lane;
-      const T yo = T(o);
-      y[i] = yo;
-      v[0] = fma(double(w[i]), double(yo), v[0]);
-      v[1] = fma(double(yo), double(yo), v[1]);
-    }
-  }
+  bsr_rows<VEC, T, T>(
+      n_brows, rp, ci, vals, [&](int64_t i) { return x[i]; },
+      [&](int64_t row, const T (&out)[VEC], int lane) {
+        if (lane < VEC) {
+          const int64_t i = row * VEC + lane;
+          const T yo = lane_pick<VEC, T>(out, lane);
+          y[i] = yo;
+          v[0] = fma(double(w[i]), double(yo), v[0]);
+          v[1] = fma(double(yo), double(yo), v[1]);
+        }
+      });
   double tot[2];
   if (last_block_reduce<2>(v, partials, counter, tot)) {
     if (mode == 0) {
@@ -416,6 +402,7 @@ int solve_impl(int method, int precond, int64_t n_brows, const int32_t* rp, cons
   FEM_CUDA_TRY(cudaMemsetAsync(work, 0, 512, st));
   KState init{};
   init.maxiter = maxiter;
+  init.first = 1;
   FEM_CUDA_TRY(cudaMemcpyAsync(S, &init, sizeof(KState), cudaMemcpyHostToDevice, st));
   // cudaMemcpyAsync from pageable memory is synchronous w.r.t. the host copy,
   // so `init` may go out of scope after this point.
@@ -424,22 +411,32 @@ int solve_impl(int method, int precond, int64_t n_brows, const int32_t* rp, cons
                                                                                 diag, vals, minv);
     FEM_LAUNCH_CHECK();
   }
-  const unsigned rg = row_grid(n_brows), vg = vec_grid(n_brows), vgn = vec_grid(n);
+  const unsigned rg = row_grid<T>(n_brows), vg = vec_grid(n_brows), vgn = vec_grid(n);
+  {
+    int rc = FEM_OK;
+    if ((rc = ensure_smem_attr(kr_residual_kernel<VEC, T>)) != FEM_OK) return rc;
+    if ((rc = ensure_smem_attr(cg_spmv_kernel<VEC, T>)) != FEM_OK) return rc;
+    if ((rc = ensure_smem_attr(bicg_spmv_kernel<VEC, T>)) != FEM_OK) return rc;
+  }
   T* r = V[0];
-  kr_residual_kernel<VEC, T><<<rg, kRowThreads, 0, st>>>(n_brows, rp, ci, vals, x, b, r);
+  kr_residual_kernel<VEC, T><<<rg, kRowThreads, bsr_rows_smem(), st>>>(n_brows, rp, ci, vals, x, b, r);
   FEM_LAUNCH_CHECK();
 
   T *z = nullptr, *p0 = nullptr, *p1 = nullptr, *q = nullptr;
   T *rhat = nullptr, *pp = nullptr, *phat = nullptr, *vv = nullptr, *s = nullptr, *shat = nullptr,
     *t = nullptr;
   if (method == FEM_KRYLOV_CG) {
-    z = (precond == FEM_PRECOND_NONE) ? r : V[1];
-    p0 = V[2];
-    p1 = V[3];
-    q = V[4];
+    z = (precond == FEM_PRECOND_NONE) ? r : V[1];  // u = M r
+    p0 = V[2];                                      // p
+    p1 = V[3];                                      // s = A p
+    q = V[4];                                       // w = A u
     FEM_CUDA_TRY(cudaMemsetAsync(p0, 0, sizeof(T) * n, st));
+    FEM_CUDA_TRY(cudaMemsetAsync(p1, 0, sizeof(T) * n, st));
     cg_init_kernel<VEC, T><<<vg, 256, 0, st>>>(precond, n_brows, minv, r, z, b, partials, counter, S,
                                                rtol, atol);
+    FEM_LAUNCH_CHECK();
+    cg_spmv_kernel<VEC, T><<<rg, kRowThreads, bsr_rows_smem(), st>>>(n_brows, rp, ci, vals, z, q,
+                                                                    partials, counter, S);
     FEM_LAUNCH_CHECK();
   } else {
     rhat = V[1];
@@ -476,24 +473,21 @@ int solve_impl(int method, int precond, int64_t n_brows, const int32_t* rp, cons
     const int chunk = check_every < (maxiter - launched) ? check_every : (maxiter - launched);
     for (int k = 0; k < chunk; ++k) {
       if (method == FEM_KRYLOV_CG) {
-        cg_spmv_kernel<VEC, T><<<rg, kRowThreads, 0, st>>>(n_brows, rp, ci, vals, z, p0, p1, q,
-                                                           partials, counter, S);
+        cg_vec_kernel<VEC, T><<<vg, 256, 0, st>>>(precond, n_brows, minv, x, r, z, p0, p1, q, partials,
+                                                  counter, S);
         FEM_LAUNCH_CHECK();
-        cg_update_kernel<VEC, T><<<vg, 256, 0, st>>>(precond, n_brows, minv, x, r, z, p1, q, partials,
-                                                     counter, S);
+        cg_spmv_kernel<VEC, T><<<rg, kRowThreads, bsr_rows_smem(), st>>>(n_brows, rp, ci, vals, z, q,
+                                                                        partials, counter, S);
         FEM_LAUNCH_CHECK();
-        T* tmp = p0;
-        p0 = p1;
-        p1 = tmp;
       } else {
         bicg_p_kernel<VEC, T><<<vg, 256, 0, st>>>(precond, n_brows, minv, r, pp, vv, phat, S);
         FEM_LAUNCH_CHECK();
-        bicg_spmv_kernel<VEC, T><<<rg, kRowThreads, 0, st>>>(0, n_brows, rp, ci, vals, phat, vv,
+        bicg_spmv_kernel<VEC, T><<<rg, kRowThreads, bsr_rows_smem(), st>>>(0, n_brows, rp, ci, vals, phat, vv,
                                                              rhat, partials, counter, S);
         FEM_LAUNCH_CHECK();
         bicg_s_kernel<VEC, T><<<vg, 256, 0, st>>>(precond, n_brows, minv, r, vv, s, shat, S);
         FEM_LAUNCH_CHECK();
-        bicg_spmv_kernel<VEC, T><<<rg, kRowThreads, 0, st>>>(1, n_brows, rp, ci, vals, shat, t, s,
+        bicg_spmv_kernel<VEC, T><<<rg, kRowThreads, bsr_rows_smem(), st>>>(1, n_brows, rp, ci, vals, shat, t, s,
                                                              partials, counter, S);
         FEM_LAUNCH_CHECK();
         bicg_x_kernel<VEC, T><<<vgn, 256, 0, st>>>(n, x, r, rhat, phat, shat, s, t, partials,

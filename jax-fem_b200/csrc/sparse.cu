@@ -9,21 +9,12 @@ template <int VEC, typename VT, typename XT, typename YT>
 __global__ void __launch_bounds__(kRowThreads) spmv_kernel(int64_t n_brows, const int32_t* rp,
                                                           const int32_t* ci, const VT* vals,
                                                           const XT* __restrict__ x, YT* y) {
-  const int lane = threadIdx.x & 31;
-  const int64_t w0 = int64_t(blockIdx.x) * (kRowThreads / 32) + (threadIdx.x >> 5);
-  const int64_t ws = int64_t(gridDim.x) * (kRowThreads / 32);
   using AT = typename std::conditional<(sizeof(VT) == 8 || sizeof(XT) == 8), double, float>::type;
-  for (int64_t row = w0; row < n_brows; row += ws) {
-    AT out[VEC];
-    bsr_row<VEC, VT, AT>(row, lane, rp, ci, vals, [&](int64_t i) { return x[i]; }, out);
-    if (lane < VEC) {
-      AT o = out[0];
-#pragma unroll
-      for (int r = 1; r < VEC; ++r)
-        if (lane == r) o = out[r];
-      y[row * VEC + lane] = YT(o);
-    }
-  }
+  bsr_rows<VEC, VT, AT>(
+      n_brows, rp, ci, vals, [&](int64_t i) { return x[i]; },
+      [&](int64_t row, const AT (&out)[VEC], int lane) {
+        if (lane < VEC) y[row * VEC + lane] = YT(lane_pick<VEC, AT>(out, lane));
+      });
 }
 
 // r = b - A x (A f32, x/b/r f64, f64 accumulation)
@@ -32,20 +23,11 @@ __global__ void __launch_bounds__(kRowThreads) residual_mixed_kernel(int64_t n_b
                                                                     const int32_t* ci, const float* vals,
                                                                     const double* __restrict__ x,
                                                                     const double* b, double* r) {
-  const int lane = threadIdx.x & 31;
-  const int64_t w0 = int64_t(blockIdx.x) * (kRowThreads / 32) + (threadIdx.x >> 5);
-  const int64_t ws = int64_t(gridDim.x) * (kRowThreads / 32);
-  for (int64_t row = w0; row < n_brows; row += ws) {
-    double out[VEC];
-    bsr_row<VEC, float, double>(row, lane, rp, ci, vals, [&](int64_t i) { return x[i]; }, out);
-    if (lane < VEC) {
-      double o = out[0];
-#pragma unroll
-      for (int rr = 1; rr < VEC; ++rr)
-        if (lane == rr) o = out[rr];
-      r[row * VEC + lane] = b[row * VEC + lane] - o;
-    }
-  }
+  bsr_rows<VEC, float, double>(
+      n_brows, rp, ci, vals, [&](int64_t i) { return x[i]; },
+      [&](int64_t row, const double (&out)[VEC], int lane) {
+        if (lane < VEC) r[row * VEC + lane] = b[row * VEC + lane] - lane_pick<VEC, double>(out, lane);
+      });
 }
 
 __global__ void dot_kernel(int64_t n, const double* x, const double* y, double* partials,
@@ -96,12 +78,12 @@ extern "C" int fem_bsr_spmv_f64(int vec, int64_t n_brows, const int32_t* d_row_p
   FEM_CHECK_ARG(n_brows >= 0, "negative size");
   if (n_brows == 0) return FEM_OK;
   auto st = as_stream(stream);
+  int rc = ensure_smem_attr(vec == 3 ? spmv_kernel<3, double, double, double> : spmv_kernel<1, double, double, double>);
+  if (rc != FEM_OK) return rc;
   if (vec == 3)
-    spmv_kernel<3, double, double, double><<<row_grid(n_brows), kRowThreads, 0, st>>>(
-        n_brows, d_row_ptr, d_col_idx, d_vals, d_x, d_y);
+    spmv_kernel<3, double, double, double><<<row_grid<double>(n_brows), kRowThreads, bsr_rows_smem(), st>>>(n_brows, d_row_ptr, d_col_idx, d_vals, d_x, d_y);
   else
-    spmv_kernel<1, double, double, double><<<row_grid(n_brows), kRowThreads, 0, st>>>(
-        n_brows, d_row_ptr, d_col_idx, d_vals, d_x, d_y);
+    spmv_kernel<1, double, double, double><<<row_grid<double>(n_brows), kRowThreads, bsr_rows_smem(), st>>>(n_brows, d_row_ptr, d_col_idx, d_vals, d_x, d_y);
   FEM_LAUNCH_CHECK();
   return FEM_OK;
 }
@@ -113,12 +95,12 @@ extern "C" int fem_bsr_spmv_f32(int vec, int64_t n_brows, const int32_t* d_row_p
   FEM_CHECK_ARG(n_brows >= 0, "negative size");
   if (n_brows == 0) return FEM_OK;
   auto st = as_stream(stream);
+  int rc = ensure_smem_attr(vec == 3 ? spmv_kernel<3, float, float, float> : spmv_kernel<1, float, float, float>);
+  if (rc != FEM_OK) return rc;
   if (vec == 3)
-    spmv_kernel<3, float, float, float><<<row_grid(n_brows), kRowThreads, 0, st>>>(
-        n_brows, d_row_ptr, d_col_idx, d_vals, d_x, d_y);
+    spmv_kernel<3, float, float, float><<<row_grid<float>(n_brows), kRowThreads, bsr_rows_smem(), st>>>(n_brows, d_row_ptr, d_col_idx, d_vals, d_x, d_y);
   else
-    spmv_kernel<1, float, float, float><<<row_grid(n_brows), kRowThreads, 0, st>>>(
-        n_brows, d_row_ptr, d_col_idx, d_vals, d_x, d_y);
+    spmv_kernel<1, float, float, float><<<row_grid<float>(n_brows), kRowThreads, bsr_rows_smem(), st>>>(n_brows, d_row_ptr, d_col_idx, d_vals, d_x, d_y);
   FEM_LAUNCH_CHECK();
   return FEM_OK;
 }
@@ -131,12 +113,12 @@ extern "C" int fem_bsr_residual_mixed(int vec, int64_t n_brows, const int32_t* d
   FEM_CHECK_ARG(n_brows >= 0, "negative size");
   if (n_brows == 0) return FEM_OK;
   auto st = as_stream(stream);
+  int rc = ensure_smem_attr(vec == 3 ? residual_mixed_kernel<3> : residual_mixed_kernel<1>);
+  if (rc != FEM_OK) return rc;
   if (vec == 3)
-    residual_mixed_kernel<3><<<row_grid(n_brows), kRowThreads, 0, st>>>(
-        n_brows, d_row_ptr, d_col_idx, d_vals, d_x, d_b, d_r);
+    residual_mixed_kernel<3><<<row_grid<float>(n_brows), kRowThreads, bsr_rows_smem(), st>>>(n_brows, d_row_ptr, d_col_idx, d_vals, d_x, d_b, d_r);
   else
-    residual_mixed_kernel<1><<<row_grid(n_brows), kRowThreads, 0, st>>>(
-        n_brows, d_row_ptr, d_col_idx, d_vals, d_x, d_b, d_r);
+    residual_mixed_kernel<1><<<row_grid<float>(n_brows), kRowThreads, bsr_rows_smem(), st>>>(n_brows, d_row_ptr, d_col_idx, d_vals, d_x, d_b, d_r);
   FEM_LAUNCH_CHECK();
   return FEM_OK;
 }

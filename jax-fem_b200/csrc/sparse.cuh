@@ -4,38 +4,148 @@
 
 namespace fem {
 
-constexpr int kRowThreads = 256;  // 8 warps per block, one warp per block row
+constexpr int kRowThreads = 256;   // 8 warps per block
+constexpr int kStageBytes = 8192;  // per-warp shared-memory stage for matrix values
 
-// One warp computes out = sum_k A(row, k) x(col_k) for one block row; lane l
-// owns blocks l, l+32, ... of the row (a HEX8 interior row has 27 blocks, so
-// one pass).  XF fetches x by dof index so callers can form x on the fly.
-template <int VEC, typename VT, typename AT, class XF>
-__device__ __forceinline__ void bsr_row(int64_t row, int lane, const int32_t* __restrict__ rp,
-                                        const int32_t* __restrict__ ci,
-                                        const VT* __restrict__ vals, XF xf, AT out[VEC]) {
-  AT acc[VEC];
-#pragma unroll
-  for (int r = 0; r < VEC; ++r) acc[r] = AT(0);
-  const int s = rp[row], e = rp[row + 1];
-  for (int k = s + lane; k < e; k += 32) {
-    const int64_t col = ci[k];
-    AT xv[VEC];
-#pragma unroll
-    for (int c = 0; c < VEC; ++c) xv[c] = AT(xf(col * VEC + c));
-    const VT* bv = vals + int64_t(k) * (VEC * VEC);
-#pragma unroll
-    for (int r = 0; r < VEC; ++r)
-#pragma unroll
-      for (int c = 0; c < VEC; ++c) acc[r] = fma(AT(__ldg(bv + r * VEC + c)), xv[c], acc[r]);
-  }
-#pragma unroll
-  for (int r = 0; r < VEC; ++r) out[r] = warp_sum(acc[r]);
+template <typename VT>
+__host__ __device__ constexpr int rows_per_warp() {
+  return sizeof(VT) == 4 ? 8 : 4;  // ~7.8 KB of 3x3 blocks per group either way
 }
 
+// Dynamic shared memory a bsr_rows kernel needs (one stage per warp).
+constexpr size_t bsr_rows_smem() { return size_t(kRowThreads / 32) * (kStageBytes + 16); }
+
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+  const unsigned sa = static_cast<unsigned>(__cvta_generic_to_shared(smem));
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() {
+  asm volatile("cp.async.commit_group;\n" ::: "memory");
+  asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+}
+
+// Grid-stride loop in which each warp owns groups of R consecutive block rows
+// (R = rows_per_warp<VT>()).  The values of a group are one contiguous byte
+// range; the warp copies it into its shared-memory stage with 16-byte
+// cp.async transfers (fully coalesced, no registers), and while those are in
+// flight it gathers the column indices and x values.  Lane l then handles
+// blocks l, l+32, ... of each row from shared memory (a HEX8 interior row has
+// 27 blocks).  XF fetches x by dof index (callers may form x on the fly);
+// EPI(row, out[VEC], lane) consumes the warp-reduced row result.  Groups too
+// large for the stage (very high-degree rows) read values directly.
+template <int VEC, typename VT, typename AT, class XF, class EPI>
+__device__ __forceinline__ void bsr_rows(int64_t n_brows, const int32_t* __restrict__ rp,
+                                         const int32_t* __restrict__ ci,
+                                         const VT* __restrict__ vals, XF xf, EPI epi) {
+  constexpr int R = rows_per_warp<VT>();
+  constexpr int VV = VEC * VEC;
+  extern __shared__ __align__(16) unsigned char bsr_smem[];
+  unsigned char* stage = bsr_smem + (threadIdx.x >> 5) * (kStageBytes + 16);
+  const int lane = threadIdx.x & 31;
+  const int64_t gw = int64_t(blockIdx.x) * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  const int64_t ngw = int64_t(gridDim.x) * (blockDim.x >> 5);
+  const int64_t total_bytes = int64_t(rp[n_brows]) * VV * int64_t(sizeof(VT));
+  const int64_t full_chunks = total_bytes >> 4;  // 16-byte chunks entirely inside vals
+  for (int64_t g = gw; g * R < n_brows; g += ngw) {
+    const int64_t row0 = g * R;
+    // rp[row0 .. row0+R] with one coalesced load
+    const int64_t nr = (n_brows - row0) < R ? (n_brows - row0) : R;
+    const int rpv = lane <= nr ? rp[row0 + lane] : 0;
+    int s[R + 1];
+#pragma unroll
+    for (int r = 0; r <= R; ++r) s[r] = __shfl_sync(0xffffffffu, rpv, r <= nr ? r : int(nr));
+    const int64_t byte0 = int64_t(s[0]) * VV * int64_t(sizeof(VT));
+    const int64_t byte1 = int64_t(s[R]) * VV * int64_t(sizeof(VT));
+    const int64_t c0 = byte0 >> 4, c1 = (byte1 + 15) >> 4;
+    const bool staged = (c1 - c0) * 16 <= kStageBytes;
+    if (staged) {
+      const unsigned char* gsrc = reinterpret_cast<const unsigned char*>(vals);
+      for (int64_t c = c0 + lane; c < c1; c += 32) {
+        unsigned char* dst = stage + (c - c0) * 16;
+        if (c < full_chunks) {
+          cp_async16(dst, gsrc + c * 16);
+        } else {  // ragged tail of the array: element-wise, inside bounds only
+          for (int k = 0; k < 16 / int(sizeof(VT)); ++k) {
+            const int64_t byte = c * 16 + k * int64_t(sizeof(VT));
+            if (byte < total_bytes)
+              reinterpret_cast<VT*>(dst)[k] = __ldg(reinterpret_cast<const VT*>(gsrc + byte));
+          }
+        }
+      }
+    }
+    // gathers while the stage fills
+    int64_t col[R];
+    AT xv[R][VEC];
+    int maxlen = 0;
+#pragma unroll
+    for (int r = 0; r < R; ++r) maxlen = max(maxlen, s[r + 1] - s[r]);
+    AT acc[R][VEC];
+#pragma unroll
+    for (int r = 0; r < R; ++r)
+#pragma unroll
+      for (int i = 0; i < VEC; ++i) acc[r][i] = AT(0);
+    for (int off = 0; off < maxlen; off += 32) {
+#pragma unroll
+      for (int r = 0; r < R; ++r) {
+        const int k = s[r] + off + lane;
+        col[r] = k < s[r + 1] ? int64_t(ci[k]) : -1;
+      }
+#pragma unroll
+      for (int r = 0; r < R; ++r)
+#pragma unroll
+        for (int c = 0; c < VEC; ++c) xv[r][c] = col[r] >= 0 ? AT(xf(col[r] * VEC + c)) : AT(0);
+      if (staged && off == 0) {
+        cp_async_wait_all();
+        __syncwarp();
+      }
+#pragma unroll
+      for (int r = 0; r < R; ++r) {
+        if (col[r] < 0) continue;
+        const int k = s[r] + off + lane;
+        const VT* bv = staged ? reinterpret_cast<const VT*>(stage + (int64_t(k) * VV * int64_t(sizeof(VT)) - c0 * 16))
+                              : vals + int64_t(k) * VV;
+#pragma unroll
+        for (int i = 0; i < VEC; ++i)
+#pragma unroll
+          for (int c = 0; c < VEC; ++c) acc[r][i] = fma(AT(bv[i * VEC + c]), xv[r][c], acc[r][i]);
+      }
+    }
+    if (staged && maxlen == 0) {
+      cp_async_wait_all();
+    }
+    __syncwarp();  // stage reused by the next group
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+#pragma unroll
+      for (int i = 0; i < VEC; ++i) acc[r][i] = warp_sum(acc[r][i]);
+      if (row0 + r < n_brows) epi(row0 + r, acc[r], lane);
+    }
+  }
+}
+
+// Select out[lane] for lane < VEC (registers cannot be indexed dynamically).
+template <int VEC, typename AT>
+__device__ __forceinline__ AT lane_pick(const AT out[VEC], int lane) {
+  AT o = out[0];
+#pragma unroll
+  for (int r = 1; r < VEC; ++r)
+    if (lane == r) o = out[r];
+  return o;
+}
+
+// Opt a bsr_rows kernel into its dynamic shared memory (> 48 KB) once per
+// kernel and device.
+int ensure_smem_attr_ptr(const void* kernel);
+template <typename K>
+inline int ensure_smem_attr(K* kernel) {
+  return ensure_smem_attr_ptr(reinterpret_cast<const void*>(kernel));
+}
+
+template <typename VT>
 inline unsigned row_grid(int64_t n_brows) {
-  // grid-stride: at most 8 resident blocks per SM worth of warps
-  const int64_t blocks_needed = (n_brows + (kRowThreads / 32) - 1) / (kRowThreads / 32);
-  const int64_t cap = int64_t(num_sms()) * 8;
+  const int64_t groups = (n_brows + rows_per_warp<VT>() - 1) / rows_per_warp<VT>();
+  const int64_t blocks_needed = (groups + (kRowThreads / 32) - 1) / (kRowThreads / 32);
+  const int64_t cap = int64_t(num_sms()) * 3;  // 3 resident blocks per SM (shared-memory stages)
   return unsigned(blocks_needed < cap ? (blocks_needed > 0 ? blocks_needed : 1) : cap);
 }
 
