@@ -206,6 +206,23 @@ FEM_API size_t fem_dot_workspace_bytes(int64_t n);
 FEM_API int fem_dot_f64(int64_t n, const double* d_x, const double* d_y, double* h_out,
                 void* d_work, size_t work_bytes, void* stream);
 
+/* ---- dot product that allocates nothing ---------------------------------
+ * No counterpart in the reference.  For callers that cannot allocate device
+ * memory: code whose device memory is owned by a host framework's pool that
+ * forbids raw cudaMalloc, or real-time loops that must not allocate once
+ * running.  Same reduction as fem_dot_f64, but its scratch (per-block
+ * partial sums, completion counter, result slot) is a file-scope static
+ * __device__ array inside the library, and the result goes to the caller's
+ * device double *d_out, asynchronously on `stream`.
+ *  - n <= 16,777,216; larger n returns FEM_ERR_ARG.
+ *  - The array (~32 KB) stays resident on every GPU that loads the library.
+ *  - All calls share it: calls whose kernels overlap on the GPU race.
+ *  - The first call on a device looks up the array's address
+ *    (cudaGetSymbolAddress); make it before any stream capture.
+ * ------------------------------------------------------------------------ */
+FEM_API int fem_dot_f64_noalloc(int64_t n, const double* d_x, const double* d_y, double* d_out,
+                                void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -71,6 +71,7 @@ _SIGS = {
     "fem_newton_rhs": (I32, [I64, P, P, P, P, P, P, P, P, DP, P, SZ, P]),
     "fem_dot_workspace_bytes": (SZ, [I64]),
     "fem_dot_f64": (I32, [I64, P, P, DP, P, SZ, P]),
+    "fem_dot_f64_noalloc": (I32, [I64, P, P, P, P]),
 }
 
 _lib = None

@@ -1,5 +1,7 @@
 // Block-CSR SpMV, mixed-precision refinement residual, dot product and the
 // Newton right-hand side.  All HBM-streaming kernels.
+#include <mutex>
+
 #include "sparse.cuh"
 
 namespace fem {
@@ -194,5 +196,84 @@ extern "C" int fem_newton_rhs(int64_t ndofs, const double* d_res, const double* 
     FEM_CUDA_TRY(cudaStreamSynchronize(st));
     *h_norm2 = mb[0];
   }
+  return FEM_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Dot product that allocates nothing.
+//
+// For callers that cannot allocate device memory themselves: code running
+// under a host framework that owns every device allocation through its own
+// pool and forbids raw cudaMalloc, or a real-time loop that must not allocate
+// (or risk an allocation failure) once it is running.  Same reduction kernel
+// as fem_dot_f64; its per-block partial sums, completion counter and result
+// slot live in the file-scope array below instead of a caller workspace.
+//
+// Limits and sharing rules:
+//  - n <= kNoAllocMaxN (16,777,216 elements): one partial sum per 4096
+//    elements, at most 4096 partial sums (32 KB).  Larger n is rejected with
+//    FEM_ERR_ARG.
+//  - Every GPU that loads this library holds the array until the process
+//    exits.  All calls share it: two calls whose kernels overlap on the GPU
+//    (e.g. on different streams) race and give wrong results.  The counter
+//    and the result slot are cleared at the start of every call, so a call
+//    never sees the previous call's contents.
+//  - The first call on a device resolves the array's device address with
+//    cudaGetSymbolAddress (once per device, that device current).  Make that
+//    first call before any stream capture.
+//  - The result is written to the caller's device double *d_out; the call is
+//    asynchronous on `stream` (no host synchronisation, no pinned buffer).
+// ---------------------------------------------------------------------------
+namespace fem {
+namespace {
+constexpr int64_t kNoAllocItemsPerBlock = 4096;  // 256 threads x 16 elements
+constexpr int64_t kNoAllocMaxBlocks = 4096;
+constexpr int64_t kNoAllocMaxN = kNoAllocItemsPerBlock * kNoAllocMaxBlocks;
+// doubles [0, 8): completion counter (first 4 bytes); [8]: reduction result;
+// [16, 16 + kNoAllocMaxBlocks): per-block partial sums
+static __device__ __align__(256) double g_noalloc_scratch[16 + kNoAllocMaxBlocks];
+
+std::mutex g_noalloc_mu;
+void* g_noalloc_addr[64] = {nullptr};
+
+int noalloc_scratch(double** out) {
+  int dev = 0;
+  FEM_CUDA_TRY(cudaGetDevice(&dev));
+  FEM_CHECK_ARG(dev >= 0 && dev < 64, "device index %d out of range", dev);
+  std::lock_guard<std::mutex> lock(g_noalloc_mu);
+  if (g_noalloc_addr[dev] == nullptr) {
+    void* p = nullptr;
+    FEM_CUDA_TRY(cudaGetSymbolAddress(&p, g_noalloc_scratch));
+    g_noalloc_addr[dev] = p;
+  }
+  *out = static_cast<double*>(g_noalloc_addr[dev]);
+  return FEM_OK;
+}
+
+__global__ void copy_scalar_kernel(const double* src, double* dst) { *dst = *src; }
+}  // namespace
+}  // namespace fem
+
+extern "C" int fem_dot_f64_noalloc(int64_t n, const double* d_x, const double* d_y, double* d_out,
+                                   void* stream) {
+  FEM_CHECK_ARG(n >= 0, "negative size");
+  FEM_CHECK_ARG(n <= fem::kNoAllocMaxN,
+                "fem_dot_f64_noalloc: n = %lld exceeds the no-alloc maximum of %lld elements",
+                (long long)n, (long long)fem::kNoAllocMaxN);
+  FEM_CHECK_ARG(d_out != nullptr && (n == 0 || (d_x != nullptr && d_y != nullptr)),
+                "NULL pointer argument");
+  double* scratch = nullptr;
+  int rc = fem::noalloc_scratch(&scratch);
+  if (rc != FEM_OK) return rc;
+  auto st = as_stream(stream);
+  unsigned int* counter = reinterpret_cast<unsigned int*>(scratch);
+  double* result = scratch + 8;
+  double* partials = scratch + 16;
+  FEM_CUDA_TRY(cudaMemsetAsync(scratch, 0, 16 * sizeof(double), st));
+  const int64_t blocks = n == 0 ? 1 : (n + fem::kNoAllocItemsPerBlock - 1) / fem::kNoAllocItemsPerBlock;
+  dot_kernel<<<unsigned(blocks), 256, 0, st>>>(n, d_x, d_y, partials, counter, result);
+  FEM_LAUNCH_CHECK();
+  fem::copy_scalar_kernel<<<1, 1, 0, st>>>(result, d_out);
+  FEM_LAUNCH_CHECK();
   return FEM_OK;
 }
