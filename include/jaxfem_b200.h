@@ -166,14 +166,21 @@ FEM_API int fem_bsr_residual_mixed(int vec, int64_t n_brows, const int32_t* d_ro
 
 /* ---- Krylov solvers -----------------------------------------------------
  * Replace linear_solver / jax_solve (solver.py:63-92, 261-284): solve
- * A x = b to ||b - A x|| <= max(rtol ||b||, atol) with the true (unpreconditioned)
- * residual, starting from the x passed in.  The iteration runs on the device;
- * the host polls a status word every `check_every` iterations.
- * *h_iters and *h_relres receive the iteration count and ||r||/||b||.
- * Returns FEM_ERR_NOT_CONVERGED / FEM_ERR_BREAKDOWN / FEM_ERR_NONFINITE with
- * x holding the last iterate.
+ * A x = b to ||b - A x|| <= max(rtol ||b||, atol), starting from the x passed
+ * in.  The iteration runs on the device; the host polls a status word every
+ * `check_every` iterations.  When the recursively updated residual meets the
+ * tolerance the true residual b - A x is recomputed; if it does not meet the
+ * tolerance the recurrence restarts from it; a breakdown (zero or
+ * non-positive denominator, typically round-off near the attainable
+ * accuracy) also restarts from the true residual.  After 3 restarts the call
+ * returns FEM_ERR_NOT_CONVERGED.  *h_iters = total iterations, *h_relres = the last
+ * true (or, while iterating, recursive) ||r||/||b||.  Returns
+ * FEM_ERR_NOT_CONVERGED / FEM_ERR_BREAKDOWN / FEM_ERR_NONFINITE with x
+ * holding the last iterate.
  * _f64: values/vectors f64.  _f32: values/vectors f32, dot products and
- * their reductions in f64.  d_work must hold fem_krylov_workspace_bytes(). */
+ * their reductions in f64 (an FP32 solve cannot push the true residual much
+ * below ~1e-6 relative; the mixed path refines in FP64 around it).
+ * d_work must hold fem_krylov_workspace_bytes() bytes. */
 FEM_API size_t fem_krylov_workspace_bytes(int method, int precond, int vec, int64_t n_brows, int fp32);
 FEM_API int fem_krylov_solve_f64(int method, int precond, int vec, int64_t n_brows,
                          const int32_t* d_row_ptr, const int32_t* d_col_idx,

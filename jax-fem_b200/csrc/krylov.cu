@@ -419,9 +419,6 @@ int solve_impl(int method, int precond, int64_t n_brows, const int32_t* rp, cons
     if ((rc = ensure_smem_attr(bicg_spmv_kernel<VEC, T>)) != FEM_OK) return rc;
   }
   T* r = V[0];
-  kr_residual_kernel<VEC, T><<<rg, kRowThreads, bsr_rows_smem(), st>>>(n_brows, rp, ci, vals, x, b, r);
-  FEM_LAUNCH_CHECK();
-
   T *z = nullptr, *p0 = nullptr, *p1 = nullptr, *q = nullptr;
   T *rhat = nullptr, *pp = nullptr, *phat = nullptr, *vv = nullptr, *s = nullptr, *shat = nullptr,
     *t = nullptr;
@@ -430,14 +427,6 @@ int solve_impl(int method, int precond, int64_t n_brows, const int32_t* rp, cons
     p0 = V[2];                                      // p
     p1 = V[3];                                      // s = A p
     q = V[4];                                       // w = A u
-    FEM_CUDA_TRY(cudaMemsetAsync(p0, 0, sizeof(T) * n, st));
-    FEM_CUDA_TRY(cudaMemsetAsync(p1, 0, sizeof(T) * n, st));
-    cg_init_kernel<VEC, T><<<vg, 256, 0, st>>>(precond, n_brows, minv, r, z, b, partials, counter, S,
-                                               rtol, atol);
-    FEM_LAUNCH_CHECK();
-    cg_spmv_kernel<VEC, T><<<rg, kRowThreads, bsr_rows_smem(), st>>>(n_brows, rp, ci, vals, z, q,
-                                                                    partials, counter, S);
-    FEM_LAUNCH_CHECK();
   } else {
     rhat = V[1];
     pp = V[2];
@@ -446,29 +435,73 @@ int solve_impl(int method, int precond, int64_t n_brows, const int32_t* rp, cons
     s = V[5];
     shat = V[6];
     t = V[7];
-    FEM_CUDA_TRY(cudaMemsetAsync(pp, 0, sizeof(T) * n, st));
-    FEM_CUDA_TRY(cudaMemsetAsync(vv, 0, sizeof(T) * n, st));
-    copy_kernel<T><<<vgn, 256, 0, st>>>(n, r, rhat);
-    FEM_LAUNCH_CHECK();
-    // init reduces r.r and b.b; rho = rhat.r = r.r for precond NONE path
-    cg_init_kernel<VEC, T><<<vg, 256, 0, st>>>(FEM_PRECOND_NONE, n_brows, minv, r, r, b, partials,
-                                               counter, S, rtol, atol);
-    FEM_LAUNCH_CHECK();
   }
-
+  // (Re)start from the true residual r = b - A x: at the start, and whenever
+  // the recursively updated residual claims a convergence that the true
+  // residual does not confirm (round-off drift, notably in FP32).
+  auto start = [&]() -> int {
+    kr_residual_kernel<VEC, T><<<rg, kRowThreads, bsr_rows_smem(), st>>>(n_brows, rp, ci, vals, x, b, r);
+    FEM_LAUNCH_CHECK();
+    if (method == FEM_KRYLOV_CG) {
+      FEM_CUDA_TRY(cudaMemsetAsync(p0, 0, sizeof(T) * n, st));
+      FEM_CUDA_TRY(cudaMemsetAsync(p1, 0, sizeof(T) * n, st));
+      cg_init_kernel<VEC, T><<<vg, 256, 0, st>>>(precond, n_brows, minv, r, z, b, partials, counter, S,
+                                                 rtol, atol);
+      FEM_LAUNCH_CHECK();
+      cg_spmv_kernel<VEC, T><<<rg, kRowThreads, bsr_rows_smem(), st>>>(n_brows, rp, ci, vals, z, q,
+                                                                      partials, counter, S);
+      FEM_LAUNCH_CHECK();
+    } else {
+      FEM_CUDA_TRY(cudaMemsetAsync(pp, 0, sizeof(T) * n, st));
+      FEM_CUDA_TRY(cudaMemsetAsync(vv, 0, sizeof(T) * n, st));
+      copy_kernel<T><<<vgn, 256, 0, st>>>(n, r, rhat);
+      FEM_LAUNCH_CHECK();
+      // rho = rhat.r = r.r, r.r and b.b (no preconditioning in this reduction)
+      cg_init_kernel<VEC, T><<<vg, 256, 0, st>>>(FEM_PRECOND_NONE, n_brows, minv, r, r, b, partials,
+                                                 counter, S, rtol, atol);
+      FEM_LAUNCH_CHECK();
+    }
+    return FEM_OK;
+  };
   double* mb = host_mailbox();
   FEM_CHECK_ARG(mb != nullptr, "pinned mailbox allocation failed");
-  int status = ST_RUNNING, iters = 0;
+  const KState* hs = reinterpret_cast<const KState*>(mb);
+  auto read_state = [&]() -> int {
+    FEM_CUDA_TRY(cudaMemcpyAsync(mb, S, sizeof(KState), cudaMemcpyDeviceToHost, st));
+    FEM_CUDA_TRY(cudaStreamSynchronize(st));
+    return FEM_OK;
+  };
+  {
+    int rc = start();
+    if (rc != FEM_OK) return rc;
+  }
+  int status = ST_RUNNING, iters = 0, iter_base = 0, restarts = 0;
   double rr = 0.0, bb = 0.0;
   int launched = 0;
   while (true) {
-    FEM_CUDA_TRY(cudaMemcpyAsync(mb, S, sizeof(KState), cudaMemcpyDeviceToHost, st));
-    FEM_CUDA_TRY(cudaStreamSynchronize(st));
-    const KState* hs = reinterpret_cast<const KState*>(mb);
+    int rc = read_state();
+    if (rc != FEM_OK) return rc;
     status = hs->status;
-    iters = hs->iter;
+    iters = iter_base + hs->iter;
     rr = hs->rr;
     bb = hs->bnorm2;
+    if ((status == ST_CONVERGED && iters > iter_base) ||
+        (status == FEM_ERR_BREAKDOWN && iters > iter_base)) {
+      // Confirm a convergence with the true residual, and answer a breakdown
+      // (a non-positive curvature or zero denominator from round-off, near
+      // the attainable accuracy) the same way: restart from r = b - A x.
+      iter_base = iters;
+      if ((rc = start()) != FEM_OK) return rc;
+      if ((rc = read_state()) != FEM_OK) return rc;
+      status = hs->status;
+      rr = hs->rr;
+      if (status != ST_RUNNING) break;
+      if (++restarts > 3 || launched >= maxiter) {
+        status = FEM_ERR_NOT_CONVERGED;
+        break;
+      }
+      continue;
+    }
     if (status != ST_RUNNING || launched >= maxiter) break;
     const int chunk = check_every < (maxiter - launched) ? check_every : (maxiter - launched);
     for (int k = 0; k < chunk; ++k) {
@@ -482,13 +515,13 @@ int solve_impl(int method, int precond, int64_t n_brows, const int32_t* rp, cons
       } else {
         bicg_p_kernel<VEC, T><<<vg, 256, 0, st>>>(precond, n_brows, minv, r, pp, vv, phat, S);
         FEM_LAUNCH_CHECK();
-        bicg_spmv_kernel<VEC, T><<<rg, kRowThreads, bsr_rows_smem(), st>>>(0, n_brows, rp, ci, vals, phat, vv,
-                                                             rhat, partials, counter, S);
+        bicg_spmv_kernel<VEC, T><<<rg, kRowThreads, bsr_rows_smem(), st>>>(
+            0, n_brows, rp, ci, vals, phat, vv, rhat, partials, counter, S);
         FEM_LAUNCH_CHECK();
         bicg_s_kernel<VEC, T><<<vg, 256, 0, st>>>(precond, n_brows, minv, r, vv, s, shat, S);
         FEM_LAUNCH_CHECK();
-        bicg_spmv_kernel<VEC, T><<<rg, kRowThreads, bsr_rows_smem(), st>>>(1, n_brows, rp, ci, vals, shat, t, s,
-                                                             partials, counter, S);
+        bicg_spmv_kernel<VEC, T><<<rg, kRowThreads, bsr_rows_smem(), st>>>(
+            1, n_brows, rp, ci, vals, shat, t, s, partials, counter, S);
         FEM_LAUNCH_CHECK();
         bicg_x_kernel<VEC, T><<<vgn, 256, 0, st>>>(n, x, r, rhat, phat, shat, s, t, partials,
                                                    counter, S);
