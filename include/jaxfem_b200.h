@@ -213,6 +213,35 @@ FEM_API size_t fem_dot_workspace_bytes(int64_t n);
 FEM_API int fem_dot_f64(int64_t n, const double* d_x, const double* d_y, double* h_out,
                 void* d_work, size_t work_bytes, void* stream);
 
+/* ---- learned warm start: tensor-core 3D convolution ----------------------
+ * No counterpart in the reference (its only network is an unrelated MLP
+ * energy surrogate, applications/surrogate_model/train.py).  BF16 operands,
+ * FP32 accumulation in TMEM (tcgen05), TMA tile loads.  Activations are
+ * NDHWC bf16, 16-byte aligned.
+ * fem_conv3d_fwd_bf16: out = [relu](conv3x3x3_pad1(in, w) + bias), w is
+ *   (Cout, 27, Cin) with tap = 9 kd + 3 kh + kw; Cin a multiple of 16,
+ *   Cout in {16,32,64,128}; N*D*H*W must tile into 128-voxel bricks (W, H, D
+ *   powers of two are fine).  bias (Cout f32) may be NULL.  The input
+ *   gradient is the same call on the output gradient with weights from
+ *   fem_conv3d_flip_weights_bf16.
+ * fem_gemm_bf16_tn_f32: C[M,N] += A[M,K] B[N,K]^T (row-major, K contiguous),
+ *   K a multiple of 16, N in {16,32,64} or a multiple of 128, split over K
+ *   into split_k slices accumulated with FP32 atomics (C must be zeroed by
+ *   the caller).  With A = im2col^T(X) (fem_conv3d_im2col_t_bf16) and
+ *   B = dZ^T (fem_transpose_bf16) this is the weight gradient dW^T.
+ * fem_tc_error: reads (and optionally resets) the device flag the tensor-core
+ *   kernels set when a pipeline wait times out (0 = none). */
+FEM_API int fem_conv3d_fwd_bf16(const void* d_in, const void* d_w, const float* d_bias, void* d_out,
+                                int N, int D, int H, int W, int Cin, int Cout, int relu, void* stream);
+FEM_API int fem_gemm_bf16_tn_f32(const void* d_a, const void* d_b, float* d_c, int M, int N, int K,
+                                 int ldc, int split_k, void* stream);
+FEM_API int fem_tc_error(int* h_err, int reset);
+FEM_API int fem_conv3d_im2col_t_bf16(const void* d_x, void* d_col, int N, int D, int H, int W, int C,
+                                     void* stream);
+FEM_API int fem_transpose_bf16(const void* d_in, void* d_out, int64_t rows, int cols, void* stream);
+FEM_API int fem_conv3d_flip_weights_bf16(const void* d_w, void* d_wt, int Cout, int Cin, void* stream);
+FEM_API int fem_relu_mask_bf16(const void* d_dy, const void* d_y, void* d_dz, int64_t n, void* stream);
+
 /* ---- dot product that allocates nothing ---------------------------------
  * No counterpart in the reference.  For callers that cannot allocate device
  * memory: code whose device memory is owned by a host framework's pool that

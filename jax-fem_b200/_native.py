@@ -72,6 +72,13 @@ _SIGS = {
     "fem_dot_workspace_bytes": (SZ, [I64]),
     "fem_dot_f64": (I32, [I64, P, P, DP, P, SZ, P]),
     "fem_dot_f64_noalloc": (I32, [I64, P, P, P, P]),
+    "fem_conv3d_fwd_bf16": (I32, [P, P, P, P, I32, I32, I32, I32, I32, I32, I32, P]),
+    "fem_gemm_bf16_tn_f32": (I32, [P, P, P, I32, I32, I32, I32, I32, P]),
+    "fem_tc_error": (I32, [IP, I32]),
+    "fem_conv3d_im2col_t_bf16": (I32, [P, P, I32, I32, I32, I32, I32, P]),
+    "fem_transpose_bf16": (I32, [P, P, I64, I32, P]),
+    "fem_conv3d_flip_weights_bf16": (I32, [P, P, I32, I32, P]),
+    "fem_relu_mask_bf16": (I32, [P, P, P, I64, P]),
 }
 
 _lib = None
