@@ -414,6 +414,76 @@ def run_profile(args, device):
     print(json.dumps({"profile": "done", "launches": nat.launch_count()}))
 
 
+def warmstart_eval(pkg, ws, prob, net, n, seed, log=None):
+    """Held-out SIMP solves from zero and from the network's prediction, on
+    the plain FP64 and the mixed path, all stopping at the same absolute
+    residual (rel.res 1e-8 of the zero-start residual, adaptive forcing).
+    Returns per-sample Krylov iterations and times per arm."""
+    linear = {"cg": {"precond": "block_jacobi", "rtol": "adaptive", "atol": 0.0, "maxiter": 50000}}
+    pred = ws.Predictor(net)
+    g = torch.Generator().manual_seed(seed)
+    dev = prob.dev().device
+    rows = []
+    for i in range(n):
+        rho = ws.random_density(g)
+        z0 = float(torch.randint(0, ws.NZ - 3 + 1, (1,), generator=g).item())
+        prob.set_patch(z0)
+        prob.set_params(ws.cell_rho_to_torch(rho, dev))
+        r = {}
+        for prec in ("fp64", "mixed"):
+            for start in ("zero", "learned"):
+                opts = {"newton": {"rel_tol": 1e-8, "tol": 1e-14, "precision": prec, "linear": linear,
+                                   "rel_tol_reference": "zero", "return_info": True,
+                                   "warm_start": pred if start == "learned" else None}}
+                torch.cuda.synchronize()
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record()
+                (sol,), info = pkg.solver(prob, opts)
+                e1.record()
+                torch.cuda.synchronize()
+                r[f"{prec}_{start}"] = {"krylov": sum(info["krylov_iters"]), "newton": info["newton_iters"],
+                                        "s": e0.elapsed_time(e1) * 1e-3}
+        rows.append(r)
+        if log and (i + 1) % 20 == 0:
+            log(f"  eval {i + 1}/{n}")
+    return rows
+
+
+def summarize_eval(rows):
+    out = {}
+    for arm in rows[0]:
+        out[arm] = {"krylov_mean": float(np.mean([r[arm]["krylov"] for r in rows])),
+                    "newton_mean": float(np.mean([r[arm]["newton"] for r in rows])),
+                    "s_mean": float(np.mean([r[arm]["s"] for r in rows]))}
+    return out
+
+
+def run_warmstart_train(args, device):
+    """Generate (rho, u) pairs with the solver, train the warm-start network on
+    the tensor-core kernels, evaluate on held-out samples, save the weights."""
+    pkg = load_package()
+    import importlib
+    ws = importlib.import_module("jax_fem_b200.warmstart")
+    prob = ws.cantilever_problem()
+    t0 = time.time()
+    train_data = ws.generate(prob, args.ws_train, seed=1000)
+    t_gen = time.time() - t0
+    print(f"generated {args.ws_train} training samples in {t_gen:.1f} s", flush=True)
+    net = ws.WarmStartNet(seed=0)
+    t0 = time.time()
+    hist = ws.train(net, train_data, epochs=args.ws_epochs, batch=16, lr=args.ws_lr, device=device)
+    torch.cuda.synchronize()
+    t_train = time.time() - t0
+    print(f"trained {args.ws_epochs} epochs in {t_train:.1f} s", flush=True)
+    rows = warmstart_eval(pkg, ws, prob, net, args.ws_test, seed=999_000, log=print)
+    meta = {"n_train": args.ws_train, "n_test": args.ws_test, "epochs": args.ws_epochs, "lr": args.ws_lr,
+            "loss_history": hist, "gen_s": t_gen, "train_s": t_train, "heldout": summarize_eval(rows),
+            "u_scale": float(net.u_scale.item())}
+    if args.ws_out:
+        ws.save(net, args.ws_out, meta)
+    print(json.dumps({k: v for k, v in meta.items() if k != "loss_history"}), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -423,6 +493,13 @@ def main():
     ap.add_argument("--n", type=int, default=50)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--profile", action="store_true", help="short kernel sequence for ncu captures")
+    ap.add_argument("--warmstart-train", action="store_true",
+                    help="generate SIMP (rho, u) pairs, train the warm-start network, evaluate, save")
+    ap.add_argument("--ws-train", type=int, default=2000)
+    ap.add_argument("--ws-test", type=int, default=200)
+    ap.add_argument("--ws-epochs", type=int, default=30)
+    ap.add_argument("--ws-lr", type=float, default=2e-3)
+    ap.add_argument("--ws-out", default="")
     ap.add_argument("--ref-newton-iters", type=int, default=25)
     ap.add_argument("--ref-krylov-iters", type=int, default=8000)
     args = ap.parse_args()
@@ -443,6 +520,9 @@ def main():
                                              device_id=device)
     if args.profile:
         run_profile(args, device)
+        return
+    if args.warmstart_train:
+        run_warmstart_train(args, device)
         return
     out = run_ours(args, rank, world, device)
     if rank == 0:

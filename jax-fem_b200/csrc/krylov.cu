@@ -13,6 +13,11 @@
 // / 3x3 block-Jacobi preconditioner u = M r while it reduces gamma = r.u and
 // r.r; a pure SpMV w = A u reduces delta = w.u, and its last block forms
 // alpha and beta for the next iteration.  Two kernels per iteration.
+#include <cstdlib>
+#include <cstring>
+#include <map>
+#include <mutex>
+
 #include "sparse.cuh"
 
 namespace fem {
@@ -136,6 +141,7 @@ __global__ void cg_init_kernel(int precond, int64_t n_brows, const T* minv, cons
     S->omega = 1.0;
     S->alpha = 1.0;
     S->iter = 0;
+    S->first = 1;  // the next CG SpMV starts a fresh recurrence (also after a restart)
     if (!finite_d(tot[0]) || !finite_d(tot[1]) || !finite_d(tot[2]))
       S->status = FEM_ERR_NONFINITE;
     else if (tot[1] <= S->tol2)
@@ -360,6 +366,69 @@ __global__ void copy_kernel(int64_t n, const T* a, T* b) {
     b[k] = a[k];
 }
 
+// ---- cached CUDA graphs of CG / BiCGSTAB iteration chunks --------------------
+struct GraphKey {
+  int method, precond, vec, tsize, chunk;
+  int64_t n;
+  const void* ptrs[24];
+  bool operator<(const GraphKey& o) const {
+    if (method != o.method) return method < o.method;
+    if (precond != o.precond) return precond < o.precond;
+    if (vec != o.vec) return vec < o.vec;
+    if (tsize != o.tsize) return tsize < o.tsize;
+    if (chunk != o.chunk) return chunk < o.chunk;
+    if (n != o.n) return n < o.n;
+    return std::memcmp(ptrs, o.ptrs, sizeof(ptrs)) < 0;
+  }
+};
+std::mutex g_graph_mu;
+std::map<GraphKey, cudaGraphExec_t>& graph_cache() {
+  static std::map<GraphKey, cudaGraphExec_t> m;
+  return m;
+}
+cudaGraphExec_t graph_lookup(const GraphKey& k) {
+  int dev = 0;
+  cudaGetDevice(&dev);
+  GraphKey kk = k;
+  kk.ptrs[23] = reinterpret_cast<const void*>(intptr_t(dev));
+  std::lock_guard<std::mutex> lock(g_graph_mu);
+  auto it = graph_cache().find(kk);
+  return it == graph_cache().end() ? nullptr : it->second;
+}
+void graph_store(const GraphKey& k, cudaGraphExec_t e) {
+  int dev = 0;
+  cudaGetDevice(&dev);
+  GraphKey kk = k;
+  kk.ptrs[23] = reinterpret_cast<const void*>(intptr_t(dev));
+  std::lock_guard<std::mutex> lock(g_graph_mu);
+  auto& m = graph_cache();
+  if (m.size() >= 64) {  // bounded: drop everything (workspaces moved)
+    for (auto& kv : m) cudaGraphExecDestroy(kv.second);
+    m.clear();
+  }
+  m[kk] = e;
+}
+// FEM_KRYLOV_GRAPHS=0 in the environment launches every kernel directly.
+bool graphs_enabled() {
+  static int on = -1;
+  if (on < 0) {
+    const char* e = std::getenv("FEM_KRYLOV_GRAPHS");
+    on = (e != nullptr && e[0] == '0') ? 0 : 1;
+  }
+  return on == 1;
+}
+
+cudaStream_t capture_stream() {
+  static std::mutex mu;
+  static cudaStream_t s[64] = {nullptr};
+  int dev = 0;
+  cudaGetDevice(&dev);
+  std::lock_guard<std::mutex> lock(mu);
+  if (s[dev] == nullptr && cudaStreamCreateWithFlags(&s[dev], cudaStreamNonBlocking) != cudaSuccess)
+    s[dev] = nullptr;
+  return s[dev];
+}
+
 // ---- workspace ----------------------------------------------------------------
 inline size_t al256(size_t x) { return (x + 255) & ~size_t(255); }
 
@@ -471,6 +540,33 @@ int solve_impl(int method, int precond, int64_t n_brows, const int32_t* rp, cons
     FEM_CUDA_TRY(cudaStreamSynchronize(st));
     return FEM_OK;
   };
+  auto launch_chunk = [&](cudaStream_t ls, int chunk) -> int {
+    for (int k = 0; k < chunk; ++k) {
+      if (method == FEM_KRYLOV_CG) {
+        cg_vec_kernel<VEC, T><<<vg, 256, 0, ls>>>(precond, n_brows, minv, x, r, z, p0, p1, q, partials,
+                                                  counter, S);
+        FEM_LAUNCH_CHECK();
+        cg_spmv_kernel<VEC, T><<<rg, kRowThreads, bsr_rows_smem(), ls>>>(n_brows, rp, ci, vals, z, q,
+                                                                        partials, counter, S);
+        FEM_LAUNCH_CHECK();
+      } else {
+        bicg_p_kernel<VEC, T><<<vg, 256, 0, ls>>>(precond, n_brows, minv, r, pp, vv, phat, S);
+        FEM_LAUNCH_CHECK();
+        bicg_spmv_kernel<VEC, T><<<rg, kRowThreads, bsr_rows_smem(), ls>>>(
+            0, n_brows, rp, ci, vals, phat, vv, rhat, partials, counter, S);
+        FEM_LAUNCH_CHECK();
+        bicg_s_kernel<VEC, T><<<vg, 256, 0, ls>>>(precond, n_brows, minv, r, vv, s, shat, S);
+        FEM_LAUNCH_CHECK();
+        bicg_spmv_kernel<VEC, T><<<rg, kRowThreads, bsr_rows_smem(), ls>>>(
+            1, n_brows, rp, ci, vals, shat, t, s, partials, counter, S);
+        FEM_LAUNCH_CHECK();
+        bicg_x_kernel<VEC, T><<<vgn, 256, 0, ls>>>(n, x, r, rhat, phat, shat, s, t, partials,
+                                                   counter, S);
+        FEM_LAUNCH_CHECK();
+      }
+    }
+    return FEM_OK;
+  };
   {
     int rc = start();
     if (rc != FEM_OK) return rc;
@@ -504,29 +600,42 @@ int solve_impl(int method, int precond, int64_t n_brows, const int32_t* rp, cons
     }
     if (status != ST_RUNNING || launched >= maxiter) break;
     const int chunk = check_every < (maxiter - launched) ? check_every : (maxiter - launched);
-    for (int k = 0; k < chunk; ++k) {
-      if (method == FEM_KRYLOV_CG) {
-        cg_vec_kernel<VEC, T><<<vg, 256, 0, st>>>(precond, n_brows, minv, x, r, z, p0, p1, q, partials,
-                                                  counter, S);
-        FEM_LAUNCH_CHECK();
-        cg_spmv_kernel<VEC, T><<<rg, kRowThreads, bsr_rows_smem(), st>>>(n_brows, rp, ci, vals, z, q,
-                                                                        partials, counter, S);
-        FEM_LAUNCH_CHECK();
-      } else {
-        bicg_p_kernel<VEC, T><<<vg, 256, 0, st>>>(precond, n_brows, minv, r, pp, vv, phat, S);
-        FEM_LAUNCH_CHECK();
-        bicg_spmv_kernel<VEC, T><<<rg, kRowThreads, bsr_rows_smem(), st>>>(
-            0, n_brows, rp, ci, vals, phat, vv, rhat, partials, counter, S);
-        FEM_LAUNCH_CHECK();
-        bicg_s_kernel<VEC, T><<<vg, 256, 0, st>>>(precond, n_brows, minv, r, vv, s, shat, S);
-        FEM_LAUNCH_CHECK();
-        bicg_spmv_kernel<VEC, T><<<rg, kRowThreads, bsr_rows_smem(), st>>>(
-            1, n_brows, rp, ci, vals, shat, t, s, partials, counter, S);
-        FEM_LAUNCH_CHECK();
-        bicg_x_kernel<VEC, T><<<vgn, 256, 0, st>>>(n, x, r, rhat, phat, shat, s, t, partials,
-                                                   counter, S);
-        FEM_LAUNCH_CHECK();
+    if (chunk == check_every && graphs_enabled()) {
+      // steady state: replay the chunk as a cached CUDA graph (kernel
+      // arguments are fixed pointers, so one capture serves every replay)
+      GraphKey key{};
+      key.method = method; key.precond = precond; key.vec = VEC; key.tsize = int(sizeof(T));
+      key.n = n_brows; key.chunk = chunk;
+      const void* kp[] = {rp, ci, vals, minv, x, r, z, p0, p1, q, rhat, pp, phat, vv, s, shat, t,
+                          partials, counter, S, b};
+      for (int i = 0; i < int(sizeof(kp) / sizeof(kp[0])); ++i) key.ptrs[i] = kp[i];
+      cudaGraphExec_t exec = graph_lookup(key);
+      if (exec == nullptr) {
+        cudaStream_t cap = capture_stream();
+        if (cap != nullptr && cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
+          const int lrc = launch_chunk(cap, chunk);
+          cudaGraph_t g = nullptr;
+          const cudaError_t ec = cudaStreamEndCapture(cap, &g);
+          if (lrc == FEM_OK && ec == cudaSuccess && g != nullptr &&
+              cudaGraphInstantiate(&exec, g, 0) == cudaSuccess) {
+            graph_store(key, exec);
+          } else {
+            exec = nullptr;
+          }
+          if (g != nullptr) cudaGraphDestroy(g);
+          cudaGetLastError();  // a failed capture falls back to direct launches
+        }
       }
+      if (exec != nullptr) {
+        FEM_CUDA_TRY(cudaGraphLaunch(exec, st));
+        launch_counter().fetch_add(int64_t(chunk) * (method == FEM_KRYLOV_CG ? 2 : 5), std::memory_order_relaxed);
+      } else {
+        int lrc = launch_chunk(st, chunk);
+        if (lrc != FEM_OK) return lrc;
+      }
+    } else {
+      int lrc = launch_chunk(st, chunk);
+      if (lrc != FEM_OK) return lrc;
     }
     launched += chunk;
   }
