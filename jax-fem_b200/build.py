@@ -80,7 +80,7 @@ def build(force=False, verbose=False, extra_flags=()):
             sys.stderr.write(f"--- {s}\n{err}\n")
         raise RuntimeError(f"{len(failed)} source(s) failed to compile")
     if jobs or not os.path.exists(LIB) or any(os.path.getmtime(o) > os.path.getmtime(LIB) for o in objs):
-        cmd = [cc, *ARCH, "-shared", "-o", LIB, *objs, "-lcudart", "-lcuda"]
+        cmd = [cc, *ARCH, "-shared", "-o", LIB, *objs, "-lcudart"]
         p = subprocess.run(cmd, capture_output=True, text=True)
         if p.returncode != 0:
             raise RuntimeError("link failed:\n" + p.stderr)

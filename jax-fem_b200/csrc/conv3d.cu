@@ -253,6 +253,25 @@ int* err_flag_device() {
   return flags[dev];
 }
 
+// cuTensorMapEncodeTiled through the runtime's driver entry-point lookup, so
+// the library does not link libcuda (and loads on hosts without a driver).
+using EncodeTiledFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                   const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                   CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+EncodeTiledFn encode_tiled() {
+  static std::mutex mu;
+  static EncodeTiledFn fn = nullptr;
+  std::lock_guard<std::mutex> lock(mu);
+  if (fn == nullptr) {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<EncodeTiledFn>(p);
+  }
+  return fn;
+}
+
 CUtensorMapSwizzle swizzle_for(int row_bytes) {
   return row_bytes == 128 ? CU_TENSOR_MAP_SWIZZLE_128B
                           : (row_bytes == 64 ? CU_TENSOR_MAP_SWIZZLE_64B : CU_TENSOR_MAP_SWIZZLE_32B);
@@ -264,7 +283,12 @@ int make_map_2d(CUtensorMap* m, const void* base, uint64_t inner, uint64_t outer
   const cuuint64_t strides[1] = {inner * 2};
   const cuuint32_t box[2] = {box_inner, box_outer};
   const cuuint32_t es[2] = {1, 1};
-  CUresult r = cuTensorMapEncodeTiled(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void*>(base), dims,
+  EncodeTiledFn enc = encode_tiled();
+  if (enc == nullptr) {
+    set_error("cuTensorMapEncodeTiled is unavailable (driver entry point lookup failed)");
+    return FEM_ERR_CUDA;
+  }
+  CUresult r = enc(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void*>(base), dims,
                                       strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE, swizzle_for(box_inner * 2),
                                       CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   if (r != CUDA_SUCCESS) {
@@ -282,7 +306,12 @@ int make_map_5d(CUtensorMap* m, const void* base, int C, int W, int H, int D, in
                                  cuuint64_t(D) * H * W * C * 2};
   const cuuint32_t box[5] = {bc, bw, bh, bd, bn};
   const cuuint32_t es[5] = {1, 1, 1, 1, 1};
-  CUresult r = cuTensorMapEncodeTiled(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 5, const_cast<void*>(base), dims,
+  EncodeTiledFn enc = encode_tiled();
+  if (enc == nullptr) {
+    set_error("cuTensorMapEncodeTiled is unavailable (driver entry point lookup failed)");
+    return FEM_ERR_CUDA;
+  }
+  CUresult r = enc(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 5, const_cast<void*>(base), dims,
                                       strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE, swizzle_for(bc * 2),
                                       CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   if (r != CUDA_SUCCESS) {
