@@ -97,7 +97,7 @@ __device__ __forceinline__ void apply_precond(int precond, int64_t nd, const T* 
 
 // r = b - A x
 template <int VEC, typename T>
-__global__ void __launch_bounds__(kRowThreads) kr_residual_kernel(int64_t n_brows, const int32_t* rp,
+__global__ void __launch_bounds__(kRowThreads, kRowBlocksPerSM) kr_residual_kernel(int64_t n_brows, const int32_t* rp,
                                                                  const int32_t* ci, const T* vals,
                                                                  const T* __restrict__ x,
                                                                  const T* b, T* r) {
@@ -155,7 +155,7 @@ __global__ void cg_init_kernel(int precond, int64_t n_brows, const T* minv, cons
 
 // CG SpMV: w = A u, delta = w . u; last block forms alpha, beta.
 template <int VEC, typename T>
-__global__ void __launch_bounds__(kRowThreads) cg_spmv_kernel(int64_t n_brows, const int32_t* rp,
+__global__ void __launch_bounds__(kRowThreads, kRowBlocksPerSM) cg_spmv_kernel(int64_t n_brows, const int32_t* rp,
                                                              const int32_t* ci, const T* vals,
                                                              const T* __restrict__ u, T* w,
                                                              double* partials, unsigned int* counter,
@@ -267,7 +267,7 @@ __global__ void bicg_p_kernel(int precond, int64_t n_brows, const T* minv, const
 // y = A x with partial dot products of y against up to two vectors.
 // mode 0: (rhat . v) -> alpha; mode 1: (t . s, t . t) -> omega
 template <int VEC, typename T>
-__global__ void __launch_bounds__(kRowThreads) bicg_spmv_kernel(int mode, int64_t n_brows, const int32_t* rp,
+__global__ void __launch_bounds__(kRowThreads, kRowBlocksPerSM) bicg_spmv_kernel(int mode, int64_t n_brows, const int32_t* rp,
                                                                const int32_t* ci, const T* vals,
                                                                const T* __restrict__ x, T* y,
                                                                const T* w, double* partials,

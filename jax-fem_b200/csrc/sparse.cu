@@ -8,7 +8,7 @@ namespace fem {
 namespace {
 
 template <int VEC, typename VT, typename XT, typename YT>
-__global__ void __launch_bounds__(kRowThreads) spmv_kernel(int64_t n_brows, const int32_t* rp,
+__global__ void __launch_bounds__(kRowThreads, kRowBlocksPerSM) spmv_kernel(int64_t n_brows, const int32_t* rp,
                                                           const int32_t* ci, const VT* vals,
                                                           const XT* __restrict__ x, YT* y) {
   using AT = typename std::conditional<(sizeof(VT) == 8 || sizeof(XT) == 8), double, float>::type;
@@ -21,7 +21,7 @@ __global__ void __launch_bounds__(kRowThreads) spmv_kernel(int64_t n_brows, cons
 
 // r = b - A x (A f32, x/b/r f64, f64 accumulation)
 template <int VEC>
-__global__ void __launch_bounds__(kRowThreads) residual_mixed_kernel(int64_t n_brows, const int32_t* rp,
+__global__ void __launch_bounds__(kRowThreads, kRowBlocksPerSM) residual_mixed_kernel(int64_t n_brows, const int32_t* rp,
                                                                     const int32_t* ci, const float* vals,
                                                                     const double* __restrict__ x,
                                                                     const double* b, double* r) {

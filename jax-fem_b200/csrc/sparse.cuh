@@ -5,11 +5,12 @@
 namespace fem {
 
 constexpr int kRowThreads = 256;   // 8 warps per block
-constexpr int kStageBytes = 8192;  // per-warp shared-memory stage for matrix values
+constexpr int kStageBytes = 4096;  // per-warp shared-memory stage for matrix values
+constexpr int kRowBlocksPerSM = 4; // resident blocks per SM the row kernels are sized for
 
 template <typename VT>
 __host__ __device__ constexpr int rows_per_warp() {
-  return sizeof(VT) == 4 ? 8 : 4;  // ~7.8 KB of 3x3 blocks per group either way
+  return sizeof(VT) == 4 ? 4 : 2;  // ~3.9 KB of 3x3 blocks per group either way
 }
 
 // Dynamic shared memory a bsr_rows kernel needs (one stage per warp).
@@ -145,7 +146,7 @@ template <typename VT>
 inline unsigned row_grid(int64_t n_brows) {
   const int64_t groups = (n_brows + rows_per_warp<VT>() - 1) / rows_per_warp<VT>();
   const int64_t blocks_needed = (groups + (kRowThreads / 32) - 1) / (kRowThreads / 32);
-  const int64_t cap = int64_t(num_sms()) * 3;  // 3 resident blocks per SM (shared-memory stages)
+  const int64_t cap = int64_t(num_sms()) * kRowBlocksPerSM;
   return unsigned(blocks_needed < cap ? (blocks_needed > 0 ? blocks_needed : 1) : cap);
 }
 

@@ -130,10 +130,15 @@ class FiniteElement:
         if dirichlet_bc_info is not None:
             location_fns, vecs, value_fns = dirichlet_bc_info
             assert len(location_fns) == len(value_fns) and len(value_fns) == len(vecs)
+            seen_loc, seen_val = {}, {}  # the same function object is evaluated once
             for lf, v, vf in zip(location_fns, vecs, value_fns):
-                flags = _location_flags(lf, self.points)
-                node_inds = np.argwhere(flags).reshape(-1)
-                vals = _batched_or_pointwise(vf, (self.points[node_inds],), ())
+                if id(lf) not in seen_loc:
+                    seen_loc[id(lf)] = np.argwhere(_location_flags(lf, self.points)).reshape(-1)
+                node_inds = seen_loc[id(lf)]
+                key = (id(vf), id(lf))
+                if key not in seen_val:
+                    seen_val[key] = _batched_or_pointwise(vf, (self.points[node_inds],), ())
+                vals = seen_val[key]
                 node_inds_list.append(node_inds)
                 vec_inds_list.append(np.full(len(node_inds), int(v), dtype=np.int32))
                 vals_list.append(np.asarray(vals, dtype=np.float64).reshape(-1))

@@ -1,0 +1,138 @@
+"""The benchmark configurations at full size, checked through properties that
+do not need an oracle solve of the whole problem:
+
+- 20^3 linear elasticity (27,783 dofs): GPU solution vs the oracle's direct
+  solve (1e-8 relative).
+- 50^3 Neo-Hookean, 30 degree twist in 5 steps (397,953 dofs): the oracle's
+  own residual of the GPU solution is <= 1e-8 of its residual at u = 0, on
+  both the plain FP64 and the mixed path; the two paths agree to 1e-6.
+- 60x30x30 SIMP (175,863 dofs), seeded Gaussian random density: compliance
+  gradient from the adjoint vs central finite differences (h = 1e-6) on 20
+  random cells (1e-5 relative).
+- 40^3 J2 with hardening, 10 increments of u_x(x=1) up to 0.02 (206,763
+  dofs): after the last increment the oracle's residual, evaluated with the
+  GPU's committed state of increment 9, is <= 1e-8 of its value at the
+  increment's start; the committed state equals the oracle's return map.
+"""
+import importlib
+import math
+
+import numpy as np
+import pytest
+import torch
+
+from oracle import fem_oracle as fo
+
+
+def _rel_residual(op, u, u_ref):
+    r = np.linalg.norm(op.apply_bc_vec(op.residual(u), u))
+    r0 = np.linalg.norm(op.apply_bc_vec(op.residual(u_ref), u_ref))
+    return r / r0
+
+
+@pytest.mark.gpu
+def test_config_linear_20(pkg, cuda):
+    n = 20
+    m = pkg.box_mesh(n, n, n, 1.0, 1.0, 1.0)
+    mesh = pkg.Mesh(m.points, m.cells_dict["hexahedron"])
+    left = lambda p: np.isclose(p[0], 0.0, atol=1e-5)  # noqa: E731
+    right = lambda p: np.isclose(p[0], 1.0, atol=1e-5)  # noqa: E731
+    bc = [[left] * 3 + [right], [0, 1, 2, 0], [lambda p: 0.0 * p[0]] * 3 + [lambda p: 0.01 + 0.0 * p[0]]]
+
+    class LE(pkg.Problem):
+        def get_tensor_map(self):
+            return pkg.LinearElastic(70e3, 0.3)
+
+    prob = LE(mesh, vec=3, dim=3, dirichlet_bc_info=bc)
+    sol = pkg.solver(prob, {"newton": {"linear": {"cg": {"precond": "jacobi", "rtol": 1e-10, "atol": 0.0}},
+                                       "tol": 1e-14}})[0].cpu().numpy().reshape(-1)
+    op = fo.OracleProblem(mesh.points, mesh.cells, 3, fo.Law("linear", E=70e3, nu=0.3), dirichlet_bc_info=bc)
+    ref = fo.newton_solve(op, tol=1e-14)
+    assert np.abs(sol - ref).max() <= 1e-8 * np.abs(ref).max()
+
+
+@pytest.mark.gpu
+def test_config_neo_hookean_50(pkg, cuda):
+    import bench
+    prob = bench.nh_problem(pkg, 50)
+    lin = {"cg": {"precond": "block_jacobi", "rtol": "adaptive", "atol": 0.0, "maxiter": 20000}}
+    sol_m, infos_m = bench.nh_solve(pkg, prob, "mixed", linear=lin)
+    sol_p, _ = bench.nh_solve(pkg, prob, "fp64")
+    um = sol_m.cpu().numpy().reshape(-1)
+    up = sol_p.cpu().numpy().reshape(-1)
+    assert np.abs(um - up).max() <= 1e-6 * np.abs(up).max()
+    bc = bench.rotation_bc(math.radians(30.0))
+    op = fo.OracleProblem(prob.mesh.points, prob.mesh.cells, 3, fo.Law("neo_hookean", E=10.0, nu=0.3),
+                          dirichlet_bc_info=bc)
+    zero = np.zeros(op.ndofs)
+    for u in (um, up):
+        assert _rel_residual(op, u, zero) <= 1e-8
+
+
+@pytest.mark.gpu
+def test_config_simp_adjoint_vs_fd(pkg, cuda):
+    ws = importlib.import_module("jax_fem_b200.warmstart")
+    prob = ws.cantilever_problem(z0=0.0)
+    g = torch.Generator().manual_seed(20261203)
+    rho0 = ws.random_density(g).reshape(-1).double()
+    lin = {"cg": {"precond": "block_jacobi", "rtol": 1e-11, "atol": 0.0, "maxiter": 50000}}
+    opts = {"newton": {"rel_tol": 1e-10, "tol": 1e-30, "linear": lin}}
+    fwd = pkg.ad_wrapper(prob, opts, lin)
+    rho = rho0.to(cuda).requires_grad_(True)
+    sol = fwd(rho)
+    c = pkg.compliance(prob, sol)
+    c.backward()
+    grad = rho.grad.cpu().numpy()
+    # each perturbed solve starts from the base solution, so Newton resolves the
+    # O(h) change to 1e-10 of itself (a cold start would bury it in the solver
+    # tolerance)
+    fd_opts = {"newton": {"rel_tol": 1e-10, "tol": 1e-30, "linear": lin,
+                          "initial_guess": sol[0].detach().clone()}}
+    rng = np.random.default_rng(7)
+    h = 1e-6
+    for cell in rng.choice(len(rho0), size=20, replace=False):
+        vals = []
+        for sgn in (1.0, -1.0):
+            r = rho0.clone()
+            r[cell] += sgn * h
+            prob.set_params(r.to(cuda))
+            vals.append(pkg.compliance(prob, pkg.solver(prob, fd_opts)).item())
+        fd = (vals[0] - vals[1]) / (2 * h)
+        assert abs(fd - grad[cell]) <= 1e-5 * abs(grad[cell]), (cell, fd, grad[cell])
+
+
+@pytest.mark.gpu
+def test_config_j2_40(pkg, cuda):
+    n = 40
+    m = pkg.box_mesh(n, n, n, 1.0, 1.0, 1.0)
+    mesh = pkg.Mesh(m.points, m.cells_dict["hexahedron"])
+    C = len(mesh.cells)
+    left = lambda p: np.isclose(p[0], 0.0, atol=1e-5)  # noqa: E731
+    right = lambda p: np.isclose(p[0], 1.0, atol=1e-5)  # noqa: E731
+    bc = [[left] * 3 + [right], [0, 1, 2, 0], [lambda p: 0.0 * p[0]] * 4]
+    z = lambda *s: torch.zeros(*s, dtype=torch.float64, device=cuda)  # noqa: E731
+
+    class J2(pkg.Problem):
+        def get_tensor_map(self):
+            return pkg.J2Plasticity(70e3, 0.3, 250.0, 700.0)
+
+    prob = J2(mesh, vec=3, dim=3, dirichlet_bc_info=bc)
+    prob.internal_vars = [z(C, 8, 3, 3), z(C, 8, 3, 3), z(C, 8)]
+    opts = {"newton": {"rel_tol": 1e-8, "tol": 1e-14,
+                       "linear": {"cg": {"precond": "block_jacobi", "rtol": 1e-10, "atol": 0.0, "maxiter": 20000}}}}
+    sol = None
+    for k in range(1, 11):
+        bc[2][-1] = (lambda v: (lambda p: v + 0.0 * p[0]))(0.02 * k / 10)
+        prob.fes[0].update_Dirichlet_boundary_conditions(bc)
+        prev_state = [t.cpu().numpy() for t in prob.internal_vars]
+        start = sol.cpu().numpy().reshape(-1) if sol is not None else np.zeros(prob.num_total_dofs_all_vars)
+        sol = pkg.solver(prob, {"newton": dict(opts["newton"], initial_guess=sol)})[0]
+        prob.update_j2_state(sol)
+    u = sol.cpu().numpy().reshape(-1)
+    op = fo.OracleProblem(mesh.points, mesh.cells, 3, fo.Law("j2", E=70e3, nu=0.3, sig0=250.0, H=700.0),
+                          dirichlet_bc_info=bc, internal_vars=[prev_state[0], prev_state[1], prev_state[2]])
+    assert _rel_residual(op, u, start) <= 1e-8
+    fo.j2_commit(op, u)
+    sig = prob.internal_vars[0].cpu().numpy()
+    assert np.abs(sig - op.internal_vars[0]).max() <= 1e-8 * np.abs(op.internal_vars[0]).max()
+    assert prob.internal_vars[2].max().item() > 0.0  # plastic flow happened
