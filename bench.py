@@ -414,13 +414,15 @@ def run_profile(args, device):
     print(json.dumps({"profile": "done", "launches": nat.launch_count()}))
 
 
-def warmstart_eval(pkg, ws, prob, net, n, seed, log=None):
+def warmstart_eval(pkg, ws, prob, net, n, seed, log=None, arms=None):
     """Held-out SIMP solves from zero and from the network's prediction, on
     the plain FP64 and the mixed path, all stopping at the same absolute
     residual (rel.res 1e-8 of the zero-start residual, adaptive forcing).
     Returns per-sample Krylov iterations and times per arm."""
     linear = {"cg": {"precond": "block_jacobi", "rtol": "adaptive", "atol": 0.0, "maxiter": 50000}}
-    pred = ws.Predictor(net)
+    preds = {"zero": None, "learned": ws.Predictor(net, galerkin=True),
+             "learned_raw": ws.Predictor(net, galerkin=False)}
+    arms = arms or [(p, s) for p in ("fp64", "mixed") for s in ("zero", "learned", "learned_raw")]
     g = torch.Generator().manual_seed(seed)
     dev = prob.dev().device
     rows = []
@@ -430,19 +432,18 @@ def warmstart_eval(pkg, ws, prob, net, n, seed, log=None):
         prob.set_patch(z0)
         prob.set_params(ws.cell_rho_to_torch(rho, dev))
         r = {}
-        for prec in ("fp64", "mixed"):
-            for start in ("zero", "learned"):
-                opts = {"newton": {"rel_tol": 1e-8, "tol": 1e-14, "precision": prec, "linear": linear,
-                                   "rel_tol_reference": "zero", "return_info": True,
-                                   "warm_start": pred if start == "learned" else None}}
-                torch.cuda.synchronize()
-                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-                e0.record()
-                (sol,), info = pkg.solver(prob, opts)
-                e1.record()
-                torch.cuda.synchronize()
-                r[f"{prec}_{start}"] = {"krylov": sum(info["krylov_iters"]), "newton": info["newton_iters"],
-                                        "s": e0.elapsed_time(e1) * 1e-3}
+        for prec, start in arms:
+            opts = {"newton": {"rel_tol": 1e-8, "tol": 1e-14, "precision": prec, "linear": linear,
+                               "rel_tol_reference": "zero", "return_info": True,
+                               "warm_start": preds[start]}}
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            (sol,), info = pkg.solver(prob, opts)
+            e1.record()
+            torch.cuda.synchronize()
+            r[f"{prec}_{start}"] = {"krylov": sum(info["krylov_iters"]), "newton": info["newton_iters"],
+                                    "s": e0.elapsed_time(e1) * 1e-3}
         rows.append(r)
         if log and (i + 1) % 20 == 0:
             log(f"  eval {i + 1}/{n}")
@@ -500,6 +501,7 @@ def main():
     ap.add_argument("--ws-epochs", type=int, default=30)
     ap.add_argument("--ws-lr", type=float, default=2e-3)
     ap.add_argument("--ws-out", default="")
+    ap.add_argument("--warmstart-eval", default="", help="evaluate a saved warm-start model on held-out samples")
     ap.add_argument("--ref-newton-iters", type=int, default=25)
     ap.add_argument("--ref-krylov-iters", type=int, default=8000)
     args = ap.parse_args()
@@ -523,6 +525,14 @@ def main():
         return
     if args.warmstart_train:
         run_warmstart_train(args, device)
+        return
+    if args.warmstart_eval:
+        import importlib
+        pkg = load_package()
+        ws = importlib.import_module("jax_fem_b200.warmstart")
+        net, meta = ws.load(args.warmstart_eval, device)
+        rows = warmstart_eval(pkg, ws, ws.cantilever_problem(), net, args.ws_test, seed=999_000)
+        print(json.dumps({"heldout": summarize_eval(rows), "n_test": args.ws_test}), flush=True)
         return
     out = run_ours(args, rank, world, device)
     if rank == 0:

@@ -328,11 +328,20 @@ def train(net, data, epochs=30, batch=16, lr=2e-3, device=None, log=print):
 
 class Predictor:
     """``warm_start`` callable for the solver: network prediction of the
-    displacement of a SIMPCantilever at its current density and load patch."""
+    displacement of a SIMPCantilever at its current density and load patch.
 
-    def __init__(self, net):
+    With ``galerkin=True`` (default) the prediction d (free dofs) is rescaled
+    by the energy-optimal factor alpha = -(f.d + d.K u_b) / (d.K d) of the
+    linear problem (K the Dirichlet-eliminated tangent, f the external load,
+    u_b the prescribed values): one tangent assembly and one SpMV remove the
+    network's error in the overall magnitude of the field."""
+
+    def __init__(self, net, galerkin=True):
         self.net = net.eval()
+        self.galerkin = galerkin
         self.calls = 0
+        self.last_alpha = None
+        self._A = None
 
     @torch.no_grad()
     def __call__(self, problem):
@@ -342,21 +351,41 @@ class Predictor:
         pad = 8 - 1  # the 4x2x2 level tiles 8 samples per 128-voxel brick
         xb = torch.cat([x, x.new_zeros((pad,) + x.shape[1:])])
         uc = self.net(xb)[:1, ..., :3].float() * self.net.u_scale
-        u = prolong(uc).reshape(-1).to(torch.float64)
+        d = prolong(uc).reshape(-1).to(torch.float64)
         mask, ubc = problem.dirichlet_device()
-        u = torch.where(mask.bool(), ubc, u)
+        mb = mask.bool()
+        d = torch.where(mb, torch.zeros_like(d), d)
+        if self.galerkin:
+            if self._A is None or self._A.vals.numel() != problem.dev().nnzb * 9:
+                self._A = problem.dev().new_matrix(torch.float64)
+            zero = torch.zeros_like(d)
+            lift = torch.empty_like(d)
+            ub = torch.where(mb, ubc, zero)
+            problem.assemble(zero, vals=self._A.vals, lift=lift, dvec=ub)
+            f = problem.external_load()
+            Kd = self._A.matvec(d)
+            dKd = float(torch.dot(d, Kd))
+            if dKd > 0:
+                alpha = -float(torch.dot(torch.where(mb, zero, f), d) + torch.dot(d, torch.where(mb, zero, lift))) / dKd
+                self.last_alpha = alpha
+                d = alpha * d
         self.calls += 1
-        return u
+        return torch.where(mb, ubc, d)
 
 
 def save(net, path, meta=None):
-    torch.save({"state": {k: v.detach().cpu() for k, v in net.state_dict().items()}, "meta": meta or {}}, path)
+    """Weights in BF16 (what the tensor-core kernels consume), buffers as-is."""
+    state = {}
+    for k, v in net.state_dict().items():
+        v = v.detach().cpu()
+        state[k] = v.to(torch.bfloat16) if k.startswith(("w.", "b.")) else v
+    torch.save({"state": state, "meta": meta or {}}, path)
 
 
 def load(path, device=None):
     ck = torch.load(path, map_location="cpu", weights_only=False)
     net = WarmStartNet()
-    net.load_state_dict(ck["state"])
+    net.load_state_dict({k: v.float() if v.dtype == torch.bfloat16 else v for k, v in ck["state"].items()})
     if device is not None:
         net.to(device)
     return net, ck.get("meta", {})
