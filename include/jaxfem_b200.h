@@ -195,6 +195,25 @@ FEM_API int fem_krylov_solve_f32(int method, int precond, int vec, int64_t n_bro
                          void* d_work, size_t work_bytes, int* h_iters, double* h_relres,
                          void* stream);
 
+/* Mixed-precision CG of the same linear solve (jax_solve / linear_solver,
+ * solver.py:63-92, 261-284): FP32 matrix values and FP32 iteration vectors,
+ * FP64 right-hand side d_b and FP64 solution d_x (initial guess in, result
+ * out), reductions in FP64.  Reliable updates: when the recursive residual
+ * has fallen below delta times its largest value since the last update
+ * (0 < delta < 1; 0.1 is the usual choice), the FP32 increment is added to
+ * d_x and the residual is replaced by the true one, b - A x with FP64
+ * accumulation; the search direction is kept.  Convergence, ||b - A x|| <=
+ * max(rtol ||b||, atol), is always confirmed on the true residual, which
+ * *h_relres reports.  Only method CG; needs fem_krylov_mixed_workspace_bytes
+ * of workspace.  *h_replacements counts the residual replacements. */
+FEM_API size_t fem_krylov_mixed_workspace_bytes(int precond, int vec, int64_t n_brows);
+FEM_API int fem_krylov_solve_mixed(int precond, int vec, int64_t n_brows,
+                         const int32_t* d_row_ptr, const int32_t* d_col_idx,
+                         const int32_t* d_diag, const float* d_vals, const double* d_b,
+                         double* d_x, double rtol, double atol, int maxiter, int check_every,
+                         double delta, void* d_work, size_t work_bytes, int* h_iters,
+                         int* h_replacements, double* h_relres, void* stream);
+
 /* ---- vector helpers of the Newton loop ----------------------------------
  * fem_newton_rhs: the BC handling of newton_update_helper + newton_step
  * (solver.py:290-304, 390-409).  With R = res + f_ext:

@@ -68,6 +68,9 @@ _SIGS = {
     "fem_krylov_workspace_bytes": (SZ, [I32, I32, I32, I64, I32]),
     "fem_krylov_solve_f64": (I32, [I32, I32, I32, I64, P, P, P, P, P, P, F64, F64, I32, I32, P, SZ, IP, DP, P]),
     "fem_krylov_solve_f32": (I32, [I32, I32, I32, I64, P, P, P, P, P, P, F64, F64, I32, I32, P, SZ, IP, DP, P]),
+    "fem_krylov_mixed_workspace_bytes": (SZ, [I32, I32, I64]),
+    "fem_krylov_solve_mixed": (I32, [I32, I32, I64, P, P, P, P, P, P, F64, F64, I32, I32, F64, P, SZ, IP, IP,
+                                     DP, P]),
     "fem_newton_rhs": (I32, [I64, P, P, P, P, P, P, P, P, DP, P, SZ, P]),
     "fem_dot_workspace_bytes": (SZ, [I64]),
     "fem_dot_f64": (I32, [I64, P, P, DP, P, SZ, P]),

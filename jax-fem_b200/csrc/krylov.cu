@@ -13,6 +13,17 @@
 // / 3x3 block-Jacobi preconditioner u = M r while it reduces gamma = r.u and
 // r.r; a pure SpMV w = A u reduces delta = w.u, and its last block forms
 // alpha and beta for the next iteration.  Two kernels per iteration.
+//
+// The mixed-precision CG (fem_krylov_solve_mixed) runs those same FP32
+// kernels on an FP32 matrix and keeps the solution in FP64 with reliable
+// updates (Sleijpen & van der Vorst 1996; the form of Clark et al. 2010 for
+// lattice QCD): whenever the recursive residual has dropped by a factor
+// `delta` below its largest value since the last update, the FP32 increment
+// is folded into the FP64 solution and the residual is replaced by the true
+// one, r = b - A x computed with FP64 accumulation.  The search direction is
+// kept, so the Krylov recurrence is not restarted and the iteration count
+// stays close to that of FP64 CG, while the true residual drives
+// convergence.
 #include <cstdlib>
 #include <cstring>
 #include <map>
@@ -23,11 +34,13 @@
 namespace fem {
 namespace {
 
-enum : int { ST_RUNNING = 0, ST_CONVERGED = 1 };
+enum : int { ST_RUNNING = 0, ST_CONVERGED = 1, ST_REPLACE = 2 };
 
 struct KState {
   double rz, rr, pq, alpha, beta, tol2, bnorm2;
   double rho, omega, rz_prev;
+  double rmax2;   // largest r.r since the last residual replacement
+  double delta2;  // replacement trigger (delta^2); 0 = never (plain CG)
   int iter, status, maxiter, first;
 };
 
@@ -108,11 +121,13 @@ __global__ void __launch_bounds__(kRowThreads, kRowBlocksPerSM) kr_residual_kern
       });
 }
 
-// z = M r; rz = r.z, rr = r.r, bb = b.b; initial status.
-template <int VEC, typename T>
+// z = M r; rz = r.z, rr = r.r, bb = b.b; initial status.  With `replace`
+// the residual r has just been replaced by the true one: only rz, rr and the
+// status are refreshed (b may be null), and the recurrence carries on.
+template <int VEC, typename T, typename BT>
 __global__ void cg_init_kernel(int precond, int64_t n_brows, const T* minv, const T* r, T* z,
-                               const T* b, double* partials, unsigned int* counter, KState* S,
-                               double rtol, double atol) {
+                               const BT* b, double* partials, unsigned int* counter, KState* S,
+                               double rtol, double atol, bool replace) {
   double v[3] = {0.0, 0.0, 0.0};
   for (int64_t nd = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; nd < n_brows;
        nd += int64_t(gridDim.x) * blockDim.x) {
@@ -123,16 +138,30 @@ __global__ void cg_init_kernel(int precond, int64_t n_brows, const T* minv, cons
 #pragma unroll
     for (int i = 0; i < VEC; ++i) {
       if (z != r) z[nd * VEC + i] = zn[i];
-      const double bi = double(b[nd * VEC + i]);
       v[0] = fma(double(rn[i]), double(zn[i]), v[0]);
       v[1] = fma(double(rn[i]), double(rn[i]), v[1]);
-      v[2] = fma(bi, bi, v[2]);
+      if (b != nullptr) {
+        const double bi = double(b[nd * VEC + i]);
+        v[2] = fma(bi, bi, v[2]);
+      }
     }
   }
   double tot[3];
   if (last_block_reduce<3>(v, partials, counter, tot)) {
     S->rz = tot[0];
     S->rr = tot[1];
+    S->rmax2 = tot[1];
+    if (replace) {
+      if (!finite_d(tot[0]) || !finite_d(tot[1]))
+        S->status = FEM_ERR_NONFINITE;
+      else if (tot[1] <= S->tol2)
+        S->status = ST_CONVERGED;
+      else if (tot[0] == 0.0)
+        S->status = FEM_ERR_BREAKDOWN;
+      else
+        S->status = ST_RUNNING;
+      return;
+    }
     S->bnorm2 = tot[2];
     const double t1 = rtol * rtol * tot[2], t2 = atol * atol;
     S->tol2 = t1 > t2 ? t1 : t2;
@@ -238,6 +267,10 @@ __global__ void cg_vec_kernel(int precond, int64_t n_brows, const T* minv, T* x,
       S->status = FEM_ERR_NOT_CONVERGED;
     } else if (tot[0] == 0.0) {
       S->status = FEM_ERR_BREAKDOWN;
+    } else if (S->delta2 > 0.0) {
+      // reliable update due: the residual fell by delta below its peak
+      if (tot[1] < S->delta2 * S->rmax2) S->status = ST_REPLACE;
+      else if (tot[1] > S->rmax2) S->rmax2 = tot[1];
     }
   }
 }
@@ -366,6 +399,28 @@ __global__ void copy_kernel(int64_t n, const T* a, T* b) {
     b[k] = a[k];
 }
 
+// ---- mixed-precision CG: FP64 solution, true residual with FP64 accumulation --
+// x64 += x32; x32 = 0
+__global__ void fold_kernel(int64_t n, double* x64, float* x32) {
+  for (int64_t k = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; k < n;
+       k += int64_t(gridDim.x) * blockDim.x) {
+    x64[k] += double(x32[k]);
+    x32[k] = 0.0f;
+  }
+}
+
+// r32 = b - A x (A f32, x and b f64, f64 accumulation, rounded once)
+template <int VEC>
+__global__ void __launch_bounds__(kRowThreads, kRowBlocksPerSM) kr_true_residual_kernel(
+    int64_t n_brows, const int32_t* rp, const int32_t* ci, const float* vals,
+    const double* __restrict__ x, const double* b, float* r) {
+  bsr_rows<VEC, float, double>(
+      n_brows, rp, ci, vals, [&](int64_t i) { return x[i]; },
+      [&](int64_t row, const double (&out)[VEC], int lane) {
+        if (lane < VEC) r[row * VEC + lane] = float(b[row * VEC + lane] - lane_pick<VEC, double>(out, lane));
+      });
+}
+
 // ---- cached CUDA graphs of CG / BiCGSTAB iteration chunks --------------------
 struct GraphKey {
   int method, precond, vec, tsize, chunk;
@@ -427,6 +482,40 @@ cudaStream_t capture_stream() {
   if (s[dev] == nullptr && cudaStreamCreateWithFlags(&s[dev], cudaStreamNonBlocking) != cudaSuccess)
     s[dev] = nullptr;
   return s[dev];
+}
+
+// Launch one chunk of iterations: replayed from a cached CUDA graph in the
+// steady state (kernel arguments are fixed pointers, so one capture serves
+// every replay), launched directly otherwise or when capture fails.
+template <class LaunchChunk>
+int run_chunk(const GraphKey& key, bool steady, int kernels_per_iter, LaunchChunk& launch_chunk,
+              cudaStream_t st) {
+  const int chunk = key.chunk;
+  if (steady && graphs_enabled()) {
+    cudaGraphExec_t exec = graph_lookup(key);
+    if (exec == nullptr) {
+      cudaStream_t cap = capture_stream();
+      if (cap != nullptr && cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
+        const int lrc = launch_chunk(cap, chunk);
+        cudaGraph_t g = nullptr;
+        const cudaError_t ec = cudaStreamEndCapture(cap, &g);
+        if (lrc == FEM_OK && ec == cudaSuccess && g != nullptr &&
+            cudaGraphInstantiate(&exec, g, 0) == cudaSuccess) {
+          graph_store(key, exec);
+        } else {
+          exec = nullptr;
+        }
+        if (g != nullptr) cudaGraphDestroy(g);
+        cudaGetLastError();  // a failed capture falls back to direct launches
+      }
+    }
+    if (exec != nullptr) {
+      FEM_CUDA_TRY(cudaGraphLaunch(exec, st));
+      launch_counter().fetch_add(int64_t(chunk) * kernels_per_iter, std::memory_order_relaxed);
+      return FEM_OK;
+    }
+  }
+  return launch_chunk(st, chunk);
 }
 
 // ---- workspace ----------------------------------------------------------------
@@ -514,8 +603,8 @@ int solve_impl(int method, int precond, int64_t n_brows, const int32_t* rp, cons
     if (method == FEM_KRYLOV_CG) {
       FEM_CUDA_TRY(cudaMemsetAsync(p0, 0, sizeof(T) * n, st));
       FEM_CUDA_TRY(cudaMemsetAsync(p1, 0, sizeof(T) * n, st));
-      cg_init_kernel<VEC, T><<<vg, 256, 0, st>>>(precond, n_brows, minv, r, z, b, partials, counter, S,
-                                                 rtol, atol);
+      cg_init_kernel<VEC, T, T><<<vg, 256, 0, st>>>(precond, n_brows, minv, r, z, b, partials, counter,
+                                                    S, rtol, atol, false);
       FEM_LAUNCH_CHECK();
       cg_spmv_kernel<VEC, T><<<rg, kRowThreads, bsr_rows_smem(), st>>>(n_brows, rp, ci, vals, z, q,
                                                                       partials, counter, S);
@@ -526,8 +615,8 @@ int solve_impl(int method, int precond, int64_t n_brows, const int32_t* rp, cons
       copy_kernel<T><<<vgn, 256, 0, st>>>(n, r, rhat);
       FEM_LAUNCH_CHECK();
       // rho = rhat.r = r.r, r.r and b.b (no preconditioning in this reduction)
-      cg_init_kernel<VEC, T><<<vg, 256, 0, st>>>(FEM_PRECOND_NONE, n_brows, minv, r, r, b, partials,
-                                                 counter, S, rtol, atol);
+      cg_init_kernel<VEC, T, T><<<vg, 256, 0, st>>>(FEM_PRECOND_NONE, n_brows, minv, r, r, b, partials,
+                                                    counter, S, rtol, atol, false);
       FEM_LAUNCH_CHECK();
     }
     return FEM_OK;
@@ -600,43 +689,14 @@ int solve_impl(int method, int precond, int64_t n_brows, const int32_t* rp, cons
     }
     if (status != ST_RUNNING || launched >= maxiter) break;
     const int chunk = check_every < (maxiter - launched) ? check_every : (maxiter - launched);
-    if (chunk == check_every && graphs_enabled()) {
-      // steady state: replay the chunk as a cached CUDA graph (kernel
-      // arguments are fixed pointers, so one capture serves every replay)
-      GraphKey key{};
-      key.method = method; key.precond = precond; key.vec = VEC; key.tsize = int(sizeof(T));
-      key.n = n_brows; key.chunk = chunk;
-      const void* kp[] = {rp, ci, vals, minv, x, r, z, p0, p1, q, rhat, pp, phat, vv, s, shat, t,
-                          partials, counter, S, b};
-      for (int i = 0; i < int(sizeof(kp) / sizeof(kp[0])); ++i) key.ptrs[i] = kp[i];
-      cudaGraphExec_t exec = graph_lookup(key);
-      if (exec == nullptr) {
-        cudaStream_t cap = capture_stream();
-        if (cap != nullptr && cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
-          const int lrc = launch_chunk(cap, chunk);
-          cudaGraph_t g = nullptr;
-          const cudaError_t ec = cudaStreamEndCapture(cap, &g);
-          if (lrc == FEM_OK && ec == cudaSuccess && g != nullptr &&
-              cudaGraphInstantiate(&exec, g, 0) == cudaSuccess) {
-            graph_store(key, exec);
-          } else {
-            exec = nullptr;
-          }
-          if (g != nullptr) cudaGraphDestroy(g);
-          cudaGetLastError();  // a failed capture falls back to direct launches
-        }
-      }
-      if (exec != nullptr) {
-        FEM_CUDA_TRY(cudaGraphLaunch(exec, st));
-        launch_counter().fetch_add(int64_t(chunk) * (method == FEM_KRYLOV_CG ? 2 : 5), std::memory_order_relaxed);
-      } else {
-        int lrc = launch_chunk(st, chunk);
-        if (lrc != FEM_OK) return lrc;
-      }
-    } else {
-      int lrc = launch_chunk(st, chunk);
-      if (lrc != FEM_OK) return lrc;
-    }
+    GraphKey key{};
+    key.method = method; key.precond = precond; key.vec = VEC; key.tsize = int(sizeof(T));
+    key.n = n_brows; key.chunk = chunk;
+    const void* kp[] = {rp, ci, vals, minv, x, r, z, p0, p1, q, rhat, pp, phat, vv, s, shat, t,
+                        partials, counter, S, b};
+    for (int i = 0; i < int(sizeof(kp) / sizeof(kp[0])); ++i) key.ptrs[i] = kp[i];
+    if ((rc = run_chunk(key, chunk == check_every, method == FEM_KRYLOV_CG ? 2 : 5, launch_chunk, st)) != FEM_OK)
+      return rc;
     launched += chunk;
   }
   if (h_iters) *h_iters = iters;
@@ -645,6 +705,168 @@ int solve_impl(int method, int precond, int64_t n_brows, const int32_t* rp, cons
   if (status == ST_RUNNING) status = FEM_ERR_NOT_CONVERGED;
   set_error("krylov: status %d after %d iterations (relres %.3e)", status, iters,
             bb > 0 ? sqrt(rr / bb) : sqrt(rr));
+  return status;
+}
+
+// Mixed-precision CG with reliable updates: FP32 matrix and iteration
+// vectors, FP64 right-hand side and solution (see the file comment).
+template <int VEC>
+int solve_mixed_impl(int precond, int64_t n_brows, const int32_t* rp, const int32_t* ci,
+                     const int32_t* diag, const float* vals, const double* b, double* x,
+                     double rtol, double atol, int maxiter, int check_every, double delta,
+                     void* work, size_t work_bytes, int* h_iters, int* h_replacements,
+                     double* h_relres, cudaStream_t st) {
+  const int64_t n = n_brows * VEC;
+  const size_t base = workspace_bytes(FEM_KRYLOV_CG, precond, VEC, n_brows, sizeof(float));
+  const size_t need = base + al256(size_t(n) * sizeof(float));
+  FEM_CHECK_ARG(work != nullptr && work_bytes >= need, "krylov workspace too small (%zu < %zu)",
+                work_bytes, need);
+  FEM_CHECK_ARG(precond == FEM_PRECOND_NONE || diag != nullptr, "preconditioner needs diag");
+  FEM_CHECK_ARG(delta > 0.0 && delta < 1.0, "replacement factor delta must be in (0, 1), got %g", delta);
+  if (check_every <= 0) check_every = 16;
+  char* p = static_cast<char*>(work);
+  KState* S = reinterpret_cast<KState*>(p);
+  unsigned int* counter = reinterpret_cast<unsigned int*>(p + 256);
+  double* partials = reinterpret_cast<double*>(p + 512);
+  p += 512 + al256(size_t(num_sms()) * 8 * 4 * sizeof(double));
+  auto take = [&](size_t cnt) {
+    float* q = reinterpret_cast<float*>(p);
+    p += al256(cnt * sizeof(float));
+    return q;
+  };
+  float* r = take(size_t(n));
+  float* zb = take(size_t(n));
+  float* p0 = take(size_t(n));  // p
+  float* p1 = take(size_t(n));  // s = A p
+  float* q = take(size_t(n));   // w = A u
+  float* minv = take((precond == FEM_PRECOND_BLOCK_JACOBI && VEC == 3) ? size_t(n_brows) * 9 : size_t(n));
+  float* x32 = reinterpret_cast<float*>(static_cast<char*>(work) + base);
+  float* z = (precond == FEM_PRECOND_NONE) ? r : zb;
+
+  FEM_CUDA_TRY(cudaMemsetAsync(work, 0, 512, st));
+  FEM_CUDA_TRY(cudaMemsetAsync(x32, 0, sizeof(float) * n, st));
+  FEM_CUDA_TRY(cudaMemsetAsync(p0, 0, sizeof(float) * n, st));
+  FEM_CUDA_TRY(cudaMemsetAsync(p1, 0, sizeof(float) * n, st));
+  KState init{};
+  init.maxiter = maxiter;
+  init.first = 1;
+  init.delta2 = delta * delta;
+  FEM_CUDA_TRY(cudaMemcpyAsync(S, &init, sizeof(KState), cudaMemcpyHostToDevice, st));
+  if (precond != FEM_PRECOND_NONE) {
+    precond_setup_kernel<VEC, float><<<unsigned((n_brows + 255) / 256), 256, 0, st>>>(precond, n_brows,
+                                                                                    diag, vals, minv);
+    FEM_LAUNCH_CHECK();
+  }
+  const unsigned rg = row_grid<float>(n_brows), vg = vec_grid(n_brows), vgn = vec_grid(n);
+  {
+    int rc = FEM_OK;
+    if ((rc = ensure_smem_attr(kr_true_residual_kernel<VEC>)) != FEM_OK) return rc;
+    if ((rc = ensure_smem_attr(cg_spmv_kernel<VEC, float>)) != FEM_OK) return rc;
+  }
+  // true residual into r, then u = M r and the reductions; `fresh` starts a
+  // new recurrence (first call, breakdown), otherwise the direction is kept
+  auto replace = [&](bool fresh) -> int {
+    fold_kernel<<<vgn, 256, 0, st>>>(n, x, x32);
+    FEM_LAUNCH_CHECK();
+    kr_true_residual_kernel<VEC><<<rg, kRowThreads, bsr_rows_smem(), st>>>(n_brows, rp, ci, vals, x, b, r);
+    FEM_LAUNCH_CHECK();
+    if (fresh) {
+      FEM_CUDA_TRY(cudaMemsetAsync(p0, 0, sizeof(float) * n, st));
+      FEM_CUDA_TRY(cudaMemsetAsync(p1, 0, sizeof(float) * n, st));
+    }
+    cg_init_kernel<VEC, float, double><<<vg, 256, 0, st>>>(precond, n_brows, minv, r, z, fresh ? b : nullptr,
+                                                           partials, counter, S, rtol, atol, !fresh);
+    FEM_LAUNCH_CHECK();
+    cg_spmv_kernel<VEC, float><<<rg, kRowThreads, bsr_rows_smem(), st>>>(n_brows, rp, ci, vals, z, q,
+                                                                        partials, counter, S);
+    FEM_LAUNCH_CHECK();
+    return FEM_OK;
+  };
+  double* mb = host_mailbox();
+  FEM_CHECK_ARG(mb != nullptr, "pinned mailbox allocation failed");
+  const KState* hs = reinterpret_cast<const KState*>(mb);
+  auto read_state = [&]() -> int {
+    FEM_CUDA_TRY(cudaMemcpyAsync(mb, S, sizeof(KState), cudaMemcpyDeviceToHost, st));
+    FEM_CUDA_TRY(cudaStreamSynchronize(st));
+    return FEM_OK;
+  };
+  auto launch_chunk = [&](cudaStream_t ls, int chunk) -> int {
+    for (int k = 0; k < chunk; ++k) {
+      cg_vec_kernel<VEC, float><<<vg, 256, 0, ls>>>(precond, n_brows, minv, x32, r, z, p0, p1, q, partials,
+                                                    counter, S);
+      FEM_LAUNCH_CHECK();
+      cg_spmv_kernel<VEC, float><<<rg, kRowThreads, bsr_rows_smem(), ls>>>(n_brows, rp, ci, vals, z, q,
+                                                                          partials, counter, S);
+      FEM_LAUNCH_CHECK();
+    }
+    return FEM_OK;
+  };
+  int rc = replace(true);
+  if (rc != FEM_OK) return rc;
+  int status = ST_RUNNING, iters = 0, iter_base = 0, restarts = 0, replacements = 0;
+  int launched = 0;
+  // Replacements are bounded: each one follows at least one iteration, and
+  // a long run of them without progress ends as "not converged".
+  const int max_replacements = maxiter;
+  while (true) {
+    if ((rc = read_state()) != FEM_OK) return rc;
+    status = hs->status;
+    iters = iter_base + hs->iter;
+    if (status == ST_REPLACE || (status == ST_CONVERGED && iters > iter_base)) {
+      // reliable update; a convergence claimed by the recursive residual is
+      // confirmed (or not) by the true one
+      if (++replacements > max_replacements) {
+        status = FEM_ERR_NOT_CONVERGED;
+        break;
+      }
+      if ((rc = replace(false)) != FEM_OK) return rc;
+      if ((rc = read_state()) != FEM_OK) return rc;
+      if (hs->status == ST_CONVERGED) {  // confirmed by the true residual
+        status = ST_CONVERGED;
+        break;
+      }
+      continue;
+    }
+    if (status == FEM_ERR_BREAKDOWN && iters > iter_base && restarts < 3 && launched < maxiter) {
+      // round-off breakdown near the attainable accuracy: fresh recurrence
+      // from the true residual
+      ++restarts;
+      iter_base = iters;
+      if ((rc = replace(true)) != FEM_OK) return rc;
+      continue;
+    }
+    if (status != ST_RUNNING || launched >= maxiter) break;
+    const int chunk = check_every < (maxiter - launched) ? check_every : (maxiter - launched);
+    GraphKey key{};
+    key.method = FEM_KRYLOV_CG + 100;  // distinct from the plain FP32 CG graphs
+    key.precond = precond; key.vec = VEC; key.tsize = int(sizeof(float));
+    key.n = n_brows; key.chunk = chunk;
+    const void* kp[] = {rp, ci, vals, minv, x32, r, z, p0, p1, q, partials, counter, S};
+    for (int i = 0; i < int(sizeof(kp) / sizeof(kp[0])); ++i) key.ptrs[i] = kp[i];
+    if ((rc = run_chunk(key, chunk == check_every, 2, launch_chunk, st)) != FEM_OK) return rc;
+    launched += chunk;
+  }
+  // the FP64 solution takes the last FP32 increment; the reported residual
+  // is the true one unless convergence was just confirmed
+  fold_kernel<<<vgn, 256, 0, st>>>(n, x, x32);
+  FEM_LAUNCH_CHECK();
+  if (status != ST_CONVERGED) {
+    kr_true_residual_kernel<VEC><<<rg, kRowThreads, bsr_rows_smem(), st>>>(n_brows, rp, ci, vals, x, b, r);
+    FEM_LAUNCH_CHECK();
+    cg_init_kernel<VEC, float, double><<<vg, 256, 0, st>>>(precond, n_brows, minv, r, z, nullptr, partials,
+                                                           counter, S, rtol, atol, true);
+    FEM_LAUNCH_CHECK();
+  }
+  if ((rc = read_state()) != FEM_OK) return rc;
+  const double rr = hs->rr, bb = hs->bnorm2;
+  if (status != ST_CONVERGED && hs->status == ST_CONVERGED) status = ST_CONVERGED;
+  if (h_iters) *h_iters = iters;
+  if (h_replacements) *h_replacements = replacements;
+  if (h_relres) *h_relres = bb > 0 ? sqrt(rr / bb) : sqrt(rr);
+  if (status == ST_CONVERGED) return FEM_OK;
+  if (status == ST_RUNNING || status == ST_REPLACE) status = FEM_ERR_NOT_CONVERGED;
+  set_error("krylov (mixed): status %d after %d iterations, %d replacements (relres %.3e)", status, iters,
+            replacements, bb > 0 ? sqrt(rr / bb) : sqrt(rr));
   return status;
 }
 
@@ -695,4 +917,30 @@ extern "C" int fem_krylov_solve_f32(int method, int precond, int vec, int64_t n_
   return fem::solve_dispatch<float>(method, precond, vec, n_brows, d_row_ptr, d_col_idx, d_diag,
                                     d_vals, d_b, d_x, rtol, atol, maxiter, check_every, d_work,
                                     work_bytes, h_iters, h_relres, stream);
+}
+
+extern "C" size_t fem_krylov_mixed_workspace_bytes(int precond, int vec, int64_t n_brows) {
+  return fem::workspace_bytes(FEM_KRYLOV_CG, precond, vec, n_brows, 4) +
+         fem::al256(size_t(n_brows) * vec * sizeof(float));
+}
+
+extern "C" int fem_krylov_solve_mixed(int precond, int vec, int64_t n_brows, const int32_t* d_row_ptr,
+                                      const int32_t* d_col_idx, const int32_t* d_diag,
+                                      const float* d_vals, const double* d_b, double* d_x, double rtol,
+                                      double atol, int maxiter, int check_every, double delta,
+                                      void* d_work, size_t work_bytes, int* h_iters,
+                                      int* h_replacements, double* h_relres, void* stream) {
+  FEM_CHECK_ARG(vec == 1 || vec == 3, "vec must be 1 or 3");
+  FEM_CHECK_ARG(precond >= FEM_PRECOND_NONE && precond <= FEM_PRECOND_BLOCK_JACOBI,
+                "unknown preconditioner %d", precond);
+  FEM_CHECK_ARG(n_brows > 0, "empty system");
+  FEM_CHECK_ARG(rtol >= 0 && atol >= 0, "negative tolerance");
+  auto st = fem::as_stream(stream);
+  if (vec == 3)
+    return fem::solve_mixed_impl<3>(precond, n_brows, d_row_ptr, d_col_idx, d_diag, d_vals, d_b, d_x, rtol,
+                                    atol, maxiter, check_every, delta, d_work, work_bytes, h_iters,
+                                    h_replacements, h_relres, st);
+  return fem::solve_mixed_impl<1>(precond, n_brows, d_row_ptr, d_col_idx, d_diag, d_vals, d_b, d_x, rtol,
+                                  atol, maxiter, check_every, delta, d_work, work_bytes, h_iters,
+                                  h_replacements, h_relres, st);
 }

@@ -60,6 +60,51 @@ def test_krylov_matches_direct_solve(pkg, cuda, method, precond, fp32):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("precond", ["none", "jacobi", "block_jacobi"])
+def test_mixed_reliable_cg_matches_direct_solve(pkg, cuda, precond):
+    """FP32 matrix, FP64 b and x: reliable-update CG reaches 1e-10 on the
+    true residual of the FP32-valued matrix (out of reach of FP32 CG alone),
+    and the solution matches a direct FP64 solve of that matrix to 1e-8."""
+    S = _solver_mod()
+    prob, A32, b = _elastic_system(pkg, cuda, fp32=True)
+    K = A32.to_scipy().astype(np.float64)
+    xref = spla.spsolve(K.tocsc(), b)
+    bd = torch.tensor(b, dtype=torch.float64, device=cuda)
+    x = torch.zeros_like(bd)
+    cfg = S.resolve_linear({"cg": {"precond": precond, "rtol": 1e-10, "atol": 0.0, "maxiter": 20000}})
+    it, nrep, rel = S.reliable_solve(A32, bd, x, cfg, S._Workspaces())
+    assert it > 0 and nrep > 0
+    xs = x.cpu().numpy()
+    assert np.abs(xs - xref).max() / np.abs(xref).max() < 1e-8
+    true_rel = np.linalg.norm(b - K @ xs) / np.linalg.norm(b)
+    assert true_rel <= 1e-10 * (1.0 + 1e-6)
+    assert abs(true_rel - rel) <= 1e-3 * true_rel
+    # a second solve from the converged x is immediate
+    it2, _, _ = S.reliable_solve(A32, bd, x, cfg, S._Workspaces())
+    assert it2 == 0
+
+
+@pytest.mark.gpu
+def test_mixed_reliable_cg_error_codes(pkg, cuda):
+    S = _solver_mod()
+    nat = pkg._native
+    prob, A32, b = _elastic_system(pkg, cuda, fp32=True)
+    bd = torch.tensor(b, dtype=torch.float64, device=cuda)
+    x = torch.zeros_like(bd)
+    with pytest.raises(nat.FEMNativeError) as ei:
+        S.reliable_solve(A32, bd, x, S.resolve_linear({"cg": {"rtol": 1e-12, "maxiter": 5}}), S._Workspaces())
+    assert ei.value.status == nat.FEM_ERR_NOT_CONVERGED
+    with pytest.raises(nat.FEMNativeError) as ei:
+        S.reliable_solve(A32, bd, x, S.resolve_linear({"cg": {"reliable_delta": 1.5}}), S._Workspaces())
+    assert ei.value.status == nat.FEM_ERR_ARG
+    bd[7] = float("nan")
+    x.zero_()
+    with pytest.raises(nat.FEMNativeError) as ei:
+        S.reliable_solve(A32, bd, x, S.resolve_linear({"cg": {}}), S._Workspaces())
+    assert ei.value.status == nat.FEM_ERR_NONFINITE
+
+
+@pytest.mark.gpu
 def test_krylov_error_codes(pkg, cuda):
     S = _solver_mod()
     nat = pkg._native
@@ -92,15 +137,19 @@ def _twist(pkg, n, deg):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("precision,rtol", [("fp64", 1e-10), ("mixed", 1e-10), ("mixed", "adaptive")])
-def test_newton_paths_match_oracle(pkg, cuda, precision, rtol):
+@pytest.mark.parametrize("precision,rtol,delta", [("fp64", 1e-10, 0.1), ("mixed", 1e-10, 0.1),
+                                                  ("mixed", "adaptive", 0.1), ("mixed", "adaptive", 0.0)])
+def test_newton_paths_match_oracle(pkg, cuda, precision, rtol, delta):
+    """delta 0.1: mixed CG with reliable updates; delta 0: FP32 CG inside
+    FP64 iterative refinement."""
     n = 6
     m = pkg.box_mesh(n, n, n, 1.0, 1.0, 1.0)
     mesh = pkg.Mesh(m.points, m.cells_dict["hexahedron"])
     bc = _twist(pkg, n, 20.0)
     prob = make_problem(pkg, mesh, pkg.NeoHookean(10.0, 0.3), bc=bc)
     opts = {"newton": {"rel_tol": 1e-8, "tol": 1e-14, "precision": precision,
-                       "linear": {"cg": {"precond": "block_jacobi", "rtol": rtol, "atol": 0.0}}}}
+                       "linear": {"cg": {"precond": "block_jacobi", "rtol": rtol, "atol": 0.0,
+                                         "reliable_delta": delta}}}}
     sol = pkg.solver(prob, opts)[0].cpu().numpy().reshape(-1)
     op = fo.OracleProblem(mesh.points, mesh.cells, 3, fo.Law("neo_hookean", E=10.0, nu=0.3), dirichlet_bc_info=bc)
     ref = fo.newton_solve(op, rel_tol=1e-12, tol=1e-14)

@@ -70,37 +70,45 @@ def test_trained_network_gain_on_heldout(pkg, cuda):
     """What the committed trained network gains over the zero start on
     held-out SIMP cantilevers (seeds disjoint from training).
 
-    Asserted: the start's relative displacement error ||u* - u0|| / ||u*||
-    falls from 1 (zero start) to below 0.15.  Recorded, not asserted: its
-    energy-norm error ||u* - u0||_K / ||u*||_K, which stays near 0.9 (the
-    coarse-grid prediction misses the fine-scale strain between cells of
-    different density), and the Krylov iterations to the same absolute
-    residual (1e-8 of the zero-start residual), which the learned start
-    leaves essentially unchanged on this problem."""
+    Asserted:
+    - the raw prediction's relative displacement error ||u* - d|| / ||u*||
+      is below 0.1 (the zero start's is 1);
+    - the Galerkin-scaled start's energy-norm error ||u* - u0||_K / ||u*||_K
+      is below 1 (the zero start's is 1).
+    Recorded: Krylov iterations from both starts to the same absolute
+    residual (1e-8 of the zero-start residual) on the FP64 path and on the
+    mixed path with FP32 CG inside FP64 refinement.  The raw prediction's
+    strain is noisy (its energy-norm error is above 1), so the Galerkin
+    factor shrinks it, and CG, which resolves the smooth error no later than
+    the rest, gains about nothing at 1e-8."""
     import os
     ws = _ws()
     path = os.path.join(os.path.dirname(ws.__file__), "weights", "warmstart_simp60.pt")
     net, meta = ws.load(path, cuda)
-    pred = ws.Predictor(net)
+    pred, raw = ws.Predictor(net), ws.Predictor(net, galerkin=False)
     prob = ws.cantilever_problem()
     g = torch.Generator().manual_seed(424242)
     lin = {"cg": {"precond": "block_jacobi", "rtol": "adaptive", "atol": 0.0, "maxiter": 50000}}
-    l2, energy, iters = [], [], {"zero": [], "learned": []}
+    l2, energy = [], []
+    iters = {f"{p}_{a}": [] for p in ("fp64", "mixed") for a in ("zero", "learned")}
     for _ in range(6):
         rho = ws.random_density(g)
         prob.set_patch(float(torch.randint(0, ws.NZ - 2, (1,), generator=g).item()))
         prob.set_params(ws.cell_rho_to_torch(rho, cuda))
         ref = pkg.solver(prob, {"newton": {"rel_tol": 1e-10, "tol": 1e-30, "linear": lin}})[0].reshape(-1)
-        u0 = pred(prob)
         K = prob.A  # FP64 eliminated tangent of the linear problem (assembled by the solve)
-        e = ref - u0
+        e = ref - raw(prob)
         l2.append((e.norm() / ref.norm()).item())
+        e = ref - pred(prob)
         energy.append((torch.dot(e, K.matvec(e)) / torch.dot(ref, K.matvec(ref))).sqrt().item())
-        for arm, start in (("zero", None), ("learned", pred)):
-            (_,), info = pkg.solver(prob, {"newton": {"rel_tol": 1e-8, "tol": 1e-30, "linear": lin,
-                                                       "rel_tol_reference": "zero", "warm_start": start,
-                                                       "return_info": True}})
-            iters[arm].append(sum(info["krylov_iters"]))
-    print(f"learned start: relative L2 error {np.round(l2, 4)}, energy-norm error {np.round(energy, 4)}; "
-          f"krylov zero {iters['zero']} learned {iters['learned']}")
-    assert max(l2) < 0.15
+        refine = {"cg": dict(lin["cg"], reliable_delta=0.0)}
+        for prec, plin in (("fp64", lin), ("mixed", refine)):
+            for arm, start in (("zero", None), ("learned", pred)):
+                (_,), info = pkg.solver(prob, {"newton": {"rel_tol": 1e-8, "tol": 1e-30, "linear": plin,
+                                                           "precision": prec, "rel_tol_reference": "zero",
+                                                           "warm_start": start, "return_info": True}})
+                iters[f"{prec}_{arm}"].append(sum(info["krylov_iters"]))
+    print(f"raw prediction L2 error {np.round(l2, 4)}; Galerkin start energy-norm error {np.round(energy, 4)}; "
+          f"krylov {iters}")
+    assert max(l2) < 0.1
+    assert max(energy) < 1.0
