@@ -140,6 +140,31 @@ FEM_API int fem_j2_commit(const double* h_params, int n_params, int64_t num_cell
                   const double* d_sigma_old, const double* d_eps_old, const double* d_alpha_old,
                   double* d_sigma_new, double* d_eps_new, double* d_alpha_new, void* stream);
 
+/* ---- J2 yield-stress sensitivity ----------------------------------------
+ * No counterpart in the reference: its ad_wrapper (solver.py:1383-1417)
+ * differentiates one static solve, not a load history.  The derivative of
+ * the return map above (stress_return_map, test_plasticity.py:42-64, with
+ * linear hardening) w.r.t. the initial yield stress sigma_y, given d_du =
+ * du/dsigma_y (NULL = 0: the explicit part) and the committed state's
+ * sensitivities (NULL = 0: the first increment).  Writes dsigma (C,8,9),
+ * deps = sym grad du (C,8,9; NULL to skip) and dalpha (C,8).  Carried over
+ * the increments this gives d(reaction)/d(sigma_y) with one extra linear
+ * solve per increment (the direct method; for a single parameter it costs
+ * what the adjoint does and needs no stored history). */
+FEM_API int fem_j2_sensitivity(const double* h_params, int n_params, int64_t num_cells,
+                  const int32_t* d_cells, const double* d_points, const double* d_u,
+                  const double* d_du, const double* d_sigma_old, const double* d_eps_old,
+                  const double* d_alpha_old, const double* d_dsigma_old, const double* d_deps_old,
+                  const double* d_dalpha_old, double* d_dsigma, double* d_deps, double* d_dalpha,
+                  void* stream);
+
+/* The internal force of a quadrature-point stress field: d_out[node*3+i] +=
+ * sum over cells and quadrature points of stress_ij dN_node/dx_j JxW (the
+ * residual of problem.py:189-214 with the stress supplied instead of
+ * computed from u).  d_stress is (C,8,9) f64; d_out (N*3) f64 accumulates. */
+FEM_API int fem_stress_divergence(int64_t num_cells, const int32_t* d_cells, const double* d_points,
+                  const double* d_stress, double* d_out, void* stream);
+
 /* ---- adjoint parameter VJP ----------------------------------------------
  * Replaces jax.vjp of the BC-applied residual w.r.t. internal variables in
  * implicit_vjp (solver.py:1340-1356, 1376-1378):

@@ -61,6 +61,8 @@ _SIGS = {
     "fem_assemble_f64": (I32, [I32, DP, I32, I32, I64, I64, P, P, P, P, P, P, P, P, I64, P, P, P, P, P, P]),
     "fem_assemble_f32": (I32, [I32, DP, I32, I32, I64, I64, P, P, P, P, P, P, P, P, I64, P, P, P, P, P, P]),
     "fem_j2_commit": (I32, [DP, I32, I64, P, P, P, P, P, P, P, P, P, P]),
+    "fem_j2_sensitivity": (I32, [DP, I32, I64, P, P, P, P, P, P, P, P, P, P, P, P, P, P]),
+    "fem_stress_divergence": (I32, [I64, P, P, P, P, P]),
     "fem_param_vjp_f64": (I32, [I32, DP, I32, I64, P, P, P, P, P, P, P]),
     "fem_bsr_spmv_f64": (I32, [I32, I64, P, P, P, P, P, P]),
     "fem_bsr_spmv_f32": (I32, [I32, I64, P, P, P, P, P, P]),

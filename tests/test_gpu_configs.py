@@ -15,7 +15,9 @@ do not need an oracle solve of the whole problem:
 - 40^3 J2 with hardening, 10 increments of u_x(x=1) up to 0.02 (206,763
   dofs): after the last increment the oracle's residual, evaluated with the
   GPU's committed state of increment 9, is <= 1e-8 of its value at the
-  increment's start; the committed state equals the oracle's return map.
+  increment's start; the committed state equals the oracle's return map;
+  the direct sensitivity of the end reaction to the yield stress matches a
+  central difference of two more histories (1e-5 relative).
 """
 import importlib
 import math
@@ -124,11 +126,10 @@ def test_config_simp_adjoint_vs_fd(pkg, cuda):
     assert abs(fd - ad) <= 1e-4 * abs(ad), (fd, ad)
 
 
-@pytest.mark.gpu
-def test_config_j2_40(pkg, cuda):
-    n = 40
-    m = pkg.box_mesh(n, n, n, 1.0, 1.0, 1.0)
-    mesh = pkg.Mesh(m.points, m.cells_dict["hexahedron"])
+def _j2_history(pkg, cuda, mesh, sy, with_sens, rel_tol=1e-8):
+    """10 increments of u_x(x=1) up to 0.02 on the J2 cube; returns the
+    problem, the last solution, the state before the last commit, the last
+    start, the bc list, the end reaction F and (with_sens) dF/dsigma_y."""
     C = len(mesh.cells)
     left = lambda p: np.isclose(p[0], 0.0, atol=1e-5)  # noqa: E731
     right = lambda p: np.isclose(p[0], 1.0, atol=1e-5)  # noqa: E731
@@ -137,11 +138,12 @@ def test_config_j2_40(pkg, cuda):
 
     class J2(pkg.Problem):
         def get_tensor_map(self):
-            return pkg.J2Plasticity(70e3, 0.3, 250.0, 700.0)
+            return pkg.J2Plasticity(70e3, 0.3, sy, 700.0)
 
     prob = J2(mesh, vec=3, dim=3, dirichlet_bc_info=bc)
     prob.internal_vars = [z(C, 8, 3, 3), z(C, 8, 3, 3), z(C, 8)]
-    opts = {"newton": {"rel_tol": 1e-8, "tol": 1e-14,
+    sens = pkg.J2YieldSensitivity(prob) if with_sens else None
+    opts = {"newton": {"rel_tol": rel_tol, "tol": 1e-14,
                        "linear": {"cg": {"precond": "block_jacobi", "rtol": 1e-10, "atol": 0.0, "maxiter": 20000}}}}
     sol = None
     for k in range(1, 11):
@@ -150,7 +152,22 @@ def test_config_j2_40(pkg, cuda):
         prev_state = [t.cpu().numpy() for t in prob.internal_vars]
         start = sol.cpu().numpy().reshape(-1) if sol is not None else np.zeros(prob.num_total_dofs_all_vars)
         sol = pkg.solver(prob, {"newton": dict(opts["newton"], initial_guess=sol)})[0]
+        if sens is not None:
+            sens.step(sol)
         prob.update_j2_state(sol)
+    mask = torch.zeros(prob.num_total_dofs_all_vars, dtype=torch.bool, device=cuda)
+    mask[torch.from_numpy(np.flatnonzero(np.isclose(mesh.points[:, 0], 1.0, atol=1e-5)) * 3).to(cuda)] = True
+    F = float(pkg.j2_reaction(prob, mask))
+    dF = float(sens.reaction(mask)) if sens is not None else None
+    return prob, sol, prev_state, start, bc, F, dF
+
+
+@pytest.mark.gpu
+def test_config_j2_40(pkg, cuda):
+    n = 40
+    m = pkg.box_mesh(n, n, n, 1.0, 1.0, 1.0)
+    mesh = pkg.Mesh(m.points, m.cells_dict["hexahedron"])
+    prob, sol, prev_state, start, bc, F, dF = _j2_history(pkg, cuda, mesh, 250.0, True)
     u = sol.cpu().numpy().reshape(-1)
     op = fo.OracleProblem(mesh.points, mesh.cells, 3, fo.Law("j2", E=70e3, nu=0.3, sig0=250.0, H=700.0),
                           dirichlet_bc_info=bc, internal_vars=[prev_state[0], prev_state[1], prev_state[2]])
@@ -159,3 +176,11 @@ def test_config_j2_40(pkg, cuda):
     sig = prob.internal_vars[0].cpu().numpy()
     assert np.abs(sig - op.internal_vars[0]).max() <= 1e-8 * np.abs(op.internal_vars[0]).max()
     assert prob.internal_vars[2].max().item() > 0.0  # plastic flow happened
+    # d(reaction)/d(sigma_y) vs a central difference of two more histories
+    # solved to 1e-11 (h = 1e-2: truncation and solve noise both below 1e-7)
+    h = 1e-2
+    Fp = _j2_history(pkg, cuda, mesh, 250.0 + h, False, rel_tol=1e-11)[5]
+    Fm = _j2_history(pkg, cuda, mesh, 250.0 - h, False, rel_tol=1e-11)[5]
+    fd = (Fp - Fm) / (2 * h)
+    print(f"J2 40^3: reaction {F:.10g}, dF/dsigma_y {dF:.10g}, central difference {fd:.10g}")
+    assert abs(dF - fd) <= 1e-5 * abs(fd), (dF, fd)

@@ -278,3 +278,65 @@ def test_j2_hardening_increments_match_oracle(pkg, cuda):
     assert alpha.max() > 0  # the bar has yielded
     np.testing.assert_allclose(sig, op.internal_vars[0], rtol=0, atol=1e-7 * np.abs(op.internal_vars[0]).max())
     np.testing.assert_allclose(alpha, op.internal_vars[2], rtol=0, atol=1e-10)
+
+
+def _oracle_j2_reaction(mesh, sig0, increments, total, mask):
+    """Reaction force at the end of an oracle J2 load history (FP64, direct
+    solves): the internal force summed over the dofs in ``mask``."""
+    C = len(mesh.cells)
+    left = lambda p: np.isclose(p[0], 0.0, atol=1e-5)  # noqa: E731
+    right = lambda p: np.isclose(p[0], 1.0, atol=1e-5)  # noqa: E731
+    bc = [[left] * 3 + [right], [0, 1, 2, 0], [lambda p: 0.0] * 4]
+    iv = [np.zeros((C, 8, 3, 3)), np.zeros((C, 8, 3, 3)), np.zeros((C, 8))]
+    op = fo.OracleProblem(mesh.points, mesh.cells, 3, fo.Law("j2", E=70e3, nu=0.3, sig0=sig0, H=700.0),
+                          dirichlet_bc_info=bc, internal_vars=iv)
+    u = None
+    for k in range(1, increments + 1):
+        bc[2][-1] = (lambda v: (lambda p: v))(total * k / increments)
+        op.update_dirichlet(bc)
+        u = fo.newton_solve(op, initial_guess=u, rel_tol=1e-12, tol=1e-11)
+        F = op.residual(u)[mask].sum()
+        fo.j2_commit(op, u)
+    return F
+
+
+@pytest.mark.gpu
+def test_j2_yield_sensitivity_matches_oracle_fd(pkg, cuda):
+    """dF/dsigma_y of the end reaction of a 4-increment J2 history (4^3
+    cells, plastic flow at the last three increments) from the direct
+    sensitivity on the GPU vs a central difference of the oracle's history
+    (h = 1e-2 on sigma_y = 250): 1e-6 relative.  The reaction itself matches
+    the oracle's to 1e-9."""
+    n, incs, total, sy = 4, 4, 0.02, 250.0
+    m = pkg.box_mesh(n, n, n, 1.0, 1.0, 1.0)
+    mesh = pkg.Mesh(m.points, m.cells_dict["hexahedron"])
+    C = len(mesh.cells)
+    left = lambda p: np.isclose(p[0], 0.0, atol=1e-5)  # noqa: E731
+    right = lambda p: np.isclose(p[0], 1.0, atol=1e-5)  # noqa: E731
+    bc = [[left] * 3 + [right], [0, 1, 2, 0], [lambda p: 0.0] * 4]
+    prob = make_problem(pkg, mesh, pkg.J2Plasticity(70e3, 0.3, sy, 700.0), bc=bc,
+                        ivars=[torch.zeros(C, 8, 3, 3, dtype=torch.float64, device=cuda),
+                               torch.zeros(C, 8, 3, 3, dtype=torch.float64, device=cuda),
+                               torch.zeros(C, 8, dtype=torch.float64, device=cuda)])
+    mask_np = np.zeros(mesh.points.shape[0] * 3, dtype=bool)
+    mask_np[np.flatnonzero(np.isclose(mesh.points[:, 0], 1.0, atol=1e-5)) * 3] = True
+    mask = torch.from_numpy(mask_np).to(cuda)
+    sens = pkg.J2YieldSensitivity(prob)
+    opts = {"newton": {"rel_tol": 1e-11, "tol": 1e-12,
+                       "linear": {"cg": {"precond": "block_jacobi", "rtol": 1e-13, "atol": 0.0}}}}
+    sol = None
+    for k in range(1, incs + 1):
+        bc[2][-1] = (lambda v: (lambda p: v))(total * k / incs)
+        prob.fes[0].update_Dirichlet_boundary_conditions(bc)
+        sol = pkg.solver(prob, {"newton": dict(opts["newton"], initial_guess=sol)})[0]
+        sens.step(sol)
+        prob.update_j2_state(sol)
+    F = float(pkg.j2_reaction(prob, mask))
+    dF = float(sens.reaction(mask))
+    assert prob.internal_vars[2].max().item() > 0.0
+    F_ref = _oracle_j2_reaction(mesh, sy, incs, total, mask_np)
+    assert abs(F - F_ref) <= 1e-9 * abs(F_ref), (F, F_ref)
+    h = 1e-2
+    fd = (_oracle_j2_reaction(mesh, sy + h, incs, total, mask_np)
+          - _oracle_j2_reaction(mesh, sy - h, incs, total, mask_np)) / (2 * h)
+    assert abs(dF - fd) <= 1e-6 * abs(fd), (dF, fd)
