@@ -39,6 +39,11 @@ int ensure_smem_attr_ptr(const void* kernel) {
   if (done.count({kernel, dev})) return FEM_OK;
   cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        int(bsr_rows_smem()));
+  // the row kernels are sized for kRowBlocksPerSM resident blocks: ask for
+  // the largest shared-memory carve-out
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(kernel, cudaFuncAttributePreferredSharedMemoryCarveout,
+                             int(cudaSharedmemCarveoutMaxShared));
   if (e != cudaSuccess) {
     set_error("cudaFuncSetAttribute(bsr smem) -> %s", cudaGetErrorString(e));
     return FEM_ERR_CUDA;

@@ -881,6 +881,7 @@ int solve_dispatch(int method, int precond, int vec, int64_t n_brows, const int3
                 "unknown preconditioner %d", precond);
   FEM_CHECK_ARG(n_brows > 0, "empty system");
   FEM_CHECK_ARG(rtol >= 0 && atol >= 0, "negative tolerance");
+  FEM_CHECK_ARG(bsr_aligned(vals, ci), "vals and col_idx must be 16-byte aligned");
   auto st = as_stream(stream);
   if (vec == 3)
     return solve_impl<3, T>(method, precond, n_brows, rp, ci, diag, vals, b, x, rtol, atol, maxiter,
@@ -935,6 +936,7 @@ extern "C" int fem_krylov_solve_mixed(int precond, int vec, int64_t n_brows, con
                 "unknown preconditioner %d", precond);
   FEM_CHECK_ARG(n_brows > 0, "empty system");
   FEM_CHECK_ARG(rtol >= 0 && atol >= 0, "negative tolerance");
+  FEM_CHECK_ARG(fem::bsr_aligned(d_vals, d_col_idx), "vals and col_idx must be 16-byte aligned");
   auto st = fem::as_stream(stream);
   if (vec == 3)
     return fem::solve_mixed_impl<3>(precond, n_brows, d_row_ptr, d_col_idx, d_diag, d_vals, d_b, d_x, rtol,

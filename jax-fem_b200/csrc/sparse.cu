@@ -78,6 +78,7 @@ extern "C" int fem_bsr_spmv_f64(int vec, int64_t n_brows, const int32_t* d_row_p
                                 double* d_y, void* stream) {
   FEM_CHECK_ARG(vec == 1 || vec == 3, "vec must be 1 or 3");
   FEM_CHECK_ARG(n_brows >= 0, "negative size");
+  FEM_CHECK_ARG(bsr_aligned(d_vals, d_col_idx), "vals and col_idx must be 16-byte aligned");
   if (n_brows == 0) return FEM_OK;
   auto st = as_stream(stream);
   int rc = ensure_smem_attr(vec == 3 ? spmv_kernel<3, double, double, double> : spmv_kernel<1, double, double, double>);
@@ -95,6 +96,7 @@ extern "C" int fem_bsr_spmv_f32(int vec, int64_t n_brows, const int32_t* d_row_p
                                 float* d_y, void* stream) {
   FEM_CHECK_ARG(vec == 1 || vec == 3, "vec must be 1 or 3");
   FEM_CHECK_ARG(n_brows >= 0, "negative size");
+  FEM_CHECK_ARG(bsr_aligned(d_vals, d_col_idx), "vals and col_idx must be 16-byte aligned");
   if (n_brows == 0) return FEM_OK;
   auto st = as_stream(stream);
   int rc = ensure_smem_attr(vec == 3 ? spmv_kernel<3, float, float, float> : spmv_kernel<1, float, float, float>);
@@ -113,6 +115,7 @@ extern "C" int fem_bsr_residual_mixed(int vec, int64_t n_brows, const int32_t* d
                                       void* stream) {
   FEM_CHECK_ARG(vec == 1 || vec == 3, "vec must be 1 or 3");
   FEM_CHECK_ARG(n_brows >= 0, "negative size");
+  FEM_CHECK_ARG(bsr_aligned(d_vals, d_col_idx), "vals and col_idx must be 16-byte aligned");
   if (n_brows == 0) return FEM_OK;
   auto st = as_stream(stream);
   int rc = ensure_smem_attr(vec == 3 ? residual_mixed_kernel<3> : residual_mixed_kernel<1>);

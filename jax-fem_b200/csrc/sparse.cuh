@@ -8,13 +8,23 @@ constexpr int kRowThreads = 256;   // 8 warps per block
 constexpr int kStageBytes = 4096;  // per-warp shared-memory stage for matrix values
 constexpr int kRowBlocksPerSM = 4; // resident blocks per SM the row kernels are sized for
 
-template <typename VT>
+// Block rows per warp group: ~3.9 KB of FP32 or FP64 3x3 blocks; FP32
+// values with FP64 accumulation take 2 rows to stay within the registers of
+// kRowBlocksPerSM resident blocks.
+template <typename VT, typename AT = VT>
 __host__ __device__ constexpr int rows_per_warp() {
-  return sizeof(VT) == 4 ? 4 : 2;  // ~3.9 KB of 3x3 blocks per group either way
+  return (sizeof(VT) == 4 && sizeof(AT) == 4) ? 4 : 2;
 }
 
 // Dynamic shared memory a bsr_rows kernel needs (one stage per warp).
 constexpr size_t bsr_rows_smem() { return size_t(kRowThreads / 32) * (kStageBytes + 16); }
+
+// The row kernels copy matrix values with 16-byte cp.async transfers: the
+// values must start on a 16-byte boundary (and the column indices, read as
+// int32, on a 4-byte one).
+inline bool bsr_aligned(const void* vals, const void* col_idx) {
+  return (reinterpret_cast<uintptr_t>(vals) & 15u) == 0 && (reinterpret_cast<uintptr_t>(col_idx) & 3u) == 0;
+}
 
 __device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
   const unsigned sa = static_cast<unsigned>(__cvta_generic_to_shared(smem));
@@ -38,7 +48,7 @@ template <int VEC, typename VT, typename AT, class XF, class EPI>
 __device__ __forceinline__ void bsr_rows(int64_t n_brows, const int32_t* __restrict__ rp,
                                          const int32_t* __restrict__ ci,
                                          const VT* __restrict__ vals, XF xf, EPI epi) {
-  constexpr int R = rows_per_warp<VT>();
+  constexpr int R = rows_per_warp<VT, AT>();
   constexpr int VV = VEC * VEC;
   extern __shared__ __align__(16) unsigned char bsr_smem[];
   unsigned char* stage = bsr_smem + (threadIdx.x >> 5) * (kStageBytes + 16);
