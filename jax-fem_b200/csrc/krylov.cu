@@ -116,8 +116,8 @@ __global__ void __launch_bounds__(kRowThreads, kRowBlocksPerSM) kr_residual_kern
                                                                  const T* b, T* r) {
   bsr_rows<VEC, T, double>(
       n_brows, rp, ci, vals, [&](int64_t i) { return x[i]; },
-      [&](int64_t row, const double (&out)[VEC], int lane) {
-        if (lane < VEC) r[row * VEC + lane] = T(double(b[row * VEC + lane]) - lane_pick<VEC, double>(out, lane));
+      [&](int64_t row, int c, double val) {
+        r[row * VEC + c] = T(double(b[row * VEC + c]) - val);
       });
 }
 
@@ -193,13 +193,10 @@ __global__ void __launch_bounds__(kRowThreads, kRowBlocksPerSM) cg_spmv_kernel(i
   double v[1] = {0.0};
   bsr_rows<VEC, T, T>(
       n_brows, rp, ci, vals, [&](int64_t i) { return u[i]; },
-      [&](int64_t row, const T (&out)[VEC], int lane) {
-        if (lane < VEC) {
-          const int64_t i = row * VEC + lane;
-          const T wo = lane_pick<VEC, T>(out, lane);
-          w[i] = wo;
-          v[0] = fma(double(u[i]), double(wo), v[0]);
-        }
+      [&](int64_t row, int c, T wo) {
+        const int64_t i = row * VEC + c;
+        w[i] = wo;
+        v[0] = fma(double(u[i]), double(wo), v[0]);
       });
   double tot[1];
   if (last_block_reduce<1>(v, partials, counter, tot)) {
@@ -309,14 +306,11 @@ __global__ void __launch_bounds__(kRowThreads, kRowBlocksPerSM) bicg_spmv_kernel
   double v[2] = {0.0, 0.0};
   bsr_rows<VEC, T, T>(
       n_brows, rp, ci, vals, [&](int64_t i) { return x[i]; },
-      [&](int64_t row, const T (&out)[VEC], int lane) {
-        if (lane < VEC) {
-          const int64_t i = row * VEC + lane;
-          const T yo = lane_pick<VEC, T>(out, lane);
-          y[i] = yo;
-          v[0] = fma(double(w[i]), double(yo), v[0]);
-          v[1] = fma(double(yo), double(yo), v[1]);
-        }
+      [&](int64_t row, int c, T yo) {
+        const int64_t i = row * VEC + c;
+        y[i] = yo;
+        v[0] = fma(double(w[i]), double(yo), v[0]);
+        v[1] = fma(double(yo), double(yo), v[1]);
       });
   double tot[2];
   if (last_block_reduce<2>(v, partials, counter, tot)) {
@@ -416,8 +410,8 @@ __global__ void __launch_bounds__(kRowThreads, kRowBlocksPerSM) kr_true_residual
     const double* __restrict__ x, const double* b, float* r) {
   bsr_rows<VEC, float, double>(
       n_brows, rp, ci, vals, [&](int64_t i) { return x[i]; },
-      [&](int64_t row, const double (&out)[VEC], int lane) {
-        if (lane < VEC) r[row * VEC + lane] = float(b[row * VEC + lane] - lane_pick<VEC, double>(out, lane));
+      [&](int64_t row, int c, double val) {
+        r[row * VEC + c] = float(b[row * VEC + c] - val);
       });
 }
 

@@ -14,8 +14,8 @@ __global__ void __launch_bounds__(kRowThreads, kRowBlocksPerSM) spmv_kernel(int6
   using AT = typename std::conditional<(sizeof(VT) == 8 || sizeof(XT) == 8), double, float>::type;
   bsr_rows<VEC, VT, AT>(
       n_brows, rp, ci, vals, [&](int64_t i) { return x[i]; },
-      [&](int64_t row, const AT (&out)[VEC], int lane) {
-        if (lane < VEC) y[row * VEC + lane] = YT(lane_pick<VEC, AT>(out, lane));
+      [&](int64_t row, int c, AT val) {
+        y[row * VEC + c] = YT(val);
       });
 }
 
@@ -27,8 +27,8 @@ __global__ void __launch_bounds__(kRowThreads, kRowBlocksPerSM) residual_mixed_k
                                                                     const double* b, double* r) {
   bsr_rows<VEC, float, double>(
       n_brows, rp, ci, vals, [&](int64_t i) { return x[i]; },
-      [&](int64_t row, const double (&out)[VEC], int lane) {
-        if (lane < VEC) r[row * VEC + lane] = b[row * VEC + lane] - lane_pick<VEC, double>(out, lane);
+      [&](int64_t row, int c, double val) {
+        r[row * VEC + c] = b[row * VEC + c] - val;
       });
 }
 

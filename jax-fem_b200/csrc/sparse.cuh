@@ -4,16 +4,30 @@
 
 namespace fem {
 
+// Compile-time tuning of the row kernels (defaults measured on B200).
+#ifndef FEM_ROW_STAGE_BYTES
+#define FEM_ROW_STAGE_BYTES 4096
+#endif
+#ifndef FEM_ROW_BLOCKS_PER_SM
+#define FEM_ROW_BLOCKS_PER_SM 4
+#endif
+#ifndef FEM_ROW_GROUP_F32
+#define FEM_ROW_GROUP_F32 4
+#endif
+#ifndef FEM_ROW_GROUP_F64
+#define FEM_ROW_GROUP_F64 2
+#endif
+
 constexpr int kRowThreads = 256;   // 8 warps per block
-constexpr int kStageBytes = 4096;  // per-warp shared-memory stage for matrix values
-constexpr int kRowBlocksPerSM = 4; // resident blocks per SM the row kernels are sized for
+constexpr int kStageBytes = FEM_ROW_STAGE_BYTES;     // per-warp shared-memory stage for matrix values
+constexpr int kRowBlocksPerSM = FEM_ROW_BLOCKS_PER_SM;  // resident blocks per SM the row kernels are sized for
 
 // Block rows per warp group: ~3.9 KB of FP32 or FP64 3x3 blocks; FP32
 // values with FP64 accumulation take 2 rows to stay within the registers of
 // kRowBlocksPerSM resident blocks.
 template <typename VT, typename AT = VT>
 __host__ __device__ constexpr int rows_per_warp() {
-  return (sizeof(VT) == 4 && sizeof(AT) == 4) ? 4 : 2;
+  return (sizeof(VT) == 4 && sizeof(AT) == 4) ? FEM_ROW_GROUP_F32 : FEM_ROW_GROUP_F64;
 }
 
 // Dynamic shared memory a bsr_rows kernel needs (one stage per warp).
@@ -125,23 +139,38 @@ __device__ __forceinline__ void bsr_rows(int64_t n_brows, const int32_t* __restr
       cp_async_wait_all();
     }
     __syncwarp();  // stage reused by the next group
+    // Transposed reduction of the NV = R*VEC row sums: each halving step
+    // trades half of the values with the partner lane, so NV sums cost
+    // P-1 + (5 - log2 P) shuffles (P = NV rounded up to a power of two)
+    // instead of 5 NV.  Value j ends in lanes j * 2^(5 - log2 P) onwards.
+    constexpr int NV = R * VEC;
+    constexpr int P = NV <= 2 ? 2 : NV <= 4 ? 4 : NV <= 8 ? 8 : NV <= 16 ? 16 : 32;
+    constexpr int L = P == 2 ? 1 : P == 4 ? 2 : P == 8 ? 3 : P == 16 ? 4 : 5;
+    static_assert(NV <= 32, "at most 32 row sums per group");
+    AT v[P];
 #pragma unroll
-    for (int r = 0; r < R; ++r) {
+    for (int j = 0; j < P; ++j) v[j] = j < NV ? acc[j / VEC][j % VEC] : AT(0);
 #pragma unroll
-      for (int i = 0; i < VEC; ++i) acc[r][i] = warp_sum(acc[r][i]);
-      if (row0 + r < n_brows) epi(row0 + r, acc[r], lane);
+    for (int step = 0; step < L; ++step) {
+      const int o = 16 >> step;
+      const bool up = (lane & o) != 0;
+      const int half = P >> (step + 1);
+#pragma unroll
+      for (int i = 0; i < half; ++i) {
+        const AT send = up ? v[i] : v[i + half];
+        const AT keep = up ? v[i + half] : v[i];
+        v[i] = keep + __shfl_xor_sync(0xffffffffu, send, o);
+      }
+    }
+    AT t = v[0];
+#pragma unroll
+    for (int o = (16 >> L); o >= 1; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
+    const int j = (lane >> (5 - L)) & (P - 1);
+    if ((lane & ((1 << (5 - L)) - 1)) == 0 && j < NV) {
+      const int64_t row = row0 + j / VEC;
+      if (row < n_brows) epi(row, j % VEC, t);
     }
   }
-}
-
-// Select out[lane] for lane < VEC (registers cannot be indexed dynamically).
-template <int VEC, typename AT>
-__device__ __forceinline__ AT lane_pick(const AT out[VEC], int lane) {
-  AT o = out[0];
-#pragma unroll
-  for (int r = 1; r < VEC; ++r)
-    if (lane == r) o = out[r];
-  return o;
 }
 
 // Opt a bsr_rows kernel into its dynamic shared memory (> 48 KB) once per
