@@ -93,6 +93,12 @@ FEM_API int64_t fem_launch_count(void);
 FEM_API int fem_bsr_pattern(const int32_t* h_cells, int64_t num_cells, int64_t num_nodes,
                     int32_t* h_row_ptr, int64_t* h_nnzb, int32_t* h_col_idx,
                     int64_t col_capacity, int32_t* h_scatter, int32_t* h_diag);
+/* Block transpose map (host, one-off): h_tmap[k] = index of block (j, i) for
+ * block k = (i, j) of a row-sorted, structurally symmetric pattern (as
+ * fem_bsr_pattern builds).  Assembly writes the lower block triangle from
+ * the upper one through it.  Part of the same pattern setup as above. */
+FEM_API int fem_bsr_transpose_map(const int32_t* h_row_ptr, const int32_t* h_col_idx, int64_t n_brows,
+                    int32_t* h_tmap);
 
 /* ---- cell assembly ------------------------------------------------------
  * Replaces Problem.newton_update / compute_residual (problem.py:439-491): the
@@ -110,6 +116,10 @@ FEM_API int fem_bsr_pattern(const int32_t* h_cells, int64_t num_cells, int64_t n
  *             system (solver.py:390-421) while staying symmetric for CG.
  * Any of d_res / d_lift / d_vals may be NULL to skip that output.  d_bc_mask
  * (uint8 per dof, 1 = Dirichlet) may be NULL (no elimination).
+ * The element tangents of every law here are symmetric: the kernel forms the
+ * 36 node pairs a <= b of each cell into the upper block triangle and a
+ * transpose pass fills the lower one, using d_transpose, the block transpose
+ * map of the pattern (fem_bsr_transpose_map; needed with d_vals).
  * d_params: host array of law parameters (see FEM_LAW_*), n_params entries.
  * d_ivar0..2: per-law internal variables (device, f64) or NULL.
  * ------------------------------------------------------------------------ */
@@ -117,7 +127,8 @@ FEM_API int fem_assemble_f64(int law, const double* h_params, int n_params, int 
                      int64_t num_cells, int64_t num_nodes, const int32_t* d_cells,
                      const double* d_points, const double* d_u,
                      const double* d_ivar0, const double* d_ivar1, const double* d_ivar2,
-                     const int32_t* d_scatter, const int32_t* d_diag, int64_t nnzb,
+                     const int32_t* d_scatter, const int32_t* d_diag,
+                     const int32_t* d_transpose, int64_t nnzb,
                      const uint8_t* d_bc_mask, const double* d_dvec,
                      double* d_res, double* d_lift, double* d_vals, void* stream);
 /* Same with the tangent computed and stored in FP32 (mixed-precision path).
@@ -127,7 +138,8 @@ FEM_API int fem_assemble_f32(int law, const double* h_params, int n_params, int 
                      int64_t num_cells, int64_t num_nodes, const int32_t* d_cells,
                      const double* d_points, const double* d_u,
                      const double* d_ivar0, const double* d_ivar1, const double* d_ivar2,
-                     const int32_t* d_scatter, const int32_t* d_diag, int64_t nnzb,
+                     const int32_t* d_scatter, const int32_t* d_diag,
+                     const int32_t* d_transpose, int64_t nnzb,
                      const uint8_t* d_bc_mask, const double* d_dvec,
                      double* d_res, double* d_lift, float* d_vals, void* stream);
 

@@ -58,8 +58,9 @@ _SIGS = {
     "fem_last_error": (_c.c_char_p, []),
     "fem_launch_count": (I64, []),
     "fem_bsr_pattern": (I32, [P, I64, I64, P, _c.POINTER(I64), P, I64, P, P]),
-    "fem_assemble_f64": (I32, [I32, DP, I32, I32, I64, I64, P, P, P, P, P, P, P, P, I64, P, P, P, P, P, P]),
-    "fem_assemble_f32": (I32, [I32, DP, I32, I32, I64, I64, P, P, P, P, P, P, P, P, I64, P, P, P, P, P, P]),
+    "fem_assemble_f64": (I32, [I32, DP, I32, I32, I64, I64, P, P, P, P, P, P, P, P, P, I64, P, P, P, P, P, P]),
+    "fem_assemble_f32": (I32, [I32, DP, I32, I32, I64, I64, P, P, P, P, P, P, P, P, P, I64, P, P, P, P, P, P]),
+    "fem_bsr_transpose_map": (I32, [P, P, I64, P]),
     "fem_j2_commit": (I32, [DP, I32, I64, P, P, P, P, P, P, P, P, P, P]),
     "fem_j2_sensitivity": (I32, [DP, I32, I64, P, P, P, P, P, P, P, P, P, P, P, P, P, P]),
     "fem_stress_divergence": (I32, [I64, P, P, P, P, P]),

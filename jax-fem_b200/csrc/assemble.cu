@@ -9,16 +9,21 @@
 // rank-structured form (see LawQuad below), so one evaluation per quadrature
 // point yields residual and tangent together.
 //
-// Work split: 8 threads per cell, 16 cells (128 threads) per block.
-//  phase 0  thread t loads node t of its cell (coords, u, Dirichlet data)
-//  phase 1  thread t = quadrature point q: geometry (J, det, grad N), grad u,
-//           the constitutive update, and per-quad tangent factors -> smem
-//  phase 2  thread t = node a: row block K_a. (two passes of 4 column nodes,
-//           36 accumulators each) and residual r_a; then scatter with
-//           Dirichlet row/column elimination into the block-CSR values via
-//           the precomputed cell->block map (no sort, no search).
-// All exchange stays inside one warp (4 cells per warp), so phases are
-// separated by __syncwarp only.
+// Work split: 12 threads per cell, 8 cells (96 threads) per block.
+//  phase 0  thread t < 8 loads node t of its cell (coords, u, Dirichlet data)
+//  phase 1  thread t < 8 = quadrature point q: geometry (J, det, grad N),
+//           grad u, the constitutive update, per-quad tangent factors -> smem
+//  phase 2  residual: thread t < 8 = node a, r_a;
+//           tangent: every element matrix here is symmetric, so only the 36
+//           node pairs a <= b are formed, three per thread.  Each pair goes
+//           to the block of the global upper triangle (row node < column
+//           node), transposed when the local order is reversed, through the
+//           precomputed cell->block map (no sort, no search), with Dirichlet
+//           row/column elimination.  The lift K d of the eliminated columns
+//           gathers per cell in shared memory.
+//  mirror   a second kernel writes each lower block as the transpose of its
+//           upper partner, so the stored matrix stays the full block CSR.
+// A cell's threads span warps, so phases are separated by __syncthreads.
 #include "common.cuh"
 
 namespace fem {
@@ -41,7 +46,9 @@ struct AsmArgs {
   double p[4];
 };
 
-constexpr int kCellsPerBlock = 16;
+constexpr int kCellsPerBlock = 8;
+constexpr int kThreadsPerCell = 12;
+constexpr int kAsmThreads = kCellsPerBlock * kThreadsPerCell;
 
 template <int LAW>
 struct LawTraits {
@@ -82,8 +89,9 @@ struct NodeLayout {
 template <int VEC, int LAW, typename T>
 __host__ __device__ constexpr size_t asm_smem_bytes() {
   return size_t(kCellsPerBlock) * padded_cell_elems<T>(8 * QuadLayout<VEC, LAW>::QF) * sizeof(T) +
-         size_t(kCellsPerBlock) * 8 * NodeLayout<VEC>::NF * sizeof(double) +
-         size_t(kCellsPerBlock) * 8 * sizeof(int);
+         size_t(kCellsPerBlock) * 8 * NodeLayout<VEC>::NF * sizeof(double) +  // node data
+         size_t(kCellsPerBlock) * 8 * VEC * sizeof(double) +                  // lift accumulators
+         size_t(kCellsPerBlock) * 8 * 2 * sizeof(int);                        // BC bits, node ids
 }
 
 // Phase 1: constitutive update at one quadrature point.
@@ -305,24 +313,32 @@ __device__ __forceinline__ void pair_block(const T* qd, int a, int b, T K[VEC][V
   }
 }
 
+// Local node pairs (a, b), a <= b, in row-major order of the upper triangle.
+__constant__ unsigned char kPairA[36] = {0, 0, 0, 0, 0, 0, 0, 0, 1, 1, 1, 1, 1, 1, 1, 2, 2, 2,
+                                         2, 2, 2, 3, 3, 3, 3, 3, 4, 4, 4, 4, 5, 5, 5, 6, 6, 7};
+__constant__ unsigned char kPairB[36] = {0, 1, 2, 3, 4, 5, 6, 7, 1, 2, 3, 4, 5, 6, 7, 2, 3, 4,
+                                         5, 6, 7, 3, 4, 5, 6, 7, 4, 5, 6, 7, 5, 6, 7, 6, 7, 7};
+
 template <int VEC, int LAW, typename T, bool WANT_K>
-__global__ void __launch_bounds__(128) assemble_kernel(const AsmArgs A) {
+__global__ void __launch_bounds__(kAsmThreads) assemble_kernel(const AsmArgs A) {
   using L = QuadLayout<VEC, LAW>;
   using N = NodeLayout<VEC>;
   constexpr int CELLF = padded_cell_elems<T>(8 * L::QF);
   extern __shared__ __align__(16) unsigned char smem[];
   T* sq = reinterpret_cast<T*>(smem);
   double* sn = reinterpret_cast<double*>(smem + size_t(kCellsPerBlock) * CELLF * sizeof(T));
-  int* sbc = reinterpret_cast<int*>(sn + kCellsPerBlock * 8 * N::NF);
+  double* slift = sn + kCellsPerBlock * 8 * N::NF;
+  int* sbc = reinterpret_cast<int*>(slift + kCellsPerBlock * 8 * VEC);
+  int* snode = sbc + kCellsPerBlock * 8;
 
-  const int cl = threadIdx.x >> 3;
-  const int t = threadIdx.x & 7;
+  const int cl = threadIdx.x / kThreadsPerCell;
+  const int t = threadIdx.x - cl * kThreadsPerCell;
   const int64_t c = int64_t(blockIdx.x) * kCellsPerBlock + cl;
   const bool valid = c < A.num_cells;
 
   // ---- phase 0: node data ----
-  const int node = valid ? A.cells[c * 8 + t] : 0;
-  {
+  if (t < 8) {
+    const int node = valid ? A.cells[c * 8 + t] : 0;
     double* nd = sn + (cl * 8 + t) * N::NF;
     if (valid) {
       nd[0] = A.points[int64_t(node) * 3 + 0];
@@ -340,17 +356,19 @@ __global__ void __launch_bounds__(128) assemble_kernel(const AsmArgs A) {
       nd[N::U + i] = valid ? A.u[dof] : 0.0;
       nd[N::D + i] = (valid && A.dvec != nullptr) ? A.dvec[dof] : 0.0;
       if (valid && A.bc != nullptr && A.bc[dof]) bits |= 1 << i;
+      slift[(cl * 8 + t) * VEC + i] = 0.0;
     }
     sbc[cl * 8 + t] = bits;
+    snode[cl * 8 + t] = node;
   }
-  __syncwarp();
+  __syncthreads();
 
   // ---- phase 1: quadrature point q = t ----
   T* cq = sq + cl * CELLF;
-  {
+  const double* nb = sn + cl * 8 * N::NF;
+  if (t < 8) {
     const int q = t;
     double X[8][3], g[8][3];
-    const double* nb = sn + cl * 8 * N::NF;
 #pragma unroll
     for (int b = 0; b < 8; ++b)
 #pragma unroll
@@ -377,15 +395,11 @@ __global__ void __launch_bounds__(128) assemble_kernel(const AsmArgs A) {
       for (int j = 0; j < 3; ++j) qd[L::G + b * 3 + j] = T(g[b][j]);
     law_quad<VEC, LAW, T>(A, valid ? c : 0, q, ug, g, jxw, qd);
   }
-  __syncwarp();
-  if (!valid) return;
+  __syncthreads();
 
-  // ---- phase 2: node a = t ----
-  const int a = t;
-  const int abits = sbc[cl * 8 + a];
-  const double* nb = sn + cl * 8 * N::NF;
-  // residual
-  if (A.res != nullptr) {
+  // ---- phase 2a: residual of node a = t ----
+  if (valid && t < 8 && A.res != nullptr) {
+    const int a = t;
     double r[VEC];
 #pragma unroll
     for (int i = 0; i < VEC; ++i) r[i] = 0.0;
@@ -397,56 +411,98 @@ __global__ void __launch_bounds__(128) assemble_kernel(const AsmArgs A) {
       for (int i = 0; i < VEC; ++i)
         r[i] += double(qd[L::P + i * 3] * g0 + qd[L::P + i * 3 + 1] * g1 + qd[L::P + i * 3 + 2] * g2);
     }
+    const int64_t node = snode[cl * 8 + a];
 #pragma unroll
-    for (int i = 0; i < VEC; ++i) atomicAdd(A.res + int64_t(node) * VEC + i, r[i]);
+    for (int i = 0; i < VEC; ++i) atomicAdd(A.res + node * VEC + i, r[i]);
   }
   if constexpr (WANT_K) {
-    if (A.vals == nullptr && A.lift == nullptr) return;
+    if (A.vals == nullptr && A.lift == nullptr) return;  // uniform over the block
     T* vals = reinterpret_cast<T*>(A.vals);
-    double lift[VEC];
-#pragma unroll
-    for (int i = 0; i < VEC; ++i) lift[i] = 0.0;
+    // ---- phase 2b: node pairs p = t, t+12, t+24 ----
+    if (valid) {
 #pragma unroll 1
-    for (int h = 0; h < 2; ++h) {
-      T K[4][VEC][VEC];
-#pragma unroll
-      for (int bb = 0; bb < 4; ++bb)
+      for (int p = t; p < 36; p += kThreadsPerCell) {
+        const int a = kPairA[p], b = kPairB[p];
+        T K[VEC][VEC];
 #pragma unroll
         for (int i = 0; i < VEC; ++i)
 #pragma unroll
-          for (int k = 0; k < VEC; ++k) K[bb][i][k] = T(0);
-#pragma unroll 1
-      for (int q = 0; q < 8; ++q) {
-        const T* qd = cq + q * L::QF;
-#pragma unroll
-        for (int bb = 0; bb < 4; ++bb) pair_block<VEC, LAW, T>(qd, a, 4 * h + bb, K[bb]);
-      }
-      const int* smap = A.scatter + c * 64 + a * 8 + 4 * h;
-#pragma unroll
-      for (int bb = 0; bb < 4; ++bb) {
-        const int b = 4 * h + bb;
-        const int bbits = sbc[cl * 8 + b];
+          for (int k = 0; k < VEC; ++k) K[i][k] = T(0);
+#pragma unroll 2
+        for (int q = 0; q < 8; ++q) pair_block<VEC, LAW, T>(cq + q * L::QF, a, b, K);
+        const int abits = sbc[cl * 8 + a], bbits = sbc[cl * 8 + b];
         if (A.lift != nullptr) {
+          // row a: K_ab d_b; row b (a != b): K_ab^T d_a
 #pragma unroll
-          for (int i = 0; i < VEC; ++i)
+          for (int i = 0; i < VEC; ++i) {
+            double la = 0.0;
 #pragma unroll
-            for (int k = 0; k < VEC; ++k) lift[i] += double(K[bb][i][k]) * nb[b * N::NF + N::D + k];
+            for (int k = 0; k < VEC; ++k) la += double(K[i][k]) * nb[b * N::NF + N::D + k];
+            atomicAdd(slift + (cl * 8 + a) * VEC + i, la);
+          }
+          if (a != b) {
+#pragma unroll
+            for (int k = 0; k < VEC; ++k) {
+              double lb = 0.0;
+#pragma unroll
+              for (int i = 0; i < VEC; ++i) lb += double(K[i][k]) * nb[a * N::NF + N::D + i];
+              atomicAdd(slift + (cl * 8 + b) * VEC + k, lb);
+            }
+          }
         }
         if (vals != nullptr) {
-          T* blk = vals + int64_t(smap[bb]) * (VEC * VEC);
+          const int na = snode[cl * 8 + a], nbn = snode[cl * 8 + b];
+          const int* smap = A.scatter + c * 64;
+          if (a == b || na < nbn) {
+            T* blk = vals + int64_t(smap[a * 8 + b]) * (VEC * VEC);
 #pragma unroll
-          for (int i = 0; i < VEC; ++i)
+            for (int i = 0; i < VEC; ++i)
+#pragma unroll
+              for (int k = 0; k < VEC; ++k)
+                if (!(((abits >> i) | (bbits >> k)) & 1)) atomicAdd(blk + i * VEC + k, K[i][k]);
+          }
+          if (a != b && na >= nbn) {  // (na == nbn only in a degenerate cell: both orientations)
+            T* blk = vals + int64_t(smap[b * 8 + a]) * (VEC * VEC);
 #pragma unroll
             for (int k = 0; k < VEC; ++k)
-              if (!(((abits >> i) | (bbits >> k)) & 1)) atomicAdd(blk + i * VEC + k, K[bb][i][k]);
+#pragma unroll
+              for (int i = 0; i < VEC; ++i)
+                if (!(((bbits >> k) | (abits >> i)) & 1)) atomicAdd(blk + k * VEC + i, K[i][k]);
+          }
         }
       }
     }
     if (A.lift != nullptr) {
+      __syncthreads();
+      if (valid && t < 8) {
+        const int abits = sbc[cl * 8 + t];
+        const int64_t node = snode[cl * 8 + t];
 #pragma unroll
-      for (int i = 0; i < VEC; ++i)
-        if (!((abits >> i) & 1)) atomicAdd(A.lift + int64_t(node) * VEC + i, lift[i]);
+        for (int i = 0; i < VEC; ++i)
+          if (!((abits >> i) & 1)) atomicAdd(A.lift + node * VEC + i, slift[(cl * 8 + t) * VEC + i]);
+      }
     }
+  }
+}
+
+// Lower-triangle blocks as transposes of their upper partners: block k of
+// row i, column j < i, takes block tmap[k] = (j, i) transposed.  In the
+// row-sorted layout tmap[k] < k holds exactly for those blocks.
+template <int VEC, typename T>
+__global__ void mirror_lower_kernel(int64_t nnzb, const int32_t* __restrict__ tmap, T* vals) {
+  for (int64_t k = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; k < nnzb;
+       k += int64_t(gridDim.x) * blockDim.x) {
+    const int64_t p = tmap[k];
+    if (p >= k) continue;
+    const T* src = vals + p * (VEC * VEC);
+    T* dst = vals + k * (VEC * VEC);
+    T v[VEC * VEC];
+#pragma unroll
+    for (int i = 0; i < VEC * VEC; ++i) v[i] = src[i];
+#pragma unroll
+    for (int i = 0; i < VEC; ++i)
+#pragma unroll
+      for (int j = 0; j < VEC; ++j) dst[i * VEC + j] = v[j * VEC + i];
   }
 }
 
@@ -472,7 +528,7 @@ int launch_law(const AsmArgs& A, bool want_k, cudaStream_t st) {
       FEM_CUDA_TRY(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sm)));
       attr = true;
     }
-    k<<<grid, 128, sm, st>>>(A);
+    k<<<grid, kAsmThreads, sm, st>>>(A);
   } else {
     auto k = assemble_kernel<VEC, LAW, T, false>;
     static bool attr = false;
@@ -480,7 +536,7 @@ int launch_law(const AsmArgs& A, bool want_k, cudaStream_t st) {
       FEM_CUDA_TRY(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sm)));
       attr = true;
     }
-    k<<<grid, 128, sm, st>>>(A);
+    k<<<grid, kAsmThreads, sm, st>>>(A);
   }
   FEM_LAUNCH_CHECK();
   return FEM_OK;
@@ -490,9 +546,9 @@ template <typename T>
 int assemble_impl(int law, const double* h_params, int n_params, int vec, int64_t num_cells,
                   int64_t num_nodes, const int32_t* d_cells, const double* d_points,
                   const double* d_u, const double* iv0, const double* iv1, const double* iv2,
-                  const int32_t* d_scatter, const int32_t* d_diag, int64_t nnzb,
-                  const uint8_t* d_bc, const double* d_dvec, double* d_res, double* d_lift,
-                  T* d_vals, void* stream) {
+                  const int32_t* d_scatter, const int32_t* d_diag, const int32_t* d_transpose,
+                  int64_t nnzb, const uint8_t* d_bc, const double* d_dvec,
+                  double* d_res, double* d_lift, T* d_vals, void* stream) {
   FEM_CHECK_ARG(num_cells >= 0 && num_nodes >= 0, "negative sizes");
   FEM_CHECK_ARG(vec == 1 || vec == 3, "vec must be 1 or 3 (got %d)", vec);
   FEM_CHECK_ARG(law == FEM_LAW_LAPLACE || vec == 3, "law %d needs vec=3", law);
@@ -503,6 +559,8 @@ int assemble_impl(int law, const double* h_params, int n_params, int vec, int64_
   FEM_CHECK_ARG(law != FEM_LAW_SIMP || iv0 != nullptr, "SIMP needs theta (ivar0)");
   FEM_CHECK_ARG(law != FEM_LAW_J2 || (iv0 && iv1 && iv2), "J2 needs sigma_old, eps_old, alpha_old");
   FEM_CHECK_ARG(d_vals == nullptr || (d_scatter != nullptr && nnzb > 0), "tangent needs scatter map");
+  FEM_CHECK_ARG(d_vals == nullptr || d_transpose != nullptr,
+                "tangent needs the block transpose map for its lower triangle");
   FEM_CHECK_ARG(d_vals == nullptr || d_bc == nullptr || d_diag != nullptr, "BC elimination needs diag");
   FEM_CHECK_ARG(d_lift == nullptr || (d_dvec != nullptr && d_scatter != nullptr), "lift needs dvec");
   cudaStream_t st = as_stream(stream);
@@ -540,6 +598,15 @@ int assemble_impl(int law, const double* h_params, int n_params, int vec, int64_
     }
   }
   if (rc != FEM_OK) return rc;
+  if (d_vals != nullptr) {
+    const int64_t blocks = (nnzb + 255) / 256;
+    const unsigned grid = unsigned(blocks < int64_t(num_sms()) * 16 ? blocks : int64_t(num_sms()) * 16);
+    if (vec == 3)
+      mirror_lower_kernel<3, T><<<grid, 256, 0, st>>>(nnzb, d_transpose, d_vals);
+    else
+      mirror_lower_kernel<1, T><<<grid, 256, 0, st>>>(nnzb, d_transpose, d_vals);
+    FEM_LAUNCH_CHECK();
+  }
   if (d_vals != nullptr && d_bc != nullptr && ndofs > 0) {
     bc_diag_kernel<T><<<unsigned((ndofs + 255) / 256), 256, 0, st>>>(vec, ndofs, d_bc, d_diag, d_vals);
     FEM_LAUNCH_CHECK();
@@ -554,22 +621,26 @@ extern "C" int fem_assemble_f64(int law, const double* h_params, int n_params, i
                                 int64_t num_cells, int64_t num_nodes, const int32_t* d_cells,
                                 const double* d_points, const double* d_u, const double* d_ivar0,
                                 const double* d_ivar1, const double* d_ivar2,
-                                const int32_t* d_scatter, const int32_t* d_diag, int64_t nnzb,
+                                const int32_t* d_scatter, const int32_t* d_diag,
+                                const int32_t* d_transpose, int64_t nnzb,
                                 const uint8_t* d_bc_mask, const double* d_dvec, double* d_res,
                                 double* d_lift, double* d_vals, void* stream) {
   return fem::assemble_impl<double>(law, h_params, n_params, vec, num_cells, num_nodes, d_cells,
                                     d_points, d_u, d_ivar0, d_ivar1, d_ivar2, d_scatter, d_diag,
-                                    nnzb, d_bc_mask, d_dvec, d_res, d_lift, d_vals, stream);
+                                    d_transpose, nnzb, d_bc_mask, d_dvec, d_res, d_lift,
+                                    d_vals, stream);
 }
 
 extern "C" int fem_assemble_f32(int law, const double* h_params, int n_params, int vec,
                                 int64_t num_cells, int64_t num_nodes, const int32_t* d_cells,
                                 const double* d_points, const double* d_u, const double* d_ivar0,
                                 const double* d_ivar1, const double* d_ivar2,
-                                const int32_t* d_scatter, const int32_t* d_diag, int64_t nnzb,
+                                const int32_t* d_scatter, const int32_t* d_diag,
+                                const int32_t* d_transpose, int64_t nnzb,
                                 const uint8_t* d_bc_mask, const double* d_dvec, double* d_res,
                                 double* d_lift, float* d_vals, void* stream) {
   return fem::assemble_impl<float>(law, h_params, n_params, vec, num_cells, num_nodes, d_cells,
                                    d_points, d_u, d_ivar0, d_ivar1, d_ivar2, d_scatter, d_diag,
-                                   nnzb, d_bc_mask, d_dvec, d_res, d_lift, d_vals, stream);
+                                   d_transpose, nnzb, d_bc_mask, d_dvec, d_res, d_lift,
+                                   d_vals, stream);
 }

@@ -123,3 +123,33 @@ extern "C" int fem_bsr_pattern(const int32_t* h_cells, int64_t num_cells, int64_
   }
   return FEM_OK;
 }
+
+// Block transpose map of a block-CSR pattern: h_tmap[k] = index of block
+// (j, i) for block k = (i, j).  Used by assembly to write the lower block
+// triangle from the upper one.  Fails if the pattern is not structurally
+// symmetric or a row's columns are not sorted.
+extern "C" int fem_bsr_transpose_map(const int32_t* h_row_ptr, const int32_t* h_col_idx, int64_t n_brows,
+                                     int32_t* h_tmap) {
+  if (h_row_ptr == nullptr || h_col_idx == nullptr || h_tmap == nullptr || n_brows < 0) {
+    fem::set_error("fem_bsr_transpose_map: NULL pointer or negative size");
+    return FEM_ERR_ARG;
+  }
+  for (int64_t i = 0; i < n_brows; ++i) {
+    for (int32_t k = h_row_ptr[i]; k < h_row_ptr[i + 1]; ++k) {
+      const int32_t j = h_col_idx[k];
+      if (j < 0 || j >= n_brows || (k > h_row_ptr[i] && h_col_idx[k - 1] >= j)) {
+        fem::set_error("fem_bsr_transpose_map: row %lld: columns not sorted or out of range", (long long)i);
+        return FEM_ERR_ARG;
+      }
+      const int32_t* b = h_col_idx + h_row_ptr[j];
+      const int32_t* e = h_col_idx + h_row_ptr[j + 1];
+      const int32_t* f = std::lower_bound(b, e, int32_t(i));
+      if (f == e || *f != int32_t(i)) {
+        fem::set_error("fem_bsr_transpose_map: block (%lld, %d) has no transpose partner", (long long)i, j);
+        return FEM_ERR_ARG;
+      }
+      h_tmap[k] = int32_t(f - h_col_idx);
+    }
+  }
+  return FEM_OK;
+}

@@ -73,6 +73,9 @@ class DeviceMesh:
         nat.check(lib.fem_bsr_pattern(cells.ctypes.data, C, N, row_ptr.ctypes.data, nnzb,
                                       col.ctypes.data, col.size, scatter.ctypes.data, diag.ctypes.data),
                   "bsr_pattern(fill)")
+        tmap = np.zeros(max(1, nnzb.value), dtype=np.int32)
+        nat.check(lib.fem_bsr_transpose_map(row_ptr.ctypes.data, col.ctypes.data, N, tmap.ctypes.data),
+                  "bsr_transpose_map")
         self.vec, self.num_cells, self.num_nodes, self.nnzb = vec, C, N, int(nnzb.value)
         self.ndofs = N * vec
         self.device = device
@@ -82,6 +85,7 @@ class DeviceMesh:
         self.col_idx = torch.from_numpy(col[: self.nnzb]).to(device)
         self.scatter = torch.from_numpy(scatter[:C]).to(device).contiguous()
         self.diag = torch.from_numpy(diag[:N]).to(device)
+        self.transpose = torch.from_numpy(tmap[: self.nnzb]).to(device)
 
     def new_matrix(self, dtype):
         vals = torch.zeros(self.nnzb * self.vec * self.vec, dtype=dtype, device=self.device)
@@ -248,7 +252,7 @@ class Problem:
         fn = nat.lib().fem_assemble_f32 if fp32 else nat.lib().fem_assemble_f64
         nat.check(fn(law.law_id, pr, n, self.vec, dv.num_cells, dv.num_nodes, nat.ptr(dv.cells),
                      nat.ptr(dv.points), nat.ptr(dofs), nat.ptr(iv[0]), nat.ptr(iv[1]), nat.ptr(iv[2]),
-                     nat.ptr(dv.scatter), nat.ptr(dv.diag), dv.nnzb,
+                     nat.ptr(dv.scatter), nat.ptr(dv.diag), nat.ptr(dv.transpose), dv.nnzb,
                      nat.ptr(mask) if bc else None, nat.ptr(dvec), nat.ptr(res), nat.ptr(lift),
                      nat.ptr(vals), nat.stream_ptr()), "assemble")
 

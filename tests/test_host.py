@@ -66,6 +66,29 @@ def test_pattern_matches_node_adjacency(pkg, shape):
     assert nnzb == (3 * Nx + 1) * (3 * Ny + 1) * (3 * Nz + 1)  # prod(3 n_i - 2) over node counts
 
 
+@pytest.mark.parametrize("shape", [(1, 1, 1), (3, 2, 4)])
+def test_transpose_map_pairs_blocks(pkg, shape):
+    """tmap[k] is the block (j, i) of block k = (i, j); it is an involution,
+    and tmap[k] < k exactly for the lower-triangle blocks."""
+    lib = pkg._native.load()
+    pts, cells = fo.box_mesh(*shape, 1.0, 1.0, 1.0)
+    N = len(pts)
+    rp, col, _, _, nnzb = _pattern(pkg, cells, N)
+    tmap = np.full(nnzb, -7, dtype=np.int32)
+    assert lib.fem_bsr_transpose_map(rp.ctypes.data, col.ctypes.data, N, tmap.ctypes.data) == 0
+    row = np.searchsorted(rp, np.arange(nnzb), side="right") - 1
+    np.testing.assert_array_equal(col[tmap], row)
+    np.testing.assert_array_equal(row[tmap], col)
+    np.testing.assert_array_equal(tmap[tmap], np.arange(nnzb))
+    np.testing.assert_array_equal(tmap < np.arange(nnzb), row > col)
+    # a pattern without the partner of block (0, 1) is rejected
+    rp2 = np.array([0, 2, 3], dtype=np.int32)
+    col2 = np.array([0, 1, 1], dtype=np.int32)
+    t2 = np.zeros(3, dtype=np.int32)
+    assert lib.fem_bsr_transpose_map(rp2.ctypes.data, col2.ctypes.data, 2, t2.ctypes.data) == -1
+    assert b"partner" in lib.fem_last_error()
+
+
 def test_pattern_rejects_bad_node(pkg):
     lib = pkg._native.load()
     cells = np.arange(8, dtype=np.int32).reshape(1, 8)
