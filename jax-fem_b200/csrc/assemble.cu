@@ -487,22 +487,21 @@ __global__ void __launch_bounds__(kAsmThreads) assemble_kernel(const AsmArgs A) 
 
 // Lower-triangle blocks as transposes of their upper partners: block k of
 // row i, column j < i, takes block tmap[k] = (j, i) transposed.  In the
-// row-sorted layout tmap[k] < k holds exactly for those blocks.
+// row-sorted layout tmap[k] < k holds exactly for those blocks.  One thread
+// per value word: consecutive threads store consecutive words (coalesced),
+// and the VEC*VEC threads of a block read one partner block.
 template <int VEC, typename T>
 __global__ void mirror_lower_kernel(int64_t nnzb, const int32_t* __restrict__ tmap, T* vals) {
-  for (int64_t k = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; k < nnzb;
-       k += int64_t(gridDim.x) * blockDim.x) {
+  constexpr int VV = VEC * VEC;
+  const int64_t nwords = nnzb * VV;
+  for (int64_t w = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; w < nwords;
+       w += int64_t(gridDim.x) * blockDim.x) {
+    const int64_t k = w / VV;
+    const int e = int(w - k * VV);
     const int64_t p = tmap[k];
     if (p >= k) continue;
-    const T* src = vals + p * (VEC * VEC);
-    T* dst = vals + k * (VEC * VEC);
-    T v[VEC * VEC];
-#pragma unroll
-    for (int i = 0; i < VEC * VEC; ++i) v[i] = src[i];
-#pragma unroll
-    for (int i = 0; i < VEC; ++i)
-#pragma unroll
-      for (int j = 0; j < VEC; ++j) dst[i * VEC + j] = v[j * VEC + i];
+    const int r = e / VEC, c = e - (e / VEC) * VEC;
+    vals[w] = vals[p * VV + c * VEC + r];
   }
 }
 
@@ -599,7 +598,7 @@ int assemble_impl(int law, const double* h_params, int n_params, int vec, int64_
   }
   if (rc != FEM_OK) return rc;
   if (d_vals != nullptr) {
-    const int64_t blocks = (nnzb + 255) / 256;
+    const int64_t blocks = (nnzb * vec * vec + 255) / 256;
     const unsigned grid = unsigned(blocks < int64_t(num_sms()) * 16 ? blocks : int64_t(num_sms()) * 16);
     if (vec == 3)
       mirror_lower_kernel<3, T><<<grid, 256, 0, st>>>(nnzb, d_transpose, d_vals);
