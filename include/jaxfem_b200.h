@@ -298,6 +298,74 @@ FEM_API int fem_transpose_bf16(const void* d_in, void* d_out, int64_t rows, int 
 FEM_API int fem_conv3d_flip_weights_bf16(const void* d_w, void* d_wt, int Cout, int Cin, void* stream);
 FEM_API int fem_relu_mask_bf16(const void* d_dy, const void* d_y, void* d_dz, int64_t n, void* stream);
 
+/* ---- geometric multigrid on box lattices ---------------------------------
+ * Replaces the reference's optional AMGX preconditioner path
+ * (solver.py:136-259) for meshes that are tensor lattices numbered as
+ * box_mesh numbers them (generate_mesh.py:151-189): node (i, j, k) =
+ * (i*ny + j)*nz + k with nx, ny, nz nodes per direction.  Levels coarsen 2:1
+ * per direction (a last odd interval stays 1 fine cell wide); prolongation
+ * is trilinear interpolation on the coarse lattice; coarse operators are
+ * Galerkin products P^T A P of the Dirichlet-eliminated fine operator, so
+ * they stay symmetric positive definite.  The smoother is Chebyshev
+ * iteration on the Jacobi-scaled operator over [lmax/ratio, lmax], lmax a
+ * Gershgorin bound; pre- and post-smoothing are the same polynomial and the
+ * coarsest level takes a longer one, so a V-cycle is a fixed symmetric
+ * operator and can precondition CG.
+ *
+ * A level describes its lattice, pattern, values and work vectors (device
+ * pointers, each n_brows*vec entries of the call's type).  stencil[(n,27)]
+ * holds the block index of neighbour (dx,dy,dz) at (dx+1)*9 + (dy+1)*3 +
+ * (dz+1), or -1.  Levels >= 1 also hold, per direction d, cpos (the fine
+ * lattice index of each coarse node), ilo (for each node of the finer level,
+ * the coarse node at or below it) and whi (the interpolation weight of the
+ * coarse node ilo+1), all concatenated over x, y, z. */
+typedef struct FemMGLevel {
+  int64_t nodes[3];
+  int64_t n_brows;
+  const int32_t* row_ptr;
+  const int32_t* col_idx;
+  const int32_t* stencil;
+  void* vals;
+  void* dinv;
+  void* x;
+  void* b;
+  void* r;
+  void* d0;
+  void* d1;
+  const int32_t* cpos;
+  const int32_t* ilo;
+  const double* whi;
+  double lmax;
+} FemMGLevel;
+
+/* Setup (once per operator): coarse values by Galerkin products, the Jacobi
+ * scaling and lmax of every level (written into levels[l].lmax; the call
+ * synchronizes `stream` to read them).  _f32: with d_fine_f64 non-NULL,
+ * level 0's values are first rounded from that FP64 operator. */
+FEM_API int fem_mg_setup_f64(int vec, int nlevels, FemMGLevel* levels, void* stream);
+FEM_API int fem_mg_setup_f32(int vec, int nlevels, FemMGLevel* levels, const double* d_fine_f64,
+                             void* stream);
+/* z = V(rhs): one V-cycle with nu Chebyshev steps before and after on each
+ * level and coarse_steps on the coarsest; ratio sets the smoothed interval
+ * [lmax/ratio, lmax].  Launches only (no synchronization). */
+FEM_API int fem_mg_vcycle_f64(int vec, int nlevels, const FemMGLevel* levels, int nu, int coarse_steps,
+                              double ratio, const double* d_rhs, double* d_z, void* stream);
+FEM_API int fem_mg_vcycle_f32(int vec, int nlevels, const FemMGLevel* levels, int nu, int coarse_steps,
+                              double ratio, const float* d_rhs, float* d_z, void* stream);
+/* CG on the FP64 operator (row_ptr, col_idx, vals) preconditioned by one
+ * V-cycle per iteration, the linear solve of solver.py:63-92 / 261-284 with
+ * a multigrid preconditioner.  levels_fp32 != 0: the hierarchy is FP32 (the
+ * V-cycle runs in FP32 on a rounded copy of r; CG, its vectors and
+ * reductions stay FP64, so the attainable accuracy is FP64's).  x holds the
+ * initial guess.  Stops when ||b - A x|| <= max(rtol ||b||, atol) on the
+ * recursive residual, then reports the true one in *h_relres. */
+FEM_API size_t fem_mg_pcg_workspace_bytes(int vec, int64_t n_brows);
+FEM_API int fem_mg_pcg_solve(int vec, int64_t n_brows, const int32_t* d_row_ptr, const int32_t* d_col_idx,
+                             const double* d_vals, const double* d_b, double* d_x, double rtol, double atol,
+                             int maxiter, int check_every, int nlevels, const FemMGLevel* levels,
+                             int levels_fp32, int nu, int coarse_steps, double ratio, void* d_work,
+                             size_t work_bytes, int* h_iters, double* h_relres, void* stream);
+
 /* ---- dot product that allocates nothing ---------------------------------
  * No counterpart in the reference.  For callers that cannot allocate device
  * memory: code whose device memory is owned by a host framework's pool that

@@ -24,6 +24,17 @@ FEM_ERR_CAPACITY = -6
 LAW_LAPLACE, LAW_LINEAR, LAW_SIMP, LAW_NEO_HOOKEAN, LAW_J2 = 0, 1, 2, 3, 4
 KRYLOV_CG, KRYLOV_BICGSTAB = 0, 1
 PRECOND_NONE, PRECOND_JACOBI, PRECOND_BLOCK_JACOBI = 0, 1, 2
+PRECOND_GMG = 100  # host-side selector: CG preconditioned by a multigrid V-cycle (multigrid.py)
+
+
+class FemMGLevel(ctypes.Structure):
+    """Mirror of ``FemMGLevel`` in include/jaxfem_b200.h."""
+    _fields_ = [("nodes", ctypes.c_int64 * 3), ("n_brows", ctypes.c_int64),
+                ("row_ptr", ctypes.c_void_p), ("col_idx", ctypes.c_void_p), ("stencil", ctypes.c_void_p),
+                ("vals", ctypes.c_void_p), ("dinv", ctypes.c_void_p), ("x", ctypes.c_void_p),
+                ("b", ctypes.c_void_p), ("r", ctypes.c_void_p), ("d0", ctypes.c_void_p), ("d1", ctypes.c_void_p),
+                ("cpos", ctypes.c_void_p), ("ilo", ctypes.c_void_p), ("whi", ctypes.c_void_p),
+                ("lmax", ctypes.c_double)]
 
 _STATUS_NAMES = {
     FEM_ERR_ARG: "invalid argument",
@@ -64,6 +75,13 @@ _SIGS = {
     "fem_j2_commit": (I32, [DP, I32, I64, P, P, P, P, P, P, P, P, P, P]),
     "fem_j2_sensitivity": (I32, [DP, I32, I64, P, P, P, P, P, P, P, P, P, P, P, P, P, P]),
     "fem_stress_divergence": (I32, [I64, P, P, P, P, P]),
+    "fem_mg_setup_f64": (I32, [I32, I32, P, P]),
+    "fem_mg_setup_f32": (I32, [I32, I32, P, P, P]),
+    "fem_mg_vcycle_f64": (I32, [I32, I32, P, I32, I32, F64, P, P, P]),
+    "fem_mg_vcycle_f32": (I32, [I32, I32, P, I32, I32, F64, P, P, P]),
+    "fem_mg_pcg_workspace_bytes": (SZ, [I32, I64]),
+    "fem_mg_pcg_solve": (I32, [I32, I64, P, P, P, P, P, F64, F64, I32, I32, I32, P, I32, I32, I32, F64, P, SZ, IP,
+                               DP, P]),
     "fem_param_vjp_f64": (I32, [I32, DP, I32, I64, P, P, P, P, P, P, P]),
     "fem_bsr_spmv_f64": (I32, [I32, I64, P, P, P, P, P, P]),
     "fem_bsr_spmv_f32": (I32, [I32, I64, P, P, P, P, P, P]),

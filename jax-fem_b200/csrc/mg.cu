@@ -1,0 +1,708 @@
+// Geometric multigrid for box-lattice meshes: Galerkin coarse operators,
+// trilinear transfer, Chebyshev-Jacobi smoothing, V-cycles and a
+// V-cycle-preconditioned CG.  Replaces the reference's optional AMGX path
+// (solver.py:136-259) on the meshes box_mesh builds (generate_mesh.py:151-189).
+//
+// Lattice: node (i, j, k) = (i*ny + j)*nz + k, nx, ny, nz nodes per direction.
+// A coarse level keeps every second node per direction (and the last node);
+// fine node i of a direction lies between coarse nodes ilo[i] and ilo[i]+1
+// with weight whi[i] on the upper one, so prolongation P is trilinear
+// interpolation and restriction is P^T.  Coarse operators are P^T A P,
+// computed per coarse block from the fine blocks (one lane per coarse block:
+// fixed summation order, no atomics).
+//
+// Smoothing: Chebyshev iteration on D^-1 A over [lmax/ratio, lmax] with
+// lmax the Gershgorin bound of D^-1 A (D = the diagonal).  Each step is one
+// SpMV with its vector updates fused into the row epilogue.  Pre- and
+// post-smoothing apply the same polynomial, the coarsest level a longer one,
+// so a V-cycle is a fixed symmetric positive operator (a CG preconditioner).
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "sparse.cuh"
+
+namespace fem {
+namespace {
+
+struct Lat {
+  int64_t n[3];
+};
+
+inline Lat lat_of(const FemMGLevel& L) { return Lat{{L.nodes[0], L.nodes[1], L.nodes[2]}}; }
+
+// 1-D interpolation weight of coarse node I at fine node i
+__device__ __forceinline__ double w1(const int32_t* ilo, const double* whi, int64_t i, int64_t I) {
+  const int64_t lo = ilo[i];
+  if (lo == I) return 1.0 - whi[i];
+  if (lo + 1 == I) return whi[i];
+  return 0.0;
+}
+
+// Fine lattice indices that interpolate from coarse node I along one
+// direction: strictly between the neighbouring coarse nodes.
+__device__ __forceinline__ void fine_range(const int32_t* cpos, int64_t I, int64_t nc, int64_t nf, int64_t* lo,
+                                           int64_t* hi) {
+  *lo = I > 0 ? int64_t(cpos[I - 1]) + 1 : 0;
+  *hi = I < nc - 1 ? int64_t(cpos[I + 1]) - 1 : nf - 1;
+}
+
+// ---- Galerkin coarse operator: one warp per coarse node, lane = slot --------
+template <int VEC, typename T>
+__global__ void rap_kernel(Lat F, const int32_t* __restrict__ fst, const T* __restrict__ fv, Lat C,
+                           const int32_t* __restrict__ cst, T* cv, const int32_t* cpos, const int32_t* ilo,
+                           const double* whi) {
+  constexpr int VV = VEC * VEC;
+  const int lane = threadIdx.x & 31;
+  const int64_t warp = (int64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+  const int64_t nwarps = (int64_t(gridDim.x) * blockDim.x) >> 5;
+  const int64_t Nc = C.n[0] * C.n[1] * C.n[2];
+  const int32_t* cp[3] = {cpos, cpos + C.n[0], cpos + C.n[0] + C.n[1]};
+  const int32_t* il[3] = {ilo, ilo + F.n[0], ilo + F.n[0] + F.n[1]};
+  const double* wh[3] = {whi, whi + F.n[0], whi + F.n[0] + F.n[1]};
+  if (lane >= 27) return;  // no warp-wide operations below
+  for (int64_t I = warp; I < Nc; I += nwarps) {
+    const int64_t Ic[3] = {I / (C.n[1] * C.n[2]), (I / C.n[2]) % C.n[1], I % C.n[2]};
+    const int s[3] = {lane / 9 - 1, (lane / 3) % 3 - 1, lane % 3 - 1};
+    int64_t J[3];
+    bool inside = true;
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      J[d] = Ic[d] + s[d];
+      inside = inside && J[d] >= 0 && J[d] < C.n[d];
+    }
+    if (!inside) continue;
+    const int32_t cblk = cst[I * 27 + lane];
+    if (cblk < 0) continue;
+    int64_t lo[3], hi[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) fine_range(cp[d], Ic[d], C.n[d], F.n[d], &lo[d], &hi[d]);
+    double acc[VV];
+#pragma unroll
+    for (int e = 0; e < VV; ++e) acc[e] = 0.0;
+    for (int64_t ix = lo[0]; ix <= hi[0]; ++ix) {
+      const double wx = w1(il[0], wh[0], ix, Ic[0]);
+      if (wx == 0.0) continue;
+      for (int64_t iy = lo[1]; iy <= hi[1]; ++iy) {
+        const double wy = w1(il[1], wh[1], iy, Ic[1]);
+        if (wy == 0.0) continue;
+        for (int64_t iz = lo[2]; iz <= hi[2]; ++iz) {
+          const double wz = w1(il[2], wh[2], iz, Ic[2]);
+          if (wz == 0.0) continue;
+          const double wi = wx * wy * wz;
+          const int64_t i = (ix * F.n[1] + iy) * F.n[2] + iz;
+          for (int o = 0; o < 27; ++o) {
+            const int64_t jx = ix + o / 9 - 1, jy = iy + (o / 3) % 3 - 1, jz = iz + o % 3 - 1;
+            if (jx < 0 || jx >= F.n[0] || jy < 0 || jy >= F.n[1] || jz < 0 || jz >= F.n[2]) continue;
+            const double wj = w1(il[0], wh[0], jx, J[0]) * w1(il[1], wh[1], jy, J[1]) * w1(il[2], wh[2], jz, J[2]);
+            if (wj == 0.0) continue;
+            const int32_t blk = fst[i * 27 + o];
+            if (blk < 0) continue;
+            const double ww = wi * wj;
+            const T* a = fv + int64_t(blk) * VV;
+#pragma unroll
+            for (int e = 0; e < VV; ++e) acc[e] = fma(ww, double(a[e]), acc[e]);
+          }
+        }
+      }
+    }
+#pragma unroll
+    for (int e = 0; e < VV; ++e) cv[int64_t(cblk) * VV + e] = T(acc[e]);
+  }
+}
+
+// ---- transfers ---------------------------------------------------------------
+// bc[I] = sum_i w_iI rf[i]   (P^T, one thread per coarse node)
+template <int VEC, typename T>
+__global__ void restrict_kernel(Lat F, Lat C, const int32_t* cpos, const int32_t* ilo, const double* whi,
+                                const T* __restrict__ rf, T* bc) {
+  const int32_t* cp[3] = {cpos, cpos + C.n[0], cpos + C.n[0] + C.n[1]};
+  const int32_t* il[3] = {ilo, ilo + F.n[0], ilo + F.n[0] + F.n[1]};
+  const double* wh[3] = {whi, whi + F.n[0], whi + F.n[0] + F.n[1]};
+  const int64_t Nc = C.n[0] * C.n[1] * C.n[2];
+  for (int64_t I = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; I < Nc; I += int64_t(gridDim.x) * blockDim.x) {
+    const int64_t Ic[3] = {I / (C.n[1] * C.n[2]), (I / C.n[2]) % C.n[1], I % C.n[2]};
+    int64_t lo[3], hi[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) fine_range(cp[d], Ic[d], C.n[d], F.n[d], &lo[d], &hi[d]);
+    double acc[VEC];
+#pragma unroll
+    for (int c = 0; c < VEC; ++c) acc[c] = 0.0;
+    for (int64_t ix = lo[0]; ix <= hi[0]; ++ix) {
+      const double wx = w1(il[0], wh[0], ix, Ic[0]);
+      if (wx == 0.0) continue;
+      for (int64_t iy = lo[1]; iy <= hi[1]; ++iy) {
+        const double wy = w1(il[1], wh[1], iy, Ic[1]);
+        if (wy == 0.0) continue;
+        for (int64_t iz = lo[2]; iz <= hi[2]; ++iz) {
+          const double w = wx * wy * w1(il[2], wh[2], iz, Ic[2]);
+          if (w == 0.0) continue;
+          const int64_t i = (ix * F.n[1] + iy) * F.n[2] + iz;
+#pragma unroll
+          for (int c = 0; c < VEC; ++c) acc[c] = fma(w, double(rf[i * VEC + c]), acc[c]);
+        }
+      }
+    }
+#pragma unroll
+    for (int c = 0; c < VEC; ++c) bc[I * VEC + c] = T(acc[c]);
+  }
+}
+
+// xf[i] += sum_J w_iJ ec[J]   (P, one thread per fine node)
+template <int VEC, typename T>
+__global__ void prolong_add_kernel(Lat F, Lat C, const int32_t* ilo, const double* whi, const T* __restrict__ ec,
+                                   T* xf) {
+  const int32_t* il[3] = {ilo, ilo + F.n[0], ilo + F.n[0] + F.n[1]};
+  const double* wh[3] = {whi, whi + F.n[0], whi + F.n[0] + F.n[1]};
+  const int64_t Nf = F.n[0] * F.n[1] * F.n[2];
+  for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < Nf; i += int64_t(gridDim.x) * blockDim.x) {
+    const int64_t ii[3] = {i / (F.n[1] * F.n[2]), (i / F.n[2]) % F.n[1], i % F.n[2]};
+    int64_t lo[3];
+    double wup[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      lo[d] = il[d][ii[d]];
+      wup[d] = wh[d][ii[d]];
+    }
+    double acc[VEC];
+#pragma unroll
+    for (int c = 0; c < VEC; ++c) acc[c] = 0.0;
+#pragma unroll
+    for (int m = 0; m < 8; ++m) {
+      const int bx = m >> 2, by = (m >> 1) & 1, bz = m & 1;
+      const double w = (bx ? wup[0] : 1.0 - wup[0]) * (by ? wup[1] : 1.0 - wup[1]) * (bz ? wup[2] : 1.0 - wup[2]);
+      if (w == 0.0) continue;
+      const int64_t J = ((lo[0] + bx) * C.n[1] + (lo[1] + by)) * C.n[2] + (lo[2] + bz);
+#pragma unroll
+      for (int c = 0; c < VEC; ++c) acc[c] = fma(w, double(ec[J * VEC + c]), acc[c]);
+    }
+#pragma unroll
+    for (int c = 0; c < VEC; ++c) xf[i * VEC + c] = T(double(xf[i * VEC + c]) + acc[c]);
+  }
+}
+
+// ---- Jacobi scaling and the Gershgorin bound of D^-1 A ----------------------
+template <int VEC, typename T>
+__global__ void jacobi_setup_kernel(int64_t n_brows, const int32_t* __restrict__ st, const T* __restrict__ vals,
+                                    T* dinv, unsigned long long* lmax_bits) {
+  constexpr int VV = VEC * VEC;
+  double local = 0.0;
+  for (int64_t dof = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; dof < n_brows * VEC;
+       dof += int64_t(gridDim.x) * blockDim.x) {
+    const int64_t row = dof / VEC;
+    const int c = int(dof - row * VEC);
+    const int32_t db = st[row * 27 + 13];
+    const double aii = db >= 0 ? double(vals[int64_t(db) * VV + c * VEC + c]) : 0.0;
+    double rs = 0.0;
+    for (int o = 0; o < 27; ++o) {
+      const int32_t blk = st[row * 27 + o];
+      if (blk < 0) continue;
+#pragma unroll
+      for (int k = 0; k < VEC; ++k) rs += fabs(double(vals[int64_t(blk) * VV + c * VEC + k]));
+    }
+    const double ad = fabs(aii);
+    dinv[dof] = T(ad > 0.0 ? 1.0 / aii : 0.0);
+    if (ad > 0.0) local = fmax(local, rs / ad);
+  }
+  local = fmax(local, __shfl_xor_sync(0xffffffffu, local, 16));
+  local = fmax(local, __shfl_xor_sync(0xffffffffu, local, 8));
+  local = fmax(local, __shfl_xor_sync(0xffffffffu, local, 4));
+  local = fmax(local, __shfl_xor_sync(0xffffffffu, local, 2));
+  local = fmax(local, __shfl_xor_sync(0xffffffffu, local, 1));
+  // non-negative doubles order like their bit patterns
+  if ((threadIdx.x & 31) == 0) atomicMax(lmax_bits, static_cast<unsigned long long>(__double_as_longlong(local)));
+}
+
+template <typename T>
+__global__ void cast_kernel(int64_t n, const double* __restrict__ a, T* b) {
+  for (int64_t k = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; k < n; k += int64_t(gridDim.x) * blockDim.x)
+    b[k] = T(a[k]);
+}
+template <typename T>
+__global__ void widen_kernel(int64_t n, const T* __restrict__ a, double* b) {
+  for (int64_t k = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; k < n; k += int64_t(gridDim.x) * blockDim.x)
+    b[k] = double(a[k]);
+}
+
+// ---- Chebyshev smoothing ------------------------------------------------------
+// First step: (zero start) r = b, x = d; otherwise x += d; d = D^-1 r / theta.
+template <typename T>
+__global__ void cheb_first_kernel(int64_t n, const T* __restrict__ dinv, const T* b, T* r, T* d, T* x,
+                                  double inv_theta, int zero_start) {
+  for (int64_t k = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; k < n; k += int64_t(gridDim.x) * blockDim.x) {
+    const T rk = zero_start ? b[k] : r[k];
+    if (zero_start) r[k] = rk;
+    const T dk = T(double(dinv[k]) * double(rk) * inv_theta);
+    d[k] = dk;
+    x[k] = zero_start ? dk : T(x[k] + dk);
+  }
+}
+
+// q = A d_old; r -= q; d_new = a d_old + c D^-1 r; x += d_new
+template <int VEC, typename T>
+__global__ void __launch_bounds__(kRowThreads, kRowBlocksPerSM)
+    cheb_step_kernel(int64_t n_brows, const int32_t* rp, const int32_t* ci, const T* vals, const T* __restrict__ dold,
+                     T* dnew, T* r, T* x, const T* __restrict__ dinv, double a, double c) {
+  bsr_rows<VEC, T, T>(
+      n_brows, rp, ci, vals, [&](int64_t i) { return dold[i]; },
+      [&](int64_t row, int comp, T q) {
+        const int64_t i = row * VEC + comp;
+        const double rn = double(r[i]) - double(q);
+        r[i] = T(rn);
+        const T dn = T(a * double(dold[i]) + c * double(dinv[i]) * rn);
+        dnew[i] = dn;
+        x[i] = T(x[i] + dn);
+      });
+}
+
+// r -= A d
+template <int VEC, typename T>
+__global__ void __launch_bounds__(kRowThreads, kRowBlocksPerSM)
+    cheb_resid_kernel(int64_t n_brows, const int32_t* rp, const int32_t* ci, const T* vals, const T* __restrict__ d,
+                      T* r) {
+  bsr_rows<VEC, T, T>(
+      n_brows, rp, ci, vals, [&](int64_t i) { return d[i]; },
+      [&](int64_t row, int comp, T q) {
+        const int64_t i = row * VEC + comp;
+        r[i] = T(double(r[i]) - double(q));
+      });
+}
+
+// r = b - A x
+template <int VEC, typename T>
+__global__ void __launch_bounds__(kRowThreads, kRowBlocksPerSM)
+    mg_residual_kernel(int64_t n_brows, const int32_t* rp, const int32_t* ci, const T* vals, const T* __restrict__ x,
+                       const T* b, T* r) {
+  bsr_rows<VEC, T, T>(
+      n_brows, rp, ci, vals, [&](int64_t i) { return x[i]; },
+      [&](int64_t row, int comp, T q) {
+        const int64_t i = row * VEC + comp;
+        r[i] = T(double(b[i]) - double(q));
+      });
+}
+
+// ---- host side -------------------------------------------------------------------
+struct Cheb {
+  double inv_theta, sigma, delta;
+};
+inline Cheb cheb_of(double lmax, double ratio) {
+  const double lmin = lmax / ratio;
+  const double theta = 0.5 * (lmax + lmin), delta = 0.5 * (lmax - lmin);
+  return Cheb{1.0 / theta, theta / delta, delta};
+}
+
+inline unsigned vgrid(int64_t n) {
+  const int64_t b = (n + 255) / 256;
+  const int64_t cap = int64_t(num_sms()) * 8;
+  return unsigned(b < 1 ? 1 : (b < cap ? b : cap));
+}
+
+template <int VEC, typename T>
+int check_levels(int nlevels, const FemMGLevel* L) {
+  FEM_CHECK_ARG(nlevels >= 1 && nlevels <= 16, "nlevels must be in [1, 16] (got %d)", nlevels);
+  FEM_CHECK_ARG(L != nullptr, "levels is NULL");
+  for (int l = 0; l < nlevels; ++l) {
+    const FemMGLevel& v = L[l];
+    FEM_CHECK_ARG(v.nodes[0] >= 2 && v.nodes[1] >= 2 && v.nodes[2] >= 2, "level %d: lattice needs >= 2 nodes per direction", l);
+    FEM_CHECK_ARG(v.n_brows == v.nodes[0] * v.nodes[1] * v.nodes[2], "level %d: n_brows != nodes product", l);
+    FEM_CHECK_ARG(v.row_ptr && v.col_idx && v.stencil && v.vals && v.dinv && v.r && v.d0 && v.d1,
+                  "level %d: NULL pattern, values or work vector", l);
+    FEM_CHECK_ARG(bsr_aligned(v.vals, v.col_idx), "level %d: vals and col_idx must be 16-byte aligned", l);
+    if (l >= 1) {
+      FEM_CHECK_ARG(v.x && v.b && v.cpos && v.ilo && v.whi, "level %d: NULL transfer data or work vector", l);
+      for (int d = 0; d < 3; ++d)
+        FEM_CHECK_ARG(v.nodes[d] <= L[l - 1].nodes[d], "level %d: coarser than its finer level expected", l);
+    }
+  }
+  return FEM_OK;
+}
+
+template <int VEC, typename T>
+int ensure_attrs() {
+  int rc;
+  if ((rc = ensure_smem_attr(cheb_step_kernel<VEC, T>)) != FEM_OK) return rc;
+  if ((rc = ensure_smem_attr(cheb_resid_kernel<VEC, T>)) != FEM_OK) return rc;
+  if ((rc = ensure_smem_attr(mg_residual_kernel<VEC, T>)) != FEM_OK) return rc;
+  return FEM_OK;
+}
+
+template <int VEC, typename T>
+int setup_impl(int nlevels, FemMGLevel* L, const double* fine64, cudaStream_t st) {
+  int rc = check_levels<VEC, T>(nlevels, L);
+  if (rc != FEM_OK) return rc;
+  constexpr int VV = VEC * VEC;
+  for (int l = 0; l < nlevels; ++l) {
+    if (l == 0 && fine64 != nullptr) {
+      // nnzb of level 0 from its row pointer (one int read)
+      int32_t nnzb = 0;
+      FEM_CUDA_TRY(cudaMemcpyAsync(&nnzb, L[0].row_ptr + L[0].n_brows, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+      FEM_CUDA_TRY(cudaStreamSynchronize(st));
+      const int64_t n = int64_t(nnzb) * VV;
+      cast_kernel<T><<<vgrid(n), 256, 0, st>>>(n, fine64, static_cast<T*>(L[0].vals));
+      FEM_LAUNCH_CHECK();
+    }
+    if (l >= 1) {
+      const int64_t nc = L[l].n_brows;
+      const int64_t blocks = (nc * 32 + 255) / 256;
+      const unsigned grid = unsigned(blocks < int64_t(num_sms()) * 32 ? blocks : int64_t(num_sms()) * 32);
+      rap_kernel<VEC, T><<<grid, 256, 0, st>>>(lat_of(L[l - 1]), L[l - 1].stencil, static_cast<const T*>(L[l - 1].vals),
+                                                lat_of(L[l]), L[l].stencil, static_cast<T*>(L[l].vals), L[l].cpos,
+                                                L[l].ilo, L[l].whi);
+      FEM_LAUNCH_CHECK();
+    }
+    unsigned long long* bits = static_cast<unsigned long long*>(L[l].d0);  // scratch (8 bytes of d0)
+    FEM_CUDA_TRY(cudaMemsetAsync(bits, 0, sizeof(unsigned long long), st));
+    jacobi_setup_kernel<VEC, T><<<vgrid(L[l].n_brows * VEC), 256, 0, st>>>(
+        L[l].n_brows, L[l].stencil, static_cast<const T*>(L[l].vals), static_cast<T*>(L[l].dinv), bits);
+    FEM_LAUNCH_CHECK();
+    unsigned long long hb = 0;
+    FEM_CUDA_TRY(cudaMemcpyAsync(&hb, bits, sizeof(hb), cudaMemcpyDeviceToHost, st));
+    FEM_CUDA_TRY(cudaStreamSynchronize(st));
+    double lm;
+    std::memcpy(&lm, &hb, sizeof(lm));
+    FEM_CHECK_ARG(std::isfinite(lm) && lm > 0.0, "level %d: operator has a zero or non-finite diagonal", l);
+    L[l].lmax = lm;
+  }
+  return ensure_attrs<VEC, T>();
+}
+
+// m Chebyshev steps on level l (x, r, d0/d1 of the level; b as rhs).  With
+// want_residual the level's r ends as b - A x.
+template <int VEC, typename T>
+int smooth(const FemMGLevel& L, const T* b, T* x, int m, double ratio, bool zero_start, bool want_residual,
+           cudaStream_t st) {
+  const int64_t n = L.n_brows * VEC;
+  const Cheb ch = cheb_of(L.lmax, ratio);
+  T* r = static_cast<T*>(L.r);
+  T* d[2] = {static_cast<T*>(L.d0), static_cast<T*>(L.d1)};
+  const T* dinv = static_cast<const T*>(L.dinv);
+  const T* vals = static_cast<const T*>(L.vals);
+  const unsigned rg = row_grid<T>(L.n_brows);
+  cheb_first_kernel<T><<<vgrid(n), 256, 0, st>>>(n, dinv, b, r, d[0], x, ch.inv_theta, zero_start ? 1 : 0);
+  FEM_LAUNCH_CHECK();
+  double rho_old = 1.0 / ch.sigma;
+  int cur = 0;
+  for (int k = 1; k < m; ++k) {
+    const double rho = 1.0 / (2.0 * ch.sigma - rho_old);
+    cheb_step_kernel<VEC, T><<<rg, kRowThreads, bsr_rows_smem(), st>>>(L.n_brows, L.row_ptr, L.col_idx, vals, d[cur],
+                                                                      d[cur ^ 1], r, x, dinv, rho * rho_old,
+                                                                      2.0 * rho / ch.delta);
+    FEM_LAUNCH_CHECK();
+    rho_old = rho;
+    cur ^= 1;
+  }
+  if (want_residual) {
+    cheb_resid_kernel<VEC, T><<<rg, kRowThreads, bsr_rows_smem(), st>>>(L.n_brows, L.row_ptr, L.col_idx, vals, d[cur], r);
+    FEM_LAUNCH_CHECK();
+  }
+  return FEM_OK;
+}
+
+template <int VEC, typename T>
+int vcycle_level(int l, int nlevels, const FemMGLevel* L, int nu, int coarse_steps, double ratio, const T* b, T* x,
+                 cudaStream_t st) {
+  int rc;
+  if (l == nlevels - 1) return smooth<VEC, T>(L[l], b, x, coarse_steps, ratio, true, false, st);
+  if ((rc = smooth<VEC, T>(L[l], b, x, nu, ratio, true, true, st)) != FEM_OK) return rc;
+  const FemMGLevel& C = L[l + 1];
+  T* bc = static_cast<T*>(C.b);
+  T* xc = static_cast<T*>(C.x);
+  restrict_kernel<VEC, T><<<vgrid(C.n_brows), 256, 0, st>>>(lat_of(L[l]), lat_of(C), C.cpos, C.ilo, C.whi,
+                                                            static_cast<const T*>(L[l].r), bc);
+  FEM_LAUNCH_CHECK();
+  if ((rc = vcycle_level<VEC, T>(l + 1, nlevels, L, nu, coarse_steps, ratio, bc, xc, st)) != FEM_OK) return rc;
+  prolong_add_kernel<VEC, T><<<vgrid(L[l].n_brows), 256, 0, st>>>(lat_of(L[l]), lat_of(C), C.ilo, C.whi, xc, x);
+  FEM_LAUNCH_CHECK();
+  mg_residual_kernel<VEC, T><<<row_grid<T>(L[l].n_brows), kRowThreads, bsr_rows_smem(), st>>>(
+      L[l].n_brows, L[l].row_ptr, L[l].col_idx, static_cast<const T*>(L[l].vals), x, b, static_cast<T*>(L[l].r));
+  FEM_LAUNCH_CHECK();
+  return smooth<VEC, T>(L[l], b, x, nu, ratio, false, false, st);
+}
+
+template <int VEC, typename T>
+int vcycle_impl(int nlevels, const FemMGLevel* L, int nu, int coarse_steps, double ratio, const T* rhs, T* z,
+                cudaStream_t st) {
+  FEM_CHECK_ARG(rhs != nullptr && z != nullptr, "rhs and z must not be NULL");
+  FEM_CHECK_ARG(nu >= 1 && nu <= 16 && coarse_steps >= 1 && coarse_steps <= 512, "nu in [1,16], coarse_steps in [1,512]");
+  FEM_CHECK_ARG(ratio > 1.0, "ratio must exceed 1");
+  for (int l = 0; l < nlevels; ++l)
+    FEM_CHECK_ARG(L[l].lmax > 0.0, "level %d has no lmax: run fem_mg_setup first", l);
+  return vcycle_level<VEC, T>(0, nlevels, L, nu, coarse_steps, ratio, rhs, z, st);
+}
+
+// ---- V-cycle preconditioned CG (FP64) -------------------------------------------
+struct PState {
+  double gamma, alpha, beta, rr, tol2, bb, pq;
+  int iter, status, maxiter, first;
+};
+enum : int { PS_RUNNING = 0, PS_CONVERGED = 1 };
+
+template <int VEC>
+__global__ void pcg_init_kernel(int64_t n, const double* r, const double* b, double* partials, unsigned* counter,
+                                PState* S, double rtol, double atol) {
+  double v[2] = {0.0, 0.0};
+  for (int64_t k = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; k < n; k += int64_t(gridDim.x) * blockDim.x) {
+    v[0] = fma(r[k], r[k], v[0]);
+    v[1] = fma(b[k], b[k], v[1]);
+  }
+  double tot[2];
+  if (last_block_reduce<2>(v, partials, counter, tot)) {
+    S->rr = tot[0];
+    S->bb = tot[1];
+    S->tol2 = fmax(rtol * rtol * tot[1], atol * atol);
+    S->iter = 0;
+    S->first = 1;
+    S->gamma = 0.0;
+    S->beta = 0.0;
+    if (!isfinite(tot[0]) || !isfinite(tot[1])) S->status = FEM_ERR_NONFINITE;
+    else if (tot[0] <= S->tol2) S->status = PS_CONVERGED;
+    else if (S->maxiter <= 0) S->status = FEM_ERR_NOT_CONVERGED;
+    else S->status = PS_RUNNING;
+  }
+}
+
+// gamma = r.z; beta = gamma / gamma_old (0 first)
+__global__ void pcg_rz_kernel(int64_t n, const double* r, const double* z, double* partials, unsigned* counter,
+                              PState* S) {
+  if (S->status != PS_RUNNING) return;
+  double v[1] = {0.0};
+  for (int64_t k = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; k < n; k += int64_t(gridDim.x) * blockDim.x)
+    v[0] = fma(r[k], z[k], v[0]);
+  double tot[1];
+  if (last_block_reduce<1>(v, partials, counter, tot)) {
+    const double g = tot[0];
+    if (!isfinite(g)) {
+      S->status = FEM_ERR_NONFINITE;
+    } else if (!(g > 0.0)) {
+      S->status = FEM_ERR_BREAKDOWN;  // preconditioner lost definiteness (or r = 0)
+    } else {
+      S->beta = S->first ? 0.0 : g / S->gamma;
+      S->gamma = g;
+      S->first = 0;
+    }
+  }
+}
+
+// p = z + beta p (from float z when the hierarchy is FP32)
+template <typename ZT>
+__global__ void pcg_dir_kernel(int64_t n, const ZT* z, double* p, const PState* S) {
+  if (S->status != PS_RUNNING) return;
+  const double beta = S->beta;
+  for (int64_t k = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; k < n; k += int64_t(gridDim.x) * blockDim.x)
+    p[k] = double(z[k]) + beta * p[k];
+}
+
+// q = A p; pq = p.q; alpha = gamma / pq
+template <int VEC>
+__global__ void __launch_bounds__(kRowThreads, kRowBlocksPerSM)
+    pcg_spmv_kernel(int64_t n_brows, const int32_t* rp, const int32_t* ci, const double* vals, const double* __restrict__ p,
+                    double* q, double* partials, unsigned* counter, PState* S) {
+  if (S->status != PS_RUNNING) return;
+  double v[1] = {0.0};
+  bsr_rows<VEC, double, double>(
+      n_brows, rp, ci, vals, [&](int64_t i) { return p[i]; },
+      [&](int64_t row, int c, double qo) {
+        const int64_t i = row * VEC + c;
+        q[i] = qo;
+        v[0] = fma(p[i], qo, v[0]);
+      });
+  double tot[1];
+  if (last_block_reduce<1>(v, partials, counter, tot)) {
+    S->pq = tot[0];
+    if (!isfinite(tot[0])) S->status = FEM_ERR_NONFINITE;
+    else if (!(tot[0] > 0.0)) S->status = FEM_ERR_BREAKDOWN;
+    else S->alpha = S->gamma / tot[0];
+  }
+}
+
+// x += alpha p; r -= alpha q; rr = r.r; bookkeeping.  Also rounds r into the
+// FP32 hierarchy's right-hand side when r32 is given.
+__global__ void pcg_update_kernel(int64_t n, double* x, double* r, const double* p, const double* q, float* r32,
+                                  double* partials, unsigned* counter, PState* S) {
+  if (S->status != PS_RUNNING) return;
+  const double alpha = S->alpha;
+  double v[1] = {0.0};
+  for (int64_t k = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; k < n; k += int64_t(gridDim.x) * blockDim.x) {
+    x[k] = fma(alpha, p[k], x[k]);
+    const double rk = fma(-alpha, q[k], r[k]);
+    r[k] = rk;
+    if (r32 != nullptr) r32[k] = float(rk);
+    v[0] = fma(rk, rk, v[0]);
+  }
+  double tot[1];
+  if (last_block_reduce<1>(v, partials, counter, tot)) {
+    S->iter += 1;
+    S->rr = tot[0];
+    if (!isfinite(tot[0])) S->status = FEM_ERR_NONFINITE;
+    else if (tot[0] <= S->tol2) S->status = PS_CONVERGED;
+    else if (S->iter >= S->maxiter) S->status = FEM_ERR_NOT_CONVERGED;
+  }
+}
+
+inline size_t al256(size_t x) { return (x + 255) & ~size_t(255); }
+
+size_t pcg_workspace_bytes(int vec, int64_t n_brows) {
+  const size_t n = size_t(n_brows) * vec;
+  return 256 + 256 + al256(size_t(num_sms()) * 8 * 4 * sizeof(double)) + 4 * al256(n * sizeof(double));
+}
+
+template <int VEC>
+int pcg_impl(int64_t n_brows, const int32_t* rp, const int32_t* ci, const double* vals, const double* b, double* x,
+             double rtol, double atol, int maxiter, int check_every, int nlevels, const FemMGLevel* L, int fp32,
+             int nu, int coarse_steps, double ratio, void* work, size_t work_bytes, int* h_iters, double* h_relres,
+             cudaStream_t st) {
+  const int64_t n = n_brows * VEC;
+  const size_t need = pcg_workspace_bytes(VEC, n_brows);
+  FEM_CHECK_ARG(work != nullptr && work_bytes >= need, "mg pcg workspace too small (%zu < %zu)", work_bytes, need);
+  FEM_CHECK_ARG(rp && ci && vals && b && x, "NULL operator or vector");
+  FEM_CHECK_ARG(bsr_aligned(vals, ci), "vals and col_idx must be 16-byte aligned");
+  FEM_CHECK_ARG(nlevels >= 1 && L != nullptr && L[0].n_brows == n_brows, "level 0 must be the operator's lattice");
+  FEM_CHECK_ARG(!fp32 || (L[0].x != nullptr && L[0].b != nullptr), "FP32 hierarchy needs level 0 x and b");
+  if (check_every <= 0) check_every = 4;
+  char* p8 = static_cast<char*>(work);
+  PState* S = reinterpret_cast<PState*>(p8);
+  unsigned* counter = reinterpret_cast<unsigned*>(p8 + 256);
+  double* partials = reinterpret_cast<double*>(p8 + 512);
+  p8 += 512 + al256(size_t(num_sms()) * 8 * 4 * sizeof(double));
+  double* r = reinterpret_cast<double*>(p8);
+  double* z = reinterpret_cast<double*>(p8 + al256(n * sizeof(double)));
+  double* pv = reinterpret_cast<double*>(p8 + 2 * al256(n * sizeof(double)));
+  double* q = reinterpret_cast<double*>(p8 + 3 * al256(n * sizeof(double)));
+  int rc;
+  if ((rc = ensure_smem_attr(pcg_spmv_kernel<VEC>)) != FEM_OK) return rc;
+  if ((rc = ensure_smem_attr(mg_residual_kernel<VEC, double>)) != FEM_OK) return rc;
+  if ((rc = (fp32 ? ensure_attrs<VEC, float>() : ensure_attrs<VEC, double>())) != FEM_OK) return rc;
+  FEM_CUDA_TRY(cudaMemsetAsync(work, 0, 512, st));
+  FEM_CUDA_TRY(cudaMemsetAsync(pv, 0, sizeof(double) * n, st));
+  PState init{};
+  init.maxiter = maxiter;
+  init.first = 1;
+  FEM_CUDA_TRY(cudaMemcpyAsync(S, &init, sizeof(PState), cudaMemcpyHostToDevice, st));
+  const unsigned rg = row_grid<double>(n_brows), vg = vgrid(n);
+  float* r32 = fp32 ? static_cast<float*>(L[0].b) : nullptr;
+  float* z32 = fp32 ? static_cast<float*>(L[0].x) : nullptr;
+  // r = b - A x, the reductions and status
+  mg_residual_kernel<VEC, double><<<rg, kRowThreads, bsr_rows_smem(), st>>>(n_brows, rp, ci, vals, x, b, r);
+  FEM_LAUNCH_CHECK();
+  pcg_init_kernel<VEC><<<vg, 256, 0, st>>>(n, r, b, partials, counter, S, rtol, atol);
+  FEM_LAUNCH_CHECK();
+  if (fp32) {
+    cast_kernel<float><<<vg, 256, 0, st>>>(n, r, r32);
+    FEM_LAUNCH_CHECK();
+  }
+  double* mb = host_mailbox();
+  FEM_CHECK_ARG(mb != nullptr, "pinned mailbox allocation failed");
+  static_assert(sizeof(PState) <= 256, "PState must fit its slot and the mailbox");
+  const PState* hs = reinterpret_cast<const PState*>(mb);
+  auto read_state = [&]() -> int {
+    FEM_CUDA_TRY(cudaMemcpyAsync(mb, S, sizeof(PState), cudaMemcpyDeviceToHost, st));
+    FEM_CUDA_TRY(cudaStreamSynchronize(st));
+    return FEM_OK;
+  };
+  int launched = 0;
+  while (true) {
+    if ((rc = read_state()) != FEM_OK) return rc;
+    if (hs->status != PS_RUNNING || launched >= maxiter) break;
+    const int chunk = check_every < maxiter - launched ? check_every : maxiter - launched;
+    for (int k = 0; k < chunk; ++k) {
+      if (fp32) {
+        // r.z needs z in FP64: widen the FP32 V-cycle output into z
+        if ((rc = vcycle_level<VEC, float>(0, nlevels, L, nu, coarse_steps, ratio, r32, z32, st)) != FEM_OK) return rc;
+        widen_kernel<float><<<vg, 256, 0, st>>>(n, z32, z);
+        FEM_LAUNCH_CHECK();
+      } else {
+        if ((rc = vcycle_level<VEC, double>(0, nlevels, L, nu, coarse_steps, ratio, r, z, st)) != FEM_OK) return rc;
+      }
+      pcg_rz_kernel<<<vg, 256, 0, st>>>(n, r, z, partials, counter, S);
+      FEM_LAUNCH_CHECK();
+      pcg_dir_kernel<double><<<vg, 256, 0, st>>>(n, z, pv, S);
+      FEM_LAUNCH_CHECK();
+      pcg_spmv_kernel<VEC><<<rg, kRowThreads, bsr_rows_smem(), st>>>(n_brows, rp, ci, vals, pv, q, partials, counter, S);
+      FEM_LAUNCH_CHECK();
+      pcg_update_kernel<<<vg, 256, 0, st>>>(n, x, r, pv, q, r32, partials, counter, S);
+      FEM_LAUNCH_CHECK();
+    }
+    launched += chunk;
+  }
+  const int status = hs->status;
+  const int iters = hs->iter;
+  const double bb = hs->bb;
+  // report the true residual ||b - A x||
+  mg_residual_kernel<VEC, double><<<rg, kRowThreads, bsr_rows_smem(), st>>>(n_brows, rp, ci, vals, x, b, q);
+  FEM_LAUNCH_CHECK();
+  FEM_CUDA_TRY(cudaMemsetAsync(counter, 0, sizeof(unsigned), st));
+  pcg_init_kernel<VEC><<<vg, 256, 0, st>>>(n, q, b, partials, counter, S, rtol, atol);
+  FEM_LAUNCH_CHECK();
+  if ((rc = read_state()) != FEM_OK) return rc;
+  const double rr = hs->rr;
+  if (h_iters) *h_iters = iters;
+  if (h_relres) *h_relres = bb > 0 ? std::sqrt(rr / bb) : std::sqrt(rr);
+  if (status == PS_CONVERGED) return FEM_OK;
+  const int st_out = (status == PS_RUNNING) ? FEM_ERR_NOT_CONVERGED : status;
+  set_error("mg pcg: status %d after %d iterations (relres %.3e)", st_out, iters, bb > 0 ? std::sqrt(rr / bb) : std::sqrt(rr));
+  return st_out;
+}
+
+}  // namespace
+}  // namespace fem
+
+using namespace fem;
+
+extern "C" int fem_mg_setup_f64(int vec, int nlevels, FemMGLevel* levels, void* stream) {
+  FEM_CHECK_ARG(vec == 1 || vec == 3, "vec must be 1 or 3");
+  return vec == 3 ? setup_impl<3, double>(nlevels, levels, nullptr, as_stream(stream))
+                  : setup_impl<1, double>(nlevels, levels, nullptr, as_stream(stream));
+}
+
+extern "C" int fem_mg_setup_f32(int vec, int nlevels, FemMGLevel* levels, const double* d_fine_f64, void* stream) {
+  FEM_CHECK_ARG(vec == 1 || vec == 3, "vec must be 1 or 3");
+  return vec == 3 ? setup_impl<3, float>(nlevels, levels, d_fine_f64, as_stream(stream))
+                  : setup_impl<1, float>(nlevels, levels, d_fine_f64, as_stream(stream));
+}
+
+extern "C" int fem_mg_vcycle_f64(int vec, int nlevels, const FemMGLevel* levels, int nu, int coarse_steps,
+                                 double ratio, const double* d_rhs, double* d_z, void* stream) {
+  FEM_CHECK_ARG(vec == 1 || vec == 3, "vec must be 1 or 3");
+  int rc = vec == 3 ? check_levels<3, double>(nlevels, levels) : check_levels<1, double>(nlevels, levels);
+  if (rc != FEM_OK) return rc;
+  rc = vec == 3 ? ensure_attrs<3, double>() : ensure_attrs<1, double>();
+  if (rc != FEM_OK) return rc;
+  return vec == 3 ? vcycle_impl<3, double>(nlevels, levels, nu, coarse_steps, ratio, d_rhs, d_z, as_stream(stream))
+                  : vcycle_impl<1, double>(nlevels, levels, nu, coarse_steps, ratio, d_rhs, d_z, as_stream(stream));
+}
+
+extern "C" int fem_mg_vcycle_f32(int vec, int nlevels, const FemMGLevel* levels, int nu, int coarse_steps,
+                                 double ratio, const float* d_rhs, float* d_z, void* stream) {
+  FEM_CHECK_ARG(vec == 1 || vec == 3, "vec must be 1 or 3");
+  int rc = vec == 3 ? check_levels<3, float>(nlevels, levels) : check_levels<1, float>(nlevels, levels);
+  if (rc != FEM_OK) return rc;
+  rc = vec == 3 ? ensure_attrs<3, float>() : ensure_attrs<1, float>();
+  if (rc != FEM_OK) return rc;
+  return vec == 3 ? vcycle_impl<3, float>(nlevels, levels, nu, coarse_steps, ratio, d_rhs, d_z, as_stream(stream))
+                  : vcycle_impl<1, float>(nlevels, levels, nu, coarse_steps, ratio, d_rhs, d_z, as_stream(stream));
+}
+
+extern "C" size_t fem_mg_pcg_workspace_bytes(int vec, int64_t n_brows) { return pcg_workspace_bytes(vec, n_brows); }
+
+extern "C" int fem_mg_pcg_solve(int vec, int64_t n_brows, const int32_t* d_row_ptr, const int32_t* d_col_idx,
+                                const double* d_vals, const double* d_b, double* d_x, double rtol, double atol,
+                                int maxiter, int check_every, int nlevels, const FemMGLevel* levels, int levels_fp32,
+                                int nu, int coarse_steps, double ratio, void* d_work, size_t work_bytes, int* h_iters,
+                                double* h_relres, void* stream) {
+  FEM_CHECK_ARG(vec == 1 || vec == 3, "vec must be 1 or 3");
+  FEM_CHECK_ARG(rtol >= 0 && atol >= 0, "negative tolerance");
+  int rc = levels_fp32 ? (vec == 3 ? check_levels<3, float>(nlevels, levels) : check_levels<1, float>(nlevels, levels))
+                       : (vec == 3 ? check_levels<3, double>(nlevels, levels) : check_levels<1, double>(nlevels, levels));
+  if (rc != FEM_OK) return rc;
+  FEM_CHECK_ARG(nu >= 1 && nu <= 16 && coarse_steps >= 1 && coarse_steps <= 512 && ratio > 1.0,
+                "nu in [1,16], coarse_steps in [1,512], ratio > 1");
+  for (int l = 0; l < nlevels; ++l)
+    FEM_CHECK_ARG(levels[l].lmax > 0.0, "level %d has no lmax: run the setup first", l);
+  auto st = as_stream(stream);
+  return vec == 3 ? pcg_impl<3>(n_brows, d_row_ptr, d_col_idx, d_vals, d_b, d_x, rtol, atol, maxiter, check_every,
+                                nlevels, levels, levels_fp32, nu, coarse_steps, ratio, d_work, work_bytes, h_iters,
+                                h_relres, st)
+                  : pcg_impl<1>(n_brows, d_row_ptr, d_col_idx, d_vals, d_b, d_x, rtol, atol, maxiter, check_every,
+                                nlevels, levels, levels_fp32, nu, coarse_steps, ratio, d_work, work_bytes, h_iters,
+                                h_relres, st);
+}

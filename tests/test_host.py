@@ -195,3 +195,34 @@ def test_no_gpu_means_loud_failure(pkg):
     p = P(pkg.Mesh(m.points, m.cells_dict["hexahedron"]), vec=3, dim=3)
     with pytest.raises(pkg._native.FEMNativeError):
         pkg.solver(p)
+
+
+def test_multigrid_lattice_hierarchy(pkg):
+    """Host side of the multigrid: lattice detection, 1-D coarsening (the
+    prolongation reproduces linear functions of the coordinates exactly, on
+    graded lattices and odd cell counts) and the 27-point stencil map."""
+    import importlib
+    mg = importlib.import_module("jax_fem_b200.multigrid")
+    m = pkg.box_mesh(5, 4, 6, 1.0, 2.0, 0.5)
+    lat = mg.lattice_of(m.points, m.cells_dict["hexahedron"])
+    assert lat is not None and lat[0] == (6, 5, 7)
+    bent = m.points.copy()
+    bent[7, 0] += 1e-3
+    assert mg.lattice_of(bent, m.cells_dict["hexahedron"]) is None
+    for coords in (np.linspace(0.0, 1.0, 6), np.linspace(0.0, 1.0, 9) ** 2, np.array([0.0, 0.3, 1.0])):
+        cc, cpos, ilo, whi = mg.coarsen_1d(coords)
+        np.testing.assert_array_equal(cc, coords[cpos])
+        assert cpos[0] == 0 and cpos[-1] == len(coords) - 1
+        P = np.zeros((len(coords), len(cc)))
+        P[np.arange(len(coords)), ilo] += 1.0 - whi
+        P[np.arange(len(coords)), ilo + 1] += whi
+        np.testing.assert_allclose(P @ (2.0 - 3.0 * cc), 2.0 - 3.0 * coords, atol=1e-14)
+        np.testing.assert_allclose(P.sum(axis=1), 1.0)
+        assert ((whi >= 0) & (whi <= 1)).all()
+    n = lat[0]
+    rp, col, _, _, _ = _pattern(pkg, mg.lattice_cells(n), n[0] * n[1] * n[2])
+    st = mg.stencil_of(n, rp, col)
+    assert (st[:, 13] >= 0).all() and (col[st[:, 13]] == np.arange(len(st))).all()
+    interior = (1 * n[1] + 1) * n[2] + 1
+    assert (st[interior] >= 0).all()
+    assert (st >= 0).sum() == len(col)
