@@ -239,30 +239,34 @@ def run_ours(args, rank, world, device):
     adaptive = {"cg": {"precond": "block_jacobi", "rtol": "adaptive", "atol": 0.0, "maxiter": 20000}}
     refine = {"cg": dict(adaptive["cg"], reliable_delta=0.0)}
     refm = {"jax_solver": {}}  # the reference's default linear solver: BiCGSTAB + Jacobi, tol = atol = 1e-10
+    gmg = {"cg": {"precond": "gmg", "rtol": "adaptive", "atol": 0.0, "maxiter": 2000}}
     variants = {  # name -> (precision, linear options)
         "reference_method_fp64": ("fp64", refm),  # the reference's exact Newton + linear settings on the GPU
         "plain_fp64": ("fp64", tight),            # tight linear solves, CG + 3x3 block-Jacobi
         "plain_fp64_adaptive": ("fp64", adaptive),
         "mixed_tight": ("mixed", tight),
         "mixed_refinement": ("mixed", refine),    # FP32 CG restarted inside FP64 iterative refinement
-        "mixed": ("mixed", adaptive),             # headline: FP32 tangent/Krylov with reliable updates
+        "mixed": ("mixed", adaptive),             # FP32 tangent/Krylov with reliable updates
+        "plain_fp64_gmg": ("fp64", gmg),          # FP64 CG + FP64 multigrid V-cycle
+        "mixed_gmg": ("mixed", gmg),              # headline: FP64 CG + FP32 multigrid V-cycle
     }
+    HEAD = "mixed_gmg"
     results = {}
     sampler = ClockSampler(torch.cuda.current_device())
     for name, (prec, lin) in variants.items():
         barrier()
-        if name == "mixed":
+        if name == HEAD:
             l0 = nat.launch_count()
             sampler.start()
         times, infos = timed(prec, args.steps, args.warmup, lin)
-        if name == "mixed":
+        if name == HEAD:
             clocks = sampler.stop()
             launches = (nat.launch_count() - l0) * args.steps // (args.steps + args.warmup)
         barrier()
         results[name] = (max_over_ranks(statistics.mean(times)), infos)
-    t_mixed = results["mixed"][0]
+    t_mixed = results[HEAD][0]
     t_plain = results["plain_fp64"][0]
-    mixed_infos, plain_infos = results["mixed"][1], results["plain_fp64"][1]
+    mixed_infos, plain_infos = results[HEAD][1], results["plain_fp64"][1]
 
     # e2e through the public API with host buffers: the step's inputs (node
     # coordinates and Dirichlet values) come from pinned host memory, the
@@ -274,7 +278,7 @@ def run_ours(args, rank, world, device):
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         dv.points.copy_(pts_h, non_blocking=True)
-        sol, _ = nh_solve(pkg, prob, "mixed", linear=variants["mixed"][1])
+        sol, _ = nh_solve(pkg, prob, variants[HEAD][0], linear=variants[HEAD][1])
         sol_h.copy_(sol.reshape(-1), non_blocking=True)
         torch.cuda.synchronize()
         if i >= args.warmup:
@@ -318,18 +322,21 @@ def run_ours(args, rank, world, device):
             sprob = ws.cantilever_problem()
             warmstart_eval(pkg, ws, sprob, net, 1, seed=77)  # warm-up
             rows = warmstart_eval(pkg, ws, sprob, net, args.simp_samples, seed=999_000,
-                                  arms=[(pr, st) for pr in ("fp64", "mixed") for st in ("zero", "learned")])
+                                  arms=[(pr, st) for pr in ("fp64", "mixed", "fp64_gmg", "mixed_gmg")
+                                        for st in ("zero", "learned")])
             simp = {"workload": "SIMP cantilever 60x30x30 (175,863 dofs), seeded Gaussian random density, "
                                 "load patch position uniform in z; rel.res 1e-8 of the zero-start residual; "
-                                "mixed = FP32 tangent, FP32 CG restarted inside FP64 refinement",
+                                "fp64/mixed = block-Jacobi CG (mixed: FP32 tangent, FP32 CG restarted inside FP64 "
+                                "refinement); *_gmg = FP64 CG with a multigrid V-cycle (FP32 in mixed_gmg)",
                     "samples": args.simp_samples, "arms": summarize_eval(rows)}
     except Exception as e:  # noqa: BLE001 - report, do not lose the headline line
         simp = {"error": str(e)[:200]}
     # J2 40^3, 10 increments, plain vs mixed
     j2 = {}
-    for arm, prec, rt in (("fp64", "fp64", 1e-10), ("fp64_adaptive", "fp64", "adaptive"),
-                          ("mixed", "mixed", "adaptive")):
-        lin_j2 = {"cg": {"precond": "block_jacobi", "rtol": rt, "atol": 0.0, "maxiter": 20000}}
+    for arm, prec, rt, pc in (("fp64", "fp64", 1e-10, "block_jacobi"), ("fp64_adaptive", "fp64", "adaptive", "block_jacobi"),
+                              ("mixed", "mixed", "adaptive", "block_jacobi"), ("fp64_gmg", "fp64", "adaptive", "gmg"),
+                              ("mixed_gmg", "mixed", "adaptive", "gmg")):
+        lin_j2 = {"cg": {"precond": pc, "rtol": rt, "atol": 0.0, "maxiter": 20000}}
         j2_run(pkg, 40, 10, prec, lin_j2)  # warm-up
         torch.cuda.synchronize()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -351,21 +358,26 @@ def run_ours(args, rank, world, device):
         "higher_is_better": False,
         "scaling": "weak",
         "vs_baseline": None,
-        "dtype": "f32 tangent/Krylov + f64 residual/refinement",
+        "dtype": "f64 tangent, residual and CG; f32 multigrid V-cycle",
         "data": "synthetic",
         "config": {"workload": f"neo-hookean {args.n}^3 HEX8, 30 deg twist in 5 load steps, "
                                "Newton rel.res 1e-8", "dofs": ndofs, "cells": dv.num_cells,
-                   "precision": "mixed", "krylov": "cg + 3x3 block-jacobi",
+                   "precision": "mixed", "krylov": "cg (f64) preconditioned by a geometric multigrid v-cycle (f32)",
                    "l2": "flushed (256 MB write) between timed steps", "parallelism": f"replicas x{world}"},
         "plain_fp64_s": round(t_plain, 6),
         "speedup_vs_plain_fp64": round(t_plain / t_mixed, 3),
+        "speedup_mixed_vs_fp64_same_method": {
+            "gmg": round(results["plain_fp64_gmg"][0] / results["mixed_gmg"][0], 3),
+            "block_jacobi_adaptive": round(results["plain_fp64_adaptive"][0] / results["mixed"][0], 3)},
         "variants_s": {k: round(v[0], 6) for k, v in results.items()},
         "variants_note": "reference_method_fp64 = the reference's default BiCGSTAB + Jacobi (tol = atol = 1e-10) in "
                          "FP64 on the GPU; plain_fp64 = tight (1e-10) CG + 3x3 block-Jacobi solves in FP64; "
                          "*_adaptive/mixed* = Eisenstat-Walker forcing; mixed = FP32 tangent and FP32 CG "
                          "iterations with reliable updates (FP64 solution, true residual, reductions); "
                          "mixed_tight = the same to the 1e-10 linear tolerance; mixed_refinement = FP32 CG "
-                         "restarted inside FP64 iterative refinement",
+                         "restarted inside FP64 iterative refinement; *_gmg = CG preconditioned by a geometric "
+                         "multigrid V-cycle (FP64 CG; V-cycle FP64 in plain_fp64_gmg, FP32 in mixed_gmg); "
+                         "value = mixed_gmg",
         "solves_per_s": round(world / t_mixed, 4),
         "newton_iters": newton,
         "krylov_iters": krylov,
@@ -461,7 +473,8 @@ def run_reference(args, rank, world):
 
 def run_profile(args, device):
     """A short fixed sequence of the hot kernels at the bench size, for ncu:
-    FP64 and FP32 assembly (x2 each), FP32/FP64 SpMV (x3 each), one mixed solve."""
+    FP64 and FP32 assembly (x2 each), FP32/FP64 SpMV (x3 each), one mixed
+    solve with block-Jacobi CG and one with the multigrid-preconditioned CG."""
     pkg = load_package()
     nat = pkg._native
     prob = nh_problem(pkg, n=args.n)
@@ -483,6 +496,8 @@ def run_profile(args, device):
         A64.matvec(x64)
     nh_solve(pkg, prob, "mixed", steps=1, total_deg=6.0,
              linear={"cg": {"precond": "block_jacobi", "rtol": "adaptive", "atol": 0.0}})
+    nh_solve(pkg, prob, "mixed", steps=1, total_deg=6.0,
+             linear={"cg": {"precond": "gmg", "rtol": "adaptive", "atol": 0.0}})
     torch.cuda.synchronize()
     print(json.dumps({"profile": "done", "launches": nat.launch_count()}))
 
@@ -496,9 +511,12 @@ def warmstart_eval(pkg, ws, prob, net, n, seed, log=None, arms=None):
     # FP32 CG restarted inside FP64 refinement: on this high-contrast problem
     # it is the faster of the two mixed CG forms (reliable updates stall)
     linear_mixed = {"cg": dict(linear["cg"], reliable_delta=0.0)}
+    linear_gmg = {"cg": {"precond": "gmg", "rtol": "adaptive", "atol": 0.0, "maxiter": 2000}}
     preds = {"zero": None, "learned": ws.Predictor(net, galerkin=True),
              "learned_raw": ws.Predictor(net, galerkin=False)}
     arms = arms or [(p, s) for p in ("fp64", "mixed") for s in ("zero", "learned", "learned_raw")]
+    lin_of = {"fp64": ("fp64", linear), "mixed": ("mixed", linear_mixed),
+              "fp64_gmg": ("fp64", linear_gmg), "mixed_gmg": ("mixed", linear_gmg)}
     g = torch.Generator().manual_seed(seed)
     dev = prob.dev().device
     rows = []
@@ -508,9 +526,9 @@ def warmstart_eval(pkg, ws, prob, net, n, seed, log=None, arms=None):
         prob.set_patch(z0)
         prob.set_params(ws.cell_rho_to_torch(rho, dev))
         r = {}
-        for prec, start in arms:
-            opts = {"newton": {"rel_tol": 1e-8, "tol": 1e-14, "precision": prec,
-                               "linear": linear if prec == "fp64" else linear_mixed,
+        for arm, start in arms:
+            prec, lin = lin_of[arm]
+            opts = {"newton": {"rel_tol": 1e-8, "tol": 1e-14, "precision": prec, "linear": lin,
                                "rel_tol_reference": "zero", "return_info": True,
                                "warm_start": preds[start]}}
             torch.cuda.synchronize()
@@ -519,7 +537,7 @@ def warmstart_eval(pkg, ws, prob, net, n, seed, log=None, arms=None):
             (sol,), info = pkg.solver(prob, opts)
             e1.record()
             torch.cuda.synchronize()
-            r[f"{prec}_{start}"] = {"krylov": sum(info["krylov_iters"]), "newton": info["newton_iters"],
+            r[f"{arm}_{start}"] = {"krylov": sum(info["krylov_iters"]), "newton": info["newton_iters"],
                                     "s": e0.elapsed_time(e1) * 1e-3}
         rows.append(r)
         if log and (i + 1) % 20 == 0:

@@ -335,16 +335,19 @@ typedef struct FemMGLevel {
   const int32_t* cpos;
   const int32_t* ilo;
   const double* whi;
-  double lmax;
+  void* lmax;             /* device, 8 bytes: the level's Gershgorin bound (FP64), written by setup */
 } FemMGLevel;
 
-/* Setup (once per operator): coarse values by Galerkin products, the Jacobi
- * scaling and lmax of every level (written into levels[l].lmax; the call
- * synchronizes `stream` to read them).  _f32: with d_fine_f64 non-NULL,
- * level 0's values are first rounded from that FP64 operator. */
-FEM_API int fem_mg_setup_f64(int vec, int nlevels, FemMGLevel* levels, void* stream);
-FEM_API int fem_mg_setup_f32(int vec, int nlevels, FemMGLevel* levels, const double* d_fine_f64,
-                             void* stream);
+/* Setup (once per operator, launches only): coarse values by Galerkin
+ * products P^T (A P), the Jacobi scaling and the bound lmax of every level.
+ * d_scratch holds A P of one level (levels[0].n_brows * 27 * vec*vec values
+ * of the call's type; fem_mg_setup_scratch_bytes).  _f32: with d_fine_f64
+ * non-NULL, level 0's values are first rounded from that FP64 operator. */
+FEM_API size_t fem_mg_setup_scratch_bytes(int vec, int64_t fine_n_brows, int fp32);
+FEM_API int fem_mg_setup_f64(int vec, int nlevels, const FemMGLevel* levels, void* d_scratch,
+                             size_t scratch_bytes, void* stream);
+FEM_API int fem_mg_setup_f32(int vec, int nlevels, const FemMGLevel* levels, const double* d_fine_f64,
+                             void* d_scratch, size_t scratch_bytes, void* stream);
 /* z = V(rhs): one V-cycle with nu Chebyshev steps before and after on each
  * level and coarse_steps on the coarsest; ratio sets the smoothed interval
  * [lmax/ratio, lmax].  Launches only (no synchronization). */

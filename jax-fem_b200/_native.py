@@ -34,7 +34,7 @@ class FemMGLevel(ctypes.Structure):
                 ("vals", ctypes.c_void_p), ("dinv", ctypes.c_void_p), ("x", ctypes.c_void_p),
                 ("b", ctypes.c_void_p), ("r", ctypes.c_void_p), ("d0", ctypes.c_void_p), ("d1", ctypes.c_void_p),
                 ("cpos", ctypes.c_void_p), ("ilo", ctypes.c_void_p), ("whi", ctypes.c_void_p),
-                ("lmax", ctypes.c_double)]
+                ("lmax", ctypes.c_void_p)]
 
 _STATUS_NAMES = {
     FEM_ERR_ARG: "invalid argument",
@@ -75,8 +75,9 @@ _SIGS = {
     "fem_j2_commit": (I32, [DP, I32, I64, P, P, P, P, P, P, P, P, P, P]),
     "fem_j2_sensitivity": (I32, [DP, I32, I64, P, P, P, P, P, P, P, P, P, P, P, P, P, P]),
     "fem_stress_divergence": (I32, [I64, P, P, P, P, P]),
-    "fem_mg_setup_f64": (I32, [I32, I32, P, P]),
-    "fem_mg_setup_f32": (I32, [I32, I32, P, P, P]),
+    "fem_mg_setup_scratch_bytes": (SZ, [I32, I64, I32]),
+    "fem_mg_setup_f64": (I32, [I32, I32, P, P, SZ, P]),
+    "fem_mg_setup_f32": (I32, [I32, I32, P, P, P, SZ, P]),
     "fem_mg_vcycle_f64": (I32, [I32, I32, P, I32, I32, F64, P, P, P]),
     "fem_mg_vcycle_f32": (I32, [I32, I32, P, I32, I32, F64, P, P, P]),
     "fem_mg_pcg_workspace_bytes": (SZ, [I32, I64]),

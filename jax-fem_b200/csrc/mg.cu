@@ -7,17 +7,24 @@
 // A coarse level keeps every second node per direction (and the last node);
 // fine node i of a direction lies between coarse nodes ilo[i] and ilo[i]+1
 // with weight whi[i] on the upper one, so prolongation P is trilinear
-// interpolation and restriction is P^T.  Coarse operators are P^T A P,
-// computed per coarse block from the fine blocks (one lane per coarse block:
+// interpolation and restriction is P^T.  Coarse operators are P^T (A P): a
+// first pass forms B = A P per fine row (27 coarse columns at most), a second
+// pass sums the <= 27 fine rows of each coarse block (one thread per block:
 // fixed summation order, no atomics).
 //
 // Smoothing: Chebyshev iteration on D^-1 A over [lmax/ratio, lmax] with
-// lmax the Gershgorin bound of D^-1 A (D = the diagonal).  Each step is one
-// SpMV with its vector updates fused into the row epilogue.  Pre- and
+// lmax the Gershgorin bound of D^-1 A (D = the diagonal), kept on the device:
+// the kernels derive their Chebyshev coefficients from it, so setup and
+// V-cycles never wait for the host.  Each step is one SpMV with its vector
+// updates fused into the row epilogue.  Pre- and
 // post-smoothing apply the same polynomial, the coarsest level a longer one,
 // so a V-cycle is a fixed symmetric positive operator (a CG preconditioner).
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
+#include <map>
+#include <mutex>
+#include <string>
 #include <vector>
 
 #include "sparse.cuh"
@@ -47,33 +54,80 @@ __device__ __forceinline__ void fine_range(const int32_t* cpos, int64_t I, int64
   *hi = I < nc - 1 ? int64_t(cpos[I + 1]) - 1 : nf - 1;
 }
 
-// ---- Galerkin coarse operator: one warp per coarse node, lane = slot --------
+// ---- Galerkin coarse operator ---------------------------------------------------
+// Window of coarse columns of fine node i along one direction: A P (i, J) can
+// be non-zero only for J in base .. base+2, base = ilo[max(i-1, 0)].
+__device__ __forceinline__ int64_t col_base(const int32_t* ilo, int64_t i) { return ilo[i > 0 ? i - 1 : 0]; }
+
+// B[i][t] = sum_j A_ij w(j, J_t), J_t = base(i) + (t/9, t/3%3, t%3): one thread
+// per (fine node, window slot).
 template <int VEC, typename T>
-__global__ void rap_kernel(Lat F, const int32_t* __restrict__ fst, const T* __restrict__ fv, Lat C,
-                           const int32_t* __restrict__ cst, T* cv, const int32_t* cpos, const int32_t* ilo,
-                           const double* whi) {
+__global__ void ap_kernel(Lat F, const int32_t* __restrict__ fst, const T* __restrict__ fv, Lat C,
+                          const int32_t* ilo, const double* whi, T* B) {
   constexpr int VV = VEC * VEC;
-  const int lane = threadIdx.x & 31;
-  const int64_t warp = (int64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
-  const int64_t nwarps = (int64_t(gridDim.x) * blockDim.x) >> 5;
-  const int64_t Nc = C.n[0] * C.n[1] * C.n[2];
+  const int32_t* il[3] = {ilo, ilo + F.n[0], ilo + F.n[0] + F.n[1]};
+  const double* wh[3] = {whi, whi + F.n[0], whi + F.n[0] + F.n[1]};
+  const int64_t Nf = F.n[0] * F.n[1] * F.n[2];
+  for (int64_t g = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; g < Nf * 27; g += int64_t(gridDim.x) * blockDim.x) {
+    const int64_t i = g / 27;
+    const int t = int(g - i * 27);
+    const int64_t ii[3] = {i / (F.n[1] * F.n[2]), (i / F.n[2]) % F.n[1], i % F.n[2]};
+    const int td[3] = {t / 9, (t / 3) % 3, t % 3};
+    double w[3][3];  // w[d][k]: weight of column J_d at fine index ii[d] + k - 1
+    bool any = true;
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      const int64_t J = col_base(il[d], ii[d]) + td[d];
+      bool nz = false;
+#pragma unroll
+      for (int k = 0; k < 3; ++k) {
+        const int64_t j = ii[d] + k - 1;
+        w[d][k] = (J < C.n[d] && j >= 0 && j < F.n[d]) ? w1(il[d], wh[d], j, J) : 0.0;
+        nz = nz || w[d][k] != 0.0;
+      }
+      any = any && nz;
+    }
+    double acc[VV];
+#pragma unroll
+    for (int e = 0; e < VV; ++e) acc[e] = 0.0;
+    if (any) {
+      for (int kx = 0; kx < 3; ++kx) {
+        if (w[0][kx] == 0.0) continue;
+        for (int ky = 0; ky < 3; ++ky) {
+          if (w[1][ky] == 0.0) continue;
+          for (int kz = 0; kz < 3; ++kz) {
+            const double ww = w[0][kx] * w[1][ky] * w[2][kz];
+            if (ww == 0.0) continue;
+            const int32_t blk = fst[i * 27 + kx * 9 + ky * 3 + kz];
+            if (blk < 0) continue;
+            const T* av = fv + int64_t(blk) * VV;
+#pragma unroll
+            for (int e = 0; e < VV; ++e) acc[e] = fma(ww, double(av[e]), acc[e]);
+          }
+        }
+      }
+    }
+#pragma unroll
+    for (int e = 0; e < VV; ++e) B[g * VV + e] = T(acc[e]);
+  }
+}
+
+// A_c(I, J) = sum_i w(i, I) B[i][J - base(i)]: one thread per coarse block.
+template <int VEC, typename T>
+__global__ void ptap_kernel(Lat F, Lat C, const int32_t* __restrict__ cst, const T* __restrict__ B, T* cv,
+                            const int32_t* cpos, const int32_t* ilo, const double* whi) {
+  constexpr int VV = VEC * VEC;
   const int32_t* cp[3] = {cpos, cpos + C.n[0], cpos + C.n[0] + C.n[1]};
   const int32_t* il[3] = {ilo, ilo + F.n[0], ilo + F.n[0] + F.n[1]};
   const double* wh[3] = {whi, whi + F.n[0], whi + F.n[0] + F.n[1]};
-  if (lane >= 27) return;  // no warp-wide operations below
-  for (int64_t I = warp; I < Nc; I += nwarps) {
-    const int64_t Ic[3] = {I / (C.n[1] * C.n[2]), (I / C.n[2]) % C.n[1], I % C.n[2]};
-    const int s[3] = {lane / 9 - 1, (lane / 3) % 3 - 1, lane % 3 - 1};
-    int64_t J[3];
-    bool inside = true;
-#pragma unroll
-    for (int d = 0; d < 3; ++d) {
-      J[d] = Ic[d] + s[d];
-      inside = inside && J[d] >= 0 && J[d] < C.n[d];
-    }
-    if (!inside) continue;
-    const int32_t cblk = cst[I * 27 + lane];
+  const int64_t Nc = C.n[0] * C.n[1] * C.n[2];
+  for (int64_t g = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; g < Nc * 27; g += int64_t(gridDim.x) * blockDim.x) {
+    const int64_t I = g / 27;
+    const int s = int(g - I * 27);
+    const int32_t cblk = cst[g];
     if (cblk < 0) continue;
+    const int64_t Ic[3] = {I / (C.n[1] * C.n[2]), (I / C.n[2]) % C.n[1], I % C.n[2]};
+    const int64_t J[3] = {Ic[0] + s / 9 - 1, Ic[1] + (s / 3) % 3 - 1, Ic[2] + s % 3 - 1};
     int64_t lo[3], hi[3];
 #pragma unroll
     for (int d = 0; d < 3; ++d) fine_range(cp[d], Ic[d], C.n[d], F.n[d], &lo[d], &hi[d]);
@@ -82,27 +136,21 @@ __global__ void rap_kernel(Lat F, const int32_t* __restrict__ fst, const T* __re
     for (int e = 0; e < VV; ++e) acc[e] = 0.0;
     for (int64_t ix = lo[0]; ix <= hi[0]; ++ix) {
       const double wx = w1(il[0], wh[0], ix, Ic[0]);
-      if (wx == 0.0) continue;
+      const int64_t tx = J[0] - col_base(il[0], ix);
+      if (wx == 0.0 || tx < 0 || tx > 2) continue;
       for (int64_t iy = lo[1]; iy <= hi[1]; ++iy) {
         const double wy = w1(il[1], wh[1], iy, Ic[1]);
-        if (wy == 0.0) continue;
+        const int64_t ty = J[1] - col_base(il[1], iy);
+        if (wy == 0.0 || ty < 0 || ty > 2) continue;
         for (int64_t iz = lo[2]; iz <= hi[2]; ++iz) {
           const double wz = w1(il[2], wh[2], iz, Ic[2]);
-          if (wz == 0.0) continue;
+          const int64_t tz = J[2] - col_base(il[2], iz);
+          if (wz == 0.0 || tz < 0 || tz > 2) continue;
           const double wi = wx * wy * wz;
           const int64_t i = (ix * F.n[1] + iy) * F.n[2] + iz;
-          for (int o = 0; o < 27; ++o) {
-            const int64_t jx = ix + o / 9 - 1, jy = iy + (o / 3) % 3 - 1, jz = iz + o % 3 - 1;
-            if (jx < 0 || jx >= F.n[0] || jy < 0 || jy >= F.n[1] || jz < 0 || jz >= F.n[2]) continue;
-            const double wj = w1(il[0], wh[0], jx, J[0]) * w1(il[1], wh[1], jy, J[1]) * w1(il[2], wh[2], jz, J[2]);
-            if (wj == 0.0) continue;
-            const int32_t blk = fst[i * 27 + o];
-            if (blk < 0) continue;
-            const double ww = wi * wj;
-            const T* a = fv + int64_t(blk) * VV;
+          const T* bv = B + ((i * 27) + tx * 9 + ty * 3 + tz) * VV;
 #pragma unroll
-            for (int e = 0; e < VV; ++e) acc[e] = fma(ww, double(a[e]), acc[e]);
-          }
+          for (int e = 0; e < VV; ++e) acc[e] = fma(wi, double(bv[e]), acc[e]);
         }
       }
     }
@@ -218,6 +266,13 @@ __global__ void cast_kernel(int64_t n, const double* __restrict__ a, T* b) {
   for (int64_t k = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; k < n; k += int64_t(gridDim.x) * blockDim.x)
     b[k] = T(a[k]);
 }
+// level 0 values rounded from FP64: the count nnzb*vv is read from row_ptr
+template <typename T>
+__global__ void cast_vals_kernel(const int32_t* rp, int64_t n_brows, int vv, const double* __restrict__ a, T* b) {
+  const int64_t n = int64_t(rp[n_brows]) * vv;
+  for (int64_t k = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; k < n; k += int64_t(gridDim.x) * blockDim.x)
+    b[k] = T(a[k]);
+}
 template <typename T>
 __global__ void widen_kernel(int64_t n, const T* __restrict__ a, double* b) {
   for (int64_t k = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; k < n; k += int64_t(gridDim.x) * blockDim.x)
@@ -225,10 +280,28 @@ __global__ void widen_kernel(int64_t n, const T* __restrict__ a, double* b) {
 }
 
 // ---- Chebyshev smoothing ------------------------------------------------------
+// Coefficients of step k (k >= 1) of Chebyshev iteration on D^-1 A over
+// [lmax/ratio, lmax]: d_k = a d_{k-1} + c D^-1 r_k; step 0 is d_0 = D^-1 r_0 / theta.
+struct ChebCoef {
+  double inv_theta, a, c;
+};
+__device__ __forceinline__ ChebCoef cheb_coef(const void* lmax_bits, double ratio, int k) {
+  const double lmax = __longlong_as_double(*static_cast<const long long*>(lmax_bits));
+  const double lmin = lmax / ratio;
+  const double theta = 0.5 * (lmax + lmin), delta = 0.5 * (lmax - lmin), sigma = theta / delta;
+  double rho_prev = 1.0 / sigma, rho = rho_prev;
+  for (int j = 1; j <= k; ++j) {
+    rho_prev = rho;
+    rho = 1.0 / (2.0 * sigma - rho_prev);
+  }
+  return ChebCoef{1.0 / theta, rho * rho_prev, 2.0 * rho / delta};
+}
+
 // First step: (zero start) r = b, x = d; otherwise x += d; d = D^-1 r / theta.
 template <typename T>
 __global__ void cheb_first_kernel(int64_t n, const T* __restrict__ dinv, const T* b, T* r, T* d, T* x,
-                                  double inv_theta, int zero_start) {
+                                  const void* lmax, double ratio, int zero_start) {
+  const double inv_theta = cheb_coef(lmax, ratio, 0).inv_theta;
   for (int64_t k = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; k < n; k += int64_t(gridDim.x) * blockDim.x) {
     const T rk = zero_start ? b[k] : r[k];
     if (zero_start) r[k] = rk;
@@ -242,7 +315,9 @@ __global__ void cheb_first_kernel(int64_t n, const T* __restrict__ dinv, const T
 template <int VEC, typename T>
 __global__ void __launch_bounds__(kRowThreads, kRowBlocksPerSM)
     cheb_step_kernel(int64_t n_brows, const int32_t* rp, const int32_t* ci, const T* vals, const T* __restrict__ dold,
-                     T* dnew, T* r, T* x, const T* __restrict__ dinv, double a, double c) {
+                     T* dnew, T* r, T* x, const T* __restrict__ dinv, const void* lmax, double ratio, int step) {
+  const ChebCoef cf = cheb_coef(lmax, ratio, step);
+  const double a = cf.a, c = cf.c;
   bsr_rows<VEC, T, T>(
       n_brows, rp, ci, vals, [&](int64_t i) { return dold[i]; },
       [&](int64_t row, int comp, T q) {
@@ -282,15 +357,6 @@ __global__ void __launch_bounds__(kRowThreads, kRowBlocksPerSM)
 }
 
 // ---- host side -------------------------------------------------------------------
-struct Cheb {
-  double inv_theta, sigma, delta;
-};
-inline Cheb cheb_of(double lmax, double ratio) {
-  const double lmin = lmax / ratio;
-  const double theta = 0.5 * (lmax + lmin), delta = 0.5 * (lmax - lmin);
-  return Cheb{1.0 / theta, theta / delta, delta};
-}
-
 inline unsigned vgrid(int64_t n) {
   const int64_t b = (n + 255) / 256;
   const int64_t cap = int64_t(num_sms()) * 8;
@@ -305,8 +371,8 @@ int check_levels(int nlevels, const FemMGLevel* L) {
     const FemMGLevel& v = L[l];
     FEM_CHECK_ARG(v.nodes[0] >= 2 && v.nodes[1] >= 2 && v.nodes[2] >= 2, "level %d: lattice needs >= 2 nodes per direction", l);
     FEM_CHECK_ARG(v.n_brows == v.nodes[0] * v.nodes[1] * v.nodes[2], "level %d: n_brows != nodes product", l);
-    FEM_CHECK_ARG(v.row_ptr && v.col_idx && v.stencil && v.vals && v.dinv && v.r && v.d0 && v.d1,
-                  "level %d: NULL pattern, values or work vector", l);
+    FEM_CHECK_ARG(v.row_ptr && v.col_idx && v.stencil && v.vals && v.dinv && v.r && v.d0 && v.d1 && v.lmax,
+                  "level %d: NULL pattern, values, bound slot or work vector", l);
     FEM_CHECK_ARG(bsr_aligned(v.vals, v.col_idx), "level %d: vals and col_idx must be 16-byte aligned", l);
     if (l >= 1) {
       FEM_CHECK_ARG(v.x && v.b && v.cpos && v.ilo && v.whi, "level %d: NULL transfer data or work vector", l);
@@ -326,42 +392,40 @@ int ensure_attrs() {
   return FEM_OK;
 }
 
+size_t setup_scratch_bytes(int vec, int64_t fine_n_brows, size_t elem) {
+  return size_t(fine_n_brows) * 27 * vec * vec * elem;
+}
+
 template <int VEC, typename T>
-int setup_impl(int nlevels, FemMGLevel* L, const double* fine64, cudaStream_t st) {
+int setup_impl(int nlevels, const FemMGLevel* L, const double* fine64, void* scratch, size_t scratch_bytes,
+               cudaStream_t st) {
   int rc = check_levels<VEC, T>(nlevels, L);
   if (rc != FEM_OK) return rc;
   constexpr int VV = VEC * VEC;
+  FEM_CHECK_ARG(nlevels == 1 || (scratch != nullptr && scratch_bytes >= setup_scratch_bytes(VEC, L[0].n_brows, sizeof(T))),
+                "setup scratch too small (%zu < %zu)", scratch_bytes, setup_scratch_bytes(VEC, L[0].n_brows, sizeof(T)));
+  T* B = static_cast<T*>(scratch);
   for (int l = 0; l < nlevels; ++l) {
     if (l == 0 && fine64 != nullptr) {
-      // nnzb of level 0 from its row pointer (one int read)
-      int32_t nnzb = 0;
-      FEM_CUDA_TRY(cudaMemcpyAsync(&nnzb, L[0].row_ptr + L[0].n_brows, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
-      FEM_CUDA_TRY(cudaStreamSynchronize(st));
-      const int64_t n = int64_t(nnzb) * VV;
-      cast_kernel<T><<<vgrid(n), 256, 0, st>>>(n, fine64, static_cast<T*>(L[0].vals));
+      cast_vals_kernel<T><<<unsigned(num_sms()) * 8, 256, 0, st>>>(L[0].row_ptr, L[0].n_brows, VV, fine64,
+                                                                  static_cast<T*>(L[0].vals));
       FEM_LAUNCH_CHECK();
     }
     if (l >= 1) {
-      const int64_t nc = L[l].n_brows;
-      const int64_t blocks = (nc * 32 + 255) / 256;
-      const unsigned grid = unsigned(blocks < int64_t(num_sms()) * 32 ? blocks : int64_t(num_sms()) * 32);
-      rap_kernel<VEC, T><<<grid, 256, 0, st>>>(lat_of(L[l - 1]), L[l - 1].stencil, static_cast<const T*>(L[l - 1].vals),
-                                                lat_of(L[l]), L[l].stencil, static_cast<T*>(L[l].vals), L[l].cpos,
-                                                L[l].ilo, L[l].whi);
+      const Lat F = lat_of(L[l - 1]), C = lat_of(L[l]);
+      ap_kernel<VEC, T><<<vgrid(L[l - 1].n_brows * 27), 256, 0, st>>>(F, L[l - 1].stencil,
+                                                                     static_cast<const T*>(L[l - 1].vals), C, L[l].ilo,
+                                                                     L[l].whi, B);
+      FEM_LAUNCH_CHECK();
+      ptap_kernel<VEC, T><<<vgrid(L[l].n_brows * 27), 256, 0, st>>>(F, C, L[l].stencil, B, static_cast<T*>(L[l].vals),
+                                                                   L[l].cpos, L[l].ilo, L[l].whi);
       FEM_LAUNCH_CHECK();
     }
-    unsigned long long* bits = static_cast<unsigned long long*>(L[l].d0);  // scratch (8 bytes of d0)
-    FEM_CUDA_TRY(cudaMemsetAsync(bits, 0, sizeof(unsigned long long), st));
+    FEM_CUDA_TRY(cudaMemsetAsync(L[l].lmax, 0, sizeof(unsigned long long), st));
     jacobi_setup_kernel<VEC, T><<<vgrid(L[l].n_brows * VEC), 256, 0, st>>>(
-        L[l].n_brows, L[l].stencil, static_cast<const T*>(L[l].vals), static_cast<T*>(L[l].dinv), bits);
+        L[l].n_brows, L[l].stencil, static_cast<const T*>(L[l].vals), static_cast<T*>(L[l].dinv),
+        static_cast<unsigned long long*>(L[l].lmax));
     FEM_LAUNCH_CHECK();
-    unsigned long long hb = 0;
-    FEM_CUDA_TRY(cudaMemcpyAsync(&hb, bits, sizeof(hb), cudaMemcpyDeviceToHost, st));
-    FEM_CUDA_TRY(cudaStreamSynchronize(st));
-    double lm;
-    std::memcpy(&lm, &hb, sizeof(lm));
-    FEM_CHECK_ARG(std::isfinite(lm) && lm > 0.0, "level %d: operator has a zero or non-finite diagonal", l);
-    L[l].lmax = lm;
   }
   return ensure_attrs<VEC, T>();
 }
@@ -372,23 +436,18 @@ template <int VEC, typename T>
 int smooth(const FemMGLevel& L, const T* b, T* x, int m, double ratio, bool zero_start, bool want_residual,
            cudaStream_t st) {
   const int64_t n = L.n_brows * VEC;
-  const Cheb ch = cheb_of(L.lmax, ratio);
   T* r = static_cast<T*>(L.r);
   T* d[2] = {static_cast<T*>(L.d0), static_cast<T*>(L.d1)};
   const T* dinv = static_cast<const T*>(L.dinv);
   const T* vals = static_cast<const T*>(L.vals);
   const unsigned rg = row_grid<T>(L.n_brows);
-  cheb_first_kernel<T><<<vgrid(n), 256, 0, st>>>(n, dinv, b, r, d[0], x, ch.inv_theta, zero_start ? 1 : 0);
+  cheb_first_kernel<T><<<vgrid(n), 256, 0, st>>>(n, dinv, b, r, d[0], x, L.lmax, ratio, zero_start ? 1 : 0);
   FEM_LAUNCH_CHECK();
-  double rho_old = 1.0 / ch.sigma;
   int cur = 0;
   for (int k = 1; k < m; ++k) {
-    const double rho = 1.0 / (2.0 * ch.sigma - rho_old);
     cheb_step_kernel<VEC, T><<<rg, kRowThreads, bsr_rows_smem(), st>>>(L.n_brows, L.row_ptr, L.col_idx, vals, d[cur],
-                                                                      d[cur ^ 1], r, x, dinv, rho * rho_old,
-                                                                      2.0 * rho / ch.delta);
+                                                                      d[cur ^ 1], r, x, dinv, L.lmax, ratio, k);
     FEM_LAUNCH_CHECK();
-    rho_old = rho;
     cur ^= 1;
   }
   if (want_residual) {
@@ -425,8 +484,6 @@ int vcycle_impl(int nlevels, const FemMGLevel* L, int nu, int coarse_steps, doub
   FEM_CHECK_ARG(rhs != nullptr && z != nullptr, "rhs and z must not be NULL");
   FEM_CHECK_ARG(nu >= 1 && nu <= 16 && coarse_steps >= 1 && coarse_steps <= 512, "nu in [1,16], coarse_steps in [1,512]");
   FEM_CHECK_ARG(ratio > 1.0, "ratio must exceed 1");
-  for (int l = 0; l < nlevels; ++l)
-    FEM_CHECK_ARG(L[l].lmax > 0.0, "level %d has no lmax: run fem_mg_setup first", l);
   return vcycle_level<VEC, T>(0, nlevels, L, nu, coarse_steps, ratio, rhs, z, st);
 }
 
@@ -541,6 +598,37 @@ __global__ void pcg_update_kernel(int64_t n, double* x, double* r, const double*
 
 inline size_t al256(size_t x) { return (x + 255) & ~size_t(255); }
 
+// Cached CUDA graphs of PCG iteration chunks (V-cycles included): the launch
+// sequence depends only on the pointers and parameters in the key, so one
+// capture serves every later solve on the same hierarchy and buffers.
+// FEM_MG_GRAPHS=0 in the environment launches every kernel directly.
+bool mg_graphs_enabled() {
+  static int on = -1;
+  if (on < 0) {
+    const char* e = std::getenv("FEM_MG_GRAPHS");
+    on = (e != nullptr && e[0] == '0') ? 0 : 1;
+  }
+  return on == 1;
+}
+std::mutex g_mg_mu;
+struct MGGraph {
+  cudaGraphExec_t exec;
+  int64_t kernels;  // launches one replay stands for
+};
+std::map<std::string, MGGraph>& mg_graph_cache() {
+  static std::map<std::string, MGGraph> m;
+  return m;
+}
+cudaStream_t mg_capture_stream() {
+  static std::mutex mu;
+  static cudaStream_t s[64] = {nullptr};
+  int dev = 0;
+  cudaGetDevice(&dev);
+  std::lock_guard<std::mutex> lock(mu);
+  if (s[dev] == nullptr && cudaStreamCreateWithFlags(&s[dev], cudaStreamNonBlocking) != cudaSuccess) s[dev] = nullptr;
+  return s[dev];
+}
+
 size_t pcg_workspace_bytes(int vec, int64_t n_brows) {
   const size_t n = size_t(n_brows) * vec;
   return 256 + 256 + al256(size_t(num_sms()) * 8 * 4 * sizeof(double)) + 4 * al256(n * sizeof(double));
@@ -604,23 +692,81 @@ int pcg_impl(int64_t n_brows, const int32_t* rp, const int32_t* ci, const double
     if ((rc = read_state()) != FEM_OK) return rc;
     if (hs->status != PS_RUNNING || launched >= maxiter) break;
     const int chunk = check_every < maxiter - launched ? check_every : maxiter - launched;
-    for (int k = 0; k < chunk; ++k) {
-      if (fp32) {
-        // r.z needs z in FP64: widen the FP32 V-cycle output into z
-        if ((rc = vcycle_level<VEC, float>(0, nlevels, L, nu, coarse_steps, ratio, r32, z32, st)) != FEM_OK) return rc;
-        widen_kernel<float><<<vg, 256, 0, st>>>(n, z32, z);
+    auto launch_chunk = [&](cudaStream_t ls) -> int {
+      for (int k = 0; k < chunk; ++k) {
+        int rc2;
+        if (fp32) {
+          // r.z needs z in FP64: widen the FP32 V-cycle output into z
+          if ((rc2 = vcycle_level<VEC, float>(0, nlevels, L, nu, coarse_steps, ratio, r32, z32, ls)) != FEM_OK)
+            return rc2;
+          widen_kernel<float><<<vg, 256, 0, ls>>>(n, z32, z);
+          FEM_LAUNCH_CHECK();
+        } else {
+          if ((rc2 = vcycle_level<VEC, double>(0, nlevels, L, nu, coarse_steps, ratio, r, z, ls)) != FEM_OK)
+            return rc2;
+        }
+        pcg_rz_kernel<<<vg, 256, 0, ls>>>(n, r, z, partials, counter, S);
         FEM_LAUNCH_CHECK();
-      } else {
-        if ((rc = vcycle_level<VEC, double>(0, nlevels, L, nu, coarse_steps, ratio, r, z, st)) != FEM_OK) return rc;
+        pcg_dir_kernel<double><<<vg, 256, 0, ls>>>(n, z, pv, S);
+        FEM_LAUNCH_CHECK();
+        pcg_spmv_kernel<VEC><<<rg, kRowThreads, bsr_rows_smem(), ls>>>(n_brows, rp, ci, vals, pv, q, partials, counter,
+                                                                        S);
+        FEM_LAUNCH_CHECK();
+        pcg_update_kernel<<<vg, 256, 0, ls>>>(n, x, r, pv, q, r32, partials, counter, S);
+        FEM_LAUNCH_CHECK();
       }
-      pcg_rz_kernel<<<vg, 256, 0, st>>>(n, r, z, partials, counter, S);
-      FEM_LAUNCH_CHECK();
-      pcg_dir_kernel<double><<<vg, 256, 0, st>>>(n, z, pv, S);
-      FEM_LAUNCH_CHECK();
-      pcg_spmv_kernel<VEC><<<rg, kRowThreads, bsr_rows_smem(), st>>>(n_brows, rp, ci, vals, pv, q, partials, counter, S);
-      FEM_LAUNCH_CHECK();
-      pcg_update_kernel<<<vg, 256, 0, st>>>(n, x, r, pv, q, r32, partials, counter, S);
-      FEM_LAUNCH_CHECK();
+      return FEM_OK;
+    };
+    cudaGraphExec_t exec = nullptr;
+    int64_t nkern = 0;
+    if (mg_graphs_enabled()) {
+      std::string key(reinterpret_cast<const char*>(L), sizeof(FemMGLevel) * size_t(nlevels));
+      const void* ptrs[] = {rp, ci, vals, b, x, work};
+      key.append(reinterpret_cast<const char*>(ptrs), sizeof(ptrs));
+      const double params[] = {double(nlevels), double(fp32), double(nu), double(coarse_steps), ratio, double(chunk),
+                               double(n_brows), double(VEC)};
+      key.append(reinterpret_cast<const char*>(params), sizeof(params));
+      int dev = 0;
+      cudaGetDevice(&dev);
+      key.append(reinterpret_cast<const char*>(&dev), sizeof(dev));
+      {
+        std::lock_guard<std::mutex> lock(g_mg_mu);
+        auto it = mg_graph_cache().find(key);
+        if (it != mg_graph_cache().end()) {
+          exec = it->second.exec;
+          nkern = it->second.kernels;
+        }
+      }
+      if (exec == nullptr) {
+        cudaStream_t cap = mg_capture_stream();
+        if (cap != nullptr && cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
+          const int64_t c0 = launch_counter().load();
+          const int lrc = launch_chunk(cap);
+          nkern = launch_counter().load() - c0;
+          launch_counter().fetch_sub(nkern, std::memory_order_relaxed);  // counted when replayed
+          cudaGraph_t g = nullptr;
+          const cudaError_t ec = cudaStreamEndCapture(cap, &g);
+          if (lrc == FEM_OK && ec == cudaSuccess && g != nullptr && cudaGraphInstantiate(&exec, g, 0) == cudaSuccess) {
+            std::lock_guard<std::mutex> lock(g_mg_mu);
+            auto& m = mg_graph_cache();
+            if (m.size() >= 32) {  // bounded: drop everything (hierarchies were rebuilt)
+              for (auto& kv : m) cudaGraphExecDestroy(kv.second.exec);
+              m.clear();
+            }
+            m[key] = MGGraph{exec, nkern};
+          } else {
+            exec = nullptr;
+          }
+          if (g != nullptr) cudaGraphDestroy(g);
+          cudaGetLastError();  // a failed capture falls back to direct launches
+        }
+      }
+    }
+    if (exec != nullptr) {
+      FEM_CUDA_TRY(cudaGraphLaunch(exec, st));
+      launch_counter().fetch_add(nkern, std::memory_order_relaxed);
+    } else if ((rc = launch_chunk(st)) != FEM_OK) {
+      return rc;
     }
     launched += chunk;
   }
@@ -648,16 +794,22 @@ int pcg_impl(int64_t n_brows, const int32_t* rp, const int32_t* ci, const double
 
 using namespace fem;
 
-extern "C" int fem_mg_setup_f64(int vec, int nlevels, FemMGLevel* levels, void* stream) {
-  FEM_CHECK_ARG(vec == 1 || vec == 3, "vec must be 1 or 3");
-  return vec == 3 ? setup_impl<3, double>(nlevels, levels, nullptr, as_stream(stream))
-                  : setup_impl<1, double>(nlevels, levels, nullptr, as_stream(stream));
+extern "C" size_t fem_mg_setup_scratch_bytes(int vec, int64_t fine_n_brows, int fp32) {
+  return setup_scratch_bytes(vec, fine_n_brows, fp32 ? sizeof(float) : sizeof(double));
 }
 
-extern "C" int fem_mg_setup_f32(int vec, int nlevels, FemMGLevel* levels, const double* d_fine_f64, void* stream) {
+extern "C" int fem_mg_setup_f64(int vec, int nlevels, const FemMGLevel* levels, void* d_scratch, size_t scratch_bytes,
+                                void* stream) {
   FEM_CHECK_ARG(vec == 1 || vec == 3, "vec must be 1 or 3");
-  return vec == 3 ? setup_impl<3, float>(nlevels, levels, d_fine_f64, as_stream(stream))
-                  : setup_impl<1, float>(nlevels, levels, d_fine_f64, as_stream(stream));
+  return vec == 3 ? setup_impl<3, double>(nlevels, levels, nullptr, d_scratch, scratch_bytes, as_stream(stream))
+                  : setup_impl<1, double>(nlevels, levels, nullptr, d_scratch, scratch_bytes, as_stream(stream));
+}
+
+extern "C" int fem_mg_setup_f32(int vec, int nlevels, const FemMGLevel* levels, const double* d_fine_f64,
+                                void* d_scratch, size_t scratch_bytes, void* stream) {
+  FEM_CHECK_ARG(vec == 1 || vec == 3, "vec must be 1 or 3");
+  return vec == 3 ? setup_impl<3, float>(nlevels, levels, d_fine_f64, d_scratch, scratch_bytes, as_stream(stream))
+                  : setup_impl<1, float>(nlevels, levels, d_fine_f64, d_scratch, scratch_bytes, as_stream(stream));
 }
 
 extern "C" int fem_mg_vcycle_f64(int vec, int nlevels, const FemMGLevel* levels, int nu, int coarse_steps,
@@ -696,8 +848,6 @@ extern "C" int fem_mg_pcg_solve(int vec, int64_t n_brows, const int32_t* d_row_p
   if (rc != FEM_OK) return rc;
   FEM_CHECK_ARG(nu >= 1 && nu <= 16 && coarse_steps >= 1 && coarse_steps <= 512 && ratio > 1.0,
                 "nu in [1,16], coarse_steps in [1,512], ratio > 1");
-  for (int l = 0; l < nlevels; ++l)
-    FEM_CHECK_ARG(levels[l].lmax > 0.0, "level %d has no lmax: run the setup first", l);
   auto st = as_stream(stream);
   return vec == 3 ? pcg_impl<3>(n_brows, d_row_ptr, d_col_idx, d_vals, d_b, d_x, rtol, atol, maxiter, check_every,
                                 nlevels, levels, levels_fp32, nu, coarse_steps, ratio, d_work, work_bytes, h_iters,

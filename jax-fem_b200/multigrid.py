@@ -116,6 +116,7 @@ class Multigrid:
         self.nlevels = 0
         self.level_nodes = []
         self.mats = []  # per level (row_ptr, col_idx, values or None for level 0 in FP64), for inspection
+        self._lmax = torch.zeros(max_levels, dtype=torch.int64, device=dev)  # FP64 bits, written by setup
         fine_rp, fine_ci = dv.row_ptr.cpu().numpy(), dv.col_idx.cpu().numpy()
         transfer = None  # (cpos, ilo, whi) from the finer level to this one
         while True:
@@ -145,6 +146,7 @@ class Multigrid:
                 L.vals = vals.data_ptr()
             if transfer is not None:
                 L.cpos, L.ilo, L.whi = (t.data_ptr() for t in transfer)
+            L.lmax = self._lmax.data_ptr() + 8 * l
             self._keep += [rp_d, ci_d, st_d, vals, *bufs.values(), *(transfer or ())]
             self.level_nodes.append(n)
             self.mats.append((rp_d, ci_d, vals))
@@ -158,6 +160,8 @@ class Multigrid:
                         torch.from_numpy(np.concatenate([q[2] for q in parts]).astype(np.int32)).to(dev),
                         torch.from_numpy(np.concatenate([q[3] for q in parts]).astype(np.float64)).to(dev))
         self._work = None
+        nb = nat.lib().fem_mg_setup_scratch_bytes(self.vec, self.levels[0].n_brows, int(fp32))
+        self._scratch = torch.empty(max(int(nb), 16), dtype=torch.uint8, device=dev)
 
     def setup(self, A):
         """Coarse operators and smoother bounds for the FP64 operator A
@@ -167,22 +171,24 @@ class Multigrid:
             raise TypeError("the multigrid hierarchy is formed from the FP64 operator")
         if self.fp32:
             nat.check(lib.fem_mg_setup_f32(self.vec, self.nlevels, ctypes.byref(self.levels), nat.ptr(A.vals),
-                                           nat.stream_ptr()), "mg_setup_f32")
+                                           nat.ptr(self._scratch), self._scratch.numel(), nat.stream_ptr()),
+                      "mg_setup_f32")
         else:
             self.levels[0].vals = A.vals.data_ptr()
             self._keep.append(A.vals)
-            nat.check(lib.fem_mg_setup_f64(self.vec, self.nlevels, ctypes.byref(self.levels), nat.stream_ptr()),
-                      "mg_setup_f64")
+            nat.check(lib.fem_mg_setup_f64(self.vec, self.nlevels, ctypes.byref(self.levels), nat.ptr(self._scratch),
+                                           self._scratch.numel(), nat.stream_ptr()), "mg_setup_f64")
 
     def lmax(self):
-        return [self.levels[l].lmax for l in range(self.nlevels)]
+        """Per-level Gershgorin bounds of the Jacobi-scaled operators (reads the device)."""
+        return self._lmax[: self.nlevels].view(torch.float64).tolist()
 
-    def vcycle(self, rhs, z, nu=2, coarse_steps=24, ratio=10.0):
+    def vcycle(self, rhs, z, nu=2, coarse_steps=8, ratio=25.0):
         fn = nat.lib().fem_mg_vcycle_f32 if self.fp32 else nat.lib().fem_mg_vcycle_f64
         nat.check(fn(self.vec, self.nlevels, ctypes.byref(self.levels), nu, coarse_steps, float(ratio),
                      nat.ptr(rhs), nat.ptr(z), nat.stream_ptr()), "mg_vcycle")
 
-    def solve(self, A, b, x, rtol, atol=0.0, maxiter=1000, nu=2, coarse_steps=24, ratio=10.0, check_every=4):
+    def solve(self, A, b, x, rtol, atol=0.0, maxiter=1000, nu=2, coarse_steps=8, ratio=25.0, check_every=4):
         """CG on A x = b (FP64) with one V-cycle per iteration; x holds the
         initial guess.  Returns (iterations, true relative residual)."""
         lib = nat.lib()
