@@ -1,0 +1,46 @@
+"""The bench's multi-GPU form is replicas: each rank solves its own copy of
+the workload and the job time is the max over ranks (one scalar all-reduce).
+Checked here on CPU with two gloo ranks; the reference arm runs on rank 0
+only."""
+import os
+import socket
+
+import pytest
+import torch
+import torch.distributed as dist
+import torch.multiprocessing as mp
+
+
+def _free_port():
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
+
+
+def _worker(rank, world, port, out):
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        import bench
+        t = bench.reduce_max(0.5 + rank, world, torch.device("cpu"))
+
+        class A:
+            n, steps, warmup = 4, 1, 0
+            ref_newton_iters, ref_krylov_iters = 1, 1
+        ref = bench.run_reference(A, rank, world) if rank == 1 else "skipped"
+        out[rank] = (t, ref)
+        dist.barrier()
+    finally:
+        dist.destroy_process_group()
+
+
+def test_replica_max_over_ranks_gloo():
+    world = 2
+    port = _free_port()
+    with mp.Manager() as m:
+        out = m.dict()
+        mp.spawn(_worker, args=(world, port, out), nprocs=world, join=True)
+        res = dict(out)
+    assert res[0][0] == pytest.approx(1.5) and res[1][0] == pytest.approx(1.5)
+    assert res[1][1] is None  # the reference arm does no work off rank 0
