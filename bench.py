@@ -42,15 +42,23 @@ METRIC = "time-to-solve @rel.res 1e-8: mixed+learned vs plain on B200; assembly 
 # workloads (shapes and values of the benchmark configurations)
 # ---------------------------------------------------------------------------
 
+def _left(p):
+    return np.isclose(p[0], 0.0, atol=1e-5)
+
+
+def _right(p):
+    return np.isclose(p[0], 1.0, atol=1e-5)
+
+
+def _zero(p):
+    return 0.0 * p[0]
+
+
 def rotation_bc(theta):
-    """x=0 clamped; x=1: u_x=0, (y,z) rotated by theta about (y,z)=(0.5,0.5)."""
+    """x=0 clamped; x=1: u_x=0, (y,z) rotated by theta about (y,z)=(0.5,0.5).
+    The faces' location functions are defined once, as a user script would;
+    only the value functions change with the load step."""
     c, s = math.cos(theta), math.sin(theta)
-
-    def left(p):
-        return np.isclose(p[0], 0.0, atol=1e-5)
-
-    def right(p):
-        return np.isclose(p[0], 1.0, atol=1e-5)
 
     def uy(p):
         return 0.5 + (p[1] - 0.5) * c - (p[2] - 0.5) * s - p[1]
@@ -58,8 +66,7 @@ def rotation_bc(theta):
     def uz(p):
         return 0.5 + (p[1] - 0.5) * s + (p[2] - 0.5) * c - p[2]
 
-    z = lambda p: 0.0 * p[0]  # noqa: E731
-    return [[left] * 3 + [right] * 3, [0, 1, 2] * 2, [z, z, z, z, uy, uz]]
+    return [[_left] * 3 + [_right] * 3, [0, 1, 2] * 2, [_zero, _zero, _zero, _zero, uy, uz]]
 
 
 def nh_problem(pkg, n=50, E=10.0, nu=0.3):

@@ -59,56 +59,55 @@ __device__ __forceinline__ void fine_range(const int32_t* cpos, int64_t I, int64
 // be non-zero only for J in base .. base+2, base = ilo[max(i-1, 0)].
 __device__ __forceinline__ int64_t col_base(const int32_t* ilo, int64_t i) { return ilo[i > 0 ? i - 1 : 0]; }
 
-// B[i][t] = sum_j A_ij w(j, J_t), J_t = base(i) + (t/9, t/3%3, t%3): one thread
-// per (fine node, window slot).
+// B[i][t] = sum_j A_ij w(j, J_t), J_t = base(i) + (t/9, t/3%3, t%3): one warp
+// per fine row.  Lane o stages the row's block of neighbour offset o in shared
+// memory (the row's blocks are contiguous); lane t then forms window slot t
+// from the 27 staged blocks.
+constexpr int kApWarps = 8;
 template <int VEC, typename T>
-__global__ void ap_kernel(Lat F, const int32_t* __restrict__ fst, const T* __restrict__ fv, Lat C,
-                          const int32_t* ilo, const double* whi, T* B) {
+__global__ void __launch_bounds__(kApWarps * 32) ap_kernel(Lat F, const int32_t* __restrict__ fst,
+                                                           const T* __restrict__ fv, Lat C, const int32_t* ilo,
+                                                           const double* whi, T* B) {
   constexpr int VV = VEC * VEC;
+  __shared__ T sA[kApWarps][27][VV];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   const int32_t* il[3] = {ilo, ilo + F.n[0], ilo + F.n[0] + F.n[1]};
   const double* wh[3] = {whi, whi + F.n[0], whi + F.n[0] + F.n[1]};
   const int64_t Nf = F.n[0] * F.n[1] * F.n[2];
-  for (int64_t g = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; g < Nf * 27; g += int64_t(gridDim.x) * blockDim.x) {
-    const int64_t i = g / 27;
-    const int t = int(g - i * 27);
+  const int64_t w0 = int64_t(blockIdx.x) * kApWarps + wid, nw = int64_t(gridDim.x) * kApWarps;
+  for (int64_t i = w0; i < Nf; i += nw) {
+    __syncwarp();  // the previous row's stage is no longer read
+    if (lane < 27) {
+      const int32_t blk = fst[i * 27 + lane];
+#pragma unroll
+      for (int e = 0; e < VV; ++e) sA[wid][lane][e] = blk >= 0 ? fv[int64_t(blk) * VV + e] : T(0);
+    }
+    __syncwarp();
+    if (lane >= 27) continue;
     const int64_t ii[3] = {i / (F.n[1] * F.n[2]), (i / F.n[2]) % F.n[1], i % F.n[2]};
-    const int td[3] = {t / 9, (t / 3) % 3, t % 3};
+    const int td[3] = {lane / 9, (lane / 3) % 3, lane % 3};
     double w[3][3];  // w[d][k]: weight of column J_d at fine index ii[d] + k - 1
-    bool any = true;
 #pragma unroll
     for (int d = 0; d < 3; ++d) {
       const int64_t J = col_base(il[d], ii[d]) + td[d];
-      bool nz = false;
 #pragma unroll
       for (int k = 0; k < 3; ++k) {
         const int64_t j = ii[d] + k - 1;
         w[d][k] = (J < C.n[d] && j >= 0 && j < F.n[d]) ? w1(il[d], wh[d], j, J) : 0.0;
-        nz = nz || w[d][k] != 0.0;
       }
-      any = any && nz;
     }
     double acc[VV];
 #pragma unroll
     for (int e = 0; e < VV; ++e) acc[e] = 0.0;
-    if (any) {
-      for (int kx = 0; kx < 3; ++kx) {
-        if (w[0][kx] == 0.0) continue;
-        for (int ky = 0; ky < 3; ++ky) {
-          if (w[1][ky] == 0.0) continue;
-          for (int kz = 0; kz < 3; ++kz) {
-            const double ww = w[0][kx] * w[1][ky] * w[2][kz];
-            if (ww == 0.0) continue;
-            const int32_t blk = fst[i * 27 + kx * 9 + ky * 3 + kz];
-            if (blk < 0) continue;
-            const T* av = fv + int64_t(blk) * VV;
 #pragma unroll
-            for (int e = 0; e < VV; ++e) acc[e] = fma(ww, double(av[e]), acc[e]);
-          }
-        }
-      }
+    for (int o = 0; o < 27; ++o) {
+      const double ww = w[0][o / 9] * w[1][(o / 3) % 3] * w[2][o % 3];
+      if (ww == 0.0) continue;
+#pragma unroll
+      for (int e = 0; e < VV; ++e) acc[e] = fma(ww, double(sA[wid][o][e]), acc[e]);
     }
 #pragma unroll
-    for (int e = 0; e < VV; ++e) B[g * VV + e] = T(acc[e]);
+    for (int e = 0; e < VV; ++e) B[(i * 27 + lane) * VV + e] = T(acc[e]);
   }
 }
 
@@ -413,7 +412,9 @@ int setup_impl(int nlevels, const FemMGLevel* L, const double* fine64, void* scr
     }
     if (l >= 1) {
       const Lat F = lat_of(L[l - 1]), C = lat_of(L[l]);
-      ap_kernel<VEC, T><<<vgrid(L[l - 1].n_brows * 27), 256, 0, st>>>(F, L[l - 1].stencil,
+      const int64_t apb = (L[l - 1].n_brows + kApWarps - 1) / kApWarps;
+      const unsigned apg = unsigned(apb < int64_t(num_sms()) * 16 ? apb : int64_t(num_sms()) * 16);
+      ap_kernel<VEC, T><<<apg, kApWarps * 32, 0, st>>>(F, L[l - 1].stencil,
                                                                      static_cast<const T*>(L[l - 1].vals), C, L[l].ilo,
                                                                      L[l].whi, B);
       FEM_LAUNCH_CHECK();

@@ -12,6 +12,8 @@ batched: a function is first called once with the coordinate axes as arrays
 kept only if it agrees with point-by-point calls on a sample; otherwise it is
 called point by point.
 """
+import weakref
+
 import numpy as np
 
 # basix hexahedron facets (vertex lists in basix numbering) and outward normals,
@@ -57,6 +59,12 @@ def face_quadrature(face):
     return pts, np.full(4, 0.25)
 
 
+# Functions whose batched evaluation was confirmed against point-wise calls
+# (a property of the function's code): later calls with the same function
+# object skip the point-wise sample.  Weak keys: no id reuse after collection.
+_BATCHED_OK = weakref.WeakKeyDictionary()
+
+
 def _batched_or_pointwise(fn, args, out_tail, sample=8):
     """Evaluate fn over leading axis of each array in ``args`` (see module doc)."""
     n = len(args[0])
@@ -76,10 +84,20 @@ def _batched_or_pointwise(fn, args, out_tail, sample=8):
             batched = np.moveaxis(r, -1, 0)
     except Exception:  # noqa: BLE001 - fall back to point-by-point
         batched = None
+    key = (len(args), out_tail)
+    try:
+        if batched is not None and key in _BATCHED_OK.get(fn, ()):
+            return np.array(batched)
+    except TypeError:  # not weak-referenceable
+        pass
     rng = np.random.default_rng(0)
     idx = np.unique(np.concatenate([[0, n - 1], rng.integers(0, n, size=min(sample, n))]))
     ref = pointwise(idx)
     if batched is not None and np.array_equal(np.asarray(batched[idx], dtype=np.float64), ref):
+        try:
+            _BATCHED_OK.setdefault(fn, set()).add(key)
+        except TypeError:
+            pass
         return np.array(batched)
     return pointwise(np.arange(n))
 
