@@ -8,7 +8,9 @@
   direct solution (1e-8) in far fewer iterations than block-Jacobi CG, with
   the hierarchy in FP64 and in FP32;
 - Newton with precond 'gmg' (plain and mixed) matches the FP64 oracle
-  (1e-8 / 1e-6), as the block-Jacobi paths do."""
+  (1e-8 / 1e-6), as the block-Jacobi paths do;
+- the scalar (Laplace) hierarchy solves Poisson to the direct solution;
+- the SIMP adjoint through 'gmg' gives the block-Jacobi path's gradient."""
 import importlib
 import math
 
@@ -152,3 +154,53 @@ def test_newton_gmg_matches_oracle(pkg, cuda, precision, rtol):
     r = np.linalg.norm(op.apply_bc_vec(op.residual(sol), sol))
     assert r / r0 <= 1e-8
     assert max(info["krylov_iters"]) < 60
+
+
+@pytest.mark.gpu
+def test_scalar_poisson_multigrid(pkg, cuda):
+    """vec = 1 (Laplace): multigrid CG on a Poisson problem matches the
+    direct solve (1e-8), and so does Newton with precond 'gmg'."""
+    mg, S = _mods()
+    m = pkg.box_mesh(10, 9, 12, 1.0, 1.0, 1.0)
+    mesh = pkg.Mesh(m.points, m.cells_dict["hexahedron"])
+    left = lambda p: np.isclose(p[0], 0.0, atol=1e-9)  # noqa: E731
+    right = lambda p: np.isclose(p[0], 1.0, atol=1e-9)  # noqa: E731
+    prob = make_problem(pkg, mesh, pkg.Laplace(), vec=1,
+                        bc=[[left, right], [0, 0], [lambda p: 0.0 * p[0], lambda p: 1.0 + 0.0 * p[0]]])
+    A = prob.dev().new_matrix(torch.float64)
+    u0 = torch.zeros(prob.num_total_dofs_all_vars, dtype=torch.float64, device=cuda)
+    prob.assemble(u0, vals=A.vals)
+    K = A.to_scipy()
+    b = np.random.default_rng(1).normal(size=K.shape[0])
+    xref = spla.spsolve(K.tocsc(), b)
+    for fp32 in (False, True):
+        M = mg.Multigrid(prob.dev(), prob.mesh.points, prob.mesh.cells, fp32=fp32)
+        M.setup(A)
+        x = torch.zeros(K.shape[0], dtype=torch.float64, device=cuda)
+        its, rel = M.solve(A, torch.tensor(b, device=cuda), x, rtol=1e-11)
+        assert its < 40 and np.abs(x.cpu().numpy() - xref).max() <= 1e-8 * np.abs(xref).max()
+    opts = lambda pc: {"newton": {"rel_tol": 1e-10, "tol": 1e-14, "linear": {"cg": {"precond": pc, "rtol": 1e-12,  # noqa: E731
+                                                                                "atol": 0.0}}}}
+    s1 = pkg.solver(prob, opts("gmg"))[0].cpu().numpy()
+    s2 = pkg.solver(prob, opts("block_jacobi"))[0].cpu().numpy()
+    assert np.abs(s1 - s2).max() <= 1e-9 * np.abs(s2).max()
+
+
+@pytest.mark.gpu
+def test_simp_adjoint_through_multigrid(pkg, cuda):
+    """ad_wrapper with 'gmg' for the forward and the transposed solve gives
+    the block-Jacobi path's compliance gradient (1e-7; both solves at rtol
+    1e-11, near where block-Jacobi CG stalls on this high-contrast system)."""
+    ws = importlib.import_module("jax_fem_b200.warmstart")
+    prob = ws.cantilever_problem(z0=3.0)
+    g = torch.Generator().manual_seed(17)
+    rho0 = ws.random_density(g).reshape(-1).double().to(cuda)
+    grads = []
+    for pc in ("gmg", "block_jacobi"):
+        lin = {"cg": {"precond": pc, "rtol": 1e-11, "atol": 0.0, "maxiter": 50000}}
+        fwd = pkg.ad_wrapper(prob, {"newton": {"rel_tol": 1e-11, "tol": 1e-30, "linear": lin}}, lin)
+        rho = rho0.clone().requires_grad_(True)
+        c = pkg.compliance(prob, fwd(rho))
+        c.backward()
+        grads.append(rho.grad.cpu().numpy())
+    assert np.abs(grads[0] - grads[1]).max() <= 1e-7 * np.abs(grads[1]).max()
