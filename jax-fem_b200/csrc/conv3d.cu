@@ -239,7 +239,6 @@ __global__ void __launch_bounds__(128, 1) tc_kernel(const __grid_constant__ CUte
 }
 
 // ---- host helpers -----------------------------------------------------------
-int g_err_host = 0;
 int* err_flag_device() {
   static std::mutex mu;
   static int* flags[64] = {nullptr};
@@ -409,11 +408,6 @@ unsigned grid_for(int64_t n) {
   const int64_t b = (n + 255) / 256;
   const int64_t cap = int64_t(num_sms()) * 16;
   return unsigned(b < 1 ? 1 : (b > cap ? cap : b));
-}
-
-int check_err(cudaStream_t st) {
-  (void)st;
-  return FEM_OK;
 }
 
 }  // namespace
