@@ -226,3 +226,11 @@ def test_multigrid_lattice_hierarchy(pkg):
     interior = (1 * n[1] + 1) * n[2] + 1
     assert (st[interior] >= 0).all()
     assert (st >= 0).sum() == len(col)
+    # a mesh that is not a box lattice is refused before any device work
+    with pytest.raises(NotImplementedError):
+        mg.Multigrid(None, bent, m.cells_dict["hexahedron"])
+    # the multigrid preconditioner is a CG preconditioner only
+    S = importlib.import_module("jax_fem_b200.solver")
+    with pytest.raises(ValueError):
+        S.resolve_linear({"bicgstab": {"precond": "gmg"}})
+    assert S.resolve_linear({"cg": {"precond": "gmg"}}).eta_max == 1e-3
