@@ -159,39 +159,53 @@ __global__ void ptap_kernel(Lat F, Lat C, const int32_t* __restrict__ cst, const
 }
 
 // ---- transfers ---------------------------------------------------------------
-// bc[I] = sum_i w_iI rf[i]   (P^T, one thread per coarse node)
+// bc[I] = sum_i w_iI rf[i]   (P^T, one thread per coarse node).  Along each
+// direction at most 3 fine nodes lie strictly between the neighbouring coarse
+// nodes, so the 27 candidates are unrolled with their weights formed first and
+// the gathers issued together; lattice indices fit in 32 bits.
 template <int VEC, typename T>
 __global__ void restrict_kernel(Lat F, Lat C, const int32_t* cpos, const int32_t* ilo, const double* whi,
                                 const T* __restrict__ rf, T* bc) {
-  const int32_t* cp[3] = {cpos, cpos + C.n[0], cpos + C.n[0] + C.n[1]};
-  const int32_t* il[3] = {ilo, ilo + F.n[0], ilo + F.n[0] + F.n[1]};
-  const double* wh[3] = {whi, whi + F.n[0], whi + F.n[0] + F.n[1]};
-  const int64_t Nc = C.n[0] * C.n[1] * C.n[2];
-  for (int64_t I = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; I < Nc; I += int64_t(gridDim.x) * blockDim.x) {
-    const int64_t Ic[3] = {I / (C.n[1] * C.n[2]), (I / C.n[2]) % C.n[1], I % C.n[2]};
-    int64_t lo[3], hi[3];
+  const int nc[3] = {int(C.n[0]), int(C.n[1]), int(C.n[2])};
+  const int nf[3] = {int(F.n[0]), int(F.n[1]), int(F.n[2])};
+  const int32_t* cp[3] = {cpos, cpos + nc[0], cpos + nc[0] + nc[1]};
+  const int32_t* il[3] = {ilo, ilo + nf[0], ilo + nf[0] + nf[1]};
+  const double* wh[3] = {whi, whi + nf[0], whi + nf[0] + nf[1]};
+  const int Nc = nc[0] * nc[1] * nc[2];
+  for (int I = blockIdx.x * blockDim.x + threadIdx.x; I < Nc; I += gridDim.x * blockDim.x) {
+    const int Ic[3] = {I / (nc[1] * nc[2]), (I / nc[2]) % nc[1], I % nc[2]};
+    int fi[3][3];
+    double fw[3][3];
 #pragma unroll
-    for (int d = 0; d < 3; ++d) fine_range(cp[d], Ic[d], C.n[d], F.n[d], &lo[d], &hi[d]);
+    for (int d = 0; d < 3; ++d) {
+      const int lo = Ic[d] > 0 ? cp[d][Ic[d] - 1] + 1 : 0;
+      const int hi = Ic[d] < nc[d] - 1 ? cp[d][Ic[d] + 1] - 1 : nf[d] - 1;
+#pragma unroll
+      for (int k = 0; k < 3; ++k) {
+        const int i = lo + k;
+        fi[d][k] = i <= hi ? i : lo;
+        fw[d][k] = i <= hi ? w1(il[d], wh[d], i, Ic[d]) : 0.0;
+      }
+    }
     double acc[VEC];
 #pragma unroll
     for (int c = 0; c < VEC; ++c) acc[c] = 0.0;
-    for (int64_t ix = lo[0]; ix <= hi[0]; ++ix) {
-      const double wx = w1(il[0], wh[0], ix, Ic[0]);
-      if (wx == 0.0) continue;
-      for (int64_t iy = lo[1]; iy <= hi[1]; ++iy) {
-        const double wy = w1(il[1], wh[1], iy, Ic[1]);
-        if (wy == 0.0) continue;
-        for (int64_t iz = lo[2]; iz <= hi[2]; ++iz) {
-          const double w = wx * wy * w1(il[2], wh[2], iz, Ic[2]);
-          if (w == 0.0) continue;
-          const int64_t i = (ix * F.n[1] + iy) * F.n[2] + iz;
 #pragma unroll
-          for (int c = 0; c < VEC; ++c) acc[c] = fma(w, double(rf[i * VEC + c]), acc[c]);
+    for (int a = 0; a < 3; ++a)
+#pragma unroll
+      for (int b = 0; b < 3; ++b) {
+        const double wab = fw[0][a] * fw[1][b];
+        const int rowab = (fi[0][a] * nf[1] + fi[1][b]) * nf[2];
+#pragma unroll
+        for (int e = 0; e < 3; ++e) {
+          const double w = wab * fw[2][e];
+          const int i = rowab + fi[2][e];
+#pragma unroll
+          for (int c = 0; c < VEC; ++c) acc[c] = fma(w, double(rf[int64_t(i) * VEC + c]), acc[c]);
         }
       }
-    }
 #pragma unroll
-    for (int c = 0; c < VEC; ++c) bc[I * VEC + c] = T(acc[c]);
+    for (int c = 0; c < VEC; ++c) bc[int64_t(I) * VEC + c] = T(acc[c]);
   }
 }
 
@@ -199,12 +213,14 @@ __global__ void restrict_kernel(Lat F, Lat C, const int32_t* cpos, const int32_t
 template <int VEC, typename T>
 __global__ void prolong_add_kernel(Lat F, Lat C, const int32_t* ilo, const double* whi, const T* __restrict__ ec,
                                    T* xf) {
-  const int32_t* il[3] = {ilo, ilo + F.n[0], ilo + F.n[0] + F.n[1]};
-  const double* wh[3] = {whi, whi + F.n[0], whi + F.n[0] + F.n[1]};
-  const int64_t Nf = F.n[0] * F.n[1] * F.n[2];
-  for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < Nf; i += int64_t(gridDim.x) * blockDim.x) {
-    const int64_t ii[3] = {i / (F.n[1] * F.n[2]), (i / F.n[2]) % F.n[1], i % F.n[2]};
-    int64_t lo[3];
+  const int nf[3] = {int(F.n[0]), int(F.n[1]), int(F.n[2])};
+  const int nc1 = int(C.n[1]), nc2 = int(C.n[2]);
+  const int32_t* il[3] = {ilo, ilo + nf[0], ilo + nf[0] + nf[1]};
+  const double* wh[3] = {whi, whi + nf[0], whi + nf[0] + nf[1]};
+  const int Nf = nf[0] * nf[1] * nf[2];
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < Nf; i += gridDim.x * blockDim.x) {
+    const int ii[3] = {i / (nf[1] * nf[2]), (i / nf[2]) % nf[1], i % nf[2]};
+    int lo[3];
     double wup[3];
 #pragma unroll
     for (int d = 0; d < 3; ++d) {
@@ -219,12 +235,12 @@ __global__ void prolong_add_kernel(Lat F, Lat C, const int32_t* ilo, const doubl
       const int bx = m >> 2, by = (m >> 1) & 1, bz = m & 1;
       const double w = (bx ? wup[0] : 1.0 - wup[0]) * (by ? wup[1] : 1.0 - wup[1]) * (bz ? wup[2] : 1.0 - wup[2]);
       if (w == 0.0) continue;
-      const int64_t J = ((lo[0] + bx) * C.n[1] + (lo[1] + by)) * C.n[2] + (lo[2] + bz);
+      const int J = ((lo[0] + bx) * nc1 + (lo[1] + by)) * nc2 + (lo[2] + bz);
 #pragma unroll
-      for (int c = 0; c < VEC; ++c) acc[c] = fma(w, double(ec[J * VEC + c]), acc[c]);
+      for (int c = 0; c < VEC; ++c) acc[c] = fma(w, double(ec[int64_t(J) * VEC + c]), acc[c]);
     }
 #pragma unroll
-    for (int c = 0; c < VEC; ++c) xf[i * VEC + c] = T(double(xf[i * VEC + c]) + acc[c]);
+    for (int c = 0; c < VEC; ++c) xf[int64_t(i) * VEC + c] = T(double(xf[int64_t(i) * VEC + c]) + acc[c]);
   }
 }
 
@@ -485,6 +501,7 @@ int vcycle_impl(int nlevels, const FemMGLevel* L, int nu, int coarse_steps, doub
   FEM_CHECK_ARG(rhs != nullptr && z != nullptr, "rhs and z must not be NULL");
   FEM_CHECK_ARG(nu >= 1 && nu <= 16 && coarse_steps >= 1 && coarse_steps <= 512, "nu in [1,16], coarse_steps in [1,512]");
   FEM_CHECK_ARG(ratio > 1.0, "ratio must exceed 1");
+  FEM_CHECK_ARG(L[0].n_brows < (int64_t(1) << 31), "lattice node indices must fit in 32 bits");
   return vcycle_level<VEC, T>(0, nlevels, L, nu, coarse_steps, ratio, rhs, z, st);
 }
 
@@ -492,6 +509,7 @@ int vcycle_impl(int nlevels, const FemMGLevel* L, int nu, int coarse_steps, doub
 struct PState {
   double gamma, alpha, beta, rr, tol2, bb, pq;
   int iter, status, maxiter, first;
+  int loops;  // bodies run by the device-side loop (its own bound)
 };
 enum : int { PS_RUNNING = 0, PS_CONVERGED = 1 };
 
@@ -597,6 +615,16 @@ __global__ void pcg_update_kernel(int64_t n, double* x, double* r, const double*
   }
 }
 
+// Condition of the device-side iteration loop (a WHILE node of the solve
+// graph): continue while the state is RUNNING.  The loop keeps its own count
+// of bodies run, so it ends after maxiter bodies whatever the state says.
+__global__ void pcg_cond_kernel(PState* S, cudaGraphConditionalHandle h, int in_body) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  if (in_body) S->loops += 1;
+  const bool go = S->status == PS_RUNNING && S->loops < S->maxiter;
+  cudaGraphSetConditional(h, go ? 1u : 0u);
+}
+
 inline size_t al256(size_t x) { return (x + 255) & ~size_t(255); }
 
 // Cached CUDA graphs of PCG iteration chunks (V-cycles included): the launch
@@ -630,6 +658,64 @@ cudaStream_t mg_capture_stream() {
   return s[dev];
 }
 
+// Graph: condition kernel -> WHILE node (body: one iteration, then the
+// condition kernel).  Returns nullptr when any step fails (the caller then
+// launches directly); *nbody = kernels per body.
+template <typename F>
+cudaGraphExec_t build_loop_graph(PState* S, F&& body_fn, int64_t* nbody) {
+  cudaStream_t cap = mg_capture_stream();
+  if (cap == nullptr) return nullptr;
+  cudaGraph_t g = nullptr;
+  if (cudaGraphCreate(&g, 0) != cudaSuccess) return nullptr;
+  cudaGraphExec_t exec = nullptr;
+  cudaGraphConditionalHandle h = 0;
+  cudaGraphNode_t kn = nullptr, wn = nullptr;
+  bool ok = cudaGraphConditionalHandleCreate(&h, g, 0, cudaGraphCondAssignDefault) == cudaSuccess;
+  if (ok) {
+    int first = 0;
+    void* args[] = {&S, &h, &first};
+    cudaKernelNodeParams kp{};
+    kp.func = reinterpret_cast<void*>(pcg_cond_kernel);
+    kp.gridDim = dim3(1);
+    kp.blockDim = dim3(32);
+    kp.sharedMemBytes = 0;
+    kp.kernelParams = args;
+    kp.extra = nullptr;
+    ok = cudaGraphAddKernelNode(&kn, g, nullptr, 0, &kp) == cudaSuccess;
+  }
+  cudaGraphNodeParams cp{};
+  if (ok) {
+    cp.type = cudaGraphNodeTypeConditional;
+    cp.conditional.handle = h;
+    cp.conditional.type = cudaGraphCondTypeWhile;
+    cp.conditional.size = 1;
+    ok = cudaGraphAddNode(&wn, g, &kn, 1, &cp) == cudaSuccess;
+  }
+  if (ok) {
+    cudaGraph_t body = cp.conditional.phGraph_out[0];
+    ok = cudaStreamBeginCaptureToGraph(cap, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal) ==
+         cudaSuccess;
+    if (ok) {
+      const int64_t c0 = launch_counter().load();
+      int lrc = body_fn(cap);
+      if (lrc == FEM_OK) {
+        pcg_cond_kernel<<<1, 32, 0, cap>>>(S, h, 1);
+        if (cudaGetLastError() != cudaSuccess) lrc = FEM_ERR_CUDA;
+      }
+      const int64_t nk = launch_counter().load() - c0;
+      launch_counter().fetch_sub(nk, std::memory_order_relaxed);  // counted when run
+      *nbody = nk + 1;
+      cudaGraph_t out = nullptr;
+      const cudaError_t ec = cudaStreamEndCapture(cap, &out);
+      ok = lrc == FEM_OK && ec == cudaSuccess;
+    }
+  }
+  if (ok && cudaGraphInstantiate(&exec, g, 0) != cudaSuccess) exec = nullptr;
+  cudaGraphDestroy(g);
+  cudaGetLastError();  // a failed build falls back to direct launches
+  return exec;
+}
+
 size_t pcg_workspace_bytes(int vec, int64_t n_brows) {
   const size_t n = size_t(n_brows) * vec;
   return 256 + 256 + al256(size_t(num_sms()) * 8 * 4 * sizeof(double)) + 4 * al256(n * sizeof(double));
@@ -646,6 +732,7 @@ int pcg_impl(int64_t n_brows, const int32_t* rp, const int32_t* ci, const double
   FEM_CHECK_ARG(rp && ci && vals && b && x, "NULL operator or vector");
   FEM_CHECK_ARG(bsr_aligned(vals, ci), "vals and col_idx must be 16-byte aligned");
   FEM_CHECK_ARG(nlevels >= 1 && L != nullptr && L[0].n_brows == n_brows, "level 0 must be the operator's lattice");
+  FEM_CHECK_ARG(n_brows < (int64_t(1) << 31), "lattice node indices must fit in 32 bits");
   FEM_CHECK_ARG(!fp32 || (L[0].x != nullptr && L[0].b != nullptr), "FP32 hierarchy needs level 0 x and b");
   if (check_every <= 0) check_every = 4;
   char* p8 = static_cast<char*>(work);
@@ -688,88 +775,78 @@ int pcg_impl(int64_t n_brows, const int32_t* rp, const int32_t* ci, const double
     FEM_CUDA_TRY(cudaStreamSynchronize(st));
     return FEM_OK;
   };
-  int launched = 0;
-  while (true) {
-    if ((rc = read_state()) != FEM_OK) return rc;
-    if (hs->status != PS_RUNNING || launched >= maxiter) break;
-    const int chunk = check_every < maxiter - launched ? check_every : maxiter - launched;
-    auto launch_chunk = [&](cudaStream_t ls) -> int {
-      for (int k = 0; k < chunk; ++k) {
-        int rc2;
-        if (fp32) {
-          // r.z needs z in FP64: widen the FP32 V-cycle output into z
-          if ((rc2 = vcycle_level<VEC, float>(0, nlevels, L, nu, coarse_steps, ratio, r32, z32, ls)) != FEM_OK)
-            return rc2;
-          widen_kernel<float><<<vg, 256, 0, ls>>>(n, z32, z);
-          FEM_LAUNCH_CHECK();
-        } else {
-          if ((rc2 = vcycle_level<VEC, double>(0, nlevels, L, nu, coarse_steps, ratio, r, z, ls)) != FEM_OK)
-            return rc2;
-        }
-        pcg_rz_kernel<<<vg, 256, 0, ls>>>(n, r, z, partials, counter, S);
-        FEM_LAUNCH_CHECK();
-        pcg_dir_kernel<double><<<vg, 256, 0, ls>>>(n, z, pv, S);
-        FEM_LAUNCH_CHECK();
-        pcg_spmv_kernel<VEC><<<rg, kRowThreads, bsr_rows_smem(), ls>>>(n_brows, rp, ci, vals, pv, q, partials, counter,
-                                                                        S);
-        FEM_LAUNCH_CHECK();
-        pcg_update_kernel<<<vg, 256, 0, ls>>>(n, x, r, pv, q, r32, partials, counter, S);
-        FEM_LAUNCH_CHECK();
-      }
-      return FEM_OK;
-    };
+  // one PCG iteration: V-cycle, r.z, direction, A p, update
+  auto launch_iter = [&](cudaStream_t ls) -> int {
+    int rc2;
+    if (fp32) {
+      // r.z needs z in FP64: widen the FP32 V-cycle output into z
+      if ((rc2 = vcycle_level<VEC, float>(0, nlevels, L, nu, coarse_steps, ratio, r32, z32, ls)) != FEM_OK) return rc2;
+      widen_kernel<float><<<vg, 256, 0, ls>>>(n, z32, z);
+      FEM_LAUNCH_CHECK();
+    } else {
+      if ((rc2 = vcycle_level<VEC, double>(0, nlevels, L, nu, coarse_steps, ratio, r, z, ls)) != FEM_OK) return rc2;
+    }
+    pcg_rz_kernel<<<vg, 256, 0, ls>>>(n, r, z, partials, counter, S);
+    FEM_LAUNCH_CHECK();
+    pcg_dir_kernel<double><<<vg, 256, 0, ls>>>(n, z, pv, S);
+    FEM_LAUNCH_CHECK();
+    pcg_spmv_kernel<VEC><<<rg, kRowThreads, bsr_rows_smem(), ls>>>(n_brows, rp, ci, vals, pv, q, partials, counter, S);
+    FEM_LAUNCH_CHECK();
+    pcg_update_kernel<<<vg, 256, 0, ls>>>(n, x, r, pv, q, r32, partials, counter, S);
+    FEM_LAUNCH_CHECK();
+    return FEM_OK;
+  };
+  bool looped = false;
+  if (mg_graphs_enabled()) {
+    // The whole iteration loop as one graph: a WHILE node whose body is one
+    // iteration and whose condition the device sets from the state, so the
+    // host waits once per solve and no iteration runs after convergence.
+    std::string key(reinterpret_cast<const char*>(L), sizeof(FemMGLevel) * size_t(nlevels));
+    const void* ptrs[] = {rp, ci, vals, b, x, work};
+    key.append(reinterpret_cast<const char*>(ptrs), sizeof(ptrs));
+    const double params[] = {double(nlevels), double(fp32), double(nu), double(coarse_steps), ratio, double(n_brows),
+                             double(VEC)};
+    key.append(reinterpret_cast<const char*>(params), sizeof(params));
+    int dev = 0;
+    cudaGetDevice(&dev);
+    key.append(reinterpret_cast<const char*>(&dev), sizeof(dev));
     cudaGraphExec_t exec = nullptr;
-    int64_t nkern = 0;
-    if (mg_graphs_enabled()) {
-      std::string key(reinterpret_cast<const char*>(L), sizeof(FemMGLevel) * size_t(nlevels));
-      const void* ptrs[] = {rp, ci, vals, b, x, work};
-      key.append(reinterpret_cast<const char*>(ptrs), sizeof(ptrs));
-      const double params[] = {double(nlevels), double(fp32), double(nu), double(coarse_steps), ratio, double(chunk),
-                               double(n_brows), double(VEC)};
-      key.append(reinterpret_cast<const char*>(params), sizeof(params));
-      int dev = 0;
-      cudaGetDevice(&dev);
-      key.append(reinterpret_cast<const char*>(&dev), sizeof(dev));
-      {
-        std::lock_guard<std::mutex> lock(g_mg_mu);
-        auto it = mg_graph_cache().find(key);
-        if (it != mg_graph_cache().end()) {
-          exec = it->second.exec;
-          nkern = it->second.kernels;
-        }
+    int64_t nbody = 0;
+    {
+      std::lock_guard<std::mutex> lock(g_mg_mu);
+      auto it = mg_graph_cache().find(key);
+      if (it != mg_graph_cache().end()) {
+        exec = it->second.exec;
+        nbody = it->second.kernels;
       }
-      if (exec == nullptr) {
-        cudaStream_t cap = mg_capture_stream();
-        if (cap != nullptr && cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
-          const int64_t c0 = launch_counter().load();
-          const int lrc = launch_chunk(cap);
-          nkern = launch_counter().load() - c0;
-          launch_counter().fetch_sub(nkern, std::memory_order_relaxed);  // counted when replayed
-          cudaGraph_t g = nullptr;
-          const cudaError_t ec = cudaStreamEndCapture(cap, &g);
-          if (lrc == FEM_OK && ec == cudaSuccess && g != nullptr && cudaGraphInstantiate(&exec, g, 0) == cudaSuccess) {
-            std::lock_guard<std::mutex> lock(g_mg_mu);
-            auto& m = mg_graph_cache();
-            if (m.size() >= 32) {  // bounded: drop everything (hierarchies were rebuilt)
-              for (auto& kv : m) cudaGraphExecDestroy(kv.second.exec);
-              m.clear();
-            }
-            m[key] = MGGraph{exec, nkern};
-          } else {
-            exec = nullptr;
-          }
-          if (g != nullptr) cudaGraphDestroy(g);
-          cudaGetLastError();  // a failed capture falls back to direct launches
-        }
+    }
+    if (exec == nullptr && (exec = build_loop_graph(S, launch_iter, &nbody)) != nullptr) {
+      std::lock_guard<std::mutex> lock(g_mg_mu);
+      auto& m = mg_graph_cache();
+      if (m.size() >= 32) {  // bounded: drop everything (hierarchies were rebuilt)
+        for (auto& kv : m) cudaGraphExecDestroy(kv.second.exec);
+        m.clear();
       }
+      m[key] = MGGraph{exec, nbody};
     }
     if (exec != nullptr) {
       FEM_CUDA_TRY(cudaGraphLaunch(exec, st));
-      launch_counter().fetch_add(nkern, std::memory_order_relaxed);
-    } else if ((rc = launch_chunk(st)) != FEM_OK) {
-      return rc;
+      if ((rc = read_state()) != FEM_OK) return rc;
+      launch_counter().fetch_add(1 + int64_t(hs->loops) * nbody, std::memory_order_relaxed);
+      looped = true;
     }
-    launched += chunk;
+  }
+  if (!looped) {
+    // direct launches, the state read every check_every iterations
+    int launched = 0;
+    while (true) {
+      if ((rc = read_state()) != FEM_OK) return rc;
+      if (hs->status != PS_RUNNING || launched >= maxiter) break;
+      const int chunk = check_every < maxiter - launched ? check_every : maxiter - launched;
+      for (int k = 0; k < chunk; ++k)
+        if ((rc = launch_iter(st)) != FEM_OK) return rc;
+      launched += chunk;
+    }
   }
   const int status = hs->status;
   const int iters = hs->iter;

@@ -123,6 +123,68 @@ def test_mg_pcg_matches_direct_solve(pkg, cuda, fp32):
     assert its * 3 < its_bj
 
 
+_DIRECT_SCRIPT = r"""
+import sys, numpy as np, torch
+sys.path[:0] = [sys.argv[1], sys.argv[1] + "/tests"]
+from __graft_entry__ import load_package
+import test_gpu_multigrid as t
+pkg = load_package()
+mg, S = t._mods()
+prob, A = t._graded_elastic(pkg, torch.device("cuda", 0), shape=(12, 10, 9))
+A.vals.copy_(torch.from_numpy(np.load(sys.argv[4])))  # the parent's operator, bit for bit
+b = torch.tensor(np.random.default_rng(5).normal(size=A.n_brows * 3), dtype=torch.float64, device="cuda")
+M = mg.Multigrid(prob.dev(), prob.mesh.points, prob.mesh.cells, fp32=sys.argv[3] == "1")
+M.setup(A)
+x = torch.zeros_like(b)
+its, rel = M.solve(A, b, x, rtol=1e-10, check_every=3)
+np.save(sys.argv[2], x.cpu().numpy())
+print(its)
+"""
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("fp32", [False, True])
+def test_mg_pcg_device_loop_matches_direct_launches(pkg, cuda, fp32, tmp_path):
+    """The solve graph (a device-side WHILE loop over iterations) runs the
+    same kernels in the same order as direct launches with a host check every
+    few iterations: identical iterates, and no iteration after convergence."""
+    import os
+    import subprocess
+    import sys
+    mg, S = _mods()
+    prob, A = _graded_elastic(pkg, cuda, shape=(12, 10, 9))
+    b = torch.tensor(np.random.default_rng(5).normal(size=A.n_brows * 3), dtype=torch.float64, device=cuda)
+    M = mg.Multigrid(prob.dev(), prob.mesh.points, prob.mesh.cells, fp32=fp32)
+    M.setup(A)
+    x = torch.zeros_like(b)
+    its, rel = M.solve(A, b, x, rtol=1e-10)
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    out, vals = tmp_path / "x_direct.npy", tmp_path / "vals.npy"
+    np.save(vals, A.vals.cpu().numpy())  # assembly sums with atomics: hand over the exact operator
+    env = dict(os.environ, FEM_MG_GRAPHS="0")
+    p = subprocess.run([sys.executable, "-c", _DIRECT_SCRIPT, root, str(out), "1" if fp32 else "0", str(vals)],
+                       env=env, capture_output=True, text=True, timeout=600)
+    assert p.returncode == 0, p.stderr[-2000:]
+    its_direct = int(p.stdout.split()[-1])
+    assert its == its_direct
+    np.testing.assert_array_equal(x.cpu().numpy(), np.load(out))
+
+
+@pytest.mark.gpu
+def test_mg_pcg_device_loop_stops_at_maxiter(pkg, cuda):
+    mg, S = _mods()
+    nat = pkg._native
+    prob, A = _graded_elastic(pkg, cuda, shape=(12, 10, 9))
+    b = torch.ones(A.n_brows * 3, dtype=torch.float64, device=cuda)
+    M = mg.Multigrid(prob.dev(), prob.mesh.points, prob.mesh.cells, fp32=True)
+    M.setup(A)
+    x = torch.zeros_like(b)
+    with pytest.raises(nat.FEMNativeError) as e:
+        M.solve(A, b, x, rtol=1e-30, maxiter=3)
+    assert e.value.status == nat.FEM_ERR_NOT_CONVERGED
+    assert "after 3 iterations" in str(e.value)
+
+
 def _twist(n, deg):
     th = math.radians(deg)
     c, s = math.cos(th), math.sin(th)
