@@ -11,7 +11,16 @@ batched: a function is first called once with the coordinate axes as arrays
 (``point[0]`` is the vector of all x coordinates) and the batched answer is
 kept only if it agrees with point-by-point calls on a sample; otherwise it is
 called point by point.
+
+A location function that is a plain Python function is evaluated once per
+function object: its node set is reused by later Dirichlet updates while its
+code, defaults, closure values and the module globals it names are unchanged
+(values compared by content: numbers, strings, tuples, small arrays; modules
+and functions by identity).  One that reads anything that can change in place
+unseen (a list, a dict, an object's attributes) is evaluated at every update,
+as the reference does.
 """
+import types
 import weakref
 
 import numpy as np
@@ -102,6 +111,59 @@ def _batched_or_pointwise(fn, args, out_tail, sample=8):
     return pointwise(np.arange(n))
 
 
+_PLAIN = (int, float, complex, str, bytes, bool, type(None), np.generic)
+
+
+def _code_names(code):
+    names = set(code.co_names)
+    for c in code.co_consts:
+        if isinstance(c, types.CodeType):
+            names |= _code_names(c)
+    return names
+
+
+def _value_state(v, depth):
+    if isinstance(v, types.ModuleType):
+        return ("module", v)
+    if isinstance(v, _PLAIN):
+        return ("value", type(v), v)
+    if isinstance(v, np.ndarray):
+        return ("array", v.dtype.str, v.shape, v.tobytes()) if v.nbytes <= (1 << 20) else None
+    if isinstance(v, tuple):
+        parts = tuple(_value_state(x, depth) for x in v)
+        return None if any(p is None for p in parts) else ("tuple", parts)
+    if isinstance(v, types.FunctionType):
+        st = function_state(v, depth - 1)
+        return None if st is None else ("function", v, st)
+    if isinstance(v, (types.BuiltinFunctionType, np.ufunc)):
+        return ("builtin", v)
+    return None
+
+
+def function_state(fn, depth=2):
+    """What a plain Python function's answer can depend on besides its
+    arguments, as a comparable value: its code, defaults, closure values and
+    the globals it names.  None when fn is not a plain function or some of
+    that state could change in place unseen."""
+    if not isinstance(fn, types.FunctionType) or depth < 0:
+        return None
+    vals = list(fn.__defaults__ or ()) + list((fn.__kwdefaults__ or {}).values())
+    for cell in fn.__closure__ or ():
+        try:
+            vals.append(cell.cell_contents)
+        except ValueError:  # empty cell
+            return None
+    g = fn.__globals__
+    vals += [g[nm] for nm in sorted(_code_names(fn.__code__)) if nm in g]
+    state = [fn.__code__]
+    for v in vals:
+        st = _value_state(v, depth)
+        if st is None:
+            return None
+        state.append(st)
+    return tuple(state)
+
+
 def _location_flags(fn, points):
     nargs = getattr(getattr(fn, "__code__", None), "co_argcount", 1)
     if nargs == 1:
@@ -151,7 +213,7 @@ class FiniteElement:
             seen_loc, seen_val = {}, {}  # the same function object is evaluated once
             for lf, v, vf in zip(location_fns, vecs, value_fns):
                 if id(lf) not in seen_loc:
-                    seen_loc[id(lf)] = np.argwhere(_location_flags(lf, self.points)).reshape(-1)
+                    seen_loc[id(lf)] = self._location_nodes(lf)
                 node_inds = seen_loc[id(lf)]
                 key = (id(vf), id(lf))
                 if key not in seen_val:
@@ -161,6 +223,24 @@ class FiniteElement:
                 vec_inds_list.append(np.full(len(node_inds), int(v), dtype=np.int32))
                 vals_list.append(np.asarray(vals, dtype=np.float64).reshape(-1))
         return node_inds_list, vec_inds_list, vals_list
+
+    def _location_nodes(self, lf):
+        """Nodes where the location function holds (reused while its state,
+        ``function_state``, is unchanged)."""
+        memo = self.__dict__.setdefault("_location_memo", {})
+        state = function_state(lf)
+        hit = memo.get(id(lf))
+        try:
+            if state is not None and hit is not None and hit[0] is lf and hit[1] == state:
+                return hit[2].copy()
+        except (TypeError, ValueError):  # a state that does not compare plainly
+            pass
+        nodes = np.argwhere(_location_flags(lf, self.points)).reshape(-1)
+        if state is not None:
+            if len(memo) >= 64:
+                memo.clear()
+            memo[id(lf)] = (lf, state, nodes.copy())
+        return nodes
 
     def update_Dirichlet_boundary_conditions(self, dirichlet_bc_info):
         self.dirichlet_bc_info = dirichlet_bc_info

@@ -122,6 +122,55 @@ def test_dirichlet_discovery_batched_and_pointwise(pkg):
         np.testing.assert_allclose(a, b, rtol=0, atol=0)
 
 
+_XCUT = 2.0
+
+
+def _below_cut(p):
+    return p[0] < _XCUT
+
+
+def test_location_node_sets_reused_only_while_unchanged(pkg, monkeypatch):
+    """A location function's node set is reused across Dirichlet updates
+    while the function and what it reads are unchanged, and recomputed when a
+    global or a closure array it reads changes; a function reading a mutable
+    container is evaluated at every update."""
+    global _XCUT
+    fe_mod = pkg.fe
+    d = golden("hyperelasticity")
+    mesh = pkg.Mesh(d["points"], d["cells"])
+    calls = []
+    real = fe_mod._location_flags
+    monkeypatch.setattr(fe_mod, "_location_flags", lambda fn, pts: calls.append(fn) or real(fn, pts))
+    zero = lambda p: 0.0 * p[0]  # noqa: E731
+    fe = fe_mod.FiniteElement(mesh, 3, 3, dirichlet_bc_info=[[_below_cut], [0], [zero]])
+    first = fe.node_inds_list[0].copy()
+    fe.update_Dirichlet_boundary_conditions([[_below_cut], [0], [zero]])
+    assert len(calls) == 1  # reused
+    np.testing.assert_array_equal(fe.node_inds_list[0], first)
+    old = _XCUT
+    try:
+        _XCUT = 5.0  # a global the function reads
+        fe.update_Dirichlet_boundary_conditions([[_below_cut], [0], [zero]])
+        assert len(calls) == 2
+        np.testing.assert_array_equal(fe.node_inds_list[0], np.flatnonzero(d["points"][:, 0] < 5.0))
+    finally:
+        _XCUT = old
+    box = np.array([1.0, 3.0])
+    inside = lambda p: (p[0] > box[0]) & (p[0] < box[1])  # noqa: E731
+    fe.update_Dirichlet_boundary_conditions([[inside], [0], [zero]])
+    box[1] = 6.0  # mutated in place
+    fe.update_Dirichlet_boundary_conditions([[inside], [0], [zero]])
+    assert len(calls) == 4  # evaluated again after the mutation
+    np.testing.assert_array_equal(fe.node_inds_list[0],
+                                  np.flatnonzero((d["points"][:, 0] > 1.0) & (d["points"][:, 0] < 6.0)))
+    lims = [1.0]
+    right_of = lambda p: p[0] > lims[0]  # noqa: E731
+    for _ in range(2):
+        fe.update_Dirichlet_boundary_conditions([[right_of], [0], [zero]])
+    assert len(calls) == 6  # a list is never trusted
+    assert fe_mod.function_state(right_of) is None and fe_mod.function_state(_below_cut) is not None
+
+
 def test_load_vectors_match_oracle(pkg):
     d = golden("linear_elasticity_cylinder")
     mesh = pkg.Mesh(d["points"], d["cells"])
