@@ -252,7 +252,9 @@ def run_ours(args, rank, world, device):
     adaptive = {"cg": {"precond": "block_jacobi", "rtol": "adaptive", "atol": 0.0, "maxiter": 20000}}
     refine = {"cg": dict(adaptive["cg"], reliable_delta=0.0)}
     refm = {"jax_solver": {}}  # the reference's default linear solver: BiCGSTAB + Jacobi, tol = atol = 1e-10
-    gmg = {"cg": {"precond": "gmg", "rtol": "adaptive", "atol": 0.0, "maxiter": 2000}}
+    # multigrid: coarse operators shared by up to 4 Newton solves (re-formed
+    # sooner when convergence slows); the finest level takes every tangent
+    gmg = {"cg": {"precond": "gmg", "rtol": "adaptive", "atol": 0.0, "maxiter": 2000, "mg_lag": 4}}
     variants = {  # name -> (precision, linear options)
         "reference_method_fp64": ("fp64", refm),  # the reference's exact Newton + linear settings on the GPU
         "plain_fp64": ("fp64", tight),            # tight linear solves, CG + 3x3 block-Jacobi
@@ -389,8 +391,8 @@ def run_ours(args, rank, world, device):
                          "iterations with reliable updates (FP64 solution, true residual, reductions); "
                          "mixed_tight = the same to the 1e-10 linear tolerance; mixed_refinement = FP32 CG "
                          "restarted inside FP64 iterative refinement; *_gmg = CG preconditioned by a geometric "
-                         "multigrid V-cycle (FP64 CG; V-cycle FP64 in plain_fp64_gmg, FP32 in mixed_gmg); "
-                         "value = mixed_gmg",
+                         "multigrid V-cycle (FP64 CG; V-cycle FP64 in plain_fp64_gmg, FP32 in mixed_gmg; "
+                         "coarse operators shared by up to 4 Newton solves, mg_lag 4); value = mixed_gmg",
         "solves_per_s": round(world / t_mixed, 4),
         "newton_iters": newton,
         "krylov_iters": krylov,

@@ -160,24 +160,37 @@ class Multigrid:
                         torch.from_numpy(np.concatenate([q[2] for q in parts]).astype(np.int32)).to(dev),
                         torch.from_numpy(np.concatenate([q[3] for q in parts]).astype(np.float64)).to(dev))
         self._work = None
+        self._fine_ref = None
+        # coarse-operator reuse bookkeeping (solver.mg_solve)
+        self.setup_for, self.solves_on_coarse, self.first_rate, self.last_rate = None, 0, None, None
         nb = nat.lib().fem_mg_setup_scratch_bytes(self.vec, self.levels[0].n_brows, int(fp32))
         self._scratch = torch.empty(max(int(nb), 16), dtype=torch.uint8, device=dev)
 
-    def setup(self, A):
+    def setup(self, A, fine_only=False):
         """Coarse operators and smoother bounds for the FP64 operator A
-        (a ``BSRMatrix`` on this mesh's pattern)."""
+        (a ``BSRMatrix`` on this mesh's pattern).  With ``fine_only`` only
+        the finest level takes A's values (and its Jacobi scaling and bound);
+        the coarse levels keep the operators of the last full setup."""
         lib = nat.lib()
         if A.vals.dtype != torch.float64:
             raise TypeError("the multigrid hierarchy is formed from the FP64 operator")
+        if fine_only and self.setup_for is None:
+            raise RuntimeError("fine_only needs an earlier full setup")
+        nl = 1 if fine_only else self.nlevels
         if self.fp32:
-            nat.check(lib.fem_mg_setup_f32(self.vec, self.nlevels, ctypes.byref(self.levels), nat.ptr(A.vals),
+            nat.check(lib.fem_mg_setup_f32(self.vec, nl, ctypes.byref(self.levels), nat.ptr(A.vals),
                                            nat.ptr(self._scratch), self._scratch.numel(), nat.stream_ptr()),
                       "mg_setup_f32")
         else:
             self.levels[0].vals = A.vals.data_ptr()
-            self._keep.append(A.vals)
-            nat.check(lib.fem_mg_setup_f64(self.vec, self.nlevels, ctypes.byref(self.levels), nat.ptr(self._scratch),
+            if self._fine_ref is not A.vals:
+                self._keep.append(A.vals)
+                self._fine_ref = A.vals
+            nat.check(lib.fem_mg_setup_f64(self.vec, nl, ctypes.byref(self.levels), nat.ptr(self._scratch),
                                            self._scratch.numel(), nat.stream_ptr()), "mg_setup_f64")
+        if not fine_only:
+            self.solves_on_coarse = 0
+        self.setup_for = A
 
     def lmax(self):
         """Per-level Gershgorin bounds of the Jacobi-scaled operators (reads the device)."""

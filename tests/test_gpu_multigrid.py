@@ -219,6 +219,36 @@ def test_newton_gmg_matches_oracle(pkg, cuda, precision, rtol):
 
 
 @pytest.mark.gpu
+def test_newton_gmg_coarse_operator_lag(pkg, cuda, monkeypatch):
+    """mg_lag = 3: the coarse operators are re-formed at most every third
+    Newton solve (the finest level takes every new tangent); Newton still
+    converges to the oracle's solution."""
+    mgm, S = _mods()
+    n = 8
+    m = pkg.box_mesh(n, n, n, 1.0, 1.0, 1.0)
+    mesh = pkg.Mesh(m.points, m.cells_dict["hexahedron"])
+    bc = _twist(n, 20.0)
+    prob = make_problem(pkg, mesh, pkg.NeoHookean(10.0, 0.3), bc=bc)
+    kinds = []
+    real = mgm.Multigrid.setup
+    monkeypatch.setattr(mgm.Multigrid, "setup", lambda self, A, fine_only=False: kinds.append(fine_only) or
+                        real(self, A, fine_only=fine_only))
+    opts = {"newton": {"rel_tol": 1e-8, "tol": 1e-14, "precision": "mixed", "return_info": True,
+                       "linear": {"cg": {"precond": "gmg", "rtol": "adaptive", "atol": 0.0, "mg_lag": 3}}}}
+    (sol,), info = pkg.solver(prob, opts)
+    assert len(kinds) == info["newton_iters"] >= 3
+    assert kinds[0] is False and any(kinds)
+    run = 0
+    for k in kinds:  # never more than 3 solves on one set of coarse operators
+        run = run + 1 if k else 1
+        assert run <= 3
+    sol = sol.cpu().numpy().reshape(-1)
+    op = fo.OracleProblem(mesh.points, mesh.cells, 3, fo.Law("neo_hookean", E=10.0, nu=0.3), dirichlet_bc_info=bc)
+    ref = fo.newton_solve(op, rel_tol=1e-12, tol=1e-14)
+    assert np.abs(sol - ref).max() <= 1e-6 * np.abs(ref).max()
+
+
+@pytest.mark.gpu
 def test_scalar_poisson_multigrid(pkg, cuda):
     """vec = 1 (Laplace): multigrid CG on a Poisson problem matches the
     direct solve (1e-8), and so does Newton with precond 'gmg'."""
