@@ -132,8 +132,9 @@ FEM_API int fem_assemble_f64(int law, const double* h_params, int n_params, int 
                      const uint8_t* d_bc_mask, const double* d_dvec,
                      double* d_res, double* d_lift, double* d_vals, void* stream);
 /* Same with the tangent computed and stored in FP32 (mixed-precision path).
- * d_res / d_lift stay FP64 but are computed in FP32 arithmetic here; the
- * mixed path takes its Newton residual from a residual-only f64 call. */
+ * Geometry, the constitutive update and d_res are FP64 as in _f64 (the
+ * Newton residual is exact); d_lift is accumulated in FP64 from the FP32
+ * tangent. */
 FEM_API int fem_assemble_f32(int law, const double* h_params, int n_params, int vec,
                      int64_t num_cells, int64_t num_nodes, const int32_t* d_cells,
                      const double* d_points, const double* d_u,
@@ -368,6 +369,15 @@ FEM_API int fem_mg_pcg_solve(int vec, int64_t n_brows, const int32_t* d_row_ptr,
                              int maxiter, int check_every, int nlevels, const FemMGLevel* levels,
                              int levels_fp32, int nu, int coarse_steps, double ratio, void* d_work,
                              size_t work_bytes, int* h_iters, double* h_relres, void* stream);
+/* The same CG on an FP32 operator (an FP32-assembled tangent): the products
+ * A p read FP32 values and accumulate in FP64, every vector and reduction is
+ * FP64.  The solve is exact for the FP32 operator; for a Newton step that
+ * operator is the tangent rounded to FP32. */
+FEM_API int fem_mg_pcg_solve_mixed(int vec, int64_t n_brows, const int32_t* d_row_ptr, const int32_t* d_col_idx,
+                                   const float* d_vals, const double* d_b, double* d_x, double rtol, double atol,
+                                   int maxiter, int check_every, int nlevels, const FemMGLevel* levels,
+                                   int levels_fp32, int nu, int coarse_steps, double ratio, void* d_work,
+                                   size_t work_bytes, int* h_iters, double* h_relres, void* stream);
 
 /* ---- dot product that allocates nothing ---------------------------------
  * No counterpart in the reference.  For callers that cannot allocate device

@@ -83,6 +83,8 @@ _SIGS = {
     "fem_mg_pcg_workspace_bytes": (SZ, [I32, I64]),
     "fem_mg_pcg_solve": (I32, [I32, I64, P, P, P, P, P, F64, F64, I32, I32, I32, P, I32, I32, I32, F64, P, SZ, IP,
                                DP, P]),
+    "fem_mg_pcg_solve_mixed": (I32, [I32, I64, P, P, P, P, P, F64, F64, I32, I32, I32, P, I32, I32, I32, F64, P, SZ, IP,
+                               DP, P]),
     "fem_param_vjp_f64": (I32, [I32, DP, I32, I64, P, P, P, P, P, P, P]),
     "fem_bsr_spmv_f64": (I32, [I32, I64, P, P, P, P, P, P]),
     "fem_bsr_spmv_f32": (I32, [I32, I64, P, P, P, P, P, P]),

@@ -6,14 +6,19 @@
 // (problem.py:426-437) and the PETSc COO insertion + zeroRows of get_A
 // (solver.py:485-491).  The reference differentiates the kernel with 24
 // forward-mode JVPs per cell; here every law supplies its exact tangent in a
-// rank-structured form (see LawQuad below), so one evaluation per quadrature
+// rank-structured form (see law_quad below), so one evaluation per quadrature
 // point yields residual and tangent together.
+//
+// Precision: geometry, the constitutive update and the residual are FP64 in
+// every variant; the tangent (its per-quad factors in shared memory, the
+// node-pair products and the stored values) is FP64 or FP32.
 //
 // Work split: 12 threads per cell, 8 cells (96 threads) per block.
 //  phase 0  thread t < 8 loads node t of its cell (coords, u, Dirichlet data)
 //  phase 1  thread t < 8 = quadrature point q: geometry (J, det, grad N),
-//           grad u, the constitutive update, per-quad tangent factors -> smem
-//  phase 2  residual: thread t < 8 = node a, r_a;
+//           grad u, the constitutive update; P*JxW (FP64) and the tangent
+//           factors -> smem
+//  phase 2  residual: thread t < 8 = node a, r_a = sum_q P_q g_a,q in FP64;
 //           tangent: every element matrix here is symmetric, so only the 36
 //           node pairs a <= b are formed, three per thread.  Each pair goes
 //           to the block of the global upper triangle (row node < column
@@ -47,6 +52,7 @@ struct AsmArgs {
 };
 
 constexpr int kCellsPerBlock = 8;
+constexpr int kLiftBit = 8;  // node flag beside the Dirichlet bits 0..2: d != 0 at the node
 constexpr int kThreadsPerCell = 12;
 constexpr int kAsmThreads = kCellsPerBlock * kThreadsPerCell;
 
@@ -55,19 +61,19 @@ struct LawTraits {
   static constexpr int NV = (LAW == FEM_LAW_NEO_HOOKEAN) ? 2 : ((LAW == FEM_LAW_J2) ? 1 : 0);
 };
 
-// Per-quad record in shared memory (type T):
+// Per-quad record in shared memory (type T, the tangent's type):
 //   [0,24)            g_b  (physical shape gradients of the 8 nodes)
 //   [24, 24+24 NV)    law vectors per node (NH: F g_b, F^-T g_b; J2: s g_b)
-//   then VEC*3        P * JxW
 //   then 4            tangent coefficients * JxW
+// The stress P * JxW (and, with an FP32 record, the shape gradients) go to a
+// separate FP64 area, so the residual is FP64 whatever T is.
 template <int VEC, int LAW>
 struct QuadLayout {
   static constexpr int NV = LawTraits<LAW>::NV;
   static constexpr int G = 0;
   static constexpr int V1 = 24;
   static constexpr int V2 = 48;
-  static constexpr int P = 24 + 24 * NV;
-  static constexpr int C = P + VEC * 3;
+  static constexpr int C = 24 + 24 * NV;
   static constexpr int QF = C + 4;
 };
 
@@ -80,34 +86,40 @@ __host__ __device__ constexpr int padded_cell_elems(int n) {
 
 template <int VEC>
 struct NodeLayout {
-  static constexpr int X = 0;
   static constexpr int U = 3;
   static constexpr int D = 3 + VEC;
   static constexpr int NF = 3 + 2 * VEC;
 };
 
+// FP64 copies of the shape gradients for the residual, kept only when the
+// tangent record is FP32 (an FP64 record already holds them).
+template <typename T>
+__host__ __device__ constexpr int residual_g_elems() {
+  return sizeof(T) == 8 ? 0 : 24;
+}
+
 template <int VEC, int LAW, typename T>
 __host__ __device__ constexpr size_t asm_smem_bytes() {
   return size_t(kCellsPerBlock) * padded_cell_elems<T>(8 * QuadLayout<VEC, LAW>::QF) * sizeof(T) +
-         size_t(kCellsPerBlock) * 8 * NodeLayout<VEC>::NF * sizeof(double) +  // node data
-         size_t(kCellsPerBlock) * 8 * VEC * sizeof(double) +                  // lift accumulators
-         size_t(kCellsPerBlock) * 8 * 2 * sizeof(int);                        // BC bits, node ids
+         size_t(kCellsPerBlock) * 8 * (VEC * 3 + residual_g_elems<T>()) * sizeof(double) +  // P*JxW, g (FP64)
+         size_t(kCellsPerBlock) * 8 * NodeLayout<VEC>::NF * sizeof(double) +              // node data
+         size_t(kCellsPerBlock) * 8 * VEC * sizeof(double) +                              // lift accumulators
+         size_t(kCellsPerBlock) * 8 * 2 * sizeof(int);                                    // BC bits, node ids
 }
 
-// Phase 1: constitutive update at one quadrature point.
-// ug = grad u (VEC x 3, f64), g = physical shape gradients (f64),
-// writes P*JxW, coefficients*JxW and the per-node law vectors.
+// Phase 1: constitutive update at one quadrature point, in FP64.
+// ug = grad u (VEC x 3), g = physical shape gradients; returns P*JxW in P and
+// writes the tangent coefficients*JxW and per-node law vectors (as T).
 template <int VEC, int LAW, typename T>
 __device__ __forceinline__ void law_quad(const AsmArgs& A, int64_t c, int q, const double ug[VEC][3],
-                                         const double g[8][3], double jxw, T* qd) {
+                                         const double g[8][3], double jxw, T* qd, double* P) {
   using L = QuadLayout<VEC, LAW>;
-  T* P = qd + L::P;
   T* cf = qd + L::C;
   if constexpr (LAW == FEM_LAW_LAPLACE) {
 #pragma unroll
     for (int i = 0; i < VEC; ++i)
 #pragma unroll
-      for (int j = 0; j < 3; ++j) P[i * 3 + j] = T(ug[i][j] * jxw);
+      for (int j = 0; j < 3; ++j) P[i * 3 + j] = ug[i][j] * jxw;
     cf[0] = T(jxw);
     cf[1] = cf[2] = cf[3] = T(0);
   } else if constexpr (LAW == FEM_LAW_LINEAR || LAW == FEM_LAW_SIMP) {
@@ -121,33 +133,31 @@ __device__ __forceinline__ void law_quad(const AsmArgs& A, int64_t c, int q, con
       nu = A.p[2];
       E = Emin + (E0 - Emin) * pow(th, pen);
     }
-    const T mu = T(E / (2.0 * (1.0 + nu)));
-    const T lm = T(E * nu / ((1.0 + nu) * (1.0 - 2.0 * nu)));
-    const T w = T(jxw);
-    T eps[3][3];
+    const double mu = E / (2.0 * (1.0 + nu));
+    const double lm = E * nu / ((1.0 + nu) * (1.0 - 2.0 * nu));
+    double eps[3][3];
 #pragma unroll
     for (int i = 0; i < 3; ++i)
 #pragma unroll
-      for (int j = 0; j < 3; ++j) eps[i][j] = T(0.5) * (T(ug[i][j]) + T(ug[j][i]));
-    const T tr = eps[0][0] + eps[1][1] + eps[2][2];
+      for (int j = 0; j < 3; ++j) eps[i][j] = 0.5 * (ug[i][j] + ug[j][i]);
+    const double tr = eps[0][0] + eps[1][1] + eps[2][2];
 #pragma unroll
     for (int i = 0; i < 3; ++i)
 #pragma unroll
-      for (int j = 0; j < 3; ++j)
-        P[i * 3 + j] = w * (T(2) * mu * eps[i][j] + (i == j ? lm * tr : T(0)));
-    cf[0] = lm * w;
-    cf[1] = mu * w;
+      for (int j = 0; j < 3; ++j) P[i * 3 + j] = jxw * (2.0 * mu * eps[i][j] + (i == j ? lm * tr : 0.0));
+    cf[0] = T(lm * jxw);
+    cf[1] = T(mu * jxw);
     cf[2] = cf[3] = T(0);
   } else if constexpr (LAW == FEM_LAW_NEO_HOOKEAN) {
-    const T E = T(A.p[0]), nu = T(A.p[1]);
-    const T mu = E / (T(2) * (T(1) + nu));
-    const T kappa = E / (T(3) * (T(1) - T(2) * nu));
-    T F[3][3];
+    const double E = A.p[0], nu = A.p[1];
+    const double mu = E / (2.0 * (1.0 + nu));
+    const double kappa = E / (3.0 * (1.0 - 2.0 * nu));
+    double F[3][3];
 #pragma unroll
     for (int i = 0; i < 3; ++i)
 #pragma unroll
-      for (int j = 0; j < 3; ++j) F[i][j] = T(ug[i][j]) + (i == j ? T(1) : T(0));
-    T cof[3][3];
+      for (int j = 0; j < 3; ++j) F[i][j] = ug[i][j] + (i == j ? 1.0 : 0.0);
+    double cof[3][3];
     cof[0][0] = F[1][1] * F[2][2] - F[1][2] * F[2][1];
     cof[0][1] = F[1][2] * F[2][0] - F[1][0] * F[2][2];
     cof[0][2] = F[1][0] * F[2][1] - F[1][1] * F[2][0];
@@ -157,10 +167,10 @@ __device__ __forceinline__ void law_quad(const AsmArgs& A, int64_t c, int q, con
     cof[2][0] = F[0][1] * F[1][2] - F[0][2] * F[1][1];
     cof[2][1] = F[0][2] * F[1][0] - F[0][0] * F[1][2];
     cof[2][2] = F[0][0] * F[1][1] - F[0][1] * F[1][0];
-    const T J = F[0][0] * cof[0][0] + F[0][1] * cof[0][1] + F[0][2] * cof[0][2];
-    const T iJ = T(1) / J;
-    T H[3][3];  // F^{-T}
-    T I1 = T(0);
+    const double J = F[0][0] * cof[0][0] + F[0][1] * cof[0][1] + F[0][2] * cof[0][2];
+    const double iJ = 1.0 / J;
+    double H[3][3];  // F^{-T}
+    double I1 = 0.0;
 #pragma unroll
     for (int i = 0; i < 3; ++i)
 #pragma unroll
@@ -168,86 +178,81 @@ __device__ __forceinline__ void law_quad(const AsmArgs& A, int64_t c, int q, con
         H[i][j] = cof[i][j] * iJ;
         I1 += F[i][j] * F[i][j];
       }
-    const T cb = cbrt(J);
-    const T m = mu / (cb * cb);  // mu J^{-2/3}
-    T scale = T(jxw);
-    if (A.iv0 != nullptr) scale *= T(A.iv0[c * 8 + q]);
-    const T kJ1 = kappa * J * (J - T(1));
+    const double cb = cbrt(J);
+    const double m = mu / (cb * cb);  // mu J^{-2/3}
+    double scale = jxw;
+    if (A.iv0 != nullptr) scale *= A.iv0[c * 8 + q];
+    const double kJ1 = kappa * J * (J - 1.0);
 #pragma unroll
     for (int i = 0; i < 3; ++i)
 #pragma unroll
-      for (int j = 0; j < 3; ++j)
-        P[i * 3 + j] = scale * (m * (F[i][j] - I1 * H[i][j] / T(3)) + kJ1 * H[i][j]);
+      for (int j = 0; j < 3; ++j) P[i * 3 + j] = scale * (m * (F[i][j] - I1 * H[i][j] / 3.0) + kJ1 * H[i][j]);
     // K_ab = m (ga.gb) I - 2/3 m (f_a (x) h_b + h_a (x) f_b)
     //        + (2/9 m I1 + kappa (2J-1) J) h_a (x) h_b + (1/3 m I1 - kappa J (J-1)) h_b (x) h_a
-    cf[0] = scale * m;
-    cf[1] = scale * (T(-2) / T(3)) * m;
-    cf[2] = scale * (T(2) / T(9) * m * I1 + kappa * (T(2) * J - T(1)) * J);
-    cf[3] = scale * (m * I1 / T(3) - kJ1);
-    T* v1 = qd + QuadLayout<VEC, LAW>::V1;
-    T* v2 = qd + QuadLayout<VEC, LAW>::V2;
+    cf[0] = T(scale * m);
+    cf[1] = T(scale * (-2.0 / 3.0) * m);
+    cf[2] = T(scale * (2.0 / 9.0 * m * I1 + kappa * (2.0 * J - 1.0) * J));
+    cf[3] = T(scale * (m * I1 / 3.0 - kJ1));
+    T* v1 = qd + L::V1;
+    T* v2 = qd + L::V2;
 #pragma unroll
     for (int b = 0; b < 8; ++b) {
-      const T gb0 = T(g[b][0]), gb1 = T(g[b][1]), gb2 = T(g[b][2]);
 #pragma unroll
       for (int i = 0; i < 3; ++i) {
-        v1[b * 3 + i] = F[i][0] * gb0 + F[i][1] * gb1 + F[i][2] * gb2;
-        v2[b * 3 + i] = H[i][0] * gb0 + H[i][1] * gb1 + H[i][2] * gb2;
+        v1[b * 3 + i] = T(F[i][0] * g[b][0] + F[i][1] * g[b][1] + F[i][2] * g[b][2]);
+        v2[b * 3 + i] = T(H[i][0] * g[b][0] + H[i][1] * g[b][1] + H[i][2] * g[b][2]);
       }
     }
   } else if constexpr (LAW == FEM_LAW_J2) {
-    const T E = T(A.p[0]), nu = T(A.p[1]), sy0 = T(A.p[2]), Hh = T(A.p[3]);
-    const T mu = E / (T(2) * (T(1) + nu));
-    const T lm = E * nu / ((T(1) + nu) * (T(1) - T(2) * nu));
+    const double E = A.p[0], nu = A.p[1], sy0 = A.p[2], Hh = A.p[3];
+    const double mu = E / (2.0 * (1.0 + nu));
+    const double lm = E * nu / ((1.0 + nu) * (1.0 - 2.0 * nu));
     const double* so = A.iv0 + (c * 8 + q) * 9;
     const double* eo = A.iv1 + (c * 8 + q) * 9;
-    const T alpha = T(A.iv2[c * 8 + q]);
-    T de[3][3], st[3][3];
+    const double alpha = A.iv2[c * 8 + q];
+    double de[3][3], st[3][3];
 #pragma unroll
     for (int i = 0; i < 3; ++i)
 #pragma unroll
-      for (int j = 0; j < 3; ++j) de[i][j] = T(0.5) * (T(ug[i][j]) + T(ug[j][i])) - T(eo[i * 3 + j]);
-    const T trd = de[0][0] + de[1][1] + de[2][2];
+      for (int j = 0; j < 3; ++j) de[i][j] = 0.5 * (ug[i][j] + ug[j][i]) - eo[i * 3 + j];
+    const double trd = de[0][0] + de[1][1] + de[2][2];
 #pragma unroll
     for (int i = 0; i < 3; ++i)
 #pragma unroll
-      for (int j = 0; j < 3; ++j)
-        st[i][j] = T(2) * mu * de[i][j] + (i == j ? lm * trd : T(0)) + T(so[i * 3 + j]);
-    const T trs = (st[0][0] + st[1][1] + st[2][2]) / T(3);
-    T s[3][3];
-    T ss = T(0);
+      for (int j = 0; j < 3; ++j) st[i][j] = 2.0 * mu * de[i][j] + (i == j ? lm * trd : 0.0) + so[i * 3 + j];
+    const double trs = (st[0][0] + st[1][1] + st[2][2]) / 3.0;
+    double s[3][3];
+    double ss = 0.0;
 #pragma unroll
     for (int i = 0; i < 3; ++i)
 #pragma unroll
       for (int j = 0; j < 3; ++j) {
-        s[i][j] = st[i][j] - (i == j ? trs : T(0));
+        s[i][j] = st[i][j] - (i == j ? trs : 0.0);
         ss += s[i][j] * s[i][j];
       }
-    const T qv = ss > T(0) ? sqrt(T(1.5) * ss) : T(0);
-    const T syc = sy0 + Hh * alpha;
-    const T f = qv - syc;
-    T beta = T(0), gam2 = T(0);
-    if (f > T(0)) {
-      const T dg = f / (T(3) * mu + Hh);
-      beta = T(3) * mu * dg / qv;
-      gam2 = T(9) * mu * mu * syc / ((T(3) * mu + Hh) * qv * qv * qv);
+    const double qv = ss > 0.0 ? sqrt(1.5 * ss) : 0.0;
+    const double syc = sy0 + Hh * alpha;
+    const double f = qv - syc;
+    double beta = 0.0, gam2 = 0.0;
+    if (f > 0.0) {
+      const double dg = f / (3.0 * mu + Hh);
+      beta = 3.0 * mu * dg / qv;
+      gam2 = 9.0 * mu * mu * syc / ((3.0 * mu + Hh) * qv * qv * qv);
     }
-    const T w = T(jxw);
 #pragma unroll
     for (int i = 0; i < 3; ++i)
 #pragma unroll
-      for (int j = 0; j < 3; ++j) P[i * 3 + j] = w * (st[i][j] - beta * s[i][j]);
+      for (int j = 0; j < 3; ++j) P[i * 3 + j] = jxw * (st[i][j] - beta * s[i][j]);
     // K_ab = cII ga (x) gb + (csym/2) ((ga.gb) I + gb (x) ga) - gam2 (s ga) (x) (s gb)
-    cf[0] = w * (lm + T(2) * mu * beta / T(3));
-    cf[1] = w * mu * (T(1) - beta);
-    cf[2] = w * gam2;
+    cf[0] = T(jxw * (lm + 2.0 * mu * beta / 3.0));
+    cf[1] = T(jxw * mu * (1.0 - beta));
+    cf[2] = T(jxw * gam2);
     cf[3] = T(0);
-    T* v1 = qd + QuadLayout<VEC, LAW>::V1;
+    T* v1 = qd + L::V1;
 #pragma unroll
     for (int b = 0; b < 8; ++b)
 #pragma unroll
-      for (int i = 0; i < 3; ++i)
-        v1[b * 3 + i] = s[i][0] * T(g[b][0]) + s[i][1] * T(g[b][1]) + s[i][2] * T(g[b][2]);
+      for (int i = 0; i < 3; ++i) v1[b * 3 + i] = T(s[i][0] * g[b][0] + s[i][1] * g[b][1] + s[i][2] * g[b][2]);
   }
 }
 
@@ -320,13 +325,24 @@ __constant__ unsigned char kPairB[36] = {0, 1, 2, 3, 4, 5, 6, 7, 1, 2, 3, 4, 5, 
                                          5, 6, 7, 3, 4, 5, 6, 7, 4, 5, 6, 7, 5, 6, 7, 6, 7, 7};
 
 template <int VEC, int LAW, typename T, bool WANT_K>
-__global__ void __launch_bounds__(kAsmThreads) assemble_kernel(const AsmArgs A) {
+#ifndef FEM_ASM_MIN_BLOCKS_F32
+#define FEM_ASM_MIN_BLOCKS_F32 5
+#endif
+#ifndef FEM_ASM_MIN_BLOCKS_F64
+#define FEM_ASM_MIN_BLOCKS_F64 4
+#endif
+// Resident blocks per SM: shared memory allows about 5 (FP32 records) and 4
+// (FP64 records); the register budget is held to match.
+__global__ void __launch_bounds__(kAsmThreads, sizeof(T) == 4 ? FEM_ASM_MIN_BLOCKS_F32 : FEM_ASM_MIN_BLOCKS_F64)
+    assemble_kernel(const AsmArgs A) {
   using L = QuadLayout<VEC, LAW>;
   using N = NodeLayout<VEC>;
   constexpr int CELLF = padded_cell_elems<T>(8 * L::QF);
   extern __shared__ __align__(16) unsigned char smem[];
   T* sq = reinterpret_cast<T*>(smem);
-  double* sn = reinterpret_cast<double*>(smem + size_t(kCellsPerBlock) * CELLF * sizeof(T));
+  constexpr int QD = VEC * 3 + residual_g_elems<T>();  // per-quad FP64 residual data: P*JxW, then g
+  double* sP = reinterpret_cast<double*>(smem + size_t(kCellsPerBlock) * CELLF * sizeof(T));
+  double* sn = sP + kCellsPerBlock * 8 * QD;
   double* slift = sn + kCellsPerBlock * 8 * N::NF;
   int* sbc = reinterpret_cast<int*>(slift + kCellsPerBlock * 8 * VEC);
   int* snode = sbc + kCellsPerBlock * 8;
@@ -356,6 +372,7 @@ __global__ void __launch_bounds__(kAsmThreads) assemble_kernel(const AsmArgs A) 
       nd[N::U + i] = valid ? A.u[dof] : 0.0;
       nd[N::D + i] = (valid && A.dvec != nullptr) ? A.dvec[dof] : 0.0;
       if (valid && A.bc != nullptr && A.bc[dof]) bits |= 1 << i;
+      if (nd[N::D + i] != 0.0) bits |= kLiftBit;
       slift[(cl * 8 + t) * VEC + i] = 0.0;
     }
     sbc[cl * 8 + t] = bits;
@@ -393,23 +410,32 @@ __global__ void __launch_bounds__(kAsmThreads) assemble_kernel(const AsmArgs A) 
     for (int b = 0; b < 8; ++b)
 #pragma unroll
       for (int j = 0; j < 3; ++j) qd[L::G + b * 3 + j] = T(g[b][j]);
-    law_quad<VEC, LAW, T>(A, valid ? c : 0, q, ug, g, jxw, qd);
+    double* pq = sP + (cl * 8 + q) * QD;
+    law_quad<VEC, LAW, T>(A, valid ? c : 0, q, ug, g, jxw, qd, pq);
+    if constexpr (residual_g_elems<T>() > 0) {
+#pragma unroll
+      for (int b = 0; b < 8; ++b)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) pq[VEC * 3 + b * 3 + j] = g[b][j];
+    }
   }
   __syncthreads();
 
-  // ---- phase 2a: residual of node a = t ----
+  // ---- phase 2a: residual of node a = t, r_a = sum_q P_q g_a,q (FP64) ----
   if (valid && t < 8 && A.res != nullptr) {
     const int a = t;
     double r[VEC];
 #pragma unroll
     for (int i = 0; i < VEC; ++i) r[i] = 0.0;
-#pragma unroll
+#pragma unroll 1
     for (int q = 0; q < 8; ++q) {
-      const T* qd = cq + q * L::QF;
-      const T g0 = qd[L::G + a * 3], g1 = qd[L::G + a * 3 + 1], g2 = qd[L::G + a * 3 + 2];
+      const double* pq = sP + (cl * 8 + q) * QD;
+      double ga[3];
 #pragma unroll
-      for (int i = 0; i < VEC; ++i)
-        r[i] += double(qd[L::P + i * 3] * g0 + qd[L::P + i * 3 + 1] * g1 + qd[L::P + i * 3 + 2] * g2);
+      for (int j = 0; j < 3; ++j)
+        ga[j] = residual_g_elems<T>() > 0 ? pq[VEC * 3 + a * 3 + j] : double(cq[q * L::QF + L::G + a * 3 + j]);
+#pragma unroll
+      for (int i = 0; i < VEC; ++i) r[i] += pq[i * 3] * ga[0] + pq[i * 3 + 1] * ga[1] + pq[i * 3 + 2] * ga[2];
     }
     const int64_t node = snode[cl * 8 + a];
 #pragma unroll
@@ -431,8 +457,8 @@ __global__ void __launch_bounds__(kAsmThreads) assemble_kernel(const AsmArgs A) 
 #pragma unroll 2
         for (int q = 0; q < 8; ++q) pair_block<VEC, LAW, T>(cq + q * L::QF, a, b, K);
         const int abits = sbc[cl * 8 + a], bbits = sbc[cl * 8 + b];
-        if (A.lift != nullptr) {
-          // row a: K_ab d_b; row b (a != b): K_ab^T d_a
+        if (A.lift != nullptr && (bbits & kLiftBit)) {
+          // row a: K_ab d_b (only a node with non-zero d contributes)
 #pragma unroll
           for (int i = 0; i < VEC; ++i) {
             double la = 0.0;
@@ -440,14 +466,15 @@ __global__ void __launch_bounds__(kAsmThreads) assemble_kernel(const AsmArgs A) 
             for (int k = 0; k < VEC; ++k) la += double(K[i][k]) * nb[b * N::NF + N::D + k];
             atomicAdd(slift + (cl * 8 + a) * VEC + i, la);
           }
-          if (a != b) {
+        }
+        if (A.lift != nullptr && a != b && (abits & kLiftBit)) {
+          // row b: K_ab^T d_a
 #pragma unroll
-            for (int k = 0; k < VEC; ++k) {
-              double lb = 0.0;
+          for (int k = 0; k < VEC; ++k) {
+            double lb = 0.0;
 #pragma unroll
-              for (int i = 0; i < VEC; ++i) lb += double(K[i][k]) * nb[a * N::NF + N::D + i];
-              atomicAdd(slift + (cl * 8 + b) * VEC + k, lb);
-            }
+            for (int i = 0; i < VEC; ++i) lb += double(K[i][k]) * nb[a * N::NF + N::D + i];
+            atomicAdd(slift + (cl * 8 + b) * VEC + k, lb);
           }
         }
         if (vals != nullptr) {
@@ -474,7 +501,11 @@ __global__ void __launch_bounds__(kAsmThreads) assemble_kernel(const AsmArgs A) 
     }
     if (A.lift != nullptr) {
       __syncthreads();
-      if (valid && t < 8) {
+      // the cell's lift is non-zero only if one of its nodes has non-zero d
+      int any = 0;
+#pragma unroll
+      for (int b = 0; b < 8; ++b) any |= sbc[cl * 8 + b];
+      if (valid && t < 8 && (any & kLiftBit)) {
         const int abits = sbc[cl * 8 + t];
         const int64_t node = snode[cl * 8 + t];
 #pragma unroll

@@ -358,12 +358,12 @@ __global__ void __launch_bounds__(kRowThreads, kRowBlocksPerSM)
       });
 }
 
-// r = b - A x
-template <int VEC, typename T>
+// r = b - A x (values VT, vectors and row sums T)
+template <int VEC, typename VT, typename T>
 __global__ void __launch_bounds__(kRowThreads, kRowBlocksPerSM)
-    mg_residual_kernel(int64_t n_brows, const int32_t* rp, const int32_t* ci, const T* vals, const T* __restrict__ x,
+    mg_residual_kernel(int64_t n_brows, const int32_t* rp, const int32_t* ci, const VT* vals, const T* __restrict__ x,
                        const T* b, T* r) {
-  bsr_rows<VEC, T, T>(
+  bsr_rows<VEC, VT, T>(
       n_brows, rp, ci, vals, [&](int64_t i) { return x[i]; },
       [&](int64_t row, int comp, T q) {
         const int64_t i = row * VEC + comp;
@@ -403,7 +403,7 @@ int ensure_attrs() {
   int rc;
   if ((rc = ensure_smem_attr(cheb_step_kernel<VEC, T>)) != FEM_OK) return rc;
   if ((rc = ensure_smem_attr(cheb_resid_kernel<VEC, T>)) != FEM_OK) return rc;
-  if ((rc = ensure_smem_attr(mg_residual_kernel<VEC, T>)) != FEM_OK) return rc;
+  if ((rc = ensure_smem_attr(mg_residual_kernel<VEC, T, T>)) != FEM_OK) return rc;
   return FEM_OK;
 }
 
@@ -489,7 +489,7 @@ int vcycle_level(int l, int nlevels, const FemMGLevel* L, int nu, int coarse_ste
   if ((rc = vcycle_level<VEC, T>(l + 1, nlevels, L, nu, coarse_steps, ratio, bc, xc, st)) != FEM_OK) return rc;
   prolong_add_kernel<VEC, T><<<vgrid(L[l].n_brows), 256, 0, st>>>(lat_of(L[l]), lat_of(C), C.ilo, C.whi, xc, x);
   FEM_LAUNCH_CHECK();
-  mg_residual_kernel<VEC, T><<<row_grid<T>(L[l].n_brows), kRowThreads, bsr_rows_smem(), st>>>(
+  mg_residual_kernel<VEC, T, T><<<row_grid<T>(L[l].n_brows), kRowThreads, bsr_rows_smem(), st>>>(
       L[l].n_brows, L[l].row_ptr, L[l].col_idx, static_cast<const T*>(L[l].vals), x, b, static_cast<T*>(L[l].r));
   FEM_LAUNCH_CHECK();
   return smooth<VEC, T>(L[l], b, x, nu, ratio, false, false, st);
@@ -569,13 +569,13 @@ __global__ void pcg_dir_kernel(int64_t n, const ZT* z, double* p, const PState* 
 }
 
 // q = A p; pq = p.q; alpha = gamma / pq
-template <int VEC>
+template <int VEC, typename VT>
 __global__ void __launch_bounds__(kRowThreads, kRowBlocksPerSM)
-    pcg_spmv_kernel(int64_t n_brows, const int32_t* rp, const int32_t* ci, const double* vals, const double* __restrict__ p,
+    pcg_spmv_kernel(int64_t n_brows, const int32_t* rp, const int32_t* ci, const VT* vals, const double* __restrict__ p,
                     double* q, double* partials, unsigned* counter, PState* S) {
   if (S->status != PS_RUNNING) return;
   double v[1] = {0.0};
-  bsr_rows<VEC, double, double>(
+  bsr_rows<VEC, VT, double>(
       n_brows, rp, ci, vals, [&](int64_t i) { return p[i]; },
       [&](int64_t row, int c, double qo) {
         const int64_t i = row * VEC + c;
@@ -721,8 +721,8 @@ size_t pcg_workspace_bytes(int vec, int64_t n_brows) {
   return 256 + 256 + al256(size_t(num_sms()) * 8 * 4 * sizeof(double)) + 4 * al256(n * sizeof(double));
 }
 
-template <int VEC>
-int pcg_impl(int64_t n_brows, const int32_t* rp, const int32_t* ci, const double* vals, const double* b, double* x,
+template <int VEC, typename VT>
+int pcg_impl(int64_t n_brows, const int32_t* rp, const int32_t* ci, const VT* vals, const double* b, double* x,
              double rtol, double atol, int maxiter, int check_every, int nlevels, const FemMGLevel* L, int fp32,
              int nu, int coarse_steps, double ratio, void* work, size_t work_bytes, int* h_iters, double* h_relres,
              cudaStream_t st) {
@@ -745,8 +745,8 @@ int pcg_impl(int64_t n_brows, const int32_t* rp, const int32_t* ci, const double
   double* pv = reinterpret_cast<double*>(p8 + 2 * al256(n * sizeof(double)));
   double* q = reinterpret_cast<double*>(p8 + 3 * al256(n * sizeof(double)));
   int rc;
-  if ((rc = ensure_smem_attr(pcg_spmv_kernel<VEC>)) != FEM_OK) return rc;
-  if ((rc = ensure_smem_attr(mg_residual_kernel<VEC, double>)) != FEM_OK) return rc;
+  if ((rc = ensure_smem_attr(pcg_spmv_kernel<VEC, VT>)) != FEM_OK) return rc;
+  if ((rc = ensure_smem_attr(mg_residual_kernel<VEC, VT, double>)) != FEM_OK) return rc;
   if ((rc = (fp32 ? ensure_attrs<VEC, float>() : ensure_attrs<VEC, double>())) != FEM_OK) return rc;
   FEM_CUDA_TRY(cudaMemsetAsync(work, 0, 512, st));
   FEM_CUDA_TRY(cudaMemsetAsync(pv, 0, sizeof(double) * n, st));
@@ -758,7 +758,7 @@ int pcg_impl(int64_t n_brows, const int32_t* rp, const int32_t* ci, const double
   float* r32 = fp32 ? static_cast<float*>(L[0].b) : nullptr;
   float* z32 = fp32 ? static_cast<float*>(L[0].x) : nullptr;
   // r = b - A x, the reductions and status
-  mg_residual_kernel<VEC, double><<<rg, kRowThreads, bsr_rows_smem(), st>>>(n_brows, rp, ci, vals, x, b, r);
+  mg_residual_kernel<VEC, VT, double><<<rg, kRowThreads, bsr_rows_smem(), st>>>(n_brows, rp, ci, vals, x, b, r);
   FEM_LAUNCH_CHECK();
   pcg_init_kernel<VEC><<<vg, 256, 0, st>>>(n, r, b, partials, counter, S, rtol, atol);
   FEM_LAUNCH_CHECK();
@@ -790,7 +790,8 @@ int pcg_impl(int64_t n_brows, const int32_t* rp, const int32_t* ci, const double
     FEM_LAUNCH_CHECK();
     pcg_dir_kernel<double><<<vg, 256, 0, ls>>>(n, z, pv, S);
     FEM_LAUNCH_CHECK();
-    pcg_spmv_kernel<VEC><<<rg, kRowThreads, bsr_rows_smem(), ls>>>(n_brows, rp, ci, vals, pv, q, partials, counter, S);
+    pcg_spmv_kernel<VEC, VT><<<rg, kRowThreads, bsr_rows_smem(), ls>>>(n_brows, rp, ci, vals, pv, q, partials, counter,
+                                                                     S);
     FEM_LAUNCH_CHECK();
     pcg_update_kernel<<<vg, 256, 0, ls>>>(n, x, r, pv, q, r32, partials, counter, S);
     FEM_LAUNCH_CHECK();
@@ -805,7 +806,7 @@ int pcg_impl(int64_t n_brows, const int32_t* rp, const int32_t* ci, const double
     const void* ptrs[] = {rp, ci, vals, b, x, work};
     key.append(reinterpret_cast<const char*>(ptrs), sizeof(ptrs));
     const double params[] = {double(nlevels), double(fp32), double(nu), double(coarse_steps), ratio, double(n_brows),
-                             double(VEC)};
+                             double(VEC), double(sizeof(VT))};
     key.append(reinterpret_cast<const char*>(params), sizeof(params));
     int dev = 0;
     cudaGetDevice(&dev);
@@ -852,7 +853,7 @@ int pcg_impl(int64_t n_brows, const int32_t* rp, const int32_t* ci, const double
   const int iters = hs->iter;
   const double bb = hs->bb;
   // report the true residual ||b - A x||
-  mg_residual_kernel<VEC, double><<<rg, kRowThreads, bsr_rows_smem(), st>>>(n_brows, rp, ci, vals, x, b, q);
+  mg_residual_kernel<VEC, VT, double><<<rg, kRowThreads, bsr_rows_smem(), st>>>(n_brows, rp, ci, vals, x, b, q);
   FEM_LAUNCH_CHECK();
   FEM_CUDA_TRY(cudaMemsetAsync(counter, 0, sizeof(unsigned), st));
   pcg_init_kernel<VEC><<<vg, 256, 0, st>>>(n, q, b, partials, counter, S, rtol, atol);
@@ -914,11 +915,13 @@ extern "C" int fem_mg_vcycle_f32(int vec, int nlevels, const FemMGLevel* levels,
 
 extern "C" size_t fem_mg_pcg_workspace_bytes(int vec, int64_t n_brows) { return pcg_workspace_bytes(vec, n_brows); }
 
-extern "C" int fem_mg_pcg_solve(int vec, int64_t n_brows, const int32_t* d_row_ptr, const int32_t* d_col_idx,
-                                const double* d_vals, const double* d_b, double* d_x, double rtol, double atol,
-                                int maxiter, int check_every, int nlevels, const FemMGLevel* levels, int levels_fp32,
-                                int nu, int coarse_steps, double ratio, void* d_work, size_t work_bytes, int* h_iters,
-                                double* h_relres, void* stream) {
+namespace fem {
+namespace {
+template <typename VT>
+int pcg_entry(int vec, int64_t n_brows, const int32_t* d_row_ptr, const int32_t* d_col_idx, const VT* d_vals,
+              const double* d_b, double* d_x, double rtol, double atol, int maxiter, int check_every, int nlevels,
+              const FemMGLevel* levels, int levels_fp32, int nu, int coarse_steps, double ratio, void* d_work,
+              size_t work_bytes, int* h_iters, double* h_relres, void* stream) {
   FEM_CHECK_ARG(vec == 1 || vec == 3, "vec must be 1 or 3");
   FEM_CHECK_ARG(rtol >= 0 && atol >= 0, "negative tolerance");
   int rc = levels_fp32 ? (vec == 3 ? check_levels<3, float>(nlevels, levels) : check_levels<1, float>(nlevels, levels))
@@ -927,10 +930,32 @@ extern "C" int fem_mg_pcg_solve(int vec, int64_t n_brows, const int32_t* d_row_p
   FEM_CHECK_ARG(nu >= 1 && nu <= 16 && coarse_steps >= 1 && coarse_steps <= 512 && ratio > 1.0,
                 "nu in [1,16], coarse_steps in [1,512], ratio > 1");
   auto st = as_stream(stream);
-  return vec == 3 ? pcg_impl<3>(n_brows, d_row_ptr, d_col_idx, d_vals, d_b, d_x, rtol, atol, maxiter, check_every,
-                                nlevels, levels, levels_fp32, nu, coarse_steps, ratio, d_work, work_bytes, h_iters,
-                                h_relres, st)
-                  : pcg_impl<1>(n_brows, d_row_ptr, d_col_idx, d_vals, d_b, d_x, rtol, atol, maxiter, check_every,
-                                nlevels, levels, levels_fp32, nu, coarse_steps, ratio, d_work, work_bytes, h_iters,
-                                h_relres, st);
+  return vec == 3 ? pcg_impl<3, VT>(n_brows, d_row_ptr, d_col_idx, d_vals, d_b, d_x, rtol, atol, maxiter, check_every,
+                                    nlevels, levels, levels_fp32, nu, coarse_steps, ratio, d_work, work_bytes, h_iters,
+                                    h_relres, st)
+                  : pcg_impl<1, VT>(n_brows, d_row_ptr, d_col_idx, d_vals, d_b, d_x, rtol, atol, maxiter, check_every,
+                                    nlevels, levels, levels_fp32, nu, coarse_steps, ratio, d_work, work_bytes, h_iters,
+                                    h_relres, st);
+}
+}  // namespace
+}  // namespace fem
+
+extern "C" int fem_mg_pcg_solve(int vec, int64_t n_brows, const int32_t* d_row_ptr, const int32_t* d_col_idx,
+                                const double* d_vals, const double* d_b, double* d_x, double rtol, double atol,
+                                int maxiter, int check_every, int nlevels, const FemMGLevel* levels, int levels_fp32,
+                                int nu, int coarse_steps, double ratio, void* d_work, size_t work_bytes, int* h_iters,
+                                double* h_relres, void* stream) {
+  return pcg_entry<double>(vec, n_brows, d_row_ptr, d_col_idx, d_vals, d_b, d_x, rtol, atol, maxiter, check_every,
+                           nlevels, levels, levels_fp32, nu, coarse_steps, ratio, d_work, work_bytes, h_iters, h_relres,
+                           stream);
+}
+
+extern "C" int fem_mg_pcg_solve_mixed(int vec, int64_t n_brows, const int32_t* d_row_ptr, const int32_t* d_col_idx,
+                                      const float* d_vals, const double* d_b, double* d_x, double rtol, double atol,
+                                      int maxiter, int check_every, int nlevels, const FemMGLevel* levels,
+                                      int levels_fp32, int nu, int coarse_steps, double ratio, void* d_work,
+                                      size_t work_bytes, int* h_iters, double* h_relres, void* stream) {
+  return pcg_entry<float>(vec, n_brows, d_row_ptr, d_col_idx, d_vals, d_b, d_x, rtol, atol, maxiter, check_every,
+                          nlevels, levels, levels_fp32, nu, coarse_steps, ratio, d_work, work_bytes, h_iters, h_relres,
+                          stream);
 }

@@ -167,18 +167,26 @@ class Multigrid:
         self._scratch = torch.empty(max(int(nb), 16), dtype=torch.uint8, device=dev)
 
     def setup(self, A, fine_only=False):
-        """Coarse operators and smoother bounds for the FP64 operator A
-        (a ``BSRMatrix`` on this mesh's pattern).  With ``fine_only`` only
-        the finest level takes A's values (and its Jacobi scaling and bound);
-        the coarse levels keep the operators of the last full setup."""
+        """Coarse operators and smoother bounds for the operator A (a
+        ``BSRMatrix`` on this mesh's pattern): FP64, or FP32 for an FP32
+        hierarchy (then its finest level is A itself).  With ``fine_only``
+        only the finest level takes A's values (and its Jacobi scaling and
+        bound); the coarse levels keep the operators of the last full setup."""
         lib = nat.lib()
-        if A.vals.dtype != torch.float64:
-            raise TypeError("the multigrid hierarchy is formed from the FP64 operator")
+        if A.vals.dtype != torch.float64 and not (self.fp32 and A.vals.dtype == torch.float32):
+            raise TypeError("the multigrid hierarchy is formed from the FP64 operator (or FP32 for an FP32 hierarchy)")
         if fine_only and self.setup_for is None:
             raise RuntimeError("fine_only needs an earlier full setup")
         nl = 1 if fine_only else self.nlevels
         if self.fp32:
-            nat.check(lib.fem_mg_setup_f32(self.vec, nl, ctypes.byref(self.levels), nat.ptr(A.vals),
+            fine64 = None
+            if A.vals.dtype == torch.float32:
+                self.levels[0].vals = A.vals.data_ptr()
+                self._fine32 = A.vals
+            else:
+                self.levels[0].vals = self.mats[0][2].data_ptr()
+                fine64 = nat.ptr(A.vals)
+            nat.check(lib.fem_mg_setup_f32(self.vec, nl, ctypes.byref(self.levels), fine64,
                                            nat.ptr(self._scratch), self._scratch.numel(), nat.stream_ptr()),
                       "mg_setup_f32")
         else:
@@ -202,8 +210,9 @@ class Multigrid:
                      nat.ptr(rhs), nat.ptr(z), nat.stream_ptr()), "mg_vcycle")
 
     def solve(self, A, b, x, rtol, atol=0.0, maxiter=1000, nu=2, coarse_steps=8, ratio=25.0, check_every=4):
-        """CG on A x = b (FP64) with one V-cycle per iteration; x holds the
-        initial guess.  Returns (iterations, true relative residual)."""
+        """CG on A x = b with one V-cycle per iteration; x holds the initial
+        guess.  CG is FP64; A is FP64, or FP32 (the products accumulate in
+        FP64).  Returns (iterations, true relative residual)."""
         lib = nat.lib()
         n_brows = A.n_brows
         nb = lib.fem_mg_pcg_workspace_bytes(self.vec, n_brows)
@@ -211,7 +220,10 @@ class Multigrid:
             self._work = torch.empty(int(nb), dtype=torch.uint8, device=b.device)
         it = ctypes.c_int(0)
         rel = ctypes.c_double(0.0)
-        nat.check(lib.fem_mg_pcg_solve(self.vec, n_brows, nat.ptr(A.row_ptr), nat.ptr(A.col_idx), nat.ptr(A.vals),
+        if A.vals.dtype == torch.float32 and not self.fp32:
+            raise TypeError("an FP32 operator needs the FP32 hierarchy")
+        fn = lib.fem_mg_pcg_solve_mixed if A.vals.dtype == torch.float32 else lib.fem_mg_pcg_solve
+        nat.check(fn(self.vec, n_brows, nat.ptr(A.row_ptr), nat.ptr(A.col_idx), nat.ptr(A.vals),
                                        nat.ptr(b), nat.ptr(x), float(rtol), float(atol), int(maxiter),
                                        int(check_every), self.nlevels, ctypes.byref(self.levels), int(self.fp32),
                                        int(nu), int(coarse_steps), float(ratio), nat.ptr(self._work), int(nb),

@@ -79,15 +79,24 @@ def test_residual_tangent_lift_f64(pkg, cuda, kind):
 @pytest.mark.gpu
 @pytest.mark.parametrize("kind", ["linear", "neo_hookean", "j2"])
 def test_tangent_f32(pkg, cuda, kind):
+    """The FP32-tangent pass: tangent within FP32 rounding of the FP64 one,
+    residual FP64 (as the FP64 pass gives it), lift from the FP32 tangent."""
     prob, oprob, u = _setup(pkg, kind, seed=1)
     ud = torch.tensor(u, device=cuda)
+    n = ud.numel()
+    mask, _ = prob.dirichlet_device()
+    dvec = torch.where(mask.bool(), torch.full_like(ud, 1e-3), torch.zeros_like(ud))
     A32 = prob.dev().new_matrix(torch.float32)
-    prob.assemble(ud, vals=A32.vals, fp32=True)
+    r32, l32 = torch.empty(n, dtype=torch.float64, device=cuda), torch.empty(n, dtype=torch.float64, device=cuda)
+    prob.assemble(ud, res=r32, vals=A32.vals, lift=l32, dvec=dvec, fp32=True)
     A64 = prob.dev().new_matrix(torch.float64)
-    prob.assemble(ud, vals=A64.vals)
+    r64, l64 = torch.empty_like(r32), torch.empty_like(l32)
+    prob.assemble(ud, res=r64, vals=A64.vals, lift=l64, dvec=dvec)
     torch.cuda.synchronize()
     d = (A32.vals.double() - A64.vals).abs().max().item()
-    assert d <= 2e-5 * A64.vals.abs().max().item()
+    assert d <= 1e-5 * A64.vals.abs().max().item()
+    assert (r32 - r64).abs().max().item() <= 1e-13 * r64.abs().max().item()
+    assert (l32 - l64).abs().max().item() <= 1e-5 * max(l64.abs().max().item(), 1e-300)
 
 
 @pytest.mark.gpu

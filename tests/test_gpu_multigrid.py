@@ -123,6 +123,32 @@ def test_mg_pcg_matches_direct_solve(pkg, cuda, fp32):
     assert its * 3 < its_bj
 
 
+@pytest.mark.gpu
+def test_mg_pcg_on_fp32_operator(pkg, cuda):
+    """FP64 CG over an FP32 V-cycle on an FP32-assembled operator: the solve
+    is exact (1e-8) for the FP32 operator, whose values are the FP64
+    tangent's to FP32 rounding."""
+    mg, S = _mods()
+    prob, A = _graded_elastic(pkg, cuda, shape=(12, 10, 9))
+    A32 = prob.dev().new_matrix(torch.float32)
+    prob.assemble(torch.zeros(A.n_brows * 3, dtype=torch.float64, device=cuda), vals=A32.vals, fp32=True)
+    K32 = A32.to_scipy()
+    rng = np.random.default_rng(6)
+    b = rng.normal(size=K32.shape[0])
+    xref = spla.spsolve(K32.tocsc().astype(np.float64), b)
+    M = mg.Multigrid(prob.dev(), prob.mesh.points, prob.mesh.cells, fp32=True)
+    M.setup(A32)
+    x = torch.zeros(len(b), dtype=torch.float64, device=cuda)
+    its, rel = M.solve(A32, torch.tensor(b, device=cuda), x, rtol=1e-10)
+    assert rel <= 1e-10 * (1 + 1e-6)
+    assert np.abs(x.cpu().numpy() - xref).max() <= 1e-8 * np.abs(xref).max()
+    x64 = torch.zeros_like(x)
+    M64 = mg.Multigrid(prob.dev(), prob.mesh.points, prob.mesh.cells, fp32=True)
+    M64.setup(A)
+    its64, _ = M64.solve(A, torch.tensor(b, device=cuda), x64, rtol=1e-10)
+    assert abs(its - its64) <= 2
+
+
 _DIRECT_SCRIPT = r"""
 import sys, numpy as np, torch
 sys.path[:0] = [sys.argv[1], sys.argv[1] + "/tests"]
