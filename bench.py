@@ -373,11 +373,11 @@ def run_ours(args, rank, world, device):
         "higher_is_better": False,
         "scaling": "weak",
         "vs_baseline": None,
-        "dtype": "f64 tangent, residual and CG; f32 multigrid V-cycle",
+        "dtype": "f64 residual, CG vectors and reductions; f32 tangent values and multigrid V-cycle",
         "data": "synthetic",
         "config": {"workload": f"neo-hookean {args.n}^3 HEX8, 30 deg twist in 5 load steps, "
                                "Newton rel.res 1e-8", "dofs": ndofs, "cells": dv.num_cells,
-                   "precision": "mixed", "krylov": "cg (f64) preconditioned by a geometric multigrid v-cycle (f32)",
+                   "precision": "mixed", "krylov": "cg (f64 vectors, f32 tangent) preconditioned by a geometric multigrid v-cycle (f32)",
                    "l2": "flushed (256 MB write) between timed steps", "parallelism": f"replicas x{world}"},
         "plain_fp64_s": round(t_plain, 6),
         "speedup_vs_plain_fp64": round(t_plain / t_mixed, 3),
@@ -391,8 +391,9 @@ def run_ours(args, rank, world, device):
                          "iterations with reliable updates (FP64 solution, true residual, reductions); "
                          "mixed_tight = the same to the 1e-10 linear tolerance; mixed_refinement = FP32 CG "
                          "restarted inside FP64 iterative refinement; *_gmg = CG preconditioned by a geometric "
-                         "multigrid V-cycle (FP64 CG; V-cycle FP64 in plain_fp64_gmg, FP32 in mixed_gmg; "
-                         "coarse operators shared by up to 4 Newton solves, mg_lag 4); value = mixed_gmg",
+                         "multigrid V-cycle (FP64 CG; plain_fp64_gmg: FP64 tangent and V-cycle; mixed_gmg: FP32 "
+                         "tangent values and V-cycle; coarse operators shared by up to 4 Newton solves, mg_lag 4); "
+                         "value = mixed_gmg",
         "solves_per_s": round(world / t_mixed, 4),
         "newton_iters": newton,
         "krylov_iters": krylov,

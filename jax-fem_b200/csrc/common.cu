@@ -22,6 +22,15 @@ std::atomic<int64_t>& launch_counter() {
   return n;
 }
 
+bool pdl_enabled() {
+  static int on = -1;
+  if (on < 0) {
+    const char* e = std::getenv("FEM_PDL");
+    on = (e != nullptr && e[0] == '0') ? 0 : 1;
+  }
+  return on == 1;
+}
+
 double* host_mailbox() {
   static double* p = nullptr;
   if (p == nullptr) {

@@ -50,6 +50,34 @@ double* host_mailbox();
 
 inline cudaStream_t as_stream(void* s) { return reinterpret_cast<cudaStream_t>(s); }
 
+// ---- programmatic dependent launch --------------------------------------------
+// A kernel launched with launch_pdl may be scheduled while its predecessor in
+// the stream is still finishing (its launch and block set-up overlap the
+// predecessor's tail).  Such a kernel calls pdl_wait() before it touches any
+// memory its predecessor reads or writes: the wait returns once the
+// predecessor has completed and its writes are visible.  Outside such a
+// launch pdl_wait() returns at once.  FEM_PDL=0 in the environment launches
+// normally.
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
+bool pdl_enabled();
+
+template <typename... KArgs, typename... Args>
+inline cudaError_t launch_pdl(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t st,
+                              Args... args) {
+  cudaLaunchConfig_t cfg{};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = st;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = pdl_enabled() ? 1 : 0;
+  return cudaLaunchKernelEx(&cfg, kernel, static_cast<KArgs>(args)...);
+}
+
 inline int num_sms() {
   static int sms = 0;
   if (sms == 0) {

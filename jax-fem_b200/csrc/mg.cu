@@ -166,6 +166,7 @@ __global__ void ptap_kernel(Lat F, Lat C, const int32_t* __restrict__ cst, const
 template <int VEC, typename T>
 __global__ void restrict_kernel(Lat F, Lat C, const int32_t* cpos, const int32_t* ilo, const double* whi,
                                 const T* __restrict__ rf, T* bc) {
+  pdl_wait();
   const int nc[3] = {int(C.n[0]), int(C.n[1]), int(C.n[2])};
   const int nf[3] = {int(F.n[0]), int(F.n[1]), int(F.n[2])};
   const int32_t* cp[3] = {cpos, cpos + nc[0], cpos + nc[0] + nc[1]};
@@ -213,6 +214,7 @@ __global__ void restrict_kernel(Lat F, Lat C, const int32_t* cpos, const int32_t
 template <int VEC, typename T>
 __global__ void prolong_add_kernel(Lat F, Lat C, const int32_t* ilo, const double* whi, const T* __restrict__ ec,
                                    T* xf) {
+  pdl_wait();
   const int nf[3] = {int(F.n[0]), int(F.n[1]), int(F.n[2])};
   const int nc1 = int(C.n[1]), nc2 = int(C.n[2]);
   const int32_t* il[3] = {ilo, ilo + nf[0], ilo + nf[0] + nf[1]};
@@ -290,6 +292,7 @@ __global__ void cast_vals_kernel(const int32_t* rp, int64_t n_brows, int vv, con
 }
 template <typename T>
 __global__ void widen_kernel(int64_t n, const T* __restrict__ a, double* b) {
+  pdl_wait();
   for (int64_t k = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; k < n; k += int64_t(gridDim.x) * blockDim.x)
     b[k] = double(a[k]);
 }
@@ -316,6 +319,7 @@ __device__ __forceinline__ ChebCoef cheb_coef(const void* lmax_bits, double rati
 template <typename T>
 __global__ void cheb_first_kernel(int64_t n, const T* __restrict__ dinv, const T* b, T* r, T* d, T* x,
                                   const void* lmax, double ratio, int zero_start) {
+  pdl_wait();
   const double inv_theta = cheb_coef(lmax, ratio, 0).inv_theta;
   for (int64_t k = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; k < n; k += int64_t(gridDim.x) * blockDim.x) {
     const T rk = zero_start ? b[k] : r[k];
@@ -331,6 +335,7 @@ template <int VEC, typename T>
 __global__ void __launch_bounds__(kRowThreads, kRowBlocksPerSM)
     cheb_step_kernel(int64_t n_brows, const int32_t* rp, const int32_t* ci, const T* vals, const T* __restrict__ dold,
                      T* dnew, T* r, T* x, const T* __restrict__ dinv, const void* lmax, double ratio, int step) {
+  pdl_wait();
   const ChebCoef cf = cheb_coef(lmax, ratio, step);
   const double a = cf.a, c = cf.c;
   bsr_rows<VEC, T, T>(
@@ -350,6 +355,7 @@ template <int VEC, typename T>
 __global__ void __launch_bounds__(kRowThreads, kRowBlocksPerSM)
     cheb_resid_kernel(int64_t n_brows, const int32_t* rp, const int32_t* ci, const T* vals, const T* __restrict__ d,
                       T* r) {
+  pdl_wait();
   bsr_rows<VEC, T, T>(
       n_brows, rp, ci, vals, [&](int64_t i) { return d[i]; },
       [&](int64_t row, int comp, T q) {
@@ -363,6 +369,7 @@ template <int VEC, typename VT, typename T>
 __global__ void __launch_bounds__(kRowThreads, kRowBlocksPerSM)
     mg_residual_kernel(int64_t n_brows, const int32_t* rp, const int32_t* ci, const VT* vals, const T* __restrict__ x,
                        const T* b, T* r) {
+  pdl_wait();
   bsr_rows<VEC, VT, T>(
       n_brows, rp, ci, vals, [&](int64_t i) { return x[i]; },
       [&](int64_t row, int comp, T q) {
@@ -458,17 +465,19 @@ int smooth(const FemMGLevel& L, const T* b, T* x, int m, double ratio, bool zero
   const T* dinv = static_cast<const T*>(L.dinv);
   const T* vals = static_cast<const T*>(L.vals);
   const unsigned rg = row_grid<T>(L.n_brows);
-  cheb_first_kernel<T><<<vgrid(n), 256, 0, st>>>(n, dinv, b, r, d[0], x, L.lmax, ratio, zero_start ? 1 : 0);
+  FEM_CUDA_TRY(launch_pdl(cheb_first_kernel<T>, vgrid(n), 256, 0, st, n, dinv, b, r, d[0], x, L.lmax, ratio,
+                          zero_start ? 1 : 0));
   FEM_LAUNCH_CHECK();
   int cur = 0;
   for (int k = 1; k < m; ++k) {
-    cheb_step_kernel<VEC, T><<<rg, kRowThreads, bsr_rows_smem(), st>>>(L.n_brows, L.row_ptr, L.col_idx, vals, d[cur],
-                                                                      d[cur ^ 1], r, x, dinv, L.lmax, ratio, k);
+    FEM_CUDA_TRY(launch_pdl(cheb_step_kernel<VEC, T>, rg, kRowThreads, bsr_rows_smem(), st, L.n_brows, L.row_ptr,
+                            L.col_idx, vals, d[cur], d[cur ^ 1], r, x, dinv, L.lmax, ratio, k));
     FEM_LAUNCH_CHECK();
     cur ^= 1;
   }
   if (want_residual) {
-    cheb_resid_kernel<VEC, T><<<rg, kRowThreads, bsr_rows_smem(), st>>>(L.n_brows, L.row_ptr, L.col_idx, vals, d[cur], r);
+    FEM_CUDA_TRY(launch_pdl(cheb_resid_kernel<VEC, T>, rg, kRowThreads, bsr_rows_smem(), st, L.n_brows, L.row_ptr,
+                            L.col_idx, vals, d[cur], r));
     FEM_LAUNCH_CHECK();
   }
   return FEM_OK;
@@ -483,14 +492,16 @@ int vcycle_level(int l, int nlevels, const FemMGLevel* L, int nu, int coarse_ste
   const FemMGLevel& C = L[l + 1];
   T* bc = static_cast<T*>(C.b);
   T* xc = static_cast<T*>(C.x);
-  restrict_kernel<VEC, T><<<vgrid(C.n_brows), 256, 0, st>>>(lat_of(L[l]), lat_of(C), C.cpos, C.ilo, C.whi,
-                                                            static_cast<const T*>(L[l].r), bc);
+  FEM_CUDA_TRY(launch_pdl(restrict_kernel<VEC, T>, vgrid(C.n_brows), 256, 0, st, lat_of(L[l]), lat_of(C), C.cpos,
+                          C.ilo, C.whi, static_cast<const T*>(L[l].r), bc));
   FEM_LAUNCH_CHECK();
   if ((rc = vcycle_level<VEC, T>(l + 1, nlevels, L, nu, coarse_steps, ratio, bc, xc, st)) != FEM_OK) return rc;
-  prolong_add_kernel<VEC, T><<<vgrid(L[l].n_brows), 256, 0, st>>>(lat_of(L[l]), lat_of(C), C.ilo, C.whi, xc, x);
+  FEM_CUDA_TRY(launch_pdl(prolong_add_kernel<VEC, T>, vgrid(L[l].n_brows), 256, 0, st, lat_of(L[l]), lat_of(C), C.ilo,
+                          C.whi, static_cast<const T*>(xc), x));
   FEM_LAUNCH_CHECK();
-  mg_residual_kernel<VEC, T, T><<<row_grid<T>(L[l].n_brows), kRowThreads, bsr_rows_smem(), st>>>(
-      L[l].n_brows, L[l].row_ptr, L[l].col_idx, static_cast<const T*>(L[l].vals), x, b, static_cast<T*>(L[l].r));
+  FEM_CUDA_TRY(launch_pdl(mg_residual_kernel<VEC, T, T>, row_grid<T>(L[l].n_brows), kRowThreads, bsr_rows_smem(), st,
+                          L[l].n_brows, L[l].row_ptr, L[l].col_idx, static_cast<const T*>(L[l].vals),
+                          static_cast<const T*>(x), b, static_cast<T*>(L[l].r)));
   FEM_LAUNCH_CHECK();
   return smooth<VEC, T>(L[l], b, x, nu, ratio, false, false, st);
 }
@@ -540,6 +551,7 @@ __global__ void pcg_init_kernel(int64_t n, const double* r, const double* b, dou
 // gamma = r.z; beta = gamma / gamma_old (0 first)
 __global__ void pcg_rz_kernel(int64_t n, const double* r, const double* z, double* partials, unsigned* counter,
                               PState* S) {
+  pdl_wait();
   if (S->status != PS_RUNNING) return;
   double v[1] = {0.0};
   for (int64_t k = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; k < n; k += int64_t(gridDim.x) * blockDim.x)
@@ -562,6 +574,7 @@ __global__ void pcg_rz_kernel(int64_t n, const double* r, const double* z, doubl
 // p = z + beta p (from float z when the hierarchy is FP32)
 template <typename ZT>
 __global__ void pcg_dir_kernel(int64_t n, const ZT* z, double* p, const PState* S) {
+  pdl_wait();
   if (S->status != PS_RUNNING) return;
   const double beta = S->beta;
   for (int64_t k = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; k < n; k += int64_t(gridDim.x) * blockDim.x)
@@ -573,6 +586,7 @@ template <int VEC, typename VT>
 __global__ void __launch_bounds__(kRowThreads, kRowBlocksPerSM)
     pcg_spmv_kernel(int64_t n_brows, const int32_t* rp, const int32_t* ci, const VT* vals, const double* __restrict__ p,
                     double* q, double* partials, unsigned* counter, PState* S) {
+  pdl_wait();
   if (S->status != PS_RUNNING) return;
   double v[1] = {0.0};
   bsr_rows<VEC, VT, double>(
@@ -595,6 +609,7 @@ __global__ void __launch_bounds__(kRowThreads, kRowBlocksPerSM)
 // FP32 hierarchy's right-hand side when r32 is given.
 __global__ void pcg_update_kernel(int64_t n, double* x, double* r, const double* p, const double* q, float* r32,
                                   double* partials, unsigned* counter, PState* S) {
+  pdl_wait();
   if (S->status != PS_RUNNING) return;
   const double alpha = S->alpha;
   double v[1] = {0.0};
@@ -781,19 +796,22 @@ int pcg_impl(int64_t n_brows, const int32_t* rp, const int32_t* ci, const VT* va
     if (fp32) {
       // r.z needs z in FP64: widen the FP32 V-cycle output into z
       if ((rc2 = vcycle_level<VEC, float>(0, nlevels, L, nu, coarse_steps, ratio, r32, z32, ls)) != FEM_OK) return rc2;
-      widen_kernel<float><<<vg, 256, 0, ls>>>(n, z32, z);
+      FEM_CUDA_TRY(launch_pdl(widen_kernel<float>, vg, 256, 0, ls, n, static_cast<const float*>(z32), z));
       FEM_LAUNCH_CHECK();
     } else {
       if ((rc2 = vcycle_level<VEC, double>(0, nlevels, L, nu, coarse_steps, ratio, r, z, ls)) != FEM_OK) return rc2;
     }
-    pcg_rz_kernel<<<vg, 256, 0, ls>>>(n, r, z, partials, counter, S);
+    FEM_CUDA_TRY(launch_pdl(pcg_rz_kernel, vg, 256, 0, ls, n, static_cast<const double*>(r),
+                            static_cast<const double*>(z), partials, counter, S));
     FEM_LAUNCH_CHECK();
-    pcg_dir_kernel<double><<<vg, 256, 0, ls>>>(n, z, pv, S);
+    FEM_CUDA_TRY(launch_pdl(pcg_dir_kernel<double>, vg, 256, 0, ls, n, static_cast<const double*>(z), pv,
+                            static_cast<const PState*>(S)));
     FEM_LAUNCH_CHECK();
-    pcg_spmv_kernel<VEC, VT><<<rg, kRowThreads, bsr_rows_smem(), ls>>>(n_brows, rp, ci, vals, pv, q, partials, counter,
-                                                                     S);
+    FEM_CUDA_TRY(launch_pdl(pcg_spmv_kernel<VEC, VT>, rg, kRowThreads, bsr_rows_smem(), ls, n_brows, rp, ci, vals,
+                            static_cast<const double*>(pv), q, partials, counter, S));
     FEM_LAUNCH_CHECK();
-    pcg_update_kernel<<<vg, 256, 0, ls>>>(n, x, r, pv, q, r32, partials, counter, S);
+    FEM_CUDA_TRY(launch_pdl(pcg_update_kernel, vg, 256, 0, ls, n, x, r, static_cast<const double*>(pv),
+                            static_cast<const double*>(q), r32, partials, counter, S));
     FEM_LAUNCH_CHECK();
     return FEM_OK;
   };
