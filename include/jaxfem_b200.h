@@ -337,7 +337,11 @@ typedef struct FemMGLevel {
   const int32_t* ilo;
   const double* whi;
   void* lmax;             /* device, 8 bytes: the level's Gershgorin bound (FP64), written by setup */
+  double* cinv;           /* coarsest level only, or NULL: device, (n_brows*vec)^2 FP64 entries
+                             (n_brows*vec <= FEM_MG_DENSE_MAX), the dense inverse of its operator,
+                             written by setup; the V-cycle then solves that level exactly */
 } FemMGLevel;
+#define FEM_MG_DENSE_MAX 128
 
 /* Setup (once per operator, launches only): coarse values by Galerkin
  * products P^T (A P), the Jacobi scaling and the bound lmax of every level.

@@ -290,12 +290,6 @@ __global__ void cast_vals_kernel(const int32_t* rp, int64_t n_brows, int vv, con
   for (int64_t k = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; k < n; k += int64_t(gridDim.x) * blockDim.x)
     b[k] = T(a[k]);
 }
-template <typename T>
-__global__ void widen_kernel(int64_t n, const T* __restrict__ a, double* b) {
-  pdl_wait();
-  for (int64_t k = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; k < n; k += int64_t(gridDim.x) * blockDim.x)
-    b[k] = double(a[k]);
-}
 
 // ---- Chebyshev smoothing ------------------------------------------------------
 // Coefficients of step k (k >= 1) of Chebyshev iteration on D^-1 A over
@@ -378,6 +372,75 @@ __global__ void __launch_bounds__(kRowThreads, kRowBlocksPerSM)
       });
 }
 
+// ---- exact solve of a small coarsest level -------------------------------------
+// Gauss-Jordan inversion in FP64 shared memory (no pivoting: the Galerkin
+// operator of an SPD operator is SPD, so every pivot is positive).  A pivot
+// that is not positive leaves the Jacobi inverse instead.
+constexpr int kDenseThreads = 1024;
+inline size_t dense_inverse_smem(int n) { return (size_t(n) * n + n) * sizeof(double); }
+
+template <int VEC, typename T>
+__global__ void __launch_bounds__(kDenseThreads)
+    dense_inverse_kernel(int n_brows, const int32_t* rp, const int32_t* ci, const T* vals, double* inv) {
+  constexpr int VV = VEC * VEC;
+  extern __shared__ __align__(16) double dsm[];
+  const int n = n_brows * VEC;
+  double* M = dsm;
+  double* f = dsm + n * n;
+  const int tid = threadIdx.x, nt = blockDim.x;
+  for (int i = tid; i < n * n; i += nt) M[i] = 0.0;
+  __syncthreads();
+  for (int br = tid; br < n_brows; br += nt)
+    for (int k = rp[br]; k < rp[br + 1]; ++k)
+      for (int e = 0; e < VV; ++e)
+        M[(br * VEC + e / VEC) * n + ci[k] * VEC + e % VEC] = double(vals[int64_t(k) * VV + e]);
+  __syncthreads();
+  bool ok = true;
+  for (int k = 0; k < n; ++k) {
+    const double piv = M[k * n + k];
+    if (!(piv > 0.0) || !isfinite(piv)) {  // same value in every thread: uniform exit
+      ok = false;
+      break;
+    }
+    __syncthreads();  // every thread holds piv before row k changes
+    for (int j = tid; j < n; j += nt) M[k * n + j] = (j == k ? 1.0 : M[k * n + j]) / piv;
+    for (int i = tid; i < n; i += nt) f[i] = i == k ? 0.0 : M[i * n + k];
+    __syncthreads();
+    for (int idx = tid; idx < n * n; idx += nt) {
+      const int i = idx / n, j = idx - i * n;
+      if (i != k) M[idx] = (j == k ? 0.0 : M[idx]) - f[i] * M[k * n + j];
+    }
+    __syncthreads();
+  }
+  if (ok) {
+    for (int idx = tid; idx < n * n; idx += nt) inv[idx] = M[idx];
+  } else {
+    for (int idx = tid; idx < n * n; idx += nt) inv[idx] = 0.0;
+    __syncthreads();
+    for (int br = tid; br < n_brows; br += nt)
+      for (int k = rp[br]; k < rp[br + 1]; ++k)
+        if (ci[k] == br)
+          for (int c = 0; c < VEC; ++c) {
+            const double a = double(vals[int64_t(k) * VV + c * VEC + c]);
+            inv[(br * VEC + c) * n + br * VEC + c] = a > 0.0 ? 1.0 / a : 0.0;
+          }
+  }
+}
+
+// x = inv b (one warp per row)
+template <typename T>
+__global__ void dense_apply_kernel(int n, const double* __restrict__ inv, const T* __restrict__ b, T* x) {
+  pdl_wait();
+  const int lane = threadIdx.x & 31;
+  for (int row = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; row < n; row += (gridDim.x * blockDim.x) >> 5) {
+    double acc = 0.0;
+    for (int j = lane; j < n; j += 32) acc = fma(inv[int64_t(row) * n + j], double(b[j]), acc);
+#pragma unroll
+    for (int o = 16; o >= 1; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    if (lane == 0) x[row] = T(acc);
+  }
+}
+
 // ---- host side -------------------------------------------------------------------
 inline unsigned vgrid(int64_t n) {
   const int64_t b = (n + 255) / 256;
@@ -396,6 +459,8 @@ int check_levels(int nlevels, const FemMGLevel* L) {
     FEM_CHECK_ARG(v.row_ptr && v.col_idx && v.stencil && v.vals && v.dinv && v.r && v.d0 && v.d1 && v.lmax,
                   "level %d: NULL pattern, values, bound slot or work vector", l);
     FEM_CHECK_ARG(bsr_aligned(v.vals, v.col_idx), "level %d: vals and col_idx must be 16-byte aligned", l);
+    FEM_CHECK_ARG(v.cinv == nullptr || (l == nlevels - 1 && v.n_brows * VEC <= FEM_MG_DENSE_MAX),
+                  "level %d: a dense inverse is for a coarsest level of at most %d unknowns", l, FEM_MG_DENSE_MAX);
     if (l >= 1) {
       FEM_CHECK_ARG(v.x && v.b && v.cpos && v.ilo && v.whi, "level %d: NULL transfer data or work vector", l);
       for (int d = 0; d < 3; ++d)
@@ -450,6 +515,15 @@ int setup_impl(int nlevels, const FemMGLevel* L, const double* fine64, void* scr
         L[l].n_brows, L[l].stencil, static_cast<const T*>(L[l].vals), static_cast<T*>(L[l].dinv),
         static_cast<unsigned long long*>(L[l].lmax));
     FEM_LAUNCH_CHECK();
+    if (L[l].cinv != nullptr) {
+      const int n = int(L[l].n_brows) * VEC;
+      const size_t sm = dense_inverse_smem(n);
+      FEM_CUDA_TRY(cudaFuncSetAttribute(dense_inverse_kernel<VEC, T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        int(dense_inverse_smem(FEM_MG_DENSE_MAX))));
+      dense_inverse_kernel<VEC, T><<<1, kDenseThreads, sm, st>>>(int(L[l].n_brows), L[l].row_ptr, L[l].col_idx,
+                                                                 static_cast<const T*>(L[l].vals), L[l].cinv);
+      FEM_LAUNCH_CHECK();
+    }
   }
   return ensure_attrs<VEC, T>();
 }
@@ -487,7 +561,16 @@ template <int VEC, typename T>
 int vcycle_level(int l, int nlevels, const FemMGLevel* L, int nu, int coarse_steps, double ratio, const T* b, T* x,
                  cudaStream_t st) {
   int rc;
-  if (l == nlevels - 1) return smooth<VEC, T>(L[l], b, x, coarse_steps, ratio, true, false, st);
+  if (l == nlevels - 1) {
+    if (L[l].cinv != nullptr) {
+      const int n = int(L[l].n_brows) * VEC;
+      FEM_CUDA_TRY(launch_pdl(dense_apply_kernel<T>, unsigned((n + 7) / 8), 256, 0, st, n,
+                              static_cast<const double*>(L[l].cinv), b, x));
+      FEM_LAUNCH_CHECK();
+      return FEM_OK;
+    }
+    return smooth<VEC, T>(L[l], b, x, coarse_steps, ratio, true, false, st);
+  }
   if ((rc = smooth<VEC, T>(L[l], b, x, nu, ratio, true, true, st)) != FEM_OK) return rc;
   const FemMGLevel& C = L[l + 1];
   T* bc = static_cast<T*>(C.b);
@@ -548,74 +631,70 @@ __global__ void pcg_init_kernel(int64_t n, const double* r, const double* b, dou
   }
 }
 
-// gamma = r.z; beta = gamma / gamma_old (0 first)
-__global__ void pcg_rz_kernel(int64_t n, const double* r, const double* z, double* partials, unsigned* counter,
-                              PState* S) {
+// Chronopoulos-Gear form of preconditioned CG: one product and one fused pair
+// of reductions per iteration.  With z = M r (the V-cycle) and w = A z,
+//   gamma = r.z, delta = z.w, beta = gamma / gamma_old,
+//   alpha = gamma / (delta - beta gamma / alpha_old)   (= gamma / p.Ap),
+//   p = z + beta p, q = w + beta q (= A p), x += alpha p, r -= alpha q.
+// w = A z with gamma and delta; the last block forms beta and alpha.  z is
+// read as ZT (FP32 when the hierarchy is FP32) and widened on the fly.
+template <int VEC, typename VT, typename ZT>
+__global__ void __launch_bounds__(kRowThreads, kRowBlocksPerSM)
+    pcg_spmv_kernel(int64_t n_brows, const int32_t* rp, const int32_t* ci, const VT* vals, const ZT* __restrict__ z,
+                    const double* __restrict__ r, double* w, double* partials, unsigned* counter, PState* S) {
   pdl_wait();
   if (S->status != PS_RUNNING) return;
-  double v[1] = {0.0};
-  for (int64_t k = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; k < n; k += int64_t(gridDim.x) * blockDim.x)
-    v[0] = fma(r[k], z[k], v[0]);
-  double tot[1];
-  if (last_block_reduce<1>(v, partials, counter, tot)) {
-    const double g = tot[0];
-    if (!isfinite(g)) {
+  double v[2] = {0.0, 0.0};
+  bsr_rows<VEC, VT, double>(
+      n_brows, rp, ci, vals, [&](int64_t i) { return double(z[i]); },
+      [&](int64_t row, int c, double wo) {
+        const int64_t i = row * VEC + c;
+        const double zi = double(z[i]);
+        w[i] = wo;
+        v[0] = fma(r[i], zi, v[0]);
+        v[1] = fma(zi, wo, v[1]);
+      });
+  double tot[2];
+  if (last_block_reduce<2>(v, partials, counter, tot)) {
+    const double g = tot[0], dl = tot[1];
+    if (!isfinite(g) || !isfinite(dl)) {
       S->status = FEM_ERR_NONFINITE;
     } else if (!(g > 0.0)) {
       S->status = FEM_ERR_BREAKDOWN;  // preconditioner lost definiteness (or r = 0)
     } else {
-      S->beta = S->first ? 0.0 : g / S->gamma;
-      S->gamma = g;
-      S->first = 0;
+      const double beta = S->first ? 0.0 : g / S->gamma;
+      const double pq = S->first ? dl : dl - beta * g / S->alpha;
+      if (!(pq > 0.0)) {
+        S->status = FEM_ERR_BREAKDOWN;  // operator not positive definite along p
+      } else {
+        S->beta = beta;
+        S->gamma = g;
+        S->pq = pq;
+        S->alpha = g / pq;
+        S->first = 0;
+      }
     }
   }
 }
 
-// p = z + beta p (from float z when the hierarchy is FP32)
+// p = z + beta p; q = w + beta q; x += alpha p; r -= alpha q; rr = r.r;
+// bookkeeping.  Also rounds r into the FP32 hierarchy's right-hand side when
+// r32 is given.
 template <typename ZT>
-__global__ void pcg_dir_kernel(int64_t n, const ZT* z, double* p, const PState* S) {
+__global__ void pcg_update_kernel(int64_t n, const ZT* __restrict__ z, const double* __restrict__ w, double* x,
+                                  double* r, double* p, double* q, float* r32, double* partials, unsigned* counter,
+                                  PState* S) {
   pdl_wait();
   if (S->status != PS_RUNNING) return;
-  const double beta = S->beta;
-  for (int64_t k = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; k < n; k += int64_t(gridDim.x) * blockDim.x)
-    p[k] = double(z[k]) + beta * p[k];
-}
-
-// q = A p; pq = p.q; alpha = gamma / pq
-template <int VEC, typename VT>
-__global__ void __launch_bounds__(kRowThreads, kRowBlocksPerSM)
-    pcg_spmv_kernel(int64_t n_brows, const int32_t* rp, const int32_t* ci, const VT* vals, const double* __restrict__ p,
-                    double* q, double* partials, unsigned* counter, PState* S) {
-  pdl_wait();
-  if (S->status != PS_RUNNING) return;
-  double v[1] = {0.0};
-  bsr_rows<VEC, VT, double>(
-      n_brows, rp, ci, vals, [&](int64_t i) { return p[i]; },
-      [&](int64_t row, int c, double qo) {
-        const int64_t i = row * VEC + c;
-        q[i] = qo;
-        v[0] = fma(p[i], qo, v[0]);
-      });
-  double tot[1];
-  if (last_block_reduce<1>(v, partials, counter, tot)) {
-    S->pq = tot[0];
-    if (!isfinite(tot[0])) S->status = FEM_ERR_NONFINITE;
-    else if (!(tot[0] > 0.0)) S->status = FEM_ERR_BREAKDOWN;
-    else S->alpha = S->gamma / tot[0];
-  }
-}
-
-// x += alpha p; r -= alpha q; rr = r.r; bookkeeping.  Also rounds r into the
-// FP32 hierarchy's right-hand side when r32 is given.
-__global__ void pcg_update_kernel(int64_t n, double* x, double* r, const double* p, const double* q, float* r32,
-                                  double* partials, unsigned* counter, PState* S) {
-  pdl_wait();
-  if (S->status != PS_RUNNING) return;
-  const double alpha = S->alpha;
+  const double alpha = S->alpha, beta = S->beta;
   double v[1] = {0.0};
   for (int64_t k = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; k < n; k += int64_t(gridDim.x) * blockDim.x) {
-    x[k] = fma(alpha, p[k], x[k]);
-    const double rk = fma(-alpha, q[k], r[k]);
+    const double pk = fma(beta, p[k], double(z[k]));
+    const double qk = fma(beta, q[k], w[k]);
+    p[k] = pk;
+    q[k] = qk;
+    x[k] = fma(alpha, pk, x[k]);
+    const double rk = fma(-alpha, qk, r[k]);
     r[k] = rk;
     if (r32 != nullptr) r32[k] = float(rk);
     v[0] = fma(rk, rk, v[0]);
@@ -733,7 +812,7 @@ cudaGraphExec_t build_loop_graph(PState* S, F&& body_fn, int64_t* nbody) {
 
 size_t pcg_workspace_bytes(int vec, int64_t n_brows) {
   const size_t n = size_t(n_brows) * vec;
-  return 256 + 256 + al256(size_t(num_sms()) * 8 * 4 * sizeof(double)) + 4 * al256(n * sizeof(double));
+  return 256 + 256 + al256(size_t(num_sms()) * 8 * 4 * sizeof(double)) + 5 * al256(n * sizeof(double));
 }
 
 template <int VEC, typename VT>
@@ -759,12 +838,15 @@ int pcg_impl(int64_t n_brows, const int32_t* rp, const int32_t* ci, const VT* va
   double* z = reinterpret_cast<double*>(p8 + al256(n * sizeof(double)));
   double* pv = reinterpret_cast<double*>(p8 + 2 * al256(n * sizeof(double)));
   double* q = reinterpret_cast<double*>(p8 + 3 * al256(n * sizeof(double)));
+  double* w = reinterpret_cast<double*>(p8 + 4 * al256(n * sizeof(double)));
   int rc;
-  if ((rc = ensure_smem_attr(pcg_spmv_kernel<VEC, VT>)) != FEM_OK) return rc;
+  if ((rc = ensure_smem_attr(pcg_spmv_kernel<VEC, VT, float>)) != FEM_OK) return rc;
+  if ((rc = ensure_smem_attr(pcg_spmv_kernel<VEC, VT, double>)) != FEM_OK) return rc;
   if ((rc = ensure_smem_attr(mg_residual_kernel<VEC, VT, double>)) != FEM_OK) return rc;
   if ((rc = (fp32 ? ensure_attrs<VEC, float>() : ensure_attrs<VEC, double>())) != FEM_OK) return rc;
   FEM_CUDA_TRY(cudaMemsetAsync(work, 0, 512, st));
   FEM_CUDA_TRY(cudaMemsetAsync(pv, 0, sizeof(double) * n, st));
+  FEM_CUDA_TRY(cudaMemsetAsync(q, 0, sizeof(double) * n, st));
   PState init{};
   init.maxiter = maxiter;
   init.first = 1;
@@ -790,29 +872,29 @@ int pcg_impl(int64_t n_brows, const int32_t* rp, const int32_t* ci, const VT* va
     FEM_CUDA_TRY(cudaStreamSynchronize(st));
     return FEM_OK;
   };
-  // one PCG iteration: V-cycle, r.z, direction, A p, update
+  // one PCG iteration: V-cycle, w = A z with r.z and z.w, update
   auto launch_iter = [&](cudaStream_t ls) -> int {
     int rc2;
     if (fp32) {
-      // r.z needs z in FP64: widen the FP32 V-cycle output into z
       if ((rc2 = vcycle_level<VEC, float>(0, nlevels, L, nu, coarse_steps, ratio, r32, z32, ls)) != FEM_OK) return rc2;
-      FEM_CUDA_TRY(launch_pdl(widen_kernel<float>, vg, 256, 0, ls, n, static_cast<const float*>(z32), z));
+      FEM_CUDA_TRY(launch_pdl(pcg_spmv_kernel<VEC, VT, float>, rg, kRowThreads, bsr_rows_smem(), ls, n_brows, rp, ci,
+                              vals, static_cast<const float*>(z32), static_cast<const double*>(r), w, partials,
+                              counter, S));
+      FEM_LAUNCH_CHECK();
+      FEM_CUDA_TRY(launch_pdl(pcg_update_kernel<float>, vg, 256, 0, ls, n, static_cast<const float*>(z32),
+                              static_cast<const double*>(w), x, r, pv, q, r32, partials, counter, S));
       FEM_LAUNCH_CHECK();
     } else {
       if ((rc2 = vcycle_level<VEC, double>(0, nlevels, L, nu, coarse_steps, ratio, r, z, ls)) != FEM_OK) return rc2;
+      FEM_CUDA_TRY(launch_pdl(pcg_spmv_kernel<VEC, VT, double>, rg, kRowThreads, bsr_rows_smem(), ls, n_brows, rp, ci,
+                              vals, static_cast<const double*>(z), static_cast<const double*>(r), w, partials,
+                              counter, S));
+      FEM_LAUNCH_CHECK();
+      FEM_CUDA_TRY(launch_pdl(pcg_update_kernel<double>, vg, 256, 0, ls, n, static_cast<const double*>(z),
+                              static_cast<const double*>(w), x, r, pv, q, static_cast<float*>(nullptr), partials,
+                              counter, S));
+      FEM_LAUNCH_CHECK();
     }
-    FEM_CUDA_TRY(launch_pdl(pcg_rz_kernel, vg, 256, 0, ls, n, static_cast<const double*>(r),
-                            static_cast<const double*>(z), partials, counter, S));
-    FEM_LAUNCH_CHECK();
-    FEM_CUDA_TRY(launch_pdl(pcg_dir_kernel<double>, vg, 256, 0, ls, n, static_cast<const double*>(z), pv,
-                            static_cast<const PState*>(S)));
-    FEM_LAUNCH_CHECK();
-    FEM_CUDA_TRY(launch_pdl(pcg_spmv_kernel<VEC, VT>, rg, kRowThreads, bsr_rows_smem(), ls, n_brows, rp, ci, vals,
-                            static_cast<const double*>(pv), q, partials, counter, S));
-    FEM_LAUNCH_CHECK();
-    FEM_CUDA_TRY(launch_pdl(pcg_update_kernel, vg, 256, 0, ls, n, x, r, static_cast<const double*>(pv),
-                            static_cast<const double*>(q), r32, partials, counter, S));
-    FEM_LAUNCH_CHECK();
     return FEM_OK;
   };
   bool looped = false;

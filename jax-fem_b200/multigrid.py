@@ -10,7 +10,8 @@ cell wide) down to a few nodes per direction.  Prolongation is trilinear
 interpolation in the lattice coordinates, restriction its transpose, and
 coarse operators are Galerkin products P^T A P formed on the device
 (``fem_mg_setup_*``).  A V-cycle smooths with Chebyshev-Jacobi polynomials
-(``fem_mg_vcycle_*``), and ``fem_mg_pcg_solve`` runs CG in FP64 with one
+(``fem_mg_vcycle_*``) and solves a small coarsest level exactly (a dense
+inverse formed by setup), and ``fem_mg_pcg_solve`` runs CG in FP64 with one
 V-cycle per iteration.  The V-cycle is in FP64 or, for the mixed-precision
 path, in FP32 on a rounded copy of the hierarchy.
 """
@@ -104,7 +105,7 @@ class Multigrid:
     one precision.  ``setup(A)`` forms the coarse operators of the FP64
     operator A; ``solve`` runs the V-cycle-preconditioned CG."""
 
-    def __init__(self, dv, mesh_points, mesh_cells, fp32=False, max_levels=10):
+    def __init__(self, dv, mesh_points, mesh_cells, fp32=False, max_levels=10, dense_coarse=True):
         lat = lattice_of(mesh_points, mesh_cells)
         if lat is None:
             raise NotImplementedError("precond 'gmg' needs a box-lattice mesh numbered as box_mesh numbers it")
@@ -159,6 +160,14 @@ class Multigrid:
             transfer = (torch.from_numpy(np.concatenate([q[1] for q in parts]).astype(np.int32)).to(dev),
                         torch.from_numpy(np.concatenate([q[2] for q in parts]).astype(np.int32)).to(dev),
                         torch.from_numpy(np.concatenate([q[3] for q in parts]).astype(np.float64)).to(dev))
+        # a coarsest level of at most FEM_MG_DENSE_MAX unknowns is solved
+        # exactly with a dense inverse (formed by setup) instead of smoothed
+        last = self.levels[self.nlevels - 1]
+        self._cinv = None
+        if dense_coarse and last.n_brows * self.vec <= nat.FEM_MG_DENSE_MAX:
+            nc = last.n_brows * self.vec
+            self._cinv = torch.zeros(nc * nc, dtype=torch.float64, device=dev)
+            last.cinv = self._cinv.data_ptr()
         self._work = None
         self._fine_ref = None
         # coarse-operator reuse bookkeeping (solver.mg_solve)

@@ -102,6 +102,40 @@ def test_vcycle_symmetric_positive(pkg, cuda):
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("fp32", [False, True])
+def test_dense_coarsest_solve(pkg, cuda, fp32):
+    """A coarsest level of at most FEM_MG_DENSE_MAX unknowns is solved with a
+    dense inverse formed at setup: inverse x coarsest Galerkin operator = I;
+    the V-cycle stays symmetric positive; CG still reaches the direct solution."""
+    mg, _ = _mods()
+    prob, A = _graded_elastic(pkg, cuda, shape=(4, 4, 4))
+    M = mg.Multigrid(prob.dev(), prob.mesh.points, prob.mesh.cells, fp32=fp32)
+    M.setup(A)
+    last = M.level_nodes[-1]
+    nc = last[0] * last[1] * last[2] * 3
+    assert M.nlevels >= 2 and nc <= pkg._native.FEM_MG_DENSE_MAX and M._cinv is not None
+    rp, ci, vals = M.mats[-1]
+    Kc = _bsr_to_scipy(rp, ci, vals, nc // 3).toarray()
+    inv = M._cinv.cpu().numpy().reshape(nc, nc)
+    assert np.abs(inv @ Kc - np.eye(nc)).max() <= (1e-5 if fp32 else 1e-10)
+    dt = torch.float32 if fp32 else torch.float64
+    n = prob.num_total_dofs_all_vars
+    g = torch.Generator().manual_seed(4)
+    r1, r2 = (torch.randn(n, generator=g, dtype=torch.float64).to(device=cuda, dtype=dt) for _ in range(2))
+    z1, z2 = torch.empty_like(r1), torch.empty_like(r2)
+    M.vcycle(r1, z1)
+    M.vcycle(r2, z2)
+    a, b = float(torch.dot(r2.double(), z1.double())), float(torch.dot(r1.double(), z2.double()))
+    assert abs(a - b) <= (1e-5 if fp32 else 1e-10) * float(torch.dot(r1.double(), z1.double()))
+    K = A.to_scipy()
+    rhs = np.random.default_rng(8).normal(size=n)
+    xref = spla.spsolve(K.tocsc(), rhs)
+    x = torch.zeros(n, dtype=torch.float64, device=cuda)
+    its, rel = M.solve(A, torch.tensor(rhs, device=cuda), x, rtol=1e-10)
+    assert np.abs(x.cpu().numpy() - xref).max() <= 1e-8 * np.abs(xref).max()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("fp32", [False, True])
 def test_mg_pcg_matches_direct_solve(pkg, cuda, fp32):
     mg, S = _mods()
     prob, A = _graded_elastic(pkg, cuda, shape=(12, 10, 9))
