@@ -317,14 +317,15 @@ def run_ours(args, rank, world, device):
     spmv_bytes = nnzb * 9 * 4 + nnzb * 4 + (dv.num_nodes + 1) * 4 + 2 * ndofs * 4
     hbm, peak_kind = peaks()
 
-    # assembly throughput (FP64 tangent+residual, FP32 tangent), DoF/s
+    # assembly throughput, DoF/s: FP64 residual with the FP64 or the FP32
+    # tangent (the plain and the mixed Newton passes)
     sol_last = torch.zeros(ndofs, dtype=torch.float64, device=device)
     res = torch.empty(ndofs, dtype=torch.float64, device=device)
     A64 = dv.new_matrix(torch.float64)
     t_asm64 = time_kernel(lambda: prob.assemble(sol_last, res=res, vals=A64.vals), reps=10)
-    t_asm32 = time_kernel(lambda: prob.assemble(sol_last, vals=A32.vals, fp32=True), reps=10)
+    t_asm32 = time_kernel(lambda: prob.assemble(sol_last, res=res, vals=A32.vals, fp32=True), reps=10)
     asm_bytes64 = dv.num_cells * (32 + 8 * 3 * 8 + 24 * 8 + 256) + nnzb * 9 * 8 + ndofs * 8
-    asm_bytes32 = dv.num_cells * (32 + 8 * 3 * 8 + 24 * 8 + 256) + nnzb * 9 * 4
+    asm_bytes32 = dv.num_cells * (32 + 8 * 3 * 8 + 24 * 8 + 256) + nnzb * 9 * 4 + ndofs * 8
 
     # SIMP 60x30x30 with the committed learned warm start (held-out samples)
     simp = None
@@ -397,7 +398,8 @@ def run_ours(args, rank, world, device):
         "solves_per_s": round(world / t_mixed, 4),
         "newton_iters": newton,
         "krylov_iters": krylov,
-        "assembly_dofs_per_s": {"fp64_residual_tangent": round(ndofs / t_asm64), "fp32_tangent": round(ndofs / t_asm32)},
+        "assembly_dofs_per_s": {"fp64_residual_tangent": round(ndofs / t_asm64),
+                                "fp64_residual_fp32_tangent": round(ndofs / t_asm32)},
         "assembly_us": {"fp64": round(t_asm64 * 1e6, 1), "fp32": round(t_asm32 * 1e6, 1)},
         "assembly_hbm_frac": {"fp64": round(asm_bytes64 / t_asm64 / 1e9 / hbm, 3),
                               "fp32": round(asm_bytes32 / t_asm32 / 1e9 / hbm, 3)},
@@ -491,8 +493,9 @@ def run_reference(args, rank, world):
 
 def run_profile(args, device):
     """A short fixed sequence of the hot kernels at the bench size, for ncu:
-    FP64 and FP32 assembly (x2 each), FP32/FP64 SpMV (x3 each), one mixed
-    solve with block-Jacobi CG and one with the multigrid-preconditioned CG."""
+    FP64 assembly and the FP64-residual/FP32-tangent assembly (x2 each),
+    FP32/FP64 SpMV (x3 each), one mixed solve with block-Jacobi CG and one
+    with the multigrid-preconditioned CG (the headline's linear solver)."""
     pkg = load_package()
     nat = pkg._native
     prob = nh_problem(pkg, n=args.n)
@@ -505,7 +508,7 @@ def run_profile(args, device):
     for _ in range(2):
         prob.assemble(u, res=res, vals=A64.vals)
     for _ in range(2):
-        prob.assemble(u, vals=A32.vals, fp32=True)
+        prob.assemble(u, res=res, vals=A32.vals, fp32=True)
     x64 = torch.randn(n, dtype=torch.float64, device=device)
     x32 = x64.float()
     for _ in range(3):
@@ -515,7 +518,7 @@ def run_profile(args, device):
     nh_solve(pkg, prob, "mixed", steps=1, total_deg=6.0,
              linear={"cg": {"precond": "block_jacobi", "rtol": "adaptive", "atol": 0.0}})
     nh_solve(pkg, prob, "mixed", steps=1, total_deg=6.0,
-             linear={"cg": {"precond": "gmg", "rtol": "adaptive", "atol": 0.0}})
+             linear={"cg": {"precond": "gmg", "rtol": "adaptive", "atol": 0.0, "mg_lag": 4}})
     torch.cuda.synchronize()
     print(json.dumps({"profile": "done", "launches": nat.launch_count()}))
 
