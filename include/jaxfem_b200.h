@@ -340,6 +340,8 @@ typedef struct FemMGLevel {
   double* cinv;           /* coarsest level only, or NULL: device, (n_brows*vec)^2 FP64 entries
                              (n_brows*vec <= FEM_MG_DENSE_MAX), the dense inverse of its operator,
                              written by setup; the V-cycle then solves that level exactly */
+  int32_t nu;             /* smoothing steps on this level; 0: the call's nu */
+  int32_t reserved;
 } FemMGLevel;
 #define FEM_MG_DENSE_MAX 128
 

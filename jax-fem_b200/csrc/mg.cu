@@ -459,6 +459,7 @@ int check_levels(int nlevels, const FemMGLevel* L) {
     FEM_CHECK_ARG(v.row_ptr && v.col_idx && v.stencil && v.vals && v.dinv && v.r && v.d0 && v.d1 && v.lmax,
                   "level %d: NULL pattern, values, bound slot or work vector", l);
     FEM_CHECK_ARG(bsr_aligned(v.vals, v.col_idx), "level %d: vals and col_idx must be 16-byte aligned", l);
+    FEM_CHECK_ARG(v.nu >= 0 && v.nu <= 16, "level %d: nu must be in [0, 16]", l);
     FEM_CHECK_ARG(v.cinv == nullptr || (l == nlevels - 1 && v.n_brows * VEC <= FEM_MG_DENSE_MAX),
                   "level %d: a dense inverse is for a coarsest level of at most %d unknowns", l, FEM_MG_DENSE_MAX);
     if (l >= 1) {
@@ -571,7 +572,8 @@ int vcycle_level(int l, int nlevels, const FemMGLevel* L, int nu, int coarse_ste
     }
     return smooth<VEC, T>(L[l], b, x, coarse_steps, ratio, true, false, st);
   }
-  if ((rc = smooth<VEC, T>(L[l], b, x, nu, ratio, true, true, st)) != FEM_OK) return rc;
+  const int nul = L[l].nu > 0 ? L[l].nu : nu;
+  if ((rc = smooth<VEC, T>(L[l], b, x, nul, ratio, true, true, st)) != FEM_OK) return rc;
   const FemMGLevel& C = L[l + 1];
   T* bc = static_cast<T*>(C.b);
   T* xc = static_cast<T*>(C.x);
@@ -586,7 +588,7 @@ int vcycle_level(int l, int nlevels, const FemMGLevel* L, int nu, int coarse_ste
                           L[l].n_brows, L[l].row_ptr, L[l].col_idx, static_cast<const T*>(L[l].vals),
                           static_cast<const T*>(x), b, static_cast<T*>(L[l].r)));
   FEM_LAUNCH_CHECK();
-  return smooth<VEC, T>(L[l], b, x, nu, ratio, false, false, st);
+  return smooth<VEC, T>(L[l], b, x, nul, ratio, false, false, st);
 }
 
 template <int VEC, typename T>

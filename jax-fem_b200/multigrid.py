@@ -105,7 +105,7 @@ class Multigrid:
     one precision.  ``setup(A)`` forms the coarse operators of the FP64
     operator A; ``solve`` runs the V-cycle-preconditioned CG."""
 
-    def __init__(self, dv, mesh_points, mesh_cells, fp32=False, max_levels=10, dense_coarse=True):
+    def __init__(self, dv, mesh_points, mesh_cells, fp32=False, max_levels=10, dense_coarse=True, nu_fine=0):
         lat = lattice_of(mesh_points, mesh_cells)
         if lat is None:
             raise NotImplementedError("precond 'gmg' needs a box-lattice mesh numbered as box_mesh numbers it")
@@ -160,6 +160,8 @@ class Multigrid:
             transfer = (torch.from_numpy(np.concatenate([q[1] for q in parts]).astype(np.int32)).to(dev),
                         torch.from_numpy(np.concatenate([q[2] for q in parts]).astype(np.int32)).to(dev),
                         torch.from_numpy(np.concatenate([q[3] for q in parts]).astype(np.float64)).to(dev))
+        # smoothing steps on the finest level (0: the V-cycle's nu)
+        self.levels[0].nu = int(nu_fine)
         # a coarsest level of at most FEM_MG_DENSE_MAX unknowns is solved
         # exactly with a dense inverse (formed by setup) instead of smoothed
         last = self.levels[self.nlevels - 1]

@@ -229,6 +229,10 @@ def test_solver_option_resolution(pkg):
         s._resolve_solver_options({"newton": {}, "arc_length": {}})
     with pytest.raises(NotImplementedError):
         s.resolve_linear({"amgx_solver": {}})
+    lc = s.resolve_linear({"cg": {"precond": "gmg", "rtol": "adaptive", "mg_lag": 4, "mg_nu_fine": 2, "mg_nu": 3}})
+    assert lc.gmg and lc.adaptive and lc.eta_max == 1e-3
+    assert lc.mg["lag"] == 4 and lc.mg["nu_fine"] == 2 and lc.mg["nu"] == 3 and lc.mg["coarse_steps"] == 8
+    assert s.resolve_linear({"cg": {"precond": "gmg"}}).mg["nu_fine"] == 1
 
 
 def test_no_gpu_means_loud_failure(pkg):
