@@ -158,15 +158,37 @@ __global__ void ptap_kernel(Lat F, Lat C, const int32_t* __restrict__ cst, const
   }
 }
 
+// Coefficients of step k (k >= 1) of Chebyshev iteration on D^-1 A over
+// [lmax/ratio, lmax]: d_k = a d_{k-1} + c D^-1 r_k; step 0 is d_0 = D^-1 r_0 / theta.
+struct ChebCoef {
+  double inv_theta, a, c;
+};
+__device__ __forceinline__ ChebCoef cheb_coef(const void* lmax_bits, double ratio, int k) {
+  const double lmax = __longlong_as_double(*static_cast<const long long*>(lmax_bits));
+  const double lmin = lmax / ratio;
+  const double theta = 0.5 * (lmax + lmin), delta = 0.5 * (lmax - lmin), sigma = theta / delta;
+  double rho_prev = 1.0 / sigma, rho = rho_prev;
+  for (int j = 1; j <= k; ++j) {
+    rho_prev = rho;
+    rho = 1.0 / (2.0 * sigma - rho_prev);
+  }
+  return ChebCoef{1.0 / theta, rho * rho_prev, 2.0 * rho / delta};
+}
+
 // ---- transfers ---------------------------------------------------------------
 // bc[I] = sum_i w_iI rf[i]   (P^T, one thread per coarse node).  Along each
 // direction at most 3 fine nodes lie strictly between the neighbouring coarse
 // nodes, so the 27 candidates are unrolled with their weights formed first and
 // the gathers issued together; lattice indices fit in 32 bits.
+// With dinvc given, the kernel also takes the coarse level's first Chebyshev
+// step from a zero start (as cheb_first_kernel: r = b, d0 = D^-1 b / theta,
+// x = d0), node by node, so that step needs no launch of its own.
 template <int VEC, typename T>
 __global__ void restrict_kernel(Lat F, Lat C, const int32_t* cpos, const int32_t* ilo, const double* whi,
-                                const T* __restrict__ rf, T* bc) {
+                                const T* __restrict__ rf, T* bc, const T* __restrict__ dinvc, T* rc, T* d0c, T* xc,
+                                const void* lmaxc, double ratio) {
   pdl_wait();
+  const double inv_theta = dinvc != nullptr ? cheb_coef(lmaxc, ratio, 0).inv_theta : 0.0;
   const int nc[3] = {int(C.n[0]), int(C.n[1]), int(C.n[2])};
   const int nf[3] = {int(F.n[0]), int(F.n[1]), int(F.n[2])};
   const int32_t* cp[3] = {cpos, cpos + nc[0], cpos + nc[0] + nc[1]};
@@ -207,6 +229,17 @@ __global__ void restrict_kernel(Lat F, Lat C, const int32_t* cpos, const int32_t
       }
 #pragma unroll
     for (int c = 0; c < VEC; ++c) bc[int64_t(I) * VEC + c] = T(acc[c]);
+    if (dinvc != nullptr) {
+#pragma unroll
+      for (int c = 0; c < VEC; ++c) {
+        const int64_t q = int64_t(I) * VEC + c;
+        const T bq = T(acc[c]);
+        rc[q] = bq;
+        const T dq = T(double(dinvc[q]) * double(bq) * inv_theta);
+        d0c[q] = dq;
+        xc[q] = dq;
+      }
+    }
   }
 }
 
@@ -292,23 +325,6 @@ __global__ void cast_vals_kernel(const int32_t* rp, int64_t n_brows, int vv, con
 }
 
 // ---- Chebyshev smoothing ------------------------------------------------------
-// Coefficients of step k (k >= 1) of Chebyshev iteration on D^-1 A over
-// [lmax/ratio, lmax]: d_k = a d_{k-1} + c D^-1 r_k; step 0 is d_0 = D^-1 r_0 / theta.
-struct ChebCoef {
-  double inv_theta, a, c;
-};
-__device__ __forceinline__ ChebCoef cheb_coef(const void* lmax_bits, double ratio, int k) {
-  const double lmax = __longlong_as_double(*static_cast<const long long*>(lmax_bits));
-  const double lmin = lmax / ratio;
-  const double theta = 0.5 * (lmax + lmin), delta = 0.5 * (lmax - lmin), sigma = theta / delta;
-  double rho_prev = 1.0 / sigma, rho = rho_prev;
-  for (int j = 1; j <= k; ++j) {
-    rho_prev = rho;
-    rho = 1.0 / (2.0 * sigma - rho_prev);
-  }
-  return ChebCoef{1.0 / theta, rho * rho_prev, 2.0 * rho / delta};
-}
-
 // First step: (zero start) r = b, x = d; otherwise x += d; d = D^-1 r / theta.
 template <typename T>
 __global__ void cheb_first_kernel(int64_t n, const T* __restrict__ dinv, const T* b, T* r, T* d, T* x,
@@ -324,11 +340,12 @@ __global__ void cheb_first_kernel(int64_t n, const T* __restrict__ dinv, const T
   }
 }
 
-// q = A d_old; r -= q; d_new = a d_old + c D^-1 r; x += d_new
+// q = A d_old; r -= q; d_new = a d_old + c D^-1 r; x += d_new (x += d_old + d_new with fold)
 template <int VEC, typename T>
 __global__ void __launch_bounds__(kRowThreads, kRowBlocksPerSM)
     cheb_step_kernel(int64_t n_brows, const int32_t* rp, const int32_t* ci, const T* vals, const T* __restrict__ dold,
-                     T* dnew, T* r, T* x, const T* __restrict__ dinv, const void* lmax, double ratio, int step) {
+                     T* dnew, T* r, T* x, const T* __restrict__ dinv, const void* lmax, double ratio, int step,
+                     int fold) {
   pdl_wait();
   const ChebCoef cf = cheb_coef(lmax, ratio, step);
   const double a = cf.a, c = cf.c;
@@ -340,7 +357,8 @@ __global__ void __launch_bounds__(kRowThreads, kRowBlocksPerSM)
         r[i] = T(rn);
         const T dn = T(a * double(dold[i]) + c * double(dinv[i]) * rn);
         dnew[i] = dn;
-        x[i] = T(x[i] + dn);
+        // fold: the first step's x += d_old was left to this step
+        x[i] = fold ? T(T(x[i] + dold[i]) + dn) : T(x[i] + dn);
       });
 }
 
@@ -362,13 +380,18 @@ __global__ void __launch_bounds__(kRowThreads, kRowBlocksPerSM)
 template <int VEC, typename VT, typename T>
 __global__ void __launch_bounds__(kRowThreads, kRowBlocksPerSM)
     mg_residual_kernel(int64_t n_brows, const int32_t* rp, const int32_t* ci, const VT* vals, const T* __restrict__ x,
-                       const T* b, T* r) {
+                       const T* b, T* r, const T* __restrict__ dinv, T* d0, const void* lmax, double ratio) {
   pdl_wait();
+  // with d0 given: also the first Chebyshev step's d0 = D^-1 r / theta (its
+  // x += d0 is folded into the next step)
+  const double inv_theta = d0 != nullptr ? cheb_coef(lmax, ratio, 0).inv_theta : 0.0;
   bsr_rows<VEC, VT, T>(
       n_brows, rp, ci, vals, [&](int64_t i) { return x[i]; },
       [&](int64_t row, int comp, T q) {
         const int64_t i = row * VEC + comp;
-        r[i] = T(double(b[i]) - double(q));
+        const T ri = T(double(b[i]) - double(q));
+        r[i] = ri;
+        if (d0 != nullptr) d0[i] = T(double(dinv[i]) * double(ri) * inv_theta);
       });
 }
 
@@ -530,23 +553,28 @@ int setup_impl(int nlevels, const FemMGLevel* L, const double* fine64, void* scr
 }
 
 // m Chebyshev steps on level l (x, r, d0/d1 of the level; b as rhs).  With
-// want_residual the level's r ends as b - A x.
+// want_residual the level's r ends as b - A x.  first_done: the first step
+// was taken by the kernel before (restriction from a zero start, or the
+// residual's d0 with fold, whose x += d0 the second step then adds).
 template <int VEC, typename T>
 int smooth(const FemMGLevel& L, const T* b, T* x, int m, double ratio, bool zero_start, bool want_residual,
-           cudaStream_t st) {
+           cudaStream_t st, bool first_done = false, bool fold = false) {
   const int64_t n = L.n_brows * VEC;
   T* r = static_cast<T*>(L.r);
   T* d[2] = {static_cast<T*>(L.d0), static_cast<T*>(L.d1)};
   const T* dinv = static_cast<const T*>(L.dinv);
   const T* vals = static_cast<const T*>(L.vals);
   const unsigned rg = row_grid<T>(L.n_brows);
-  FEM_CUDA_TRY(launch_pdl(cheb_first_kernel<T>, vgrid(n), 256, 0, st, n, dinv, b, r, d[0], x, L.lmax, ratio,
-                          zero_start ? 1 : 0));
-  FEM_LAUNCH_CHECK();
+  if (!first_done) {
+    FEM_CUDA_TRY(launch_pdl(cheb_first_kernel<T>, vgrid(n), 256, 0, st, n, dinv, b, r, d[0], x, L.lmax, ratio,
+                            zero_start ? 1 : 0));
+    FEM_LAUNCH_CHECK();
+  }
   int cur = 0;
   for (int k = 1; k < m; ++k) {
     FEM_CUDA_TRY(launch_pdl(cheb_step_kernel<VEC, T>, rg, kRowThreads, bsr_rows_smem(), st, L.n_brows, L.row_ptr,
-                            L.col_idx, vals, d[cur], d[cur ^ 1], r, x, dinv, L.lmax, ratio, k));
+                            L.col_idx, vals, static_cast<const T*>(d[cur]), d[cur ^ 1], r, x, dinv, L.lmax, ratio, k,
+                            (fold && k == 1) ? 1 : 0));
     FEM_LAUNCH_CHECK();
     cur ^= 1;
   }
@@ -558,9 +586,11 @@ int smooth(const FemMGLevel& L, const T* b, T* x, int m, double ratio, bool zero
   return FEM_OK;
 }
 
+// pre_done: the restriction into this level already took its first
+// smoothing step.
 template <int VEC, typename T>
 int vcycle_level(int l, int nlevels, const FemMGLevel* L, int nu, int coarse_steps, double ratio, const T* b, T* x,
-                 cudaStream_t st) {
+                 cudaStream_t st, bool pre_done = false) {
   int rc;
   if (l == nlevels - 1) {
     if (L[l].cinv != nullptr) {
@@ -570,25 +600,36 @@ int vcycle_level(int l, int nlevels, const FemMGLevel* L, int nu, int coarse_ste
       FEM_LAUNCH_CHECK();
       return FEM_OK;
     }
-    return smooth<VEC, T>(L[l], b, x, coarse_steps, ratio, true, false, st);
+    return smooth<VEC, T>(L[l], b, x, coarse_steps, ratio, true, false, st, pre_done);
   }
   const int nul = L[l].nu > 0 ? L[l].nu : nu;
-  if ((rc = smooth<VEC, T>(L[l], b, x, nul, ratio, true, true, st)) != FEM_OK) return rc;
+  if ((rc = smooth<VEC, T>(L[l], b, x, nul, ratio, true, true, st, pre_done)) != FEM_OK) return rc;
   const FemMGLevel& C = L[l + 1];
   T* bc = static_cast<T*>(C.b);
   T* xc = static_cast<T*>(C.x);
+  // the next level starts with a zero-start Chebyshev step unless it is a
+  // coarsest level solved by its dense inverse: the restriction takes it
+  const bool fuse_next = !(l + 1 == nlevels - 1 && C.cinv != nullptr);
   FEM_CUDA_TRY(launch_pdl(restrict_kernel<VEC, T>, vgrid(C.n_brows), 256, 0, st, lat_of(L[l]), lat_of(C), C.cpos,
-                          C.ilo, C.whi, static_cast<const T*>(L[l].r), bc));
+                          C.ilo, C.whi, static_cast<const T*>(L[l].r), bc,
+                          fuse_next ? static_cast<const T*>(C.dinv) : static_cast<const T*>(nullptr),
+                          static_cast<T*>(C.r), static_cast<T*>(C.d0), xc, static_cast<const void*>(C.lmax), ratio));
   FEM_LAUNCH_CHECK();
-  if ((rc = vcycle_level<VEC, T>(l + 1, nlevels, L, nu, coarse_steps, ratio, bc, xc, st)) != FEM_OK) return rc;
+  if ((rc = vcycle_level<VEC, T>(l + 1, nlevels, L, nu, coarse_steps, ratio, bc, xc, st, fuse_next)) != FEM_OK)
+    return rc;
   FEM_CUDA_TRY(launch_pdl(prolong_add_kernel<VEC, T>, vgrid(L[l].n_brows), 256, 0, st, lat_of(L[l]), lat_of(C), C.ilo,
                           C.whi, static_cast<const T*>(xc), x));
   FEM_LAUNCH_CHECK();
+  // post-smoothing with two or more steps: the residual kernel forms the
+  // first step's d0 and the second step adds its x += d0
+  const bool fuse_post = nul >= 2;
   FEM_CUDA_TRY(launch_pdl(mg_residual_kernel<VEC, T, T>, row_grid<T>(L[l].n_brows), kRowThreads, bsr_rows_smem(), st,
                           L[l].n_brows, L[l].row_ptr, L[l].col_idx, static_cast<const T*>(L[l].vals),
-                          static_cast<const T*>(x), b, static_cast<T*>(L[l].r)));
+                          static_cast<const T*>(x), b, static_cast<T*>(L[l].r),
+                          static_cast<const T*>(L[l].dinv), fuse_post ? static_cast<T*>(L[l].d0) : static_cast<T*>(nullptr),
+                          static_cast<const void*>(L[l].lmax), ratio));
   FEM_LAUNCH_CHECK();
-  return smooth<VEC, T>(L[l], b, x, nul, ratio, false, false, st);
+  return smooth<VEC, T>(L[l], b, x, nul, ratio, false, false, st, fuse_post, fuse_post);
 }
 
 template <int VEC, typename T>
@@ -857,7 +898,8 @@ int pcg_impl(int64_t n_brows, const int32_t* rp, const int32_t* ci, const VT* va
   float* r32 = fp32 ? static_cast<float*>(L[0].b) : nullptr;
   float* z32 = fp32 ? static_cast<float*>(L[0].x) : nullptr;
   // r = b - A x, the reductions and status
-  mg_residual_kernel<VEC, VT, double><<<rg, kRowThreads, bsr_rows_smem(), st>>>(n_brows, rp, ci, vals, x, b, r);
+  mg_residual_kernel<VEC, VT, double><<<rg, kRowThreads, bsr_rows_smem(), st>>>(
+      n_brows, rp, ci, vals, x, b, r, static_cast<const double*>(nullptr), static_cast<double*>(nullptr), nullptr, 0.0);
   FEM_LAUNCH_CHECK();
   pcg_init_kernel<VEC><<<vg, 256, 0, st>>>(n, r, b, partials, counter, S, rtol, atol);
   FEM_LAUNCH_CHECK();
@@ -955,7 +997,8 @@ int pcg_impl(int64_t n_brows, const int32_t* rp, const int32_t* ci, const VT* va
   const int iters = hs->iter;
   const double bb = hs->bb;
   // report the true residual ||b - A x||
-  mg_residual_kernel<VEC, VT, double><<<rg, kRowThreads, bsr_rows_smem(), st>>>(n_brows, rp, ci, vals, x, b, q);
+  mg_residual_kernel<VEC, VT, double><<<rg, kRowThreads, bsr_rows_smem(), st>>>(
+      n_brows, rp, ci, vals, x, b, q, static_cast<const double*>(nullptr), static_cast<double*>(nullptr), nullptr, 0.0);
   FEM_LAUNCH_CHECK();
   FEM_CUDA_TRY(cudaMemsetAsync(counter, 0, sizeof(unsigned), st));
   pcg_init_kernel<VEC><<<vg, 256, 0, st>>>(n, q, b, partials, counter, S, rtol, atol);
