@@ -1,0 +1,156 @@
+"""Mesh and result files (jax-fem_b200/utils.py), on the CPU.
+
+- save_sol writes what the reference's save_sol (utils.py:13-57) writes: the
+  mesh, the solution as FP32 point field ``sol``, FP32 cell and point fields;
+  read back bit for bit (binary and ASCII VTU);
+- the reader takes zlib-compressed inline arrays (meshio's default) and the
+  dolfinx ASCII form of the reference's FEniCSx fixtures (VTK type 72);
+- Gmsh 2.2 / 4.1 ASCII and Abaqus meshes give the same hexahedral Mesh,
+  unused nodes and non-hexahedral elements dropped."""
+import base64
+import struct
+import zlib
+
+import numpy as np
+import pytest
+
+from __graft_entry__ import load_package
+
+
+@pytest.fixture(scope="module")
+def io():
+    pkg = load_package()
+    import importlib
+    return pkg, importlib.import_module("jax_fem_b200.utils")
+
+
+def _fe(pkg):
+    m = pkg.box_mesh(3, 2, 2, 1.5, 1.0, 1.0)
+    return pkg.fe.FiniteElement(pkg.Mesh(m.points, m.cells_dict["hexahedron"]), 3, 3)
+
+
+@pytest.mark.parametrize("fmt", ["binary", "ascii"])
+def test_save_sol_round_trip(io, tmp_path, fmt):
+    pkg, ut = io
+    fe = _fe(pkg)
+    rng = np.random.default_rng(0)
+    sol = rng.normal(size=(len(fe.points), 3))
+    rho = rng.uniform(size=len(fe.cells))
+    T = rng.normal(size=len(fe.points))
+    path = str(tmp_path / "out" / "u.vtu")
+    if fmt == "binary":
+        ut.save_sol(fe, sol, path, cell_infos=[("rho", rho)], point_infos=[("T", T)])
+    else:
+        ut.write_vtu(path, fe.points, fe.cells, {"sol": sol.astype(np.float32), "T": T.astype(np.float32)},
+                     {"rho": rho.astype(np.float32)}, fmt="ascii")
+    pts, cells, pd, cd = ut.read_vtu(path)
+    np.testing.assert_array_equal(pts, fe.points)
+    np.testing.assert_array_equal(cells, fe.cells)
+    np.testing.assert_array_equal(pd["sol"], sol.astype(np.float32))
+    np.testing.assert_array_equal(pd["T"], T.astype(np.float32))
+    np.testing.assert_array_equal(cd["rho"], rho.astype(np.float32))
+    assert pd["sol"].dtype == np.float32 and pd["sol"].shape == (len(fe.points), 3)
+    with pytest.raises(ValueError):
+        ut.save_sol(fe, sol, path, cell_infos=[("bad", np.zeros(len(fe.cells) + 1))])
+    m = ut.read_mesh(path)
+    np.testing.assert_array_equal(m.cells, fe.cells)
+
+
+def _zlib_inline(arr, blocksize=64):
+    raw = np.ascontiguousarray(arr).tobytes()
+    blocks = [raw[i:i + blocksize] for i in range(0, len(raw), blocksize)]
+    comp = [zlib.compress(b) for b in blocks]
+    last = len(blocks[-1]) if len(blocks[-1]) < blocksize else blocksize
+    hdr = struct.pack("<%dI" % (3 + len(comp)), len(comp), blocksize, last, *[len(c) for c in comp])
+    return base64.b64encode(hdr).decode() + base64.b64encode(b"".join(comp)).decode()
+
+
+def test_read_compressed_vtu(io, tmp_path):
+    """Inline zlib blocks with UInt32 headers, header and data encoded apart."""
+    pkg, ut = io
+    fe = _fe(pkg)
+    sol = np.random.default_rng(1).normal(size=(len(fe.points), 3)).astype(np.float32)
+    conn, offs = fe.cells.astype(np.int64).reshape(-1), np.arange(1, len(fe.cells) + 1, dtype=np.int64) * 8
+    types = np.full(len(fe.cells), 12, dtype=np.uint8)
+    def arr(a, t, extra=""):
+        return f'<DataArray type="{t}" {extra} format="binary">{_zlib_inline(a)}</DataArray>'
+
+    text = ('<?xml version="1.0"?><VTKFile type="UnstructuredGrid" version="0.1" byte_order="LittleEndian" '
+            'compressor="vtkZLibDataCompressor"><UnstructuredGrid>'
+            f'<Piece NumberOfPoints="{len(fe.points)}" NumberOfCells="{len(fe.cells)}">'
+            '<Points>' + arr(fe.points, "Float64", 'NumberOfComponents="3"') + '</Points><Cells>'
+            + arr(conn, "Int64", 'Name="connectivity"') + arr(offs, "Int64", 'Name="offsets"')
+            + arr(types, "UInt8", 'Name="types"') + '</Cells><PointData>'
+            + arr(sol, "Float32", 'Name="sol" NumberOfComponents="3"')
+            + '</PointData></Piece></UnstructuredGrid></VTKFile>')
+    path = tmp_path / "c.vtu"
+    path.write_text(text)
+    pts, cells, pd, cd = ut.read_vtu(str(path))
+    np.testing.assert_array_equal(pts, fe.points)
+    np.testing.assert_array_equal(cells, fe.cells)
+    np.testing.assert_array_equal(pd["sol"], sol)
+    assert cd == {}
+
+
+def test_read_dolfinx_ascii_vtu(io, tmp_path):
+    """The ASCII form dolfinx writes (version 2.2, no header type, Lagrange
+    hexahedra, type 72), as in the reference's FEniCSx fixtures."""
+    pkg, ut = io
+    pts = np.array([[0, 0, 0], [1, 0, 0], [1, 1, 0], [0, 1, 0], [0, 0, 1], [1, 0, 1], [1, 1, 1], [0, 1, 1]], float)
+    sol = np.arange(8, dtype=float) * 0.5
+    text = ('<?xml version="1.0"?>\n<VTKFile type="UnstructuredGrid" version="2.2">\n<UnstructuredGrid>\n'
+            '<Piece NumberOfPoints="8" NumberOfCells="1">\n<Points>\n'
+            '<DataArray type="Float64" NumberOfComponents="3" format="ascii">'
+            + " ".join(str(v) for v in pts.reshape(-1)) + '</DataArray>\n</Points>\n<Cells>\n'
+            '<DataArray type="Int64" Name="connectivity" format="ascii">0 1 2 3 4 5 6 7</DataArray>\n'
+            '<DataArray type="Int64" Name="offsets" format="ascii">8</DataArray>\n'
+            '<DataArray type="Int8" Name="types" format="ascii">72</DataArray>\n</Cells>\n<PointData>\n'
+            '<DataArray type="Float64" Name="sol" format="ascii">' + " ".join(str(v) for v in sol)
+            + '</DataArray>\n</PointData>\n</Piece>\n</UnstructuredGrid>\n</VTKFile>\n')
+    path = tmp_path / "d.vtu"
+    path.write_text(text)
+    p, c, pd, _ = ut.read_vtu(str(path))
+    np.testing.assert_array_equal(p, pts)
+    np.testing.assert_array_equal(c, np.arange(8)[None])
+    np.testing.assert_array_equal(pd["sol"], sol)
+
+
+# Two hexahedra side by side in x; node 99 is unused; element 3 is a boundary quad.
+_NODES = {1: (0, 0, 0), 2: (1, 0, 0), 3: (1, 1, 0), 4: (0, 1, 0), 5: (0, 0, 1), 6: (1, 0, 1), 7: (1, 1, 1),
+          8: (0, 1, 1), 9: (2, 0, 0), 10: (2, 1, 0), 11: (2, 0, 1), 12: (2, 1, 1), 99: (5, 5, 5)}
+_HEXES = [[1, 2, 3, 4, 5, 6, 7, 8], [2, 9, 10, 3, 6, 11, 12, 7]]
+
+
+def _expected(pkg):
+    used = sorted({t for h in _HEXES for t in h}, key=list(_NODES).index)
+    index = {t: i for i, t in enumerate(used)}
+    return (np.array([_NODES[t] for t in used], float),
+            np.array([[index[t] for t in h] for h in _HEXES], np.int32))
+
+
+def test_read_gmsh_and_abaqus(io, tmp_path):
+    pkg, ut = io
+    pts, cells = _expected(pkg)
+    nodes22 = "\n".join(f"{t} {x} {y} {z}" for t, (x, y, z) in _NODES.items())
+    msh22 = (f"$MeshFormat\n2.2 0 8\n$EndMeshFormat\n$Nodes\n{len(_NODES)}\n{nodes22}\n$EndNodes\n"
+             f"$Elements\n3\n1 5 2 1 1 {' '.join(map(str, _HEXES[0]))}\n2 5 2 1 1 {' '.join(map(str, _HEXES[1]))}\n"
+             f"3 3 2 2 2 1 2 6 5\n$EndElements\n")
+    ids = list(_NODES)
+    msh41 = ("$MeshFormat\n4.1 0 8\n$EndMeshFormat\n$Nodes\n2 13 1 99\n"
+             f"3 1 0 12\n" + "\n".join(map(str, ids[:12])) + "\n"
+             + "\n".join(" ".join(map(str, _NODES[t])) for t in ids[:12]) + "\n"
+             f"0 2 0 1\n99\n5 5 5\n$EndNodes\n$Elements\n2 3 1 3\n"
+             f"2 1 3 1\n3 1 2 6 5\n3 1 5 2\n1 {' '.join(map(str, _HEXES[0]))}\n2 {' '.join(map(str, _HEXES[1]))}\n"
+             "$EndElements\n")
+    inp = ("*HEADING\n** two hexahedra\n*NODE\n" + "\n".join(f"{t}, {x}, {y}, {z}" for t, (x, y, z) in _NODES.items())
+           + "\n*ELEMENT, TYPE=S4R\n3, 1, 2, 6, 5\n*ELEMENT, TYPE=C3D8, ELSET=body\n"
+           + f"1, {', '.join(map(str, _HEXES[0]))}\n2, {', '.join(map(str, _HEXES[1][:5]))},\n"
+           + f"{', '.join(map(str, _HEXES[1][5:]))}\n*END STEP\n")
+    for name, text in (("a.msh", msh22), ("b.msh", msh41), ("c.inp", inp)):
+        path = tmp_path / name
+        path.write_text(text)
+        m = ut.read_mesh(str(path))
+        np.testing.assert_array_equal(m.points, pts, err_msg=name)
+        np.testing.assert_array_equal(m.cells, cells, err_msg=name)
+    with pytest.raises(NotImplementedError):
+        ut.read_mesh(str(tmp_path / "x.stl"))
