@@ -38,7 +38,7 @@ def _worker(rank, world, port, out):
 def test_replica_max_over_ranks_gloo():
     world = 2
     port = _free_port()
-    with mp.Manager() as m:
+    with mp.get_context("spawn").Manager() as m:  # no fork of a process that already runs threads
         out = m.dict()
         mp.spawn(_worker, args=(world, port, out), nprocs=world, join=True)
         res = dict(out)
