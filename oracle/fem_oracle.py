@@ -526,6 +526,49 @@ def newton_solve(problem, initial_guess=None, rel_tol=1e-8, tol=1e-6, linear="sp
     return dofs
 
 
+def arc_length_disp(problem, Delta_l=0.1, psi=1.0, max_steps=600, tol=1e-6):
+    """Displacement-controlled arc-length continuation (solver.py:521-597,
+    721-756): Dirichlet values scaled by lambda, Crisfield's spherical
+    constraint, direct solves; then a Newton solve at full load
+    (solver.py:686-718).  Returns (u, [lambda after each step])."""
+    u = np.zeros(problem.ndofs)
+    lam, du_dir, dl_dir = 0.0, np.zeros_like(u), 0.0
+    u_b = problem.assign_bc(np.zeros_like(u))
+    ub2 = float(np.sum(u_b ** 2))
+    lams = []
+    for _ in range(max_steps):
+        u_prev, l_prev = u.copy(), lam
+        res_val = 1.0
+        while res_val > tol:
+            R = problem.newton_update(u)
+            res = problem.apply_bc_vec(R, u, lam)
+            A = problem.get_A().tocsc()
+            res_val = np.linalg.norm(res)
+            du_bar = spla.spsolve(A, -res)
+            du_t = spla.spsolve(A, u_b)
+            w = u - u_prev + du_bar
+            Dl = lam - l_prev
+            a1 = np.sum(du_t ** 2) + psi ** 2 * ub2
+            a2 = 2.0 * np.sum(w * du_t) + 2.0 * psi ** 2 * Dl * ub2
+            a3 = np.sum(w ** 2) + psi ** 2 * Dl ** 2 * ub2 - Delta_l ** 2
+            disc = np.sqrt(a2 ** 2 - 4.0 * a1 * a3)
+            roots = ((-a2 + disc) / (2.0 * a1), (-a2 - disc) / (2.0 * a1))
+            dots = [np.sum(du_dir * (w + dl * du_t)) + psi ** 2 * dl_dir * (Dl + dl) * ub2 for dl in roots]
+            if abs(dots[0]) < 1e-10 and abs(dots[1]) < 1e-10:
+                dl = max(roots)
+            else:
+                dl = roots[0] if dots[0] > dots[1] else roots[1]
+            lam += dl
+            u = u + du_bar + dl * du_t
+            du_dir, dl_dir = u - u_prev, lam - l_prev
+        lams.append(lam)
+        if lam >= 1.0:
+            break
+    if lams[-1] >= 1.0:
+        u = newton_solve(problem, initial_guess=u, rel_tol=1e-12, tol=1e-14)
+    return u, lams
+
+
 # --------------------------------------------------------------------------
 # Plasticity state commit (test_plasticity.py:67-78, fe.py:366-382)
 # --------------------------------------------------------------------------

@@ -162,6 +162,31 @@ def test_newton_paths_match_oracle(pkg, cuda, precision, rtol, delta):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("precond", ["block_jacobi", "gmg"])
+def test_arc_length_matches_oracle(pkg, cuda, precond):
+    """Displacement-controlled arc-length continuation of a 30-degree twist
+    (solver.py:521-597, 721-756): the load factor after every step equals the
+    oracle's (direct solves) to 1e-8, the path reaches lambda >= 1, and the
+    polished solution equals the oracle's Newton solution (1e-8)."""
+    n = 4
+    m = pkg.box_mesh(n, n, n, 1.0, 1.0, 1.0)
+    mesh = pkg.Mesh(m.points, m.cells_dict["hexahedron"])
+    bc = _twist(pkg, n, 30.0)
+    prob = make_problem(pkg, mesh, pkg.NeoHookean(10.0, 0.3), bc=bc)
+    lin = {"cg": {"precond": precond, "rtol": 1e-12, "atol": 0.0}}
+    (sol,), info = pkg.solver(prob, {"arc_length": {"control": "displacement", "Delta_l": 0.3, "psi": 1.0,
+                                                    "linear": lin, "return_info": True,
+                                                    "newton": {"rel_tol": 1e-10, "tol": 1e-14}}})
+    op = fo.OracleProblem(mesh.points, mesh.cells, 3, fo.Law("neo_hookean", E=10.0, nu=0.3), dirichlet_bc_info=bc)
+    ref_u, ref_lams = fo.arc_length_disp(op, Delta_l=0.3, psi=1.0)
+    lams = [h["lam"] for h in info["history"]]
+    assert len(lams) == len(ref_lams) and info["polished"] and lams[-1] >= 1.0
+    np.testing.assert_allclose(lams, ref_lams, rtol=1e-8)
+    sol = sol.cpu().numpy().reshape(-1)
+    assert np.abs(sol - ref_u).max() <= 1e-8 * np.abs(ref_u).max()
+
+
+@pytest.mark.gpu
 def test_line_search_and_custom_solver(pkg, cuda):
     S = _solver_mod()
     n = 4

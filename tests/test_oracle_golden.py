@@ -179,3 +179,23 @@ def test_closed_form_tangent_matches_complex_step(kind):
             K += _closed_form_tangent(kind, pb.shape_grads[c, q], pb.JxW[c, q], ug[c, q], params, ivq)
         Kf = K.transpose(0, 2, 1, 3).reshape(24, 24)
         np.testing.assert_allclose(Kf, jac[c], rtol=0, atol=1e-10 * np.abs(jac[c]).max())
+
+
+def test_oracle_arc_length_reaches_newton_solution():
+    """The oracle's displacement-controlled arc-length path (solver.py:521-597,
+    721-756) climbs to lambda >= 1 in increasing steps, and its polished
+    end point is the Newton solution of the full-load problem."""
+    import math
+    pts, cells = fo.box_mesh(3, 3, 3, 1.0, 1.0, 1.0)
+    c, s = math.cos(math.radians(30.0)), math.sin(math.radians(30.0))
+    left = lambda p: np.isclose(p[0], 0.0, atol=1e-5)  # noqa: E731
+    right = lambda p: np.isclose(p[0], 1.0, atol=1e-5)  # noqa: E731
+    uy = lambda p: 0.5 + (p[1] - 0.5) * c - (p[2] - 0.5) * s - p[1]  # noqa: E731
+    uz = lambda p: 0.5 + (p[1] - 0.5) * s + (p[2] - 0.5) * c - p[2]  # noqa: E731
+    z = lambda p: 0.0 * p[0]  # noqa: E731
+    bc = [[left] * 3 + [right] * 3, [0, 1, 2] * 2, [z, z, z, z, uy, uz]]
+    op = fo.OracleProblem(pts, cells, 3, fo.Law("neo_hookean", E=10.0, nu=0.3), dirichlet_bc_info=bc)
+    u, lams = fo.arc_length_disp(op, Delta_l=0.3)
+    assert lams[-1] >= 1.0 and all(b > a for a, b in zip(lams, lams[1:])) and len(lams) >= 4
+    ref = fo.newton_solve(op, rel_tol=1e-12, tol=1e-14)
+    assert np.abs(u - ref).max() <= 1e-12 * np.abs(ref).max()
