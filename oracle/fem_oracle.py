@@ -569,6 +569,51 @@ def arc_length_disp(problem, Delta_l=0.1, psi=1.0, max_steps=600, tol=1e-6):
     return u, lams
 
 
+def arc_length_force(problem, q_aux, Delta_l=0.1, psi=0.5, Delta_l_late=1.0, switch_step=200, max_steps=500,
+                     tol=1e-6):
+    """Force-controlled arc-length continuation (solver.py:607-685, 758-801):
+    residual R(u) + (1 - lambda) q with q = q_aux zeroed on Dirichlet rows,
+    direct solves; then a Newton solve at full load.  Returns (u, lambdas)."""
+    u = np.zeros(problem.ndofs)
+    lam, du_dir, dl_dir = 0.0, np.zeros_like(u), 0.0
+    q = np.asarray(q_aux, dtype=np.float64).reshape(-1).copy()
+    q[problem.bc_rows()] = 0.0
+    q2 = float(np.sum(q ** 2))
+    lams = []
+    for step in range(max_steps):
+        dl_len = Delta_l if step < switch_step else Delta_l_late
+        u_prev, l_prev = u.copy(), lam
+        res_val = 1.0
+        while res_val > tol:
+            R = problem.newton_update(u)
+            res = problem.apply_bc_vec(R, u) + (1.0 - lam) * q
+            A = problem.get_A().tocsc()
+            res_val = np.linalg.norm(res)
+            du_bar = spla.spsolve(A, -res)
+            du_t = spla.spsolve(A, q)
+            w = u - u_prev + du_bar
+            Dl = lam - l_prev
+            a1 = np.sum(du_t ** 2) + psi ** 2 * q2
+            a2 = 2.0 * np.sum(w * du_t) + 2.0 * psi ** 2 * Dl * q2
+            a3 = np.sum(w ** 2) + psi ** 2 * Dl ** 2 * q2 - dl_len ** 2
+            disc = np.sqrt(a2 ** 2 - 4.0 * a1 * a3)
+            roots = ((-a2 + disc) / (2.0 * a1), (-a2 - disc) / (2.0 * a1))
+            dots = [np.sum(du_dir * (w + dl * du_t)) + psi ** 2 * dl_dir * (Dl + dl) * q2 for dl in roots]
+            if abs(dots[0]) < 1e-10 and abs(dots[1]) < 1e-10:
+                dl = max(roots)
+            else:
+                dl = roots[0] if dots[0] > dots[1] else roots[1]
+            lam += dl
+            u = u + du_bar + dl * du_t
+            du_dir, dl_dir = u - u_prev, lam - l_prev
+        lams.append(lam)
+        if lam >= 1.0:
+            break
+    if lams[-1] >= 1.0:
+        u = newton_solve(problem, initial_guess=u, rel_tol=1e-12, tol=1e-14)
+    return u, lams
+
+
 # --------------------------------------------------------------------------
 # Plasticity state commit (test_plasticity.py:67-78, fe.py:366-382)
 # --------------------------------------------------------------------------

@@ -187,6 +187,47 @@ def test_arc_length_matches_oracle(pkg, cuda, precond):
 
 
 @pytest.mark.gpu
+def test_arc_length_force_control_matches_oracle(pkg, cuda):
+    """Force-controlled arc-length (solver.py:607-685, 758-801) of a
+    Neo-Hookean cantilever under an end traction: q_vec_aux is the residual
+    at u = 0 of the same beam under the opposite traction (get_q_vec), so
+    lambda = 0 is unloaded and lambda = 1 the full load.  Load factors step by
+    step and the polished solution match the oracle (1e-8)."""
+    S = _solver_mod()
+    m = pkg.box_mesh(6, 2, 2, 3.0, 1.0, 1.0)
+    mesh = pkg.Mesh(m.points, m.cells_dict["hexahedron"])
+    left = lambda p: np.isclose(p[0], 0.0, atol=1e-5)  # noqa: E731
+    right = lambda p: np.isclose(p[0], 3.0, atol=1e-5)  # noqa: E731
+    z = lambda p: 0.0 * p[0]  # noqa: E731
+    bc = [[left] * 3, [0, 1, 2], [z] * 3]
+    T = 0.05
+    law = pkg.NeoHookean(10.0, 0.3)
+    prob = make_problem(pkg, mesh, law, bc=bc, location_fns=[right],
+                        surface_maps=[lambda u, x: np.array([0.0, 0.0, T])])
+    aux = make_problem(pkg, mesh, law, bc=bc, location_fns=[right],
+                       surface_maps=[lambda u, x: np.array([0.0, 0.0, -T])])
+    q = S.get_q_vec(aux)
+    (sol,), info = pkg.solver(prob, {"arc_length": {"control": "force", "q_vec_aux": q, "Delta_l": 0.15,
+                                                    "psi": 0.5, "return_info": True,
+                                                    "newton": {"rel_tol": 1e-10, "tol": 1e-14}}})
+    olaw = fo.Law("neo_hookean", E=10.0, nu=0.3)
+    op = fo.OracleProblem(mesh.points, mesh.cells, 3, olaw, dirichlet_bc_info=bc, location_fns=[right],
+                          surface_maps=[lambda u, x: np.array([0.0, 0.0, T])])
+    oaux = fo.OracleProblem(mesh.points, mesh.cells, 3, olaw, dirichlet_bc_info=bc, location_fns=[right],
+                            surface_maps=[lambda u, x: np.array([0.0, 0.0, -T])])
+    qo = oaux.residual(np.zeros(oaux.ndofs))
+    np.testing.assert_allclose(q.cpu().numpy(), qo, atol=1e-14)
+    ref_u, ref_lams = fo.arc_length_force(op, qo, Delta_l=0.15, psi=0.5)
+    lams = [h["lam"] for h in info["history"]]
+    assert len(lams) == len(ref_lams) >= 5 and info["polished"] and info["control"] == "force"
+    np.testing.assert_allclose(lams, ref_lams, rtol=1e-8)
+    sol = sol.cpu().numpy().reshape(-1)
+    assert np.abs(sol - ref_u).max() <= 1e-8 * np.abs(ref_u).max()
+    with pytest.raises(ValueError):
+        pkg.solver(prob, {"arc_length": {"control": "force"}})
+
+
+@pytest.mark.gpu
 def test_line_search_and_custom_solver(pkg, cuda):
     S = _solver_mod()
     n = 4

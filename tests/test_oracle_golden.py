@@ -199,3 +199,23 @@ def test_oracle_arc_length_reaches_newton_solution():
     assert lams[-1] >= 1.0 and all(b > a for a, b in zip(lams, lams[1:])) and len(lams) >= 4
     ref = fo.newton_solve(op, rel_tol=1e-12, tol=1e-14)
     assert np.abs(u - ref).max() <= 1e-12 * np.abs(ref).max()
+
+
+def test_oracle_force_arc_length_reaches_newton_solution():
+    """The oracle's force-controlled path (solver.py:607-685, 758-801) on a
+    cantilever: counter-load q from the opposite traction, lambda climbs to 1,
+    the polished end point is the Newton solution under the full load."""
+    pts, cells = fo.box_mesh(6, 2, 2, 3.0, 1.0, 1.0)
+    left = lambda p: np.isclose(p[0], 0.0, atol=1e-5)  # noqa: E731
+    right = lambda p: np.isclose(p[0], 3.0, atol=1e-5)  # noqa: E731
+    z = lambda p: 0.0 * p[0]  # noqa: E731
+    bc = [[left] * 3, [0, 1, 2], [z] * 3]
+    law = fo.Law("neo_hookean", E=10.0, nu=0.3)
+    op = fo.OracleProblem(pts, cells, 3, law, dirichlet_bc_info=bc, location_fns=[right],
+                          surface_maps=[lambda u, x: np.array([0.0, 0.0, 0.05])])
+    aux = fo.OracleProblem(pts, cells, 3, law, dirichlet_bc_info=bc, location_fns=[right],
+                           surface_maps=[lambda u, x: np.array([0.0, 0.0, -0.05])])
+    u, lams = fo.arc_length_force(op, aux.residual(np.zeros(aux.ndofs)), Delta_l=0.15, psi=0.5)
+    assert lams[-1] >= 1.0 and all(b > a for a, b in zip(lams, lams[1:]))
+    ref = fo.newton_solve(op, rel_tol=1e-12, tol=1e-14)
+    assert np.abs(u - ref).max() <= 1e-12 * np.abs(ref).max()
