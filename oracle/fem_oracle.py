@@ -614,6 +614,54 @@ def arc_length_force(problem, q_aux, Delta_l=0.1, psi=0.5, Delta_l_late=1.0, swi
     return u, lams
 
 
+def dynamic_relax(problem, tol=1e-6, nKMat=1000, initial_guess=None, max_iters=1000000):  # noqa: N803
+    """Dynamic relaxation (solver.py:837-1047): one direct Newton step from
+    u = 0 (or the initial guess with its Dirichlet values), then the damped
+    pseudo-dynamic march until max |R| <= tol.  Returns (u, iterations)."""
+    dofs = np.zeros(problem.ndofs)
+    res = problem.apply_bc_vec(problem.newton_update(dofs), dofs)
+    dofs = dofs + spla.spsolve(problem.get_A().tocsc(), -res)
+    if initial_guess is not None:
+        dofs = problem.assign_bc(np.asarray(initial_guess, dtype=np.float64).reshape(-1))
+    rows = problem.bc_rows()
+    cmin, cmax, h_tilde, h = 1e-3, 3.9, 1.1, 1.0
+
+    def residual(d):
+        r = problem.residual(d)
+        r[rows] = 0.0
+        return r
+
+    def mass(d):
+        problem.newton_update(d)
+        return h_tilde ** 2 / 4.0 * np.asarray(abs(problem.get_A()).sum(axis=1)).reshape(-1)
+
+    R = residual(dofs)
+    M = mass(dofs)
+    q = dofs.copy()
+    qdot = -h / 2.0 * R / M
+    qdotdot, qdotdot_old = np.zeros_like(q), np.zeros_like(q)
+    n_iters, i_kmat = 0, 0
+    error = np.max(np.abs(R))
+    while error > tol and n_iters < max_iters:
+        q_old, R_old = q.copy(), R.copy()
+        q = q + h * qdot
+        R = residual(q)
+        n_iters += 1
+        i_kmat += 1
+        error = np.max(np.abs(R))
+        t = np.dot((R - R_old) / h, qdot) / np.sum(qdot * M * qdot)
+        c = min(max(2.0 * np.sqrt(max(t, 0.0)), cmin), cmax)
+        dq = q - q_old
+        eps = h_tilde ** 2 / 4.0 * np.abs(np.divide(qdotdot - qdotdot_old, dq, out=np.zeros_like(dq), where=dq != 0))
+        if np.max(eps) > 1 and i_kmat > nKMat:
+            i_kmat = 0
+            M = mass(q)
+        qdot_old, qdotdot_old = qdot.copy(), qdotdot.copy()
+        qdot = (2.0 - c * h) / (2.0 + c * h) * qdot_old - 2.0 * h / (2.0 + c * h) * R / M
+        qdotdot = (qdot - qdot_old) / h
+    return q, n_iters
+
+
 # --------------------------------------------------------------------------
 # Plasticity state commit (test_plasticity.py:67-78, fe.py:366-382)
 # --------------------------------------------------------------------------

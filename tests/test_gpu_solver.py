@@ -228,6 +228,29 @@ def test_arc_length_force_control_matches_oracle(pkg, cuda):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("nkmat", [1000, 5])
+def test_dynamic_relax_matches_oracle(pkg, cuda, nkmat):
+    """Dynamic relaxation (solver.py:837-1047) of a 20-degree twist: the
+    iteration count and the end point equal the oracle's (1e-9), and the end
+    point is the Newton solution to within the tolerance (1e-6).  nKMat = 5
+    also exercises the mass re-formed from a new tangent."""
+    n = 3
+    m = pkg.box_mesh(n, n, n, 1.0, 1.0, 1.0)
+    mesh = pkg.Mesh(m.points, m.cells_dict["hexahedron"])
+    bc = _twist(pkg, n, 20.0)
+    prob = make_problem(pkg, mesh, pkg.NeoHookean(10.0, 0.3), bc=bc)
+    (sol,) = pkg.solver(prob, {"dynamic_relax": {"tol": 1e-8, "nKMat": nkmat, "info": False, "info_force": False}})
+    its = prob.last_solve_info["dr_iters"]
+    op = fo.OracleProblem(mesh.points, mesh.cells, 3, fo.Law("neo_hookean", E=10.0, nu=0.3), dirichlet_bc_info=bc)
+    ref_u, ref_its = fo.dynamic_relax(op, tol=1e-8, nKMat=nkmat)
+    sol = sol.cpu().numpy().reshape(-1)
+    assert abs(its - ref_its) <= 1, (its, ref_its)
+    assert np.abs(sol - ref_u).max() <= 1e-9 * np.abs(ref_u).max()
+    newton = fo.newton_solve(op, rel_tol=1e-12, tol=1e-14)
+    assert np.abs(sol - newton).max() <= 1e-6 * np.abs(newton).max()
+
+
+@pytest.mark.gpu
 def test_line_search_and_custom_solver(pkg, cuda):
     S = _solver_mod()
     n = 4

@@ -219,3 +219,23 @@ def test_oracle_force_arc_length_reaches_newton_solution():
     assert lams[-1] >= 1.0 and all(b > a for a, b in zip(lams, lams[1:]))
     ref = fo.newton_solve(op, rel_tol=1e-12, tol=1e-14)
     assert np.abs(u - ref).max() <= 1e-12 * np.abs(ref).max()
+
+
+def test_oracle_dynamic_relax_reaches_newton_solution():
+    """The oracle's dynamic relaxation (solver.py:837-1047) ends within its
+    residual tolerance of the Newton solution."""
+    import math
+    pts, cells = fo.box_mesh(3, 3, 3, 1.0, 1.0, 1.0)
+    c, s = math.cos(math.radians(20.0)), math.sin(math.radians(20.0))
+    left = lambda p: np.isclose(p[0], 0.0, atol=1e-5)  # noqa: E731
+    right = lambda p: np.isclose(p[0], 1.0, atol=1e-5)  # noqa: E731
+    uy = lambda p: 0.5 + (p[1] - 0.5) * c - (p[2] - 0.5) * s - p[1]  # noqa: E731
+    uz = lambda p: 0.5 + (p[1] - 0.5) * s + (p[2] - 0.5) * c - p[2]  # noqa: E731
+    z = lambda p: 0.0 * p[0]  # noqa: E731
+    bc = [[left] * 3 + [right] * 3, [0, 1, 2] * 2, [z, z, z, z, uy, uz]]
+    op = fo.OracleProblem(pts, cells, 3, fo.Law("neo_hookean", E=10.0, nu=0.3), dirichlet_bc_info=bc)
+    u, its = fo.dynamic_relax(op, tol=1e-8)
+    assert 0 < its < 1000
+    assert np.max(np.abs(np.delete(op.residual(u), op.bc_rows()))) <= 1e-8
+    ref = fo.newton_solve(op, rel_tol=1e-12, tol=1e-14)
+    assert np.abs(u - ref).max() <= 1e-6 * np.abs(ref).max()
