@@ -207,8 +207,9 @@ def test_arc_length_force_control_matches_oracle(pkg, cuda):
     aux = make_problem(pkg, mesh, law, bc=bc, location_fns=[right],
                        surface_maps=[lambda u, x: np.array([0.0, 0.0, -T])])
     q = S.get_q_vec(aux)
+    lin = {"cg": {"precond": "block_jacobi", "rtol": 1e-12, "atol": 0.0}}  # also the polishing solve's
     (sol,), info = pkg.solver(prob, {"arc_length": {"control": "force", "q_vec_aux": q, "Delta_l": 0.15,
-                                                    "psi": 0.5, "return_info": True,
+                                                    "psi": 0.5, "return_info": True, "linear": lin,
                                                     "newton": {"rel_tol": 1e-10, "tol": 1e-14}}})
     olaw = fo.Law("neo_hookean", E=10.0, nu=0.3)
     op = fo.OracleProblem(mesh.points, mesh.cells, 3, olaw, dirichlet_bc_info=bc, location_fns=[right],
