@@ -2,7 +2,7 @@
 
 A 3D convolutional encoder-decoder maps the density field rho and the load
 patch to a displacement field that seeds Newton/CG.  The exact FP64 Newton
-residual remains the judge: the converged answer is always the solver's, the
+residual still decides convergence: the converged answer is always the solver's, the
 network only changes where the iteration starts (``solver_options
 ['newton']['warm_start']``); with no network the start is zero.
 
