@@ -17,17 +17,23 @@ namespace fem {
 #ifndef FEM_ROW_GROUP_F64
 #define FEM_ROW_GROUP_F64 2
 #endif
+#ifndef FEM_ROW_GROUP_MIXED
+#define FEM_ROW_GROUP_MIXED 3
+#endif
 
 constexpr int kRowThreads = 256;   // 8 warps per block
 constexpr int kStageBytes = FEM_ROW_STAGE_BYTES;     // per-warp shared-memory stage for matrix values
 constexpr int kRowBlocksPerSM = FEM_ROW_BLOCKS_PER_SM;  // resident blocks per SM the row kernels are sized for
 
 // Block rows per warp group: ~3.9 KB of FP32 or FP64 3x3 blocks; FP32
-// values with FP64 accumulation take 2 rows to stay within the registers of
-// kRowBlocksPerSM resident blocks.
+// values with FP64 accumulation take 3 rows, the most that stay within the
+// registers of kRowBlocksPerSM resident blocks without spills (3 measured
+// ~1 % faster per multigrid CG iteration than 2 on the 50^3 tangent).
 template <typename VT, typename AT = VT>
 __host__ __device__ constexpr int rows_per_warp() {
-  return (sizeof(VT) == 4 && sizeof(AT) == 4) ? FEM_ROW_GROUP_F32 : FEM_ROW_GROUP_F64;
+  return (sizeof(VT) == 4 && sizeof(AT) == 4) ? FEM_ROW_GROUP_F32
+         : (sizeof(VT) == 4)                      ? FEM_ROW_GROUP_MIXED
+                                                  : FEM_ROW_GROUP_F64;
 }
 
 // Dynamic shared memory a bsr_rows kernel needs (one stage per warp).
