@@ -97,6 +97,64 @@ def nh_solve(pkg, prob, precision, steps=5, total_deg=30.0, linear=None, extrapo
     return sol, infos
 
 
+def element_problem(pkg, ele, n):
+    """The Neo-Hookean twist on an n^3 box of another element type."""
+    import importlib
+    gm = importlib.import_module("jax_fem_b200.generate_mesh")
+    m = gm.box_mesh_gmsh(n, n, n, 1.0, 1.0, 1.0, None, ele)
+    mesh = pkg.Mesh(m.points, m.cells_dict[gm.get_meshio_cell_type(ele)], ele)
+
+    class HyperElasticity(pkg.Problem):
+        def get_tensor_map(self):
+            return pkg.NeoHookean(10.0, 0.3)
+
+    return HyperElasticity(mesh, vec=3, dim=3, ele_type=ele, dirichlet_bc_info=rotation_bc(0.0))
+
+
+# element type -> box divisions: 51^3 nodes (397,953 dofs, the HEX8 50^3
+# node count) for TET4, TET10 and HEX27; HEX20 has no face or cell nodes
+ELEMENT_BOXES = (("TET4", 50), ("TET10", 25), ("HEX27", 25), ("HEX20", 25))
+
+
+def element_bench(pkg, device):
+    """General-element kernel: Neo-Hookean assembly (FP64 residual with the
+    FP64 or FP32 tangent) and the 5-step twist solved in mixed precision
+    (block-Jacobi CG, adaptive forcing; multigrid needs the HEX8 lattice)."""
+    out = {}
+    for ele, n in ELEMENT_BOXES:
+        prob = element_problem(pkg, ele, n)
+        dv = prob.dev()
+        nd = dv.ndofs
+        u = torch.zeros(nd, dtype=torch.float64, device=device)
+        res = torch.empty_like(u)
+        A64, A32 = dv.new_matrix(torch.float64), dv.new_matrix(torch.float32)
+        t64 = time_kernel(lambda: prob.assemble(u, res=res, vals=A64.vals), reps=5)
+        t32 = time_kernel(lambda: prob.assemble(u, res=res, vals=A32.vals, fp32=True), reps=5)
+        nen, nq = dv.nen, prob.fes[0].num_quads
+        # cells: connectivity + node coordinates + u; the tangent values once; the residual
+        asm_bytes = dv.num_cells * nen * (4 + 3 * 8 + 3 * 8) + dv.nnzb * 9 * 8 + nd * 8
+        del A64, A32
+        lin = {"cg": {"precond": "block_jacobi", "rtol": "adaptive", "atol": 0.0, "maxiter": 20000}}
+        nh_solve(pkg, prob, "mixed", linear=lin)  # warm-up
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        _, infos = nh_solve(pkg, prob, "mixed", linear=lin)
+        e1.record()
+        torch.cuda.synchronize()
+        hbm, _ = peaks()
+        out[ele] = {"cells": dv.num_cells, "dofs": nd, "nodes_per_cell": nen, "quad_points": nq, "nnzb": dv.nnzb,
+                    "assembly_us": {"fp64": round(t64 * 1e6, 1), "fp32": round(t32 * 1e6, 1)},
+                    "assembly_dofs_per_s": {"fp64": round(nd / t64), "fp32": round(nd / t32)},
+                    "assembly_hbm_frac_fp64": round(asm_bytes / t64 / 1e9 / hbm, 3),
+                    "twist_solve_s": round(e0.elapsed_time(e1) * 1e-3, 4),
+                    "newton_iters": sum(i["newton_iters"] for i in infos),
+                    "krylov_iters": sum(sum(i["krylov_iters"]) for i in infos)}
+        del prob, dv
+        torch.cuda.empty_cache()
+    return out
+
+
 def j2_run(pkg, n=40, increments=10, precision="fp64", linear=None):
     """40^3 J2 cube with hardening: u_x(x=1) ramped to 0.02 over the increments,
     Newton to 1e-8 per increment, state committed after each."""
@@ -361,6 +419,12 @@ def run_ours(args, rank, world, device):
         e1.record()
         torch.cuda.synchronize()
         j2[arm] = {"s": round(e0.elapsed_time(e1) * 1e-3, 4), "newton": jn, "krylov": jk}
+    elements = None
+    if not args.no_elements:
+        try:
+            elements = element_bench(pkg, device)
+        except Exception as e:  # noqa: BLE001 - report, do not lose the headline line
+            elements = {"error": str(e)[:300]}
     newton = {k: sum(i["newton_iters"] for i in v[1]) for k, v in results.items()}
     krylov = {k: sum(sum(i["krylov_iters"]) for i in v[1]) for k, v in results.items()}
     out = {
@@ -413,6 +477,7 @@ def run_ours(args, rank, world, device):
                      "algorithmic_bytes": spmv_bytes, "us_per_launch": round(t_spmv * 1e6, 2)},
         "simp60_learned_warm_start": simp,
         "j2_40_10_increments": j2,
+        "other_elements_neo_hookean_twist": elements,
         "e2e": {"value": round(t_e2e, 6), "unit": "s", "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": int(ndofs * 8)},
         "gpu_launches": int(launches),
@@ -614,6 +679,7 @@ def main():
     ap.add_argument("--n", type=int, default=50)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--simp-samples", type=int, default=12)
+    ap.add_argument("--no-elements", action="store_true", help="skip the TET4/TET10/HEX20/HEX27 measurements")
     ap.add_argument("--profile", action="store_true", help="short kernel sequence for ncu captures")
     ap.add_argument("--warmstart-train", action="store_true",
                     help="generate SIMP (rho, u) pairs, train the warm-start network, evaluate, save")

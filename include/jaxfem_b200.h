@@ -93,6 +93,13 @@ FEM_API int64_t fem_launch_count(void);
 FEM_API int fem_bsr_pattern(const int32_t* h_cells, int64_t num_cells, int64_t num_nodes,
                     int32_t* h_row_ptr, int64_t* h_nnzb, int32_t* h_col_idx,
                     int64_t col_capacity, int32_t* h_scatter, int32_t* h_diag);
+/* The same for cells of nen nodes (the element types of basis.py:19-114:
+ * TET4 4, HEX8 8, TET10 10, HEX20 20, HEX27 27); h_cells is (num_cells, nen)
+ * and h_scatter (num_cells, nen*nen) with the block index of local pair
+ * (a, b) at [c*nen*nen + a*nen + b].  fem_bsr_pattern is the nen = 8 case. */
+FEM_API int fem_bsr_pattern_nen(const int32_t* h_cells, int64_t num_cells, int nen, int64_t num_nodes,
+                    int32_t* h_row_ptr, int64_t* h_nnzb, int32_t* h_col_idx,
+                    int64_t col_capacity, int32_t* h_scatter, int32_t* h_diag);
 /* Block transpose map (host, one-off): h_tmap[k] = index of block (j, i) for
  * block k = (i, j) of a row-sorted, structurally symmetric pattern (as
  * fem_bsr_pattern builds).  Assembly writes the lower block triangle from
@@ -143,6 +150,44 @@ FEM_API int fem_assemble_f32(int law, const double* h_params, int n_params, int 
                      const int32_t* d_transpose, int64_t nnzb,
                      const uint8_t* d_bc_mask, const double* d_dvec,
                      double* d_res, double* d_lift, float* d_vals, void* stream);
+
+/* ---- general elements ---------------------------------------------------
+ * The same cell assembly for the element types of basis.py:19-114 other than
+ * the HEX8 fast path above (TET4, TET10, HEX20, HEX27; HEX8 is accepted too).
+ * The element enters through its tabulation (get_shape_vals_and_grads,
+ * basis.py:141-175): d_gref (nq, nen, 3) f64, the reference shape gradients
+ * at the quadrature points in mesh node order, and d_wq (nq) the weights.
+ *   nen in {4, 8, 10, 20, 27}; 1 <= nq <= 4096
+ *   d_cells (num_cells, nen); d_scatter (num_cells, nen*nen) from
+ *   fem_bsr_pattern_nen; internal variables are per (cell, quadrature
+ *   point): theta / psi scale (num_cells, nq), J2 state (num_cells, nq, 3, 3)
+ *   and (num_cells, nq).
+ * Outputs, Dirichlet elimination and the lift are those of fem_assemble_*.
+ * The _f32 variant accumulates the tangent in FP64 and stores it in FP32. */
+FEM_API int fem_assemble_elem_f64(int law, const double* h_params, int n_params, int vec, int nen, int nq,
+                     const double* d_gref, const double* d_wq, int64_t num_cells, int64_t num_nodes,
+                     const int32_t* d_cells, const double* d_points, const double* d_u,
+                     const double* d_ivar0, const double* d_ivar1, const double* d_ivar2,
+                     const int32_t* d_scatter, const int32_t* d_diag, const int32_t* d_transpose,
+                     int64_t nnzb, const uint8_t* d_bc_mask, const double* d_dvec,
+                     double* d_res, double* d_lift, double* d_vals, void* stream);
+FEM_API int fem_assemble_elem_f32(int law, const double* h_params, int n_params, int vec, int nen, int nq,
+                     const double* d_gref, const double* d_wq, int64_t num_cells, int64_t num_nodes,
+                     const int32_t* d_cells, const double* d_points, const double* d_u,
+                     const double* d_ivar0, const double* d_ivar1, const double* d_ivar2,
+                     const int32_t* d_scatter, const int32_t* d_diag, const int32_t* d_transpose,
+                     int64_t nnzb, const uint8_t* d_bc_mask, const double* d_dvec,
+                     double* d_res, double* d_lift, float* d_vals, void* stream);
+/* fem_j2_commit for these elements (state arrays (num_cells, nq, ...)). */
+FEM_API int fem_j2_commit_elem(const double* h_params, int n_params, int nen, int nq, const double* d_gref,
+                     int64_t num_cells, const int32_t* d_cells, const double* d_points, const double* d_u,
+                     const double* d_sigma_old, const double* d_eps_old, const double* d_alpha_old,
+                     double* d_sigma_new, double* d_eps_new, double* d_alpha_new, void* stream);
+/* fem_param_vjp_f64 for these elements: d_grad (num_cells, nq). */
+FEM_API int fem_param_vjp_elem_f64(int law, const double* h_params, int n_params, int nen, int nq,
+                     const double* d_gref, const double* d_wq, int64_t num_cells, const int32_t* d_cells,
+                     const double* d_points, const double* d_u, const double* d_ivar0,
+                     const double* d_lambda, double* d_grad, void* stream);
 
 /* ---- J2 state commit ----------------------------------------------------
  * Replaces the reference plasticity update (test_plasticity.py:67-78 with

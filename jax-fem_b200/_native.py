@@ -74,6 +74,13 @@ _SIGS = {
     "fem_bsr_pattern": (I32, [P, I64, I64, P, _c.POINTER(I64), P, I64, P, P]),
     "fem_assemble_f64": (I32, [I32, DP, I32, I32, I64, I64, P, P, P, P, P, P, P, P, P, I64, P, P, P, P, P, P]),
     "fem_assemble_f32": (I32, [I32, DP, I32, I32, I64, I64, P, P, P, P, P, P, P, P, P, I64, P, P, P, P, P, P]),
+    "fem_bsr_pattern_nen": (I32, [P, I64, I32, I64, P, _c.POINTER(I64), P, I64, P, P]),
+    "fem_assemble_elem_f64": (I32, [I32, DP, I32, I32, I32, I32, P, P, I64, I64, P, P, P, P, P, P, P, P, P, I64, P,
+                                    P, P, P, P, P]),
+    "fem_assemble_elem_f32": (I32, [I32, DP, I32, I32, I32, I32, P, P, I64, I64, P, P, P, P, P, P, P, P, P, I64, P,
+                                    P, P, P, P, P]),
+    "fem_j2_commit_elem": (I32, [DP, I32, I32, I32, P, I64, P, P, P, P, P, P, P, P, P, P]),
+    "fem_param_vjp_elem_f64": (I32, [I32, DP, I32, I32, I32, P, P, I64, P, P, P, P, P, P, P]),
     "fem_bsr_transpose_map": (I32, [P, P, I64, P]),
     "fem_j2_commit": (I32, [DP, I32, I64, P, P, P, P, P, P, P, P, P, P]),
     "fem_j2_sensitivity": (I32, [DP, I32, I64, P, P, P, P, P, P, P, P, P, P, P, P, P, P]),

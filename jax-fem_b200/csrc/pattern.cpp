@@ -6,7 +6,9 @@
 // adjacency graph (one vec x vec block per pair of nodes sharing a cell);
 // the scatter map gives, for every cell and local node pair (a, b), the
 // index of block (cells[c,a], cells[c,b]) so assembly adds straight into the
-// values array.  Columns are sorted within each block row.
+// values array.  Columns are sorted within each block row.  Any number of
+// nodes per cell (nen): HEX8 and the other element types of basis.py:19-114
+// share this code.
 #include <algorithm>
 #include <cstdint>
 #include <vector>
@@ -21,26 +23,26 @@ struct Adjacency {
   std::vector<int32_t> cells;  // incident cells
 };
 
-int build_adjacency(const int32_t* cells, int64_t C, int64_t N, Adjacency* adj) {
+int build_adjacency(const int32_t* cells, int64_t C, int nen, int64_t N, Adjacency* adj) {
   adj->start.assign(size_t(N) + 1, 0);
-  for (int64_t i = 0; i < C * 8; ++i) {
+  for (int64_t i = 0; i < C * nen; ++i) {
     const int32_t n = cells[i];
     if (n < 0 || n >= N) {
       fem::set_error("fem_bsr_pattern: cell %lld references node %d outside [0, %lld)",
-                     (long long)(i / 8), n, (long long)N);
+                     (long long)(i / nen), n, (long long)N);
       return FEM_ERR_ARG;
     }
     adj->start[size_t(n) + 1]++;
   }
   for (int64_t n = 0; n < N; ++n) adj->start[n + 1] += adj->start[n];
-  adj->cells.resize(size_t(C) * 8);
+  adj->cells.resize(size_t(C) * nen);
   std::vector<int64_t> fill(adj->start.begin(), adj->start.end() - 1);
   for (int64_t c = 0; c < C; ++c)
-    for (int a = 0; a < 8; ++a) {
-      const int32_t n = cells[c * 8 + a];
+    for (int a = 0; a < nen; ++a) {
+      const int32_t n = cells[c * nen + a];
       // a cell listing the same node twice is adjacent once
       bool dup = false;
-      for (int b = 0; b < a; ++b) dup |= (cells[c * 8 + b] == n);
+      for (int b = 0; b < a; ++b) dup |= (cells[c * nen + b] == n);
       if (!dup) adj->cells[fill[n]++] = int32_t(c);
     }
   // shrink ranges to the filled part (duplicates leave holes at the end)
@@ -48,12 +50,12 @@ int build_adjacency(const int32_t* cells, int64_t C, int64_t N, Adjacency* adj) 
 }
 
 // Sorted unique neighbours of node n.
-void neighbours(const int32_t* cells, const Adjacency& adj, const std::vector<int64_t>& fill_end,
+void neighbours(const int32_t* cells, int nen, const Adjacency& adj, const std::vector<int64_t>& fill_end,
                 int64_t n, std::vector<int32_t>* out) {
   out->clear();
   for (int64_t k = adj.start[n]; k < fill_end[n]; ++k) {
     const int32_t c = adj.cells[k];
-    for (int b = 0; b < 8; ++b) out->push_back(cells[int64_t(c) * 8 + b]);
+    for (int b = 0; b < nen; ++b) out->push_back(cells[int64_t(c) * nen + b]);
   }
   std::sort(out->begin(), out->end());
   out->erase(std::unique(out->begin(), out->end()), out->end());
@@ -61,24 +63,25 @@ void neighbours(const int32_t* cells, const Adjacency& adj, const std::vector<in
 
 }  // namespace
 
-extern "C" int fem_bsr_pattern(const int32_t* h_cells, int64_t num_cells, int64_t num_nodes,
-                               int32_t* h_row_ptr, int64_t* h_nnzb, int32_t* h_col_idx,
-                               int64_t col_capacity, int32_t* h_scatter, int32_t* h_diag) {
+extern "C" int fem_bsr_pattern_nen(const int32_t* h_cells, int64_t num_cells, int nen, int64_t num_nodes,
+                                   int32_t* h_row_ptr, int64_t* h_nnzb, int32_t* h_col_idx,
+                                   int64_t col_capacity, int32_t* h_scatter, int32_t* h_diag) {
   FEM_CHECK_ARG(num_cells >= 0 && num_nodes >= 0, "negative sizes");
+  FEM_CHECK_ARG(nen >= 1 && nen <= 64, "nodes per cell %d outside [1, 64]", nen);
   FEM_CHECK_ARG(num_cells == 0 || h_cells != nullptr, "cells is NULL");
   FEM_CHECK_ARG(h_row_ptr != nullptr && h_nnzb != nullptr, "row_ptr/nnzb is NULL");
   Adjacency adj;
-  int rc = build_adjacency(h_cells, num_cells, num_nodes, &adj);
+  int rc = build_adjacency(h_cells, num_cells, nen, num_nodes, &adj);
   if (rc != FEM_OK) return rc;
   // end of the filled range of each node
   std::vector<int64_t> fill_end(size_t(num_nodes), 0);
   {
     std::vector<int64_t> fill(adj.start.begin(), adj.start.end() - 1);
     for (int64_t c = 0; c < num_cells; ++c)
-      for (int a = 0; a < 8; ++a) {
-        const int32_t n = h_cells[c * 8 + a];
+      for (int a = 0; a < nen; ++a) {
+        const int32_t n = h_cells[c * nen + a];
         bool dup = false;
-        for (int b = 0; b < a; ++b) dup |= (h_cells[c * 8 + b] == n);
+        for (int b = 0; b < a; ++b) dup |= (h_cells[c * nen + b] == n);
         if (!dup) fill[n]++;
       }
     for (int64_t n = 0; n < num_nodes; ++n) fill_end[n] = fill[n];
@@ -87,7 +90,7 @@ extern "C" int fem_bsr_pattern(const int32_t* h_cells, int64_t num_cells, int64_
   int64_t nnzb = 0;
   h_row_ptr[0] = 0;
   for (int64_t n = 0; n < num_nodes; ++n) {
-    neighbours(h_cells, adj, fill_end, n, &nb);
+    neighbours(h_cells, nen, adj, fill_end, n, &nb);
     if (nb.empty()) nb.push_back(int32_t(n));  // isolated node keeps its diagonal block
     if (h_col_idx != nullptr) {
       if (nnzb + int64_t(nb.size()) > col_capacity) {
@@ -109,19 +112,27 @@ extern "C" int fem_bsr_pattern(const int32_t* h_cells, int64_t num_cells, int64_
   }
   *h_nnzb = nnzb;
   if (h_col_idx != nullptr && h_scatter != nullptr) {
+    const int64_t nn = int64_t(nen) * nen;
     for (int64_t c = 0; c < num_cells; ++c)
-      for (int a = 0; a < 8; ++a) {
-        const int32_t na = h_cells[c * 8 + a];
+      for (int a = 0; a < nen; ++a) {
+        const int32_t na = h_cells[c * nen + a];
         const int32_t* b0 = h_col_idx + h_row_ptr[na];
         const int32_t* b1 = h_col_idx + h_row_ptr[na + 1];
-        for (int b = 0; b < 8; ++b) {
-          const int32_t nbn = h_cells[c * 8 + b];
+        for (int b = 0; b < nen; ++b) {
+          const int32_t nbn = h_cells[c * nen + b];
           const int32_t* it = std::lower_bound(b0, b1, nbn);
-          h_scatter[c * 64 + a * 8 + b] = int32_t(it - h_col_idx);
+          h_scatter[c * nn + a * nen + b] = int32_t(it - h_col_idx);
         }
       }
   }
   return FEM_OK;
+}
+
+extern "C" int fem_bsr_pattern(const int32_t* h_cells, int64_t num_cells, int64_t num_nodes,
+                               int32_t* h_row_ptr, int64_t* h_nnzb, int32_t* h_col_idx,
+                               int64_t col_capacity, int32_t* h_scatter, int32_t* h_diag) {
+  return fem_bsr_pattern_nen(h_cells, num_cells, 8, num_nodes, h_row_ptr, h_nnzb, h_col_idx, col_capacity,
+                             h_scatter, h_diag);
 }
 
 // Block transpose map of a block-CSR pattern: h_tmap[k] = index of block

@@ -1,5 +1,6 @@
-"""Host-side HEX8 finite-element setup: Dirichlet and boundary-face discovery,
-face geometry and the (u-independent) body/surface load vectors.
+"""Host-side finite-element setup: element tables, Dirichlet and
+boundary-face discovery, face geometry and the (u-independent) body/surface
+load vectors.
 
 Mirrors ``FiniteElement`` (fe.py:20-322 in the reference) for what runs once
 per problem or per load step.  Nothing here is on the per-iteration path:
@@ -25,48 +26,7 @@ import weakref
 
 import numpy as np
 
-# basix hexahedron facets (vertex lists in basix numbering) and outward normals,
-# in the order the reference's face tables use (basis.py:215-240).
-_BASIX_FACETS = np.array([[0, 1, 2, 3], [0, 1, 4, 5], [0, 2, 4, 6],
-                          [1, 3, 5, 7], [2, 3, 6, 7], [4, 5, 6, 7]])
-_FACET_NORMALS = np.array([[0, 0, -1], [0, -1, 0], [-1, 0, 0],
-                           [1, 0, 0], [0, 1, 0], [0, 0, 1]], dtype=np.float64)
-# VTK <-> basix HEX8 node permutation (basis.py:53); it is its own inverse.
-_REORDER = np.array([0, 1, 3, 2, 4, 5, 7, 6])
-# basix vertex coordinates of the unit hexahedron (x fastest)
-_BASIX_VERTS = np.array([[(v >> 0) & 1, (v >> 1) & 1, (v >> 2) & 1] for v in range(8)], dtype=np.float64)
-VTK_NODE_XI = _BASIX_VERTS[_REORDER]  # reference coordinates of VTK node a
-FACE_INDS = _REORDER[_BASIX_FACETS]   # (6,4) VTK node numbers of each face
-
-_G = 0.5 / np.sqrt(3.0)
-_GAUSS = np.array([0.5 - _G, 0.5 + _G])
-
-
-def hex8_eval(xi):
-    """Shape values (n,8) and reference gradients (n,8,3) at points xi (n,3)."""
-    xi = np.atleast_2d(np.asarray(xi, dtype=np.float64))
-    X = VTK_NODE_XI
-    f = np.where(X[None] > 0.5, xi[:, None, :], 1.0 - xi[:, None, :])  # (n,8,3)
-    s = np.where(X > 0.5, 1.0, -1.0)[None]
-    vals = f.prod(axis=2)
-    grads = np.stack([s[..., 0] * f[..., 1] * f[..., 2],
-                      f[..., 0] * s[..., 1] * f[..., 2],
-                      f[..., 0] * f[..., 1] * s[..., 2]], axis=2)
-    return vals, grads
-
-
-def volume_quadrature():
-    """2x2x2 Gauss points (x slowest) and weights on [0,1]^3."""
-    pts = np.array([[a, b, c] for a in _GAUSS for b in _GAUSS for c in _GAUSS])
-    return pts, np.full(8, 0.125)
-
-
-def face_quadrature(face):
-    """2x2 Gauss points of one face (reference coords, basix facet map) and weights."""
-    v = _BASIX_VERTS[_BASIX_FACETS[face]]
-    pts = np.array([v[0] + s * (v[1] - v[0]) + t * (v[2] - v[0]) for s in _GAUSS for t in _GAUSS])
-    return pts, np.full(4, 0.25)
-
+from . import basis
 
 # Functions whose batched evaluation was confirmed against point-wise calls
 # (a property of the function's code): later calls with the same function
@@ -178,27 +138,33 @@ def _location_flags(fn, points):
 
 
 class FiniteElement:
-    """One HEX8 field (fe.py:20-110).  Holds Dirichlet data as host arrays."""
+    """One field on a mesh of one 3D element type (fe.py:20-110).  Holds the
+    element tables (basis.py) and Dirichlet data as host arrays."""
 
     def __init__(self, mesh, vec, dim, ele_type="HEX8", quadrature_rule=None, quadrature_order=None,
                  dirichlet_bc_info=None):
-        if ele_type != "HEX8":
-            raise NotImplementedError(f"element {ele_type}: only HEX8 is on this path")
+        basis.check_ele_type(ele_type)
         if dim != 3:
             raise NotImplementedError("only dim=3 is supported")
-        if quadrature_order not in (None, 2) or quadrature_rule not in (None, "default"):
-            raise NotImplementedError("only the default 2x2x2 Gauss rule is supported")
+        if quadrature_rule not in (None, "default"):
+            raise NotImplementedError("only basix's default quadrature rule is supported")
+        if mesh.cells.shape[1] != basis.NODES_PER_CELL[ele_type]:
+            raise ValueError(f"{ele_type} needs cells of {basis.NODES_PER_CELL[ele_type]} nodes, "
+                             f"the mesh has {mesh.cells.shape[1]}")
         self.mesh = mesh
         self.points = mesh.points
         self.cells = mesh.cells
         self.vec, self.dim, self.ele_type = vec, dim, ele_type
+        self.quadrature_order = basis.DEFAULT_ORDER[ele_type] if quadrature_order is None else int(quadrature_order)
         self.num_cells = len(self.cells)
         self.num_total_nodes = len(self.points)
         self.num_total_dofs = self.num_total_nodes * vec
-        self.num_nodes, self.num_quads, self.num_faces, self.num_face_quads = 8, 8, 6, 4
-        self.face_inds = FACE_INDS
-        qp, self.quad_weights = volume_quadrature()
-        self.shape_vals, self.shape_grads_ref = hex8_eval(qp)
+        self.shape_vals, self.shape_grads_ref, self.quad_weights = basis.get_shape_vals_and_grads(
+            ele_type, self.quadrature_order)
+        (self.face_shape_vals, self.face_shape_grads_ref, self.face_quad_weights, self.face_normals,
+         self.face_inds) = basis.get_face_shape_vals_and_grads(ele_type, self.quadrature_order)
+        self.num_quads, self.num_nodes = self.shape_vals.shape
+        self.num_faces, self.num_face_quads = self.face_quad_weights.shape
         self.dirichlet_bc_info = dirichlet_bc_info
         self.bc_version = 0
         self.node_inds_list, self.vec_inds_list, self.vals_list = self.Dirichlet_boundary_conditions(
@@ -266,37 +232,27 @@ class FiniteElement:
             return out
         for lf in location_fns:
             flags = _location_flags(lf, self.points)
-            cf = flags[self.cells[:, FACE_INDS]]  # (C,6,4)
+            cf = flags[self.cells[:, self.face_inds]]  # (C, faces, face vertices)
             out.append(np.argwhere(cf.all(axis=2)))
         return out
 
     def get_face_shape_grads(self, boundary_inds):
-        """Physical face shape gradients (F,4,8,3) and Nanson scale (F,4) (fe.py:143-183)."""
+        """Physical face shape gradients (F,fq,nen,3) and Nanson scale (F,fq) (fe.py:143-183)."""
         binds = np.asarray(boundary_inds).reshape(-1, 2)
         F = len(binds)
-        grads = np.zeros((F, 4, 8, 3))
-        scale = np.zeros((F, 4))
-        X = self.points[self.cells[binds[:, 0]]] if F else np.zeros((0, 8, 3))
-        for face in range(6):
-            sel = np.nonzero(binds[:, 1] == face)[0]
-            if len(sel) == 0:
-                continue
-            pts, w = face_quadrature(face)
-            _, gref = hex8_eval(pts)  # (4,8,3)
-            J = np.einsum("fai,qaj->fqij", X[sel], gref)
-            Jinv = np.linalg.inv(J)
-            grads[sel] = np.einsum("qaj,fqjk->fqak", gref, Jinv)
-            nJ = np.einsum("i,fqij->fqj", _FACET_NORMALS[face], Jinv)
-            scale[sel] = np.linalg.norm(nJ, axis=-1) * np.linalg.det(J) * w[None]
+        gref = self.face_shape_grads_ref[binds[:, 1]]  # (F,fq,nen,3)
+        X = self.points[self.cells[binds[:, 0]]] if F else np.zeros((0, self.num_nodes, 3))
+        J = np.einsum("fai,fqaj->fqij", X, gref)
+        if F == 0:
+            return np.zeros((0, self.num_face_quads, self.num_nodes, 3)), np.zeros((0, self.num_face_quads))
+        Jinv = np.linalg.inv(J)
+        grads = np.einsum("fqaj,fqjk->fqak", gref, Jinv)
+        nJ = np.einsum("fi,fqij->fqj", self.face_normals[binds[:, 1]], Jinv)
+        scale = np.linalg.norm(nJ, axis=-1) * np.linalg.det(J) * self.face_quad_weights[binds[:, 1]]
         return grads, scale
 
     def face_shape_vals_at(self, faces):
-        out = np.zeros((len(faces), 4, 8))
-        for face in range(6):
-            sel = np.nonzero(np.asarray(faces) == face)[0]
-            if len(sel):
-                out[sel] = hex8_eval(face_quadrature(face)[0])[0][None]
-        return out
+        return self.face_shape_vals[np.asarray(faces, dtype=np.int64)]
 
     # -- load vectors of u-independent maps (problem.py:216-259) ---------------
     def _check_u_independent(self, fn, x):
@@ -312,13 +268,14 @@ class FiniteElement:
 
     def body_load(self, mass_map):
         """int mass_map(u, x) . v dx as a (ndofs,) vector."""
-        X = self.points[self.cells]  # (C,8,3)
+        X = self.points[self.cells]  # (C,nen,3)
         J = np.einsum("cai,qaj->cqij", X, self.shape_grads_ref)
         jxw = np.linalg.det(J) * self.quad_weights[None]
         xq = np.einsum("qa,cai->cqi", self.shape_vals, X).reshape(-1, 3)
         self._check_u_independent(mass_map, xq)
         u0 = np.zeros((len(xq), self.vec))
-        val = _batched_or_pointwise(mass_map, (u0, xq), (self.vec,)).reshape(self.num_cells, 8, self.vec)
+        val = _batched_or_pointwise(mass_map, (u0, xq), (self.vec,)).reshape(self.num_cells, self.num_quads,
+                                                                             self.vec)
         r = np.einsum("cqi,qa,cq->cai", val, self.shape_vals, jxw)
         f = np.zeros((self.num_total_nodes, self.vec))
         np.add.at(f, self.cells.reshape(-1), r.reshape(-1, self.vec))
@@ -331,12 +288,13 @@ class FiniteElement:
         if len(binds) == 0:
             return f.reshape(-1)
         _, scale = self.get_face_shape_grads(binds)
-        fv = self.face_shape_vals_at(binds[:, 1])  # (F,4,8)
+        fv = self.face_shape_vals_at(binds[:, 1])  # (F,fq,nen)
         X = self.points[self.cells[binds[:, 0]]]
         xq = np.einsum("fqa,fai->fqi", fv, X).reshape(-1, 3)
         self._check_u_independent(surface_map, xq)
         u0 = np.zeros((len(xq), self.vec))
-        val = _batched_or_pointwise(surface_map, (u0, xq), (self.vec,)).reshape(len(binds), 4, self.vec)
+        val = _batched_or_pointwise(surface_map, (u0, xq), (self.vec,)).reshape(len(binds), self.num_face_quads,
+                                                                                self.vec)
         r = np.einsum("fqi,fqa,fq->fai", val, fv, scale)
         np.add.at(f, self.cells[binds[:, 0]].reshape(-1), r.reshape(-1, self.vec))
         return f.reshape(-1)

@@ -1,22 +1,41 @@
-"""Mesh container and structured HEX8 box generator.
+"""Mesh container and structured box generators.
 
 Mirrors ``Mesh`` (generate_mesh.py:13-27 in the reference) and ``box_mesh``
 (generate_mesh.py:151-189): node (i, j, k) of an (Nx+1, Ny+1, Nz+1) grid has
 index (i*(Ny+1) + j)*(Nz+1) + k and cells list their nodes in VTK HEX8 order,
 so meshes, solutions and per-cell data line up with the reference's.
+
+``box_mesh_gmsh`` (generate_mesh.py:192-260) meshes the same box with gmsh,
+which is not available here; this version builds the structured mesh of
+the requested element type directly: HEX8 as ``box_mesh``, TET4 by
+splitting every hexahedron into the six tetrahedra around its (0,0,0)-(1,1,1)
+diagonal (a conforming split, every tetrahedron positively oriented), and
+the quadratic types by adding one node per edge (TET10, HEX20, HEX27), per
+face and per cell (HEX27), in VTK node order.  Corner nodes keep the
+numbering of ``box_mesh``; added nodes follow them.
 """
 import numpy as np
 
+from .basis import HEX_EDGES, HEX_FACE_CORNERS, MESHIO_CELL_TYPE, NODES_PER_CELL, TET_EDGES, check_ele_type
+
+_ELE_OF_NEN = {n: e for e, n in NODES_PER_CELL.items()}
+
 
 class Mesh:
-    """points (num_nodes, dim) float64 and cells (num_cells, 8) int32."""
+    """points (num_nodes, dim) float64 and cells (num_cells, nen) int32.
 
-    def __init__(self, points, cells, ele_type="HEX8"):
+    ``ele_type`` defaults to the element type with ``nen`` nodes."""
+
+    def __init__(self, points, cells, ele_type=None):
         self.points = np.ascontiguousarray(np.asarray(points, dtype=np.float64))
         self.cells = np.ascontiguousarray(np.asarray(cells, dtype=np.int32))
-        self.ele_type = ele_type
-        if self.cells.ndim != 2 or self.cells.shape[1] != 8:
-            raise NotImplementedError("only HEX8 meshes (cells of 8 nodes) are supported")
+        if self.cells.ndim != 2 or self.cells.shape[1] not in _ELE_OF_NEN:
+            raise NotImplementedError("cells must be (num_cells, nen) with nen in 4, 8, 10, 20, 27 "
+                                      "(TET4, HEX8, TET10, HEX20, HEX27)")
+        self.ele_type = _ELE_OF_NEN[self.cells.shape[1]] if ele_type is None else check_ele_type(ele_type)
+        if NODES_PER_CELL[self.ele_type] != self.cells.shape[1]:
+            raise ValueError(f"{self.ele_type} cells have {NODES_PER_CELL[self.ele_type]} nodes, "
+                             f"got {self.cells.shape[1]}")
 
 
 class _BoxMesh:
@@ -43,6 +62,69 @@ def box_mesh(Nx, Ny, Nz, domain_x, domain_y, domain_z):
 
 
 def get_meshio_cell_type(ele_type):
-    if ele_type != "HEX8":
-        raise NotImplementedError(f"element {ele_type} is not supported (HEX8 only)")
-    return "hexahedron"
+    """meshio cell type of an element type (generate_mesh.py:83-117)."""
+    return MESHIO_CELL_TYPE[check_ele_type(ele_type)]
+
+
+# Six tetrahedra of a hexahedron around its corner-0 -> corner-6 diagonal:
+# one per order of the axes along the path (0,0,0) -> (1,1,1).  VTK corner of
+# each (x, y, z) bit triple.
+_CORNER_OF_BITS = {(0, 0, 0): 0, (1, 0, 0): 1, (1, 1, 0): 2, (0, 1, 0): 3,
+                   (0, 0, 1): 4, (1, 0, 1): 5, (1, 1, 1): 6, (0, 1, 1): 7}
+
+
+def _kuhn_tets():
+    tets = []
+    for order in ((0, 1, 2), (0, 2, 1), (1, 0, 2), (1, 2, 0), (2, 0, 1), (2, 1, 0)):
+        b = [0, 0, 0]
+        path = [_CORNER_OF_BITS[tuple(b)]]
+        for ax in order:
+            b[ax] = 1
+            path.append(_CORNER_OF_BITS[tuple(b)])
+        tets.append(path)
+    return np.array(tets)
+
+
+def _add_entity_nodes(points, cells, groups):
+    """One new node per distinct corner set (rows of ``groups``: (C, k, m)
+    corner numbers per cell), at the mean of its corners; returns points and
+    the (C, k) new node numbers."""
+    C, k, m = groups.shape
+    keys = np.sort(groups.reshape(-1, m), axis=1)
+    uniq, inv = np.unique(keys, axis=0, return_inverse=True)
+    new = points[uniq].mean(axis=1)
+    return np.vstack([points, new]), (len(points) + inv.reshape(C, k)).astype(np.int32)
+
+
+def box_mesh_gmsh(Nx, Ny, Nz, domain_x, domain_y, domain_z, data_dir=None, ele_type="HEX8"):
+    """Structured mesh of [0,Lx]x[0,Ly]x[0,Lz] with Nx*Ny*Nz hexahedral
+    blocks in the given element type (see the module docstring); returns a
+    meshio-like object with ``points`` and ``cells_dict[cell_type]``.
+    ``data_dir`` is accepted for the reference's signature; nothing is
+    written."""
+    check_ele_type(ele_type)
+    hexmesh = box_mesh(Nx, Ny, Nz, domain_x, domain_y, domain_z)
+    points, hexes = hexmesh.points, hexmesh.cells_dict["hexahedron"]
+    if ele_type.startswith("TET"):
+        tets = hexes[:, _kuhn_tets()].reshape(-1, 4)
+        X = points[tets]
+        vol = np.einsum("ci,ci->c", np.cross(X[:, 1] - X[:, 0], X[:, 2] - X[:, 0]), X[:, 3] - X[:, 0])
+        flip = vol < 0
+        tets[flip] = tets[flip][:, [0, 2, 1, 3]]
+        cells = tets
+        if ele_type == "TET10":
+            points, mid = _add_entity_nodes(points, tets, tets[:, TET_EDGES])
+            cells = np.hstack([tets, mid])
+    else:
+        cells = hexes
+        if ele_type in ("HEX20", "HEX27"):
+            points, mid = _add_entity_nodes(points, hexes, hexes[:, HEX_EDGES])
+            cells = np.hstack([hexes, mid])
+        if ele_type == "HEX27":
+            points, fc = _add_entity_nodes(points, hexes, hexes[:, HEX_FACE_CORNERS])
+            centre = (len(points) + np.arange(len(hexes), dtype=np.int32))[:, None]
+            points = np.vstack([points, points[hexes].mean(axis=1)])
+            cells = np.hstack([cells, fc, centre])
+    out = _BoxMesh(np.ascontiguousarray(points), np.ascontiguousarray(cells, dtype=np.int32))
+    out.cells_dict = {get_meshio_cell_type(ele_type): out.cells_dict.pop("hexahedron")}
+    return out

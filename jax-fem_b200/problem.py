@@ -62,21 +62,22 @@ class DeviceMesh:
     def __init__(self, mesh, vec, device):
         cells = np.ascontiguousarray(mesh.cells, dtype=np.int32)
         C, N = cells.shape[0], mesh.points.shape[0]
+        nen = cells.shape[1]
         lib = nat.lib()
         row_ptr = np.zeros(N + 1, dtype=np.int32)
         nnzb = nat.I64(0)
-        nat.check(lib.fem_bsr_pattern(cells.ctypes.data, C, N, row_ptr.ctypes.data, nnzb, None, 0,
-                                      None, None), "bsr_pattern(count)")
+        nat.check(lib.fem_bsr_pattern_nen(cells.ctypes.data, C, nen, N, row_ptr.ctypes.data, nnzb, None, 0,
+                                          None, None), "bsr_pattern(count)")
         col = np.zeros(max(1, nnzb.value), dtype=np.int32)
-        scatter = np.zeros((max(1, C), 64), dtype=np.int32)
+        scatter = np.zeros((max(1, C), nen * nen), dtype=np.int32)
         diag = np.zeros(max(1, N), dtype=np.int32)
-        nat.check(lib.fem_bsr_pattern(cells.ctypes.data, C, N, row_ptr.ctypes.data, nnzb,
-                                      col.ctypes.data, col.size, scatter.ctypes.data, diag.ctypes.data),
+        nat.check(lib.fem_bsr_pattern_nen(cells.ctypes.data, C, nen, N, row_ptr.ctypes.data, nnzb,
+                                          col.ctypes.data, col.size, scatter.ctypes.data, diag.ctypes.data),
                   "bsr_pattern(fill)")
         tmap = np.zeros(max(1, nnzb.value), dtype=np.int32)
         nat.check(lib.fem_bsr_transpose_map(row_ptr.ctypes.data, col.ctypes.data, N, tmap.ctypes.data),
                   "bsr_transpose_map")
-        self.vec, self.num_cells, self.num_nodes, self.nnzb = vec, C, N, int(nnzb.value)
+        self.vec, self.num_cells, self.num_nodes, self.nnzb, self.nen = vec, C, N, int(nnzb.value), nen
         self.ndofs = N * vec
         self.device = device
         self.points = torch.from_numpy(np.ascontiguousarray(mesh.points, dtype=np.float64)).to(device)
@@ -100,7 +101,8 @@ def _to_dev(x, device, dtype=torch.float64):
 
 @dataclass
 class Problem:
-    """One HEX8 field; see the module docstring.  Fields as the reference's."""
+    """One field on a mesh of one 3D element type; see the module docstring.
+    Fields as the reference's."""
     mesh: Mesh
     vec: int
     dim: int
@@ -123,7 +125,7 @@ class Problem:
                     and len(self.dirichlet_bc_info[0]) == 3 and isinstance(self.dirichlet_bc_info[0][0], list)):
                 self.dirichlet_bc_info = self.dirichlet_bc_info[0]
         if not isinstance(self.mesh, Mesh):
-            self.mesh = Mesh(self.mesh.points, self.mesh.cells)
+            self.mesh = Mesh(self.mesh.points, self.mesh.cells, self.ele_type)
         self.fes = [FiniteElement(mesh=self.mesh, vec=self.vec, dim=self.dim, ele_type=self.ele_type,
                                   quadrature_rule=self.quadrature_rule,
                                   quadrature_order=self.quadrature_order,
@@ -137,6 +139,7 @@ class Problem:
         self.internal_vars = ()
         self.internal_vars_surfaces = [() for _ in range(len(self.boundary_inds_list))]
         self._dev = None
+        self._elem = None
         self._bc_cache = None
         self._fext = None
         self._law = None
@@ -173,6 +176,22 @@ class Problem:
             nat.load()
             self._dev = DeviceMesh(self.mesh, self.vec, self.device())
         return self._dev
+
+    @property
+    def hex8_kernel(self):
+        """True when cells go through the HEX8 kernel (HEX8 with its default
+        2x2x2 rule); other element types and rules use the general one."""
+        fe = self.fes[0]
+        return fe.ele_type == "HEX8" and fe.num_quads == 8 and fe.quadrature_order == 2
+
+    def element_tables(self):
+        """(reference shape gradients (nq, nen, 3), weights (nq,)) on the device."""
+        if self._elem is None:
+            fe = self.fes[0]
+            d = self.dev().device
+            self._elem = (torch.from_numpy(np.ascontiguousarray(fe.shape_grads_ref, dtype=np.float64)).to(d),
+                          torch.from_numpy(np.ascontiguousarray(fe.quad_weights, dtype=np.float64)).to(d))
+        return self._elem
 
     def unflatten_fn_sol_list(self, dofs):
         return [dofs.reshape(-1, self.vec)]
@@ -211,32 +230,33 @@ class Problem:
         return self._fext
 
     def law_ivars(self, ivars=None):
-        """Device pointers (iv0, iv1, iv2) of the law's internal variables."""
+        """Device tensors (iv0, iv1, iv2) of the law's internal variables,
+        per (cell, quadrature point)."""
         ivars = self.internal_vars if ivars is None else ivars
         law = self.law
         d = self.dev().device
-        C = self.num_cells
+        C, Q = self.num_cells, self.fes[0].num_quads
         if isinstance(law, SIMPElastic):
             if len(ivars) < 1:
                 raise ValueError("SIMPElastic needs internal_vars = [theta] (set_params)")
             th = _to_dev(ivars[0], d)
             if th.numel() == C:
-                th = th.reshape(C, 1).expand(C, 8).contiguous()
-            return (th.reshape(C, 8), None, None)
+                th = th.reshape(C, 1).expand(C, Q).contiguous()
+            return (th.reshape(C, Q), None, None)
         if isinstance(law, NeoHookean):
             if len(ivars) == 0:
                 return (None, None, None)
             sc = _to_dev(ivars[0], d)
             if sc.numel() == C:
-                sc = sc.reshape(C, 1).expand(C, 8).contiguous()
-            return (sc.reshape(C, 8), None, None)
+                sc = sc.reshape(C, 1).expand(C, Q).contiguous()
+            return (sc.reshape(C, Q), None, None)
         if isinstance(law, J2Plasticity):
             if len(ivars) < 2:
                 raise ValueError("J2Plasticity needs internal_vars = [sigma_old, eps_old(, alpha_old)]")
-            so = _to_dev(ivars[0], d).reshape(C, 8, 9)
-            eo = _to_dev(ivars[1], d).reshape(C, 8, 9)
-            ao = _to_dev(ivars[2], d).reshape(C, 8) if len(ivars) > 2 else torch.zeros(
-                C, 8, dtype=torch.float64, device=d)
+            so = _to_dev(ivars[0], d).reshape(C, Q, 9)
+            eo = _to_dev(ivars[1], d).reshape(C, Q, 9)
+            ao = _to_dev(ivars[2], d).reshape(C, Q) if len(ivars) > 2 else torch.zeros(
+                C, Q, dtype=torch.float64, device=d)
             return (so, eo, ao)
         return (None, None, None)
 
@@ -249,12 +269,18 @@ class Problem:
         mask, _ = self.dirichlet_device() if bc else (None, None)
         iv = self.law_ivars(ivars)
         pr, n = nat.params_array(law.params())
-        fn = nat.lib().fem_assemble_f32 if fp32 else nat.lib().fem_assemble_f64
-        nat.check(fn(law.law_id, pr, n, self.vec, dv.num_cells, dv.num_nodes, nat.ptr(dv.cells),
-                     nat.ptr(dv.points), nat.ptr(dofs), nat.ptr(iv[0]), nat.ptr(iv[1]), nat.ptr(iv[2]),
-                     nat.ptr(dv.scatter), nat.ptr(dv.diag), nat.ptr(dv.transpose), dv.nnzb,
-                     nat.ptr(mask) if bc else None, nat.ptr(dvec), nat.ptr(res), nat.ptr(lift),
-                     nat.ptr(vals), nat.stream_ptr()), "assemble")
+        tail = (dv.num_cells, dv.num_nodes, nat.ptr(dv.cells), nat.ptr(dv.points), nat.ptr(dofs), nat.ptr(iv[0]),
+                nat.ptr(iv[1]), nat.ptr(iv[2]), nat.ptr(dv.scatter), nat.ptr(dv.diag), nat.ptr(dv.transpose),
+                dv.nnzb, nat.ptr(mask) if bc else None, nat.ptr(dvec), nat.ptr(res), nat.ptr(lift),
+                nat.ptr(vals), nat.stream_ptr())
+        if self.hex8_kernel:
+            fn = nat.lib().fem_assemble_f32 if fp32 else nat.lib().fem_assemble_f64
+            nat.check(fn(law.law_id, pr, n, self.vec, *tail), "assemble")
+        else:
+            gref, wq = self.element_tables()
+            fn = nat.lib().fem_assemble_elem_f32 if fp32 else nat.lib().fem_assemble_elem_f64
+            nat.check(fn(law.law_id, pr, n, self.vec, dv.nen, wq.numel(), nat.ptr(gref), nat.ptr(wq), *tail),
+                      "assemble_elem")
 
     def _flat_dofs(self, sol_list):
         s = sol_list[0] if isinstance(sol_list, (list, tuple)) else sol_list
@@ -287,12 +313,16 @@ class Problem:
         sn, en, an = torch.empty_like(so), torch.empty_like(eo), torch.empty_like(ao)
         dofs = self._flat_dofs(sol)
         pr, n = nat.params_array(law.params())
-        nat.check(nat.lib().fem_j2_commit(pr, n, dv.num_cells, nat.ptr(dv.cells), nat.ptr(dv.points),
-                                          nat.ptr(dofs), nat.ptr(so), nat.ptr(eo), nat.ptr(ao),
-                                          nat.ptr(sn), nat.ptr(en), nat.ptr(an), nat.stream_ptr()),
-                  "j2_commit")
-        C = self.num_cells
-        self.internal_vars = [sn.reshape(C, 8, 3, 3), en.reshape(C, 8, 3, 3), an]
+        state = (nat.ptr(dv.cells), nat.ptr(dv.points), nat.ptr(dofs), nat.ptr(so), nat.ptr(eo), nat.ptr(ao),
+                 nat.ptr(sn), nat.ptr(en), nat.ptr(an), nat.stream_ptr())
+        if self.hex8_kernel:
+            nat.check(nat.lib().fem_j2_commit(pr, n, dv.num_cells, *state), "j2_commit")
+        else:
+            gref, wq = self.element_tables()
+            nat.check(nat.lib().fem_j2_commit_elem(pr, n, dv.nen, wq.numel(), nat.ptr(gref), dv.num_cells, *state),
+                      "j2_commit_elem")
+        C, Q = self.num_cells, self.fes[0].num_quads
+        self.internal_vars = [sn.reshape(C, Q, 3, 3), en.reshape(C, Q, 3, 3), an]
         return self.internal_vars
 
     def JxW(self):

@@ -1,4 +1,5 @@
-"""FP64 numpy restatement of the reference's HEX8 assemble-and-solve path.
+"""FP64 numpy restatement of the reference's assemble-and-solve path (HEX8,
+and the TET4, TET10, HEX20 and HEX27 element types).
 
 TEST INFRASTRUCTURE ONLY: the parity checker and the CPU baseline.  The
 product (``jax-fem_b200``) never imports this module.
@@ -97,6 +98,162 @@ def hex8_face_tables(quadrature_order=2):
     nf, nq = fpts.shape[:2]
     return (vals.reshape(nf, nq, 8), grads.reshape(nf, nq, 8, 3), np.stack(fw),
             BASIX_HEX_NORMALS.copy(), np.array(finds))
+
+
+# --------------------------------------------------------------------------
+# Other element types (basis.py:19-114): TET4, TET10, HEX20, HEX27
+# --------------------------------------------------------------------------
+# Restated from basix's element definitions in basix numbering, then moved
+# to mesh order with the reference's re_order tables, the way
+# get_shape_vals_and_grads does (basis.py:168-173).  Each element is the
+# dual basis of its degrees of freedom in its polynomial space, computed by
+# inverting the functionals applied to a monomial basis:
+#   P1/P2 on the tetrahedron, Q2 on the hexahedron: point values at the
+#   vertices, edge midpoints, face centres and cell centre (basix's dof
+#   entity order: vertices, edges, faces, interior);
+#   serendipity degree 2 on the hexahedron: vertex values and edge means
+#   (moments against the degree-0 DPC space on each edge).
+BASIX_TET_VERTICES = np.array([[0, 0, 0], [1, 0, 0], [0, 1, 0], [0, 0, 1]], dtype=np.float64)
+BASIX_TET_EDGES = np.array([[2, 3], [1, 3], [1, 2], [0, 3], [0, 2], [0, 1]])
+BASIX_TET_FACETS = np.array([[1, 2, 3], [0, 2, 3], [0, 1, 3], [0, 1, 2]])
+BASIX_TET_NORMALS = np.array([[1, 1, 1], [-1, 0, 0], [0, -1, 0], [0, 0, -1]], dtype=np.float64)
+BASIX_TET_NORMALS[0] /= np.sqrt(3.0)
+BASIX_HEX_EDGES = np.array([[0, 1], [0, 2], [0, 4], [1, 3], [1, 5], [2, 3], [2, 6], [3, 7],
+                            [4, 5], [4, 6], [5, 7], [6, 7]])
+# re_order of basis.py:53-76 (mesh position -> basix dof)
+RE_ORDER = {
+    "HEX8": [0, 1, 3, 2, 4, 5, 7, 6],
+    "HEX27": [0, 1, 3, 2, 4, 5, 7, 6, 8, 11, 13, 9, 16, 18, 19, 17, 10, 12, 15, 14, 22, 23, 21, 24, 20, 25, 26],
+    "HEX20": [0, 1, 3, 2, 4, 5, 7, 6, 8, 11, 13, 9, 16, 18, 19, 17, 10, 12, 15, 14],
+    "TET4": [0, 1, 2, 3],
+    "TET10": [0, 1, 2, 3, 9, 6, 8, 7, 5, 4],
+}
+DEFAULT_QUADRATURE_ORDER = {"HEX8": 2, "HEX27": 10, "HEX20": 2, "TET4": 0, "TET10": 2}
+
+
+def _monomial_table(pts, exps):
+    """Values (n, m) and gradients (n, m, 3) of monomials x^e at points."""
+    pts = np.atleast_2d(pts)
+    n, m = len(pts), len(exps)
+    vals = np.ones((n, m))
+    grads = np.zeros((n, m, 3))
+    for k, e in enumerate(exps):
+        vals[:, k] = np.prod([pts[:, d] ** e[d] for d in range(3)], axis=0)
+        for d in range(3):
+            if e[d] == 0:
+                continue
+            g = e[d] * pts[:, d] ** (e[d] - 1)
+            for o in range(3):
+                if o != d:
+                    g = g * pts[:, o] ** e[o]
+            grads[:, k, d] = g
+    return vals, grads
+
+
+def _element_space(ele_type):
+    """Monomial exponents of the element's polynomial space."""
+    if ele_type == "TET4":
+        return [e for e in np.ndindex(2, 2, 2) if sum(e) <= 1]
+    if ele_type == "TET10":
+        return [e for e in np.ndindex(3, 3, 3) if sum(e) <= 2]
+    if ele_type == "HEX27":
+        return list(np.ndindex(3, 3, 3))
+    if ele_type == "HEX20":  # superlinear degree (degree minus linearly entering variables) <= 2
+        return [e for e in np.ndindex(4, 4, 4) if sum(e) - sum(x == 1 for x in e) <= 2]
+    raise ValueError(ele_type)
+
+
+def _basix_dof_functionals(ele_type):
+    """The element's dofs in basix order, each (points, weights): a point
+    value is one point with weight 1; an edge mean is a Gauss rule on the edge."""
+    tet = ele_type.startswith("TET")
+    V = BASIX_TET_VERTICES if tet else BASIX_HEX_VERTICES
+    E = BASIX_TET_EDGES if tet else BASIX_HEX_EDGES
+    dofs = [(V[i][None], np.ones(1)) for i in range(len(V))]
+    if ele_type in ("TET10", "HEX27"):
+        dofs += [(0.5 * (V[a] + V[b])[None], np.ones(1)) for a, b in E]
+    if ele_type == "HEX20":
+        t, w = gauss_jacobi_01(3)
+        dofs += [(V[a][None] + t[:, None] * (V[b] - V[a])[None], w) for a, b in E]
+    if ele_type == "HEX27":
+        dofs += [(V[f].mean(axis=0)[None], np.ones(1)) for f in BASIX_HEX_FACETS]
+        dofs += [(np.full((1, 3), 0.5), np.ones(1))]
+    return dofs
+
+
+def element_shape(ele_type, xi):
+    """vals (n, nen), grads (n, nen, 3) in mesh node order at points xi."""
+    if ele_type == "HEX8":
+        return hex8_shape(xi)
+    exps = _element_space(ele_type)
+    dofs = _basix_dof_functionals(ele_type)
+    assert len(exps) == len(dofs), (ele_type, len(exps), len(dofs))
+    L = np.array([w @ _monomial_table(p, exps)[0] for p, w in dofs])  # (dof, monomial)
+    C = np.linalg.inv(L)  # column k: coefficients of basis function k
+    v, g = _monomial_table(xi, exps)
+    vals, grads = v @ C, np.einsum("nmd,mk->nkd", g, C)
+    ro = RE_ORDER[ele_type]
+    return vals[:, ro], grads[:, ro]
+
+
+def simplex_quadrature(dim, order):
+    """basix default (Xiao-Gimbutas) rules of orders 0-2 on the reference
+    triangle / tetrahedron."""
+    if dim == 3:
+        if order <= 1:
+            return np.array([[0.25, 0.25, 0.25]]), np.array([1.0 / 6.0])
+        a = 0.1381966011250105
+        b = 1.0 - 3.0 * a
+        return np.array([[a, a, a], [b, a, a], [a, b, a], [a, a, b]]), np.full(4, 1.0 / 24.0)
+    if order <= 1:
+        return np.array([[1.0 / 3.0, 1.0 / 3.0]]), np.array([0.5])
+    return np.array([[1 / 6, 1 / 6], [2 / 3, 1 / 6], [1 / 6, 2 / 3]]), np.full(3, 1.0 / 6.0)
+
+
+def element_tables(ele_type, quadrature_order=None):
+    """shape_vals (Q,nen), shape_grads_ref (Q,nen,3), weights (Q,) (basis.py:141-175)."""
+    order = DEFAULT_QUADRATURE_ORDER[ele_type] if quadrature_order is None else quadrature_order
+    if ele_type.startswith("TET"):
+        pts, wts = simplex_quadrature(3, order)
+    else:
+        m = (order + 2) // 2
+        p, w = gauss_jacobi_01(m)
+        pts = np.array([[a, b, c] for a in p for b in p for c in p])
+        wts = np.array([wa * wb * wc for wa in w for wb in w for wc in w])
+    vals, grads = element_shape(ele_type, pts)
+    return vals, grads, wts
+
+
+def element_face_tables(ele_type, quadrature_order=None):
+    """Face tables (basis.py:178-250) for any element type: vals (nf,F,nen),
+    grads (nf,F,nen,3), weights (nf,F), normals (nf,3), face_inds (nf,nfv)."""
+    order = DEFAULT_QUADRATURE_ORDER[ele_type] if quadrature_order is None else quadrature_order
+    if ele_type.startswith("TET"):
+        qp, qw = simplex_quadrature(2, order)
+        s, t = qp[:, 0], qp[:, 1]
+        lag = np.stack([1 - s - t, s, t], axis=1)
+        V, facets, normals = BASIX_TET_VERTICES, BASIX_TET_FACETS, BASIX_TET_NORMALS
+    else:
+        m = (order + 2) // 2
+        p, w = gauss_jacobi_01(m)
+        qp = np.array([[a, b] for a in p for b in p])
+        qw = np.array([wa * wb for wa in w for wb in w])
+        s, t = qp[:, 0], qp[:, 1]
+        lag = np.stack([(1 - s) * (1 - t), s * (1 - t), (1 - s) * t, s * t], axis=1)
+        V, facets, normals = BASIX_HEX_VERTICES, BASIX_HEX_FACETS, BASIX_HEX_NORMALS
+    ro = np.array(RE_ORDER[ele_type])
+    fpts, fw, finds = [], [], []
+    for facet in facets:
+        v = V[facet]
+        fpts.append(lag @ v)
+        fw.append(qw * np.linalg.norm(np.cross(v[1] - v[0], v[2] - v[0])))
+        finds.append([int(np.argwhere(ro == i)[0, 0]) for i in facet])
+    fpts = np.stack(fpts)
+    nf, nq = fpts.shape[:2]
+    vals, grads = element_shape(ele_type, fpts.reshape(-1, 3))
+    nen = vals.shape[1]
+    return (vals.reshape(nf, nq, nen), grads.reshape(nf, nq, nen, 3), np.stack(fw), normals.copy(),
+            np.array(finds))
 
 
 # --------------------------------------------------------------------------
@@ -347,15 +504,23 @@ class OracleProblem:
     """
 
     def __init__(self, points, cells, vec, law, dirichlet_bc_info=None, location_fns=None,
-                 mass_map=None, surface_maps=None, internal_vars=()):
+                 mass_map=None, surface_maps=None, internal_vars=(), ele_type="HEX8", quadrature_order=None):
         self.points = np.asarray(points, dtype=np.float64)
         self.cells = np.asarray(cells, dtype=np.int64)
         self.vec, self.law = vec, law
+        self.ele_type = ele_type
         self.num_cells, self.num_nodes = len(self.cells), len(self.points)
         self.ndofs = self.num_nodes * vec
-        self.vals, self.grads_ref, self.weights = hex8_tables()
-        (self.fvals, self.fgrads_ref, self.fweights, self.normals,
-         self.face_inds) = hex8_face_tables()
+        if ele_type == "HEX8" and quadrature_order in (None, 2):
+            self.vals, self.grads_ref, self.weights = hex8_tables()
+            (self.fvals, self.fgrads_ref, self.fweights, self.normals,
+             self.face_inds) = hex8_face_tables()
+        else:
+            self.vals, self.grads_ref, self.weights = element_tables(ele_type, quadrature_order)
+            (self.fvals, self.fgrads_ref, self.fweights, self.normals,
+             self.face_inds) = element_face_tables(ele_type, quadrature_order)
+        self.nen = self.vals.shape[1]
+        self.num_quads = self.vals.shape[0]
         self.shape_grads, self.JxW = shape_grads(self.points, self.cells, self.grads_ref, self.weights)
         self.quad_points = physical_quad_points(self.points, self.cells, self.vals)
         self.bc_info = dirichlet_bc_info
@@ -388,9 +553,9 @@ class OracleProblem:
         return np.einsum("cqij,cqaj,cq->cai", P, self.shape_grads, self.JxW)
 
     def cell_residual_and_jacobian(self, cell_u, ivars, h=1e-30):
-        """Residual (C,8*vec) and Jacobian (C,8*vec,8*vec) via forward
+        """Residual (C,nen*vec) and Jacobian (C,nen*vec,nen*vec) via forward
         directional derivatives along each cell dof (problem.py:262-266,299-301)."""
-        C, n = self.num_cells, 8 * self.vec
+        C, n = self.num_cells, self.nen * self.vec
         r = self.cell_residual(cell_u, ivars).reshape(C, n)
         jac = np.empty((C, n, n))
         base = cell_u.reshape(C, n).astype(np.complex128)
@@ -398,7 +563,7 @@ class OracleProblem:
         for d in range(n):
             up = base.copy()
             up[:, d] += 1j * h
-            jac[:, :, d] = np.imag(self.cell_residual(up.reshape(C, 8, self.vec), civars).reshape(C, n)) / h
+            jac[:, :, d] = np.imag(self.cell_residual(up.reshape(C, self.nen, self.vec), civars).reshape(C, n)) / h
         return r, jac
 
     def body_load(self):
@@ -408,7 +573,7 @@ class OracleProblem:
             return f.reshape(-1)
         x = self.quad_points.reshape(-1, 3)
         u0 = np.zeros((len(x), self.vec))
-        val = eval_pointwise(self.mass_map, u0, x).reshape(self.num_cells, 8, self.vec)
+        val = eval_pointwise(self.mass_map, u0, x).reshape(self.num_cells, self.num_quads, self.vec)
         r = np.einsum("cqi,qa,cq->cai", val, self.vals, self.JxW)
         np.add.at(f, self.cells.reshape(-1), r.reshape(-1, self.vec))
         return f.reshape(-1)

@@ -16,28 +16,29 @@ def perturbed_box(pkg, N, L=(1.0, 1.0, 1.0), amp=0.15, seed=0):
     return pkg.Mesh(pts, m.cells_dict["hexahedron"])
 
 
-def law_pair(pkg, kind, C, rng):
-    """(product law, oracle law, product ivars, oracle ivars) for a law kind."""
+def law_pair(pkg, kind, C, rng, Q=8):
+    """(product law, oracle law, product ivars, oracle ivars) for a law kind;
+    internal variables per (cell, quadrature point), Q points per cell."""
     if kind == "laplace":
         return pkg.Laplace(), fo.Law("laplace", vec=3), [], []
     if kind == "linear":
         return pkg.LinearElastic(70e3, 0.3), fo.Law("linear", E=70e3, nu=0.3), [], []
     if kind == "simp":
-        th = rng.uniform(0.05, 1.0, size=(C, 8))
+        th = rng.uniform(0.05, 1.0, size=(C, Q))
         return (pkg.SIMPElastic(70e3, 70.0, 0.3, 3.0), fo.Law("simp", E0=70e3, Emin=70.0, nu=0.3, penal=3.0),
                 [th], [th])
     if kind == "neo_hookean":
         return pkg.NeoHookean(10.0, 0.3), fo.Law("neo_hookean", E=10.0, nu=0.3), [], []
     if kind == "neo_hookean_scaled":
-        s = rng.uniform(0.5, 1.5, size=(C, 8))
+        s = rng.uniform(0.5, 1.5, size=(C, Q))
         return pkg.NeoHookean(10.0, 0.3), fo.Law("neo_hookean", E=10.0, nu=0.3), [s], [s]
     if kind == "j2":
         # a history with some points yielded: random prior stress / strain
-        so = rng.normal(0, 150.0, size=(C, 8, 3, 3))
+        so = rng.normal(0, 150.0, size=(C, Q, 3, 3))
         so = 0.5 * (so + np.swapaxes(so, -1, -2))
-        eo = rng.normal(0, 2e-3, size=(C, 8, 3, 3))
+        eo = rng.normal(0, 2e-3, size=(C, Q, 3, 3))
         eo = 0.5 * (eo + np.swapaxes(eo, -1, -2))
-        ao = rng.uniform(0, 0.01, size=(C, 8))
+        ao = rng.uniform(0, 0.01, size=(C, Q))
         return (pkg.J2Plasticity(70e3, 0.3, 250.0, 700.0), fo.Law("j2", E=70e3, nu=0.3, sig0=250.0, H=700.0),
                 [so, eo, ao], [so, eo, ao])
     raise ValueError(kind)
@@ -56,6 +57,74 @@ def make_problem(pkg, mesh, law, vec=3, bc=None, location_fns=None, ivars=(), ma
     p = P(mesh, vec=vec, dim=3, dirichlet_bc_info=bc, location_fns=location_fns)
     p.internal_vars = list(ivars)
     return p
+
+
+def element_box(pkg, ele_type, N, L=(1.0, 1.0, 1.0), amp=0.0, seed=0):
+    """Structured box mesh of one element type; with amp > 0 every node off
+    the boundary moves by up to amp * h (curved, general cells)."""
+    import importlib
+    gm = importlib.import_module("jax_fem_b200.generate_mesh")
+    m = gm.box_mesh_gmsh(N[0], N[1], N[2], *L, None, ele_type)
+    pts = m.points.copy()
+    if amp > 0:
+        rng = np.random.default_rng(seed)
+        h = np.array(L) / np.array(N)
+        inner = np.all((pts > 1e-9) & (pts < np.array(L) - 1e-9), axis=1)
+        pts[inner] += amp * h * rng.uniform(-1, 1, size=(inner.sum(), 3))
+    return pkg.Mesh(pts, m.cells_dict[gm.get_meshio_cell_type(ele_type)], ele_type)
+
+
+def face_fn(axis, value):
+    """Location function of the plane x[axis] = value."""
+    return lambda p: np.isclose(p[axis], value, atol=1e-5)
+
+
+# Manufactured Poisson solution of the reference's convergence-rate study
+# (applications/convergence_rate/example.py:56-61): -lap u = -f with
+# f = lap u_true as the mass map and u = u_true on the six faces.
+def mms_u(p):
+    x, y, z = p[..., 0], p[..., 1], p[..., 2]
+    return 1e2 * ((x - 0.5) ** 3 + 2.0 * (y - 0.5) ** 3 + 1e1 * np.exp(-(z - 0.5) ** 2))
+
+
+def mms_grad(p):
+    x, y, z = p[..., 0], p[..., 1], p[..., 2]
+    return 1e2 * np.stack([3.0 * (x - 0.5) ** 2, 6.0 * (y - 0.5) ** 2,
+                           -2e1 * (z - 0.5) * np.exp(-(z - 0.5) ** 2)], axis=-1)
+
+
+def mms_lap(p):
+    x, y, z = p[..., 0], p[..., 1], p[..., 2]
+    s = z - 0.5
+    return 1e2 * (6.0 * (x - 0.5) + 12.0 * (y - 0.5) + 1e1 * (4.0 * s * s - 2.0) * np.exp(-s * s))
+
+
+def mms_bc():
+    """Dirichlet data of the study; the value function takes one point, or
+    the coordinate arrays (p[0] = all x) in a batched call."""
+    faces = [face_fn(a, v) for a in range(3) for v in (0.0, 1.0)]
+    return [faces, [0] * 6, [lambda p: mms_u(np.stack([p[0], p[1], p[2]], axis=-1))] * 6]
+
+
+def mms_mass_map(u, x):
+    """mass_map of the study: lap u_true at x (one point or coordinate arrays)."""
+    return np.array([mms_lap(np.stack([x[0], x[1], x[2]], axis=-1))])
+
+
+def mms_errors(points, cells, vals, grads_ref, weights, sol):
+    """L2 and H1 errors of sol against the manufactured solution, with the
+    element's own quadrature, as compute_l2_norm_error / compute_h1_norm_error
+    of the study (example.py:21-49; H1 = L2 of u plus L2 of grad u)."""
+    X = points[cells]
+    J = np.einsum("cai,qaj->cqij", X, grads_ref)
+    jxw = np.linalg.det(J) * weights[None]
+    g = np.einsum("qaj,cqjk->cqak", grads_ref, np.linalg.inv(J))
+    cu = np.asarray(sol).reshape(-1)[cells]
+    xq = np.einsum("qa,cai->cqi", vals, X)
+    uq = np.einsum("qa,ca->cq", vals, cu)
+    gq = np.einsum("ca,cqaj->cqj", cu, g)
+    l2 = np.sqrt(np.sum((uq - mms_u(xq)) ** 2 * jxw))
+    return l2, l2 + np.sqrt(np.sum(((gq - mms_grad(xq)) ** 2).sum(-1) * jxw))
 
 
 def golden(name):
