@@ -556,6 +556,29 @@ def run_reference(args, rank, world):
             "e2e": {"value": round(v, 3), "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
 
 
+def run_profile_element(args, device):
+    """For ncu: the general-element kernel on one element type at its bench
+    size (ELEMENT_BOXES), Neo-Hookean at a twisted state: FP64 assembly x2,
+    then FP64-residual/FP32-tangent assembly x2."""
+    pkg = load_package()
+    nat = pkg._native
+    n = dict(ELEMENT_BOXES)[args.profile_element]
+    prob = element_problem(pkg, args.profile_element, n)
+    dv = prob.dev()
+    prob.fes[0].update_Dirichlet_boundary_conditions(rotation_bc(math.radians(6.0)))
+    mask, vals = prob.dirichlet_device()
+    u = torch.where(mask.bool(), vals, torch.zeros_like(vals))
+    res = torch.empty_like(u)
+    A64, A32 = dv.new_matrix(torch.float64), dv.new_matrix(torch.float32)
+    for _ in range(2):
+        prob.assemble(u, res=res, vals=A64.vals)
+    for _ in range(2):
+        prob.assemble(u, res=res, vals=A32.vals, fp32=True)
+    torch.cuda.synchronize()
+    print(json.dumps({"profile": args.profile_element, "cells": dv.num_cells, "dofs": dv.ndofs, "nnzb": dv.nnzb,
+                      "launches": nat.launch_count()}))
+
+
 def run_profile(args, device):
     """A short fixed sequence of the hot kernels at the bench size, for ncu:
     FP64 assembly and the FP64-residual/FP32-tangent assembly (x2 each),
@@ -680,7 +703,10 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--simp-samples", type=int, default=12)
     ap.add_argument("--no-elements", action="store_true", help="skip the TET4/TET10/HEX20/HEX27 measurements")
+    ap.add_argument("--elements-only", action="store_true", help="only the TET4/TET10/HEX20/HEX27 measurements")
     ap.add_argument("--profile", action="store_true", help="short kernel sequence for ncu captures")
+    ap.add_argument("--profile-element", default="", choices=["", "TET4", "TET10", "HEX20", "HEX27"],
+                    help="general-element assembly sequence for ncu captures")
     ap.add_argument("--warmstart-train", action="store_true",
                     help="generate SIMP (rho, u) pairs, train the warm-start network, evaluate, save")
     ap.add_argument("--ws-train", type=int, default=2000)
@@ -711,6 +737,12 @@ def main():
                                              device_id=device)
     if args.profile:
         run_profile(args, device)
+        return
+    if args.profile_element:
+        run_profile_element(args, device)
+        return
+    if args.elements_only:
+        print(json.dumps({"other_elements_neo_hookean_twist": element_bench(load_package(), device)}), flush=True)
         return
     if args.warmstart_train:
         run_warmstart_train(args, device)

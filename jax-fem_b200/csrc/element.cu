@@ -79,8 +79,8 @@ struct ElemShape<20> {
   static constexpr int TPC = 128, CPB = 1, QC = 8;
 };
 template <>
-struct ElemShape<27> {
-  static constexpr int TPC = 128, CPB = 1, QC = 8;
+struct ElemShape<27> {  // 216 points at the default order: 8 chunks with 27 threads in phase 1
+  static constexpr int TPC = 128, CPB = 1, QC = 27;
 };
 
 template <int LAW>

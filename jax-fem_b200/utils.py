@@ -1,18 +1,22 @@
-"""Mesh and result files without meshio: VTU output and hexahedral mesh input.
+"""Mesh and result files without meshio: VTU output and mesh input.
 
 Mirrors ``save_sol`` (utils.py:13-57 in the reference), which writes the
 solution and optional point/cell fields of a finite element to a VTK XML
 UnstructuredGrid (.vtu) through meshio, and gives the reading side the
 reference gets from ``meshio.read``: VTU files (ASCII, base64 binary, zlib
 compressed; what dolfinx and meshio write), Gmsh ``.msh`` (ASCII, formats 2.2
-and 4.1) and Abaqus ``.inp`` meshes, returning the hexahedra as a ``Mesh``.
+and 4.1) and Abaqus ``.inp`` meshes, returning the cells of one 3D element
+type (TET4, TET10, HEX8, HEX20, HEX27) as a ``Mesh``.
 
 File formats followed: the VTK XML file format (UnstructuredGrid, inline
 DataArrays, ``header_type`` UInt32/UInt64, ``vtkZLibDataCompressor`` block
-layout), the Gmsh MSH 2.2 / 4.1 ASCII formats (8-node hexahedron = type 5)
-and the Abaqus input format (``*NODE``, ``*ELEMENT, TYPE=C3D8``/``C3D8R``/
-``C3D8I``).  The 8-node hexahedron node order is the same in VTK, Gmsh and
-Abaqus, and it is the order ``Mesh`` uses.
+layout; cell types 10, 24, 12, 25, 29 and the order-1 Lagrange cells 71, 72),
+the Gmsh MSH 2.2 / 4.1 ASCII formats (element types 4, 11, 5, 17, 12) and the
+Abaqus input format (``*NODE``, ``*ELEMENT, TYPE=C3D4 / C3D10 / C3D8 /
+C3D20`` and their R/I/M/H variants).  ``Mesh`` uses the VTK (= meshio) node
+order; Abaqus lists the same order, Gmsh numbers the edge (and face) nodes of
+its quadratic cells differently and is permuted on reading (Gmsh node
+ordering: edges in the order of their corner pairs listed below).
 """
 import base64
 import os
@@ -23,10 +27,14 @@ import zlib
 
 import numpy as np
 
-from .generate_mesh import Mesh, get_meshio_cell_type
+from . import basis
+from .generate_mesh import Mesh
 
-_VTK_HEXAHEDRON = 12
-_VTK_LAGRANGE_HEXAHEDRON = 72  # order 1: the same 8 nodes in the same order
+# VTK cell type of each element type, and the types read back: the order-1
+# Lagrange cells of dolfinx (71 tetrahedron, 72 hexahedron) list the same
+# nodes in the same order as 10 and 12.
+_VTK_CELL = {"TET4": 10, "TET10": 24, "HEX8": 12, "HEX20": 25, "HEX27": 29}
+_VTK_READ = {10: "TET4", 24: "TET10", 12: "HEX8", 25: "HEX20", 29: "HEX27", 71: "TET4", 72: "HEX8"}
 _VTK_TYPES = {"Float32": np.float32, "Float64": np.float64, "Int8": np.int8, "UInt8": np.uint8,
               "Int16": np.int16, "UInt16": np.uint16, "Int32": np.int32, "UInt32": np.uint32,
               "Int64": np.int64, "UInt64": np.uint64}
@@ -51,16 +59,23 @@ def _data_array(arr, name=None, ncomp=None, fmt="binary"):
     return el
 
 
-def write_vtu(path, points, cells, point_data=None, cell_data=None, fmt="binary"):
-    """Write a hexahedral mesh with point and cell fields as a .vtu file.
+def write_vtu(path, points, cells, point_data=None, cell_data=None, fmt="binary", ele_type=None):
+    """Write a mesh of one element type with point and cell fields as a .vtu file.
 
-    points (N, 3); cells (C, 8) in VTK hexahedron order; point_data /
-    cell_data: dicts name -> array with N (or C) rows.  ``fmt`` is "binary"
-    (inline base64, UInt64 headers) or "ascii"."""
+    points (N, 3); cells (C, nen) in VTK node order (the element type follows
+    from nen unless given); point_data / cell_data: dicts name -> array with
+    N (or C) rows.  ``fmt`` is "binary" (inline base64, UInt64 headers) or
+    "ascii"."""
     points = np.asarray(points, dtype=np.float64)
     if points.shape[1] == 2:
         points = np.hstack([points, np.zeros((len(points), 1))])
     cells = np.asarray(cells, dtype=np.int64)
+    if ele_type is None:
+        by_nen = {n: e for e, n in basis.NODES_PER_CELL.items()}
+        if cells.shape[1] not in by_nen:
+            raise NotImplementedError(f"cells of {cells.shape[1]} nodes: no 3D element type has that many")
+        ele_type = by_nen[cells.shape[1]]
+    vtk_type = _VTK_CELL[basis.check_ele_type(ele_type)]
     root = ET.Element("VTKFile", {"type": "UnstructuredGrid", "version": "1.0", "byte_order": "LittleEndian",
                                   "header_type": "UInt64"})
     piece = ET.SubElement(ET.SubElement(root, "UnstructuredGrid"), "Piece",
@@ -69,7 +84,7 @@ def write_vtu(path, points, cells, point_data=None, cell_data=None, fmt="binary"
     ce = ET.SubElement(piece, "Cells")
     ce.append(_data_array(cells.reshape(-1), "connectivity", fmt=fmt))
     ce.append(_data_array(np.arange(1, len(cells) + 1, dtype=np.int64) * cells.shape[1], "offsets", fmt=fmt))
-    ce.append(_data_array(np.full(len(cells), _VTK_HEXAHEDRON, dtype=np.uint8), "types", fmt=fmt))
+    ce.append(_data_array(np.full(len(cells), vtk_type, dtype=np.uint8), "types", fmt=fmt))
     for tag, fields, rows in (("PointData", point_data, len(points)), ("CellData", cell_data, len(cells))):
         if not fields:
             continue
@@ -91,7 +106,7 @@ def save_sol(fe, sol, sol_file, cell_infos=None, point_infos=None):
     save_sol (utils.py:13-57): the solution as point field ``sol``, every
     field in FP32, cell fields of shape (num_cells,)."""
     fe = fe.fes[0] if hasattr(fe, "fes") else fe
-    get_meshio_cell_type(fe.ele_type)  # HEX8 only
+    basis.check_ele_type(fe.ele_type)
     sol = _host(sol)
     num_cells = len(fe.cells)
     point_data = {"sol": np.asarray(sol, dtype=np.float32).reshape(len(fe.points), -1)}
@@ -106,7 +121,7 @@ def save_sol(fe, sol, sol_file, cell_infos=None, point_infos=None):
         if len(data) != len(point_data["sol"]):
             raise ValueError("point data wrong shape!")
         point_data[name] = np.asarray(data, dtype=np.float32)
-    write_vtu(sol_file, fe.points, fe.cells, point_data, cell_data)
+    write_vtu(sol_file, fe.points, fe.cells, point_data, cell_data, ele_type=fe.ele_type)
 
 
 def _host(a):
@@ -164,10 +179,11 @@ def _read_array(el, header, compressor):
     return data.reshape(-1, int(nc)) if nc is not None and int(nc) > 1 else data
 
 
-def read_vtu(path):
-    """Read a .vtu file: returns (points (N,3) float64, cells (C,8) int32,
-    point_data dict, cell_data dict).  Only hexahedra (VTK types 12, and 72
-    of order 1) are returned; other cells raise NotImplementedError."""
+def read_vtu(path, with_type=False):
+    """Read a .vtu file: returns (points (N,3) float64, cells (C,nen) int32,
+    point_data dict, cell_data dict), and the element type when
+    ``with_type``.  All cells must be of one supported type (VTK 10, 24, 12,
+    25, 29, or 71 / 72 of order 1); others raise NotImplementedError."""
     root = ET.parse(path).getroot()
     if root.get("type") != "UnstructuredGrid":
         raise NotImplementedError("only VTK UnstructuredGrid files are read")
@@ -180,30 +196,74 @@ def read_vtu(path):
     cd = {el.get("Name"): _read_array(el, header, compressor) for el in piece.find("Cells")}
     conn, offs, types = cd["connectivity"].astype(np.int64), cd["offsets"].astype(np.int64), cd["types"]
     sizes = np.diff(np.concatenate([[0], offs]))
-    if not np.all(np.isin(types, (_VTK_HEXAHEDRON, _VTK_LAGRANGE_HEXAHEDRON))) or not np.all(sizes == 8):
-        raise NotImplementedError("only 8-node hexahedral cells are read")
-    cells = conn.reshape(-1, 8).astype(np.int32)
+    eles = {_VTK_READ.get(int(t)) for t in np.unique(types)}
+    ele = eles.pop() if len(eles) == 1 else None
+    if ele is None or not np.all(sizes == basis.NODES_PER_CELL[ele]):
+        raise NotImplementedError("the cells must be of one type: TET4, TET10, HEX8, HEX20 or HEX27 "
+                                  "(VTK 10, 24, 12, 25, 29; 71/72 of order 1)")
+    cells = conn.reshape(-1, basis.NODES_PER_CELL[ele]).astype(np.int32)
     fields = []
     for tag in ("PointData", "CellData"):
         sec = piece.find(tag)
         fields.append({} if sec is None else {el.get("Name"): _read_array(el, header, compressor) for el in sec})
+    if with_type:
+        return points, cells, fields[0], fields[1], ele
     return points, cells, fields[0], fields[1]
 
 
 # ---- Gmsh and Abaqus meshes -------------------------------------------------------
 
-def _compact(points, node_ids, cells_ids):
-    """Mesh from node ids and cells of ids: points ordered by first use in
-    the hexahedra (unused nodes, e.g. geometry points, are dropped)."""
+# Gmsh element type -> element; Gmsh's corner pairs of the edge nodes of the
+# quadratic tetrahedron and hexahedron, and the corner sets of the
+# hexahedron's face nodes (Gmsh node ordering).
+_GMSH_TYPES = {4: "TET4", 11: "TET10", 5: "HEX8", 17: "HEX20", 12: "HEX27"}
+_GMSH_TET_EDGES = [(0, 1), (1, 2), (2, 0), (3, 0), (3, 2), (3, 1)]
+_GMSH_HEX_EDGES = [(0, 1), (0, 3), (0, 4), (1, 2), (1, 5), (2, 3), (2, 6), (3, 7), (4, 5), (4, 7), (5, 6), (6, 7)]
+_GMSH_HEX_FACES = [(0, 1, 2, 3), (0, 1, 4, 5), (0, 3, 4, 7), (1, 2, 5, 6), (2, 3, 6, 7), (4, 5, 6, 7)]
+
+
+def _gmsh_to_vtk(ele):
+    """perm with vtk_cell = gmsh_cell[perm]."""
+    tet = ele.startswith("TET")
+    nc = 4 if tet else 8
+    perm = list(range(nc))
+    if ele in ("TET10", "HEX20", "HEX27"):
+        g_edges = [frozenset(e) for e in (_GMSH_TET_EDGES if tet else _GMSH_HEX_EDGES)]
+        v_edges = basis.TET_EDGES if tet else basis.HEX_EDGES
+        perm += [nc + g_edges.index(frozenset(int(c) for c in e)) for e in v_edges]
+    if ele == "HEX27":
+        g_faces = [frozenset(f) for f in _GMSH_HEX_FACES]
+        perm += [20 + g_faces.index(frozenset(int(c) for c in f)) for f in basis.HEX_FACE_CORNERS]
+        perm.append(26)
+    return np.array(perm)
+
+
+def _pick(found, ele_type, path, what):
+    """The cells of the requested element type, or of the single one found."""
+    if ele_type is not None:
+        if ele_type not in found:
+            raise ValueError(f"{path}: no {ele_type} {what}")
+        return ele_type
+    if len(found) != 1:
+        raise ValueError(f"{path}: {'no' if not found else 'several'} 3D element types "
+                         f"({sorted(found)}); pass ele_type")
+    return next(iter(found))
+
+
+def _compact(points, node_ids, cells_ids, ele):
+    """Mesh from node ids and cells of ids: the points the cells use, in the
+    order of the node table (unused nodes, e.g. geometry points, dropped)."""
+    nen = basis.NODES_PER_CELL[ele]
     index = {int(t): i for i, t in enumerate(node_ids)}
-    cells = np.array([[index[int(t)] for t in c] for c in cells_ids], dtype=np.int64).reshape(-1, 8)
+    cells = np.array([[index[int(t)] for t in c] for c in cells_ids], dtype=np.int64).reshape(-1, nen)
     used, inv = np.unique(cells.reshape(-1), return_inverse=True)
-    return Mesh(points[used], inv.reshape(-1, 8).astype(np.int32))
+    return Mesh(points[used], inv.reshape(-1, nen).astype(np.int32), ele)
 
 
-def read_gmsh(path):
-    """Hexahedral mesh from a Gmsh ASCII .msh file (format 2.2 or 4.1):
-    the 8-node hexahedra (element type 5); nodes not used by them dropped."""
+def read_gmsh(path, ele_type=None):
+    """Mesh from a Gmsh ASCII .msh file (format 2.2 or 4.1): the cells of
+    one 3D element type (``ele_type``, or the only one in the file), in VTK
+    node order; nodes not used by them dropped."""
     with open(path) as f:
         lines = [ln.strip() for ln in f]
     sec = {}
@@ -218,7 +278,7 @@ def read_gmsh(path):
     version = float(sec["MeshFormat"][0].split()[0])
     if int(sec["MeshFormat"][0].split()[1]) != 0:
         raise NotImplementedError("binary .msh files are not read")
-    ids, xyz, hexes = [], [], []
+    ids, xyz, found = [], [], {}
     if version >= 4.0:
         nodes = sec["Nodes"]
         nblocks = int(nodes[0].split()[0])
@@ -233,8 +293,10 @@ def read_gmsh(path):
         p = 1
         for _ in range(nblocks):
             _, _, etype, n = (int(v) for v in els[p].split())
-            if etype == 5:
-                hexes += [[int(v) for v in ln.split()[1:9]] for ln in els[p + 1:p + 1 + n]]
+            if etype in _GMSH_TYPES:
+                nen = basis.NODES_PER_CELL[_GMSH_TYPES[etype]]
+                found.setdefault(_GMSH_TYPES[etype], []).extend(
+                    [int(v) for v in ln.split()[1:1 + nen]] for ln in els[p + 1:p + 1 + n])
             p += 1 + n
     else:
         nodes = sec["Nodes"]
@@ -245,17 +307,25 @@ def read_gmsh(path):
         els = sec["Elements"]
         for ln in els[1:1 + int(els[0])]:
             v = [int(t) for t in ln.split()]
-            if v[1] == 5:
-                hexes.append(v[3 + v[2]:3 + v[2] + 8])
-    if not hexes:
-        raise ValueError(f"{path}: no 8-node hexahedra (Gmsh element type 5)")
-    return _compact(np.array(xyz, dtype=np.float64), ids, hexes)
+            if v[1] in _GMSH_TYPES:
+                nen = basis.NODES_PER_CELL[_GMSH_TYPES[v[1]]]
+                found.setdefault(_GMSH_TYPES[v[1]], []).append(v[3 + v[2]:3 + v[2] + nen])
+    ele = _pick(found, ele_type, path, "cells (Gmsh element types 4, 11, 5, 17, 12)")
+    cells = np.array(found[ele], dtype=np.int64)[:, _gmsh_to_vtk(ele)]
+    return _compact(np.array(xyz, dtype=np.float64), ids, cells, ele)
 
 
-def read_abaqus(path):
-    """Hexahedral mesh from an Abaqus .inp file: the *NODE table and the
-    *ELEMENT blocks of TYPE=C3D8, C3D8R or C3D8I."""
-    ids, xyz, hexes = [], [], []
+_ABAQUS_TYPES = {"C3D4": "TET4", "C3D4H": "TET4", "C3D10": "TET10", "C3D10H": "TET10", "C3D10M": "TET10",
+                 "C3D10MH": "TET10", "C3D8": "HEX8", "C3D8R": "HEX8", "C3D8I": "HEX8", "C3D8H": "HEX8",
+                 "C3D20": "HEX20", "C3D20R": "HEX20", "C3D20H": "HEX20", "C3D20RH": "HEX20"}
+
+
+def read_abaqus(path, ele_type=None):
+    """Mesh from an Abaqus .inp file: the *NODE table and the *ELEMENT
+    blocks of one 3D element type (C3D4, C3D10, C3D8, C3D20 and their
+    R/I/M/H variants; ``ele_type`` or the only one in the file).  Abaqus
+    lists the nodes of these cells in VTK order."""
+    ids, xyz, found = [], [], {}
     mode, pending = None, []
     with open(path) as f:
         for raw in f:
@@ -268,7 +338,7 @@ def read_abaqus(path):
                     mode = "node"
                 elif kw.startswith("*ELEMENT") and not kw.startswith("*ELEMENT OUTPUT"):
                     m = re.search(r"TYPE\s*=\s*([A-Z0-9]+)", kw)
-                    mode = "hex" if m and m.group(1) in ("C3D8", "C3D8R", "C3D8I") else None
+                    mode = _ABAQUS_TYPES.get(m.group(1)) if m else None
                 else:
                     mode = None
                 pending = []
@@ -277,24 +347,27 @@ def read_abaqus(path):
             if mode == "node":
                 ids.append(int(vals[0]))
                 xyz.append([float(v) for v in vals[1:4]] + [0.0] * (3 - len(vals[1:4])))
-            elif mode == "hex":  # a row may continue on the next line after a trailing comma
+            elif mode is not None:  # a row may continue on the next line after a trailing comma
                 pending += [int(v) for v in vals]
-                if len(pending) >= 9:
-                    hexes.append(pending[1:9])
+                nen = basis.NODES_PER_CELL[mode]
+                if len(pending) >= nen + 1:
+                    found.setdefault(mode, []).append(pending[1:nen + 1])
                     pending = []
-    if not hexes:
-        raise ValueError(f"{path}: no C3D8 elements")
-    return _compact(np.array(xyz, dtype=np.float64), ids, hexes)
+    ele = _pick(found, ele_type, path, "elements (C3D4, C3D10, C3D8, C3D20)")
+    return _compact(np.array(xyz, dtype=np.float64), ids, found[ele], ele)
 
 
-def read_mesh(path):
-    """``Mesh`` of the hexahedra in a .vtu, .msh or .inp file (by extension)."""
+def read_mesh(path, ele_type=None):
+    """``Mesh`` of the cells of one 3D element type in a .vtu, .msh or .inp
+    file (by extension)."""
     ext = os.path.splitext(path)[1].lower()
     if ext == ".vtu":
-        points, cells, _, _ = read_vtu(path)
-        return Mesh(points, cells)
+        points, cells, _, _, ele = read_vtu(path, with_type=True)
+        if ele_type is not None and ele_type != ele:
+            raise ValueError(f"{path}: holds {ele} cells, not {ele_type}")
+        return Mesh(points, cells, ele)
     if ext == ".msh":
-        return read_gmsh(path)
+        return read_gmsh(path, ele_type)
     if ext == ".inp":
-        return read_abaqus(path)
+        return read_abaqus(path, ele_type)
     raise NotImplementedError(f"mesh file type '{ext}' (read .vtu, .msh or .inp)")

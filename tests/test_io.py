@@ -6,7 +6,11 @@
 - the reader takes zlib-compressed inline arrays (meshio's default) and the
   dolfinx ASCII form of the reference's FEniCSx fixtures (VTK type 72);
 - Gmsh 2.2 / 4.1 ASCII and Abaqus meshes give the same hexahedral Mesh,
-  unused nodes and non-hexahedral elements dropped."""
+  unused nodes and non-hexahedral elements dropped;
+- TET4, TET10, HEX20 and HEX27 meshes and solutions round-trip through VTU
+  with their VTK cell types; their Gmsh (edge and face nodes renumbered)
+  and Abaqus cells come back in VTK order, checked by geometry: every
+  edge / face / centre node sits where the cell's corners put it."""
 import base64
 import struct
 import zlib
@@ -154,3 +158,104 @@ def test_read_gmsh_and_abaqus(io, tmp_path):
         np.testing.assert_array_equal(m.cells, cells, err_msg=name)
     with pytest.raises(NotImplementedError):
         ut.read_mesh(str(tmp_path / "x.stl"))
+
+
+@pytest.mark.parametrize("ele", ["TET4", "TET10", "HEX20", "HEX27"])
+def test_element_types_round_trip(io, tmp_path, ele):
+    pkg, ut = io
+    from helpers import element_box
+    m = element_box(pkg, ele, (2, 1, 2))
+    fe = pkg.fe.FiniteElement(m, 1, 3, ele_type=ele)
+    sol = np.random.default_rng(2).normal(size=len(m.points))
+    path = str(tmp_path / f"{ele}.vtu")
+    ut.save_sol(fe, sol, path)
+    pts, cells, pd, _, got = ut.read_vtu(path, with_type=True)
+    assert got == ele
+    np.testing.assert_array_equal(cells, m.cells)
+    np.testing.assert_array_equal(pd["sol"].reshape(-1), sol.astype(np.float32))
+    mm = ut.read_mesh(path)
+    assert mm.ele_type == ele and mm.cells.shape == m.cells.shape
+    with pytest.raises(ValueError):
+        ut.read_mesh(path, ele_type="HEX8")
+
+
+def _isoparametric_ok(pkg, mesh):
+    """Every node of every cell sits at the linear map of its reference
+    position from the cell's corners (straight-sided cells)."""
+    import importlib
+    B = importlib.import_module("jax_fem_b200.basis")
+    lin = "TET4" if mesh.ele_type.startswith("TET") else "HEX8"
+    vn = B.shape_fn(lin, B.node_coords(mesh.ele_type))[0]
+    X = mesh.points[mesh.cells]
+    return np.allclose(np.einsum("ka,cai->cki", vn, X[:, :vn.shape[1]]), X, atol=1e-12)
+
+
+# Gmsh node numbering of quadratic cells (edge corner pairs, hexahedron face
+# corner sets), used here to write the cells in Gmsh order.
+_GMSH_TET_EDGES = [(0, 1), (1, 2), (2, 0), (3, 0), (3, 2), (3, 1)]
+_GMSH_HEX_EDGES = [(0, 1), (0, 3), (0, 4), (1, 2), (1, 5), (2, 3), (2, 6), (3, 7), (4, 5), (4, 7), (5, 6), (6, 7)]
+_GMSH_HEX_FACES = [(0, 1, 2, 3), (0, 1, 4, 5), (0, 3, 4, 7), (1, 2, 5, 6), (2, 3, 6, 7), (4, 5, 6, 7)]
+
+
+def _gmsh_cell(corner_xyz, ele, add_node):
+    """Node numbers of one cell in Gmsh order, new nodes created by add_node(xyz)."""
+    ids = [add_node(x) for x in corner_xyz]
+    if ele in ("TET10", "HEX20", "HEX27"):
+        edges = _GMSH_TET_EDGES if ele == "TET10" else _GMSH_HEX_EDGES
+        ids += [add_node(0.5 * (corner_xyz[a] + corner_xyz[b])) for a, b in edges]
+    if ele == "HEX27":
+        ids += [add_node(corner_xyz[list(f)].mean(axis=0)) for f in _GMSH_HEX_FACES]
+        ids.append(add_node(corner_xyz.mean(axis=0)))
+    return ids
+
+
+@pytest.mark.parametrize("ele,gtype", [("TET4", 4), ("TET10", 11), ("HEX20", 17), ("HEX27", 12)])
+def test_gmsh_quadratic_cells_come_back_in_vtk_order(io, tmp_path, ele, gtype):
+    pkg, ut = io
+    rng = np.random.default_rng(4)
+    if ele.startswith("TET"):
+        corners = np.array([[0, 0, 0], [1, 0, 0], [0, 1, 0], [0, 0, 1]], float)
+    else:
+        corners = np.array([[0, 0, 0], [1, 0, 0], [1, 1, 0], [0, 1, 0], [0, 0, 1], [1, 0, 1], [1, 1, 1],
+                            [0, 1, 1]], float)
+    corners = corners @ np.array([[1.0, 0.2, 0.1], [0.0, 1.1, 0.3], [0.1, 0.0, 0.9]]) + rng.normal(size=3)
+    nodes = {}
+
+    def add(x):
+        nodes[100 + 3 * len(nodes)] = x  # sparse Gmsh node tags
+        return 100 + 3 * (len(nodes) - 1)
+
+    cell = _gmsh_cell(corners, ele, add)
+    node_lines = "\n".join(f"{t} {float(x[0])!r} {float(x[1])!r} {float(x[2])!r}" for t, x in nodes.items())
+    msh22 = (f"$MeshFormat\n2.2 0 8\n$EndMeshFormat\n$Nodes\n{len(nodes)}\n{node_lines}\n$EndNodes\n"
+             f"$Elements\n2\n1 15 2 0 1 {cell[0]}\n2 {gtype} 2 0 1 {' '.join(map(str, cell))}\n$EndElements\n")
+    tags = list(nodes)
+    msh41 = ("$MeshFormat\n4.1 0 8\n$EndMeshFormat\n"
+             f"$Nodes\n1 {len(tags)} {min(tags)} {max(tags)}\n3 1 0 {len(tags)}\n"
+             + "\n".join(map(str, tags)) + "\n" + "\n".join(" ".join(repr(float(v)) for v in nodes[t]) for t in tags)
+             + f"\n$EndNodes\n$Elements\n1 1 1 1\n3 1 {gtype} 1\n1 {' '.join(map(str, cell))}\n$EndElements\n")
+    for name, text in (("a.msh", msh22), ("b.msh", msh41)):
+        (tmp_path / name).write_text(text)
+        m = ut.read_mesh(str(tmp_path / name))
+        assert m.ele_type == ele and m.cells.shape == (1, len(cell))
+        assert _isoparametric_ok(pkg, m), name
+
+
+def test_abaqus_tet10_and_hex20(io, tmp_path):
+    pkg, ut = io
+    from helpers import element_box
+    for ele, typ in (("TET10", "C3D10"), ("HEX20", "C3D20R")):
+        m = element_box(pkg, ele, (1, 1, 1))
+        lines = ["*HEADING", "*NODE"] + [f"{i + 1}, {float(x)!r}, {float(y)!r}, {float(z)!r}"
+                                         for i, (x, y, z) in enumerate(m.points)]
+        lines.append(f"*ELEMENT, TYPE={typ}, ELSET=body")
+        for k, c in enumerate(m.cells):
+            vals = [str(k + 1)] + [str(int(v) + 1) for v in c]
+            lines += [", ".join(vals[:8]) + ",", ", ".join(vals[8:16]) + ("," if len(vals) > 16 else "")]
+            if len(vals) > 16:
+                lines.append(", ".join(vals[16:]))
+        (tmp_path / f"{ele}.inp").write_text("\n".join(lines) + "\n")
+        got = ut.read_mesh(str(tmp_path / f"{ele}.inp"))
+        assert got.ele_type == ele
+        np.testing.assert_array_equal(got.points[got.cells], m.points[m.cells])
+        assert _isoparametric_ok(pkg, got)
