@@ -1,5 +1,7 @@
 /*
- * jaxfem_b200.h -- C ABI of the B200 (sm_100a) HEX8 assemble-and-solve library.
+ * jaxfem_b200.h -- C ABI of the B200 (sm_100a) assemble-and-solve library
+ * (HEX8 fast path; TET4, TET10, HEX20, HEX27 through the general element
+ * entry points).
  *
  * The reference (JAX-FEM) is pure Python: its hot path is a chain of Python
  * functions with no foreign-function boundary.  Each entry point below
@@ -17,10 +19,12 @@
  *    (query with the *_workspace_bytes functions).  A workspace must not be
  *    shared by two calls that may run concurrently.
  *  - Layouts: points (num_nodes,3) f64 row-major; cells (num_cells,8) int32
- *    in VTK/meshio HEX8 order; dof = node*vec + component; block-CSR (BSR)
+ *    in VTK/meshio HEX8 order ((num_cells,nen) for the general element
+ *    entry points); dof = node*vec + component; block-CSR (BSR)
  *    matrices with vec x vec row-major blocks, sorted columns per block row.
  *  - Per-quadrature-point data is (num_cells, 8, ...) with the quadrature
- *    points in basix order (2x2x2 Gauss-Legendre on [0,1]^3, x slowest).
+ *    points in basix order (2x2x2 Gauss-Legendre on [0,1]^3, x slowest);
+ *    (num_cells, nq, ...) for the general element entry points.
  */
 #ifndef JAXFEM_B200_H
 #define JAXFEM_B200_H
