@@ -100,7 +100,8 @@ FEM_API int fem_bsr_pattern(const int32_t* h_cells, int64_t num_cells, int64_t n
 /* The same for cells of nen nodes (the element types of basis.py:19-114:
  * TET4 4, HEX8 8, TET10 10, HEX20 20, HEX27 27); h_cells is (num_cells, nen)
  * and h_scatter (num_cells, nen*nen) with the block index of local pair
- * (a, b) at [c*nen*nen + a*nen + b].  fem_bsr_pattern is the nen = 8 case. */
+ * (a, b) at [c*nen*nen + a*nen + b].  fem_bsr_pattern is the nen = 8 case.
+ * 1 <= nen <= 256 (the cell-kernel path passes cell dof tables). */
 FEM_API int fem_bsr_pattern_nen(const int32_t* h_cells, int64_t num_cells, int nen, int64_t num_nodes,
                     int32_t* h_row_ptr, int64_t* h_nnzb, int32_t* h_col_idx,
                     int64_t col_capacity, int32_t* h_scatter, int32_t* h_diag);
@@ -192,6 +193,40 @@ FEM_API int fem_param_vjp_elem_f64(int law, const double* h_params, int n_params
                      const double* d_gref, const double* d_wq, int64_t num_cells, const int32_t* d_cells,
                      const double* d_points, const double* d_u, const double* d_ivar0,
                      const double* d_lambda, double* d_grad, void* stream);
+
+/* ---- cell-kernel path ---------------------------------------------------
+ * For problems whose weak form is user code evaluated by the host on the
+ * device (universal kernels, multi-variable problems, tensor maps that are
+ * not registered laws; problem.py:260-300): the global system is a scalar
+ * CSR matrix over all dofs (a BSR with vec = 1), its pattern from
+ * fem_bsr_pattern_nen with the cell dof table (num_cells, nd) as "cells".
+ * fem_scatter_cells_* replaces the residual scatter of
+ * compute_residual_vars_helper (problem.py:471-483) and the COO insertion +
+ * zeroRows of get_A (solver.py:466-491).  It ACCUMULATES (the caller zeroes
+ * d_res / d_lift / d_vals once, then calls it for the cells and for each
+ * set of boundary faces):
+ *   d_item_res (items, nd), d_item_jac (items, nd, nd) row-major (NULL: no
+ *   tangent or lift); item i belongs to cell d_item_cell[i] (NULL: cell i),
+ *   whose dofs are d_cell_dofs[cell] and whose scatter row is
+ *   d_scatter[cell] (nd*nd entries);
+ *   d_res[dofs[a]] += res[i, a];
+ *   d_vals[scatter[cell, a*nd+b]] += jac[i, a, b] unless dofs[a] or dofs[b]
+ *   is a Dirichlet dof (d_bc_mask);
+ *   d_lift[dofs[a]] += jac[i, a, b] * d_dvec[dofs[b]] for free dofs[a].
+ * No symmetry is assumed.  1 <= nd <= 256.
+ * fem_bsr_bc_diag_* then writes the unit diagonal at Dirichlet dofs. */
+FEM_API int fem_scatter_cells_f64(int nd, int64_t num_items, const int32_t* d_item_cell,
+                     const int32_t* d_cell_dofs, const int32_t* d_scatter, const double* d_item_res,
+                     const double* d_item_jac, const uint8_t* d_bc_mask, const double* d_dvec,
+                     double* d_res, double* d_lift, double* d_vals, void* stream);
+FEM_API int fem_scatter_cells_f32(int nd, int64_t num_items, const int32_t* d_item_cell,
+                     const int32_t* d_cell_dofs, const int32_t* d_scatter, const double* d_item_res,
+                     const double* d_item_jac, const uint8_t* d_bc_mask, const double* d_dvec,
+                     double* d_res, double* d_lift, float* d_vals, void* stream);
+FEM_API int fem_bsr_bc_diag_f64(int vec, int64_t n_brows, const uint8_t* d_bc_mask, const int32_t* d_diag,
+                     double* d_vals, void* stream);
+FEM_API int fem_bsr_bc_diag_f32(int vec, int64_t n_brows, const uint8_t* d_bc_mask, const int32_t* d_diag,
+                     float* d_vals, void* stream);
 
 /* ---- J2 state commit ----------------------------------------------------
  * Replaces the reference plasticity update (test_plasticity.py:67-78 with

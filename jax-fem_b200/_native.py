@@ -81,6 +81,10 @@ _SIGS = {
                                     P, P, P, P, P]),
     "fem_j2_commit_elem": (I32, [DP, I32, I32, I32, P, I64, P, P, P, P, P, P, P, P, P, P]),
     "fem_param_vjp_elem_f64": (I32, [I32, DP, I32, I32, I32, P, P, I64, P, P, P, P, P, P, P]),
+    "fem_scatter_cells_f64": (I32, [I32, I64, P, P, P, P, P, P, P, P, P, P, P]),
+    "fem_scatter_cells_f32": (I32, [I32, I64, P, P, P, P, P, P, P, P, P, P, P]),
+    "fem_bsr_bc_diag_f64": (I32, [I32, I64, P, P, P, P]),
+    "fem_bsr_bc_diag_f32": (I32, [I32, I64, P, P, P, P]),
     "fem_bsr_transpose_map": (I32, [P, P, I64, P]),
     "fem_j2_commit": (I32, [DP, I32, I64, P, P, P, P, P, P, P, P, P, P]),
     "fem_j2_sensitivity": (I32, [DP, I32, I64, P, P, P, P, P, P, P, P, P, P, P, P, P, P]),

@@ -67,7 +67,7 @@ extern "C" int fem_bsr_pattern_nen(const int32_t* h_cells, int64_t num_cells, in
                                    int32_t* h_row_ptr, int64_t* h_nnzb, int32_t* h_col_idx,
                                    int64_t col_capacity, int32_t* h_scatter, int32_t* h_diag) {
   FEM_CHECK_ARG(num_cells >= 0 && num_nodes >= 0, "negative sizes");
-  FEM_CHECK_ARG(nen >= 1 && nen <= 64, "nodes per cell %d outside [1, 64]", nen);
+  FEM_CHECK_ARG(nen >= 1 && nen <= 256, "nodes per cell %d outside [1, 256]", nen);
   FEM_CHECK_ARG(num_cells == 0 || h_cells != nullptr, "cells is NULL");
   FEM_CHECK_ARG(h_row_ptr != nullptr && h_nnzb != nullptr, "row_ptr/nnzb is NULL");
   Adjacency adj;

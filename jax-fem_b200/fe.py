@@ -266,6 +266,17 @@ class FiniteElement:
                     "mass/surface maps that depend on u are not supported on this path; "
                     "only u-independent loads (evaluated once into a load vector) are")
 
+    def depends_on_u(self, fn):
+        """Whether a mass / surface map's value changes with u (checked at a
+        few nodes with random u): such maps go to the cell-kernel path."""
+        try:
+            self._check_u_independent(fn, self.points[: min(4, len(self.points))])
+        except NotImplementedError:
+            return True
+        except Exception:  # noqa: BLE001 - needs internal variables or torch input: user code
+            return True
+        return False
+
     def body_load(self, mass_map):
         """int mass_map(u, x) . v dx as a (ndofs,) vector."""
         X = self.points[self.cells]  # (C,nen,3)

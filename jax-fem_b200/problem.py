@@ -93,6 +93,16 @@ class DeviceMesh:
         return BSRMatrix(self.vec, self.row_ptr, self.col_idx, self.diag, vals)
 
 
+class CellKernelLaw:
+    """What ``problem.law`` is on the cell-kernel path: no registered kernel
+    (law_id None: treated as nonlinear by the Newton forcing)."""
+    law_id = None
+    vec = None
+
+    def params(self):
+        return []
+
+
 def _to_dev(x, device, dtype=torch.float64):
     if isinstance(x, torch.Tensor):
         return x.detach().to(device=device, dtype=dtype).contiguous()
@@ -114,31 +124,41 @@ class Problem:
     additional_info: tuple = ()
 
     def __post_init__(self):
+        # one variable, or one per entry of a mesh list (problem.py:56-84)
         if isinstance(self.mesh, list):
-            if len(self.mesh) != 1:
-                raise NotImplementedError("multi-variable problems are not on this path")
-            self.mesh = self.mesh[0]
-            self.vec = self.vec[0] if isinstance(self.vec, list) else self.vec
-            self.ele_type = self.ele_type[0] if isinstance(self.ele_type, list) else self.ele_type
-            if isinstance(self.dirichlet_bc_info, list) and len(self.dirichlet_bc_info) == 1 and (
-                    self.dirichlet_bc_info[0] is None or isinstance(self.dirichlet_bc_info[0], list)
-                    and len(self.dirichlet_bc_info[0]) == 3 and isinstance(self.dirichlet_bc_info[0][0], list)):
-                self.dirichlet_bc_info = self.dirichlet_bc_info[0]
-        if not isinstance(self.mesh, Mesh):
-            self.mesh = Mesh(self.mesh.points, self.mesh.cells, self.ele_type)
-        self.fes = [FiniteElement(mesh=self.mesh, vec=self.vec, dim=self.dim, ele_type=self.ele_type,
-                                  quadrature_rule=self.quadrature_rule,
-                                  quadrature_order=self.quadrature_order,
-                                  dirichlet_bc_info=self.dirichlet_bc_info)]
-        self.num_vars = 1
-        self.cells_list = [self.fes[0].cells]
+            n = len(self.mesh)
+            meshes = list(self.mesh)
+            vecs = list(self.vec) if isinstance(self.vec, list) else [self.vec] * n
+            etypes = list(self.ele_type) if isinstance(self.ele_type, list) else [self.ele_type] * n
+            bcs = list(self.dirichlet_bc_info) if self.dirichlet_bc_info is not None else [None] * n
+        else:
+            n, meshes, vecs, etypes, bcs = 1, [self.mesh], [self.vec], [self.ele_type], [self.dirichlet_bc_info]
+        pick = lambda v, i: v[i] if isinstance(v, list) else v  # noqa: E731
+        meshes = [m if isinstance(m, Mesh) else Mesh(m.points, m.cells, e) for m, e in zip(meshes, etypes)]
+        self.fes = [FiniteElement(mesh=meshes[i], vec=vecs[i], dim=self.dim, ele_type=etypes[i],
+                                  quadrature_rule=pick(self.quadrature_rule, i),
+                                  quadrature_order=pick(self.quadrature_order, i),
+                                  dirichlet_bc_info=bcs[i]) for i in range(n)]
+        self.num_vars = n
+        if n == 1:
+            self.mesh, self.vec, self.ele_type, self.dirichlet_bc_info = meshes[0], vecs[0], etypes[0], bcs[0]
+        else:
+            self.mesh, self.vec, self.ele_type, self.dirichlet_bc_info = meshes, vecs, etypes, bcs
+        self.cells_list = [fe.cells for fe in self.fes]
+        if any(fe.num_cells != self.fes[0].num_cells for fe in self.fes):
+            raise ValueError("all variables must have the same number of cells")
         self.num_cells = self.fes[0].num_cells
         self.boundary_inds_list = self.fes[0].get_boundary_conditions_inds(self.location_fns)
         self.offset = [0]
-        self.num_total_dofs_all_vars = self.fes[0].num_total_dofs
+        for fe in self.fes[:-1]:
+            self.offset.append(self.offset[-1] + fe.num_total_dofs)
+        self.num_total_dofs_all_vars = self.offset[-1] + self.fes[-1].num_total_dofs
+        self.num_nodes_cumsum = np.cumsum([0] + [fe.num_nodes for fe in self.fes])
         self.internal_vars = ()
         self.internal_vars_surfaces = [() for _ in range(len(self.boundary_inds_list))]
         self._dev = None
+        self._cells = None
+        self._cell_path = None
         self._elem = None
         self._bc_cache = None
         self._fext = None
@@ -146,6 +166,8 @@ class Problem:
         self.custom_init(*self.additional_info)
         if hasattr(self, "get_surface_maps"):
             assert len(self.boundary_inds_list) == len(self.get_surface_maps())
+        elif hasattr(self, "get_universal_kernels_surface"):
+            assert len(self.boundary_inds_list) == len(self.get_universal_kernels_surface())
         else:
             assert len(self.boundary_inds_list) == 0, "Missing definitions for surface integral"
 
@@ -158,23 +180,52 @@ class Problem:
 
     # ---- helpers ---------------------------------------------------------------
     @property
+    def cell_path(self):
+        """True when the weak form is user code run by the cell-kernel path
+        (cellpath.py): a universal kernel, several variables, a tensor map
+        that is not a registered law, no tensor map, or mass / surface maps
+        that depend on u.  False: the registered-law kernels."""
+        if self._cell_path is None:
+            cp = (self.num_vars > 1 or hasattr(self, "get_universal_kernel")
+                  or hasattr(self, "get_universal_kernels_surface") or not hasattr(self, "get_tensor_map"))
+            if not cp:
+                try:
+                    as_law(self.get_tensor_map(), self.vec, self.dim)
+                except NotImplementedError:
+                    cp = True
+            fe = self.fes[0]
+            if not cp and hasattr(self, "get_mass_map"):
+                cp = fe.depends_on_u(self.get_mass_map())
+            if not cp and hasattr(self, "get_surface_maps"):
+                cp = any(fe.depends_on_u(m) for m in self.get_surface_maps())
+            self._cell_path = cp
+        return self._cell_path
+
+    @property
     def law(self):
         if self._law is None:
-            if not hasattr(self, "get_tensor_map"):
-                raise NotImplementedError("a Problem on this path needs get_tensor_map")
-            self._law = as_law(self.get_tensor_map(), self.vec, self.dim)
+            if self.cell_path:
+                self._law = CellKernelLaw()
+            else:
+                self._law = as_law(self.get_tensor_map(), self.vec, self.dim)
         return self._law
 
     def device(self):
         return torch.device("cuda", torch.cuda.current_device())
 
     def dev(self):
-        """Device mesh + pattern, built on first use."""
+        """Device mesh + pattern, built on first use (the scalar CSR system of
+        all dofs on the cell-kernel path)."""
         if self._dev is None:
             if not torch.cuda.is_available():
                 raise nat.FEMNativeError(nat.FEM_ERR_CUDA, "no CUDA device: this path has no CPU fallback")
             nat.load()
-            self._dev = DeviceMesh(self.mesh, self.vec, self.device())
+            if self.cell_path:
+                from .cellpath import CellPath
+                self._cells = CellPath(self, self.device())
+                self._dev = self._cells.sys
+            else:
+                self._dev = DeviceMesh(self.mesh, self.vec, self.device())
         return self._dev
 
     @property
@@ -194,14 +245,25 @@ class Problem:
         return self._elem
 
     def unflatten_fn_sol_list(self, dofs):
-        return [dofs.reshape(-1, self.vec)]
+        """Flat dofs -> [(num_nodes_i, vec_i), ...] (views)."""
+        dofs = dofs.reshape(-1)
+        return [dofs[off:off + fe.num_total_dofs].reshape(-1, fe.vec) for off, fe in zip(self.offset, self.fes)]
+
+    def unflatten_fn_dof(self, cell_sol_flat):
+        """A cell's flat dofs -> [(num_nodes_i, vec_i), ...] per variable (for kernels)."""
+        out, k = [], 0
+        for fe in self.fes:
+            out.append(cell_sol_flat[k:k + fe.num_nodes * fe.vec].reshape(fe.num_nodes, fe.vec))
+            k += fe.num_nodes * fe.vec
+        return out
 
     def dirichlet_device(self):
-        """(mask uint8, values f64) on the device, refreshed after BC updates."""
-        fe = self.fes[0]
-        key = fe.bc_version
+        """(mask uint8, values f64) over all dofs on the device, refreshed after BC updates."""
+        key = tuple(fe.bc_version for fe in self.fes)
         if self._bc_cache is None or self._bc_cache[0] != key:
-            mask, vals = fe.dirichlet_arrays()
+            arrays = [fe.dirichlet_arrays() for fe in self.fes]
+            mask = np.concatenate([a[0] for a in arrays])
+            vals = np.concatenate([a[1] for a in arrays])
             d = self.dev().device
             self._bc_cache = (key, torch.from_numpy(mask).to(d), torch.from_numpy(vals).to(d))
         return self._bc_cache[1], self._bc_cache[2]
@@ -218,10 +280,14 @@ class Problem:
         return self._surface_loads
 
     def external_load(self):
-        """f_ext = int mass_map . v dx + sum_surfaces int surface_map . v ds (device f64)."""
+        """f_ext = int mass_map . v dx + sum_surfaces int surface_map . v ds (device f64);
+        zero on the cell-kernel path, whose kernels hold these terms."""
         if self._fext is None:
             d = self.dev().device
             f = torch.zeros(self.num_total_dofs_all_vars, dtype=torch.float64, device=d)
+            if self.cell_path:
+                self._fext = f
+                return f
             if hasattr(self, "get_mass_map"):
                 f += torch.from_numpy(self.fes[0].body_load(self.get_mass_map())).to(d)
             for fs in self.surface_load_vectors():
@@ -265,6 +331,9 @@ class Problem:
                  ivars=None):
         """One fused pass of the cell kernel: residual, tangent, Dirichlet lift."""
         dv = self.dev()
+        if self.cell_path:
+            self._cells.assemble(dofs, res=res, vals=vals, lift=lift, dvec=dvec, bc=bc, fp32=fp32, ivars=ivars)
+            return
         law = self.law
         mask, _ = self.dirichlet_device() if bc else (None, None)
         iv = self.law_ivars(ivars)
@@ -283,15 +352,17 @@ class Problem:
                       "assemble_elem")
 
     def _flat_dofs(self, sol_list):
-        s = sol_list[0] if isinstance(sol_list, (list, tuple)) else sol_list
-        return _to_dev(s, self.dev().device).reshape(-1)
+        d = self.dev().device
+        if isinstance(sol_list, (list, tuple)):
+            return torch.cat([_to_dev(s, d).reshape(-1) for s in sol_list[: self.num_vars]])
+        return _to_dev(sol_list, d).reshape(-1)
 
     def compute_residual(self, sol_list):
         """Residual list (without Dirichlet rows applied), as the reference's."""
         dofs = self._flat_dofs(sol_list)
         res = torch.empty_like(dofs)
         self.assemble(dofs, res=res, bc=False)
-        return [(res + self.external_load()).reshape(-1, self.vec)]
+        return self.unflatten_fn_sol_list(res + self.external_load())
 
     def newton_update(self, sol_list):
         """Residual list; also assembles the BC-eliminated tangent into ``self.A``."""
@@ -300,7 +371,7 @@ class Problem:
         if getattr(self, "A", None) is None or self.A.vals.dtype != torch.float64:
             self.A = self.dev().new_matrix(torch.float64)
         self.assemble(dofs, res=res, vals=self.A.vals)
-        return [(res + self.external_load()).reshape(-1, self.vec)]
+        return self.unflatten_fn_sol_list(res + self.external_load())
 
     # ---- J2 state commit (test_plasticity.py:67-78) -----------------------------
     def update_j2_state(self, sol):

@@ -656,6 +656,190 @@ class OracleProblem:
         return out
 
 
+class KernelProblem:
+    """Multi-variable problem with user kernels (problem.py:56-128, 130-190,
+    189-340, 426-483): cell residual = laplace kernel of ``tensor_map`` on
+    the first variable + mass kernel of ``mass_map`` + ``universal_kernel``;
+    face residual = surface kernel of ``surface_maps[i]`` + universal surface
+    kernel ``universal_surface[i]``.  Kernels are numpy functions with the
+    reference's per-cell signatures (complex-step safe); a Python loop over
+    cells stands in for jax.vmap.  Jacobians by complex step along each
+    cell dof (the reference's forward JVPs), COO assembly with the variables'
+    dof offsets, BC rows zeroed (solver.py:466-491).
+
+    ``vars``: list of dicts with points, cells, vec, ele_type, order and
+    dirichlet (a [location_fns, vecs, value_fns] triple or None)."""
+
+    def __init__(self, vars, tensor_map=None, mass_map=None, universal_kernel=None, location_fns=None,
+                 surface_maps=None, universal_surface=None, internal_vars=(), internal_vars_surfaces=()):
+        self.vars = []
+        off = 0
+        for v in vars:
+            ele, order = v.get("ele_type", "HEX8"), v.get("order")
+            if ele == "HEX8" and order in (None, 2):
+                vals, grads_ref, w = hex8_tables()
+                fv, fg, fw, normals, finds = hex8_face_tables()
+            else:
+                vals, grads_ref, w = element_tables(ele, order)
+                fv, fg, fw, normals, finds = element_face_tables(ele, order)
+            pts = np.asarray(v["points"], dtype=np.float64)
+            cells = np.asarray(v["cells"], dtype=np.int64)
+            g, jxw = shape_grads(pts, cells, grads_ref, w)
+            nodes, vecs, bvals = dirichlet_bcs(pts, v.get("dirichlet"))
+            self.vars.append(dict(points=pts, cells=cells, vec=v["vec"], vals=vals, grads_ref=grads_ref, w=w,
+                                  fvals=fv, fgrads=fg, fw=fw, normals=normals, face_inds=finds, g=g, jxw=jxw,
+                                  off=off, nodes=nodes, vecs=vecs, bvals=bvals))
+            off += len(pts) * v["vec"]
+        self.ndofs = off
+        v0 = self.vars[0]
+        self.num_cells = len(v0["cells"])
+        # (C, nd) global dofs of each cell (problem.py:86-97)
+        self.cell_dofs = np.hstack([(v["vec"] * v["cells"][:, :, None] + np.arange(v["vec"])[None, None, :]
+                                     + v["off"]).reshape(self.num_cells, -1) for v in self.vars])
+        self.shape_grads = np.concatenate([v["g"] for v in self.vars], axis=2)          # (C,Q,sum nen,3)
+        self.JxW = np.stack([v["jxw"] for v in self.vars], axis=1)                      # (C,V,Q)
+        self.v_grads_JxW = np.concatenate([v["g"][:, :, :, None, :] * v["jxw"][:, :, None, None, None]
+                                           for v in self.vars], axis=2)
+        self.x = np.einsum("qa,cai->cqi", v0["vals"], v0["points"][v0["cells"]])
+        self.tensor_map, self.mass_map, self.universal = tensor_map, mass_map, universal_kernel
+        self.surface_maps, self.universal_surface = surface_maps, universal_surface
+        self.internal_vars = list(internal_vars)
+        self.internal_vars_surfaces = list(internal_vars_surfaces)
+        self.boundary_inds = boundary_faces(v0["points"], v0["cells"], location_fns, v0["face_inds"])
+        self.faces = []
+        for binds in self.boundary_inds:
+            fvals, fgrads, scales = [], [], []
+            for v in self.vars:
+                X = v["points"][v["cells"][binds[:, 0]]]
+                gr = v["fgrads"][binds[:, 1]]
+                Jf = np.einsum("fai,fqaj->fqij", X, gr)
+                fgrads.append(np.einsum("fqaj,fqjk->fqak", gr, np.linalg.inv(Jf)))
+                scales.append(face_geometry(v["points"], v["cells"], binds, v["fgrads"], v["fw"], v["normals"]))
+                fvals.append(v["fvals"][binds[:, 1]])
+            xs = np.einsum("fqa,fai->fqi", v0["fvals"][binds[:, 1]], v0["points"][v0["cells"][binds[:, 0]]])
+            self.faces.append(dict(binds=binds, vals=np.concatenate(fvals, axis=2),
+                                   grads=np.concatenate(fgrads, axis=2), nanson=np.stack(scales, axis=1), x=xs))
+
+    def unflatten_fn_dof(self, flat):
+        out, k = [], 0
+        for v in self.vars:
+            n = v["vals"].shape[1] * v["vec"]
+            out.append(flat[k:k + n].reshape(-1, v["vec"]))
+            k += n
+        return out
+
+    def _first(self, val, nd):
+        out = np.zeros(nd, dtype=val.dtype)
+        out[: val.size] = val.reshape(-1)
+        return out
+
+    def cell_kernel(self, c, sol, ivars):
+        """problem.py:278-300 for cell c."""
+        v0 = self.vars[0]
+        n0 = v0["vals"].shape[1]
+        nd = sol.size
+        val = np.zeros(nd, dtype=sol.dtype)
+        u = sol[: n0 * v0["vec"]].reshape(n0, v0["vec"])
+        iv = [np.asarray(a)[c] for a in ivars]
+        if self.tensor_map is not None:  # laplace kernel, problem.py:189-214
+            ug = np.einsum("ai,qaj->qij", u, self.shape_grads[c][:, :n0, :])
+            P = np.array([self.tensor_map(ug[q], *[a[q] for a in iv]) for q in range(ug.shape[0])])
+            val = val + self._first(np.einsum("qij,qaj->ai", P, self.v_grads_JxW[c][:, :n0, 0, :]), nd)
+        if self.mass_map is not None:  # mass kernel, problem.py:216-236
+            uq = np.einsum("ai,qa->qi", u, v0["vals"])
+            m = np.array([self.mass_map(uq[q], self.x[c][q], *[a[q] for a in iv]) for q in range(uq.shape[0])])
+            val = val + self._first(np.einsum("qi,qa,q->ai", m, v0["vals"], self.JxW[c][0]), nd)
+        if self.universal is not None:
+            val = val + self.universal(sol, self.x[c], self.shape_grads[c], self.JxW[c], self.v_grads_JxW[c], *iv)
+        return val
+
+    def face_kernel(self, i, f, sol, ivars):
+        """problem.py:305-332 for face f of surface i."""
+        face = self.faces[i]
+        v0 = self.vars[0]
+        n0 = v0["vals"].shape[1]
+        nd = sol.size
+        val = np.zeros(nd, dtype=sol.dtype)
+        iv = [np.asarray(a)[f] for a in ivars]
+        fsv = face["vals"][f]
+        if self.surface_maps is not None:  # surface kernel, problem.py:238-259
+            u = sol[: n0 * v0["vec"]].reshape(n0, v0["vec"])
+            uq = np.einsum("ai,qa->qi", u, fsv[:, :n0])
+            t = np.array([self.surface_maps[i](uq[q], face["x"][f][q], *[a[q] for a in iv])
+                          for q in range(uq.shape[0])])
+            val = val + self._first(np.einsum("qi,qa,q->ai", t, fsv[:, :n0], face["nanson"][f][0]), nd)
+        if self.universal_surface is not None:
+            val = val + self.universal_surface[i](sol, face["x"][f], fsv, face["grads"][f], face["nanson"][f], *iv)
+        return val
+
+    def _items(self):
+        """(global dofs, kernel(sol) -> residual) of every cell and selected face."""
+        out = []
+        for c in range(self.num_cells):
+            out.append((self.cell_dofs[c], lambda s, c=c: self.cell_kernel(c, s, self.internal_vars)))
+        for i, face in enumerate(self.faces):
+            ivs = self.internal_vars_surfaces[i] if i < len(self.internal_vars_surfaces) else ()
+            for f, (c, _) in enumerate(face["binds"]):
+                out.append((self.cell_dofs[c], lambda s, i=i, f=f, ivs=ivs: self.face_kernel(i, f, s, ivs)))
+        return out
+
+    def residual(self, dofs):
+        R = np.zeros(self.ndofs)
+        for idx, k in self._items():
+            np.add.at(R, idx, k(dofs[idx]))
+        return R
+
+    def residual_and_tangent(self, dofs, h=1e-30):
+        R = np.zeros(self.ndofs)
+        I, J, V = [], [], []
+        for idx, k in self._items():
+            base = dofs[idx].astype(np.complex128)
+            np.add.at(R, idx, k(dofs[idx]))
+            nd = len(idx)
+            jac = np.empty((nd, nd))
+            for d in range(nd):
+                up = base.copy()
+                up[d] += 1j * h
+                jac[:, d] = np.imag(k(up)) / h
+            I.append(np.repeat(idx, nd))
+            J.append(np.tile(idx, nd))
+            V.append(jac.reshape(-1))
+        K = sp.csr_matrix((np.concatenate(V), (np.concatenate(I), np.concatenate(J))), shape=(self.ndofs,) * 2)
+        return R, K
+
+    def bc_rows(self):
+        rows, vals = [], []
+        for v in self.vars:
+            for n, vi, bv in zip(v["nodes"], v["vecs"], v["bvals"]):
+                rows.append(v["off"] + n * v["vec"] + vi)
+                vals.append(bv)
+        if not rows:
+            return np.zeros(0, dtype=np.int64), np.zeros(0)
+        return np.concatenate(rows), np.concatenate(vals)
+
+    def newton(self, rel_tol=1e-10, tol=1e-12, max_iter=30):
+        """The Newton loop of solver.py:1232-1318 with spsolve and zeroRows."""
+        rows, bvals = self.bc_rows()
+        dofs = np.zeros(self.ndofs)
+
+        def system(d):
+            R, K = self.residual_and_tangent(d)
+            R[rows] = d[rows] - bvals
+            keep = np.ones(self.ndofs)
+            keep[rows] = 0.0
+            unit = 1.0 - keep
+            return R, (sp.diags(keep) @ K + sp.diags(unit)).tocsc()
+
+        R, K = system(dofs)
+        r0 = np.linalg.norm(R)
+        it = 0
+        while np.linalg.norm(R) > tol and np.linalg.norm(R) / r0 > rel_tol and it < max_iter:
+            dofs = dofs + spla.spsolve(K, -R)
+            R, K = system(dofs)
+            it += 1
+        return dofs
+
+
 def newton_solve(problem, initial_guess=None, rel_tol=1e-8, tol=1e-6, linear="spsolve",
                  max_iter=50, return_info=False):
     """Newton loop of ``solver`` (solver.py:1232-1318) with the step of

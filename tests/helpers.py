@@ -131,3 +131,40 @@ def golden(name):
     import os
     here = os.path.dirname(os.path.abspath(__file__))
     return dict(np.load(os.path.join(here, "golden", name + ".npz")))
+
+
+def thermo_meshes(pkg):
+    """A 2x1x1 box (length 2) of TET10 cells and the TET4 mesh of its corner nodes."""
+    m10 = element_box(pkg, "TET10", (2, 1, 1), L=(2.0, 1.0, 1.0))
+    ncorner = int(m10.cells[:, :4].max()) + 1
+    m4 = pkg.Mesh(m10.points[:ncorner], m10.cells[:, :4], "TET4")
+    return m10, m4
+
+
+def thermo_problem(pkg, m10, m4, h=2.0, T_inf=1.0):
+    """The two-variable thermo-elastic problem (u on TET10, T on TET4) with a
+    Robin condition on x = 2, as a product Problem (torch kernels) and an
+    oracle KernelProblem (numpy kernels)."""
+    import torch
+
+    import kernels as K
+    bc_u = [[face_fn(0, 0.0)] * 3, [0, 1, 2], [lambda p: 0.0] * 3]
+    bc_T = [[face_fn(0, 0.0)], [0], [lambda p: 0.0]]
+    right = face_fn(0, 2.0)
+
+    class Thermo(pkg.Problem):
+        def get_universal_kernel(self):
+            return K.thermoelastic_universal(torch, 10, self.fes[1].shape_vals_t, 100.0, 0.3, 2.0, 3.0, 1.0)
+
+        def get_universal_kernels_surface(self):
+            return [K.robin_surface(torch, 10, h, T_inf)]
+
+    p = Thermo([m10, m4], vec=[3, 1], dim=3, ele_type=["TET10", "TET4"], quadrature_order=[2, 2],
+               dirichlet_bc_info=[bc_u, bc_T], location_fns=[right])
+    oracle = fo.KernelProblem(
+        [dict(points=m10.points, cells=m10.cells, vec=3, ele_type="TET10", order=2, dirichlet=bc_u),
+         dict(points=m4.points, cells=m4.cells, vec=1, ele_type="TET4", order=2, dirichlet=bc_T)],
+        universal_kernel=K.thermoelastic_universal(np, 10, fo.element_tables("TET4", 2)[0], 100.0, 0.3, 2.0, 3.0,
+                                                   1.0),
+        location_fns=[right], universal_surface=[K.robin_surface(np, 10, h, T_inf)])
+    return p, oracle, bc_u, bc_T
