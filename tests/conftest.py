@@ -16,6 +16,8 @@ GOLDEN = os.path.join(ROOT, "tests", "golden")
 
 def pytest_configure(config):
     config.addinivalue_line("markers", "gpu: needs a CUDA device (B200) and the built library")
+    # raised inside torch.func's linear-algebra rules, not by this package
+    config.addinivalue_line("filterwarnings", "ignore:`torch.jit.script` is deprecated:DeprecationWarning")
 
 
 @pytest.fixture(scope="session")
