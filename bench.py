@@ -155,6 +155,65 @@ def element_bench(pkg, device):
     return out
 
 
+def _nh_universal(E=10.0, nu=0.3):
+    """The compressible Neo-Hookean weak form written as a torch universal
+    kernel (the reference's form of a user-written weak form)."""
+    mu = E / (2.0 * (1.0 + nu))
+    kappa = E / (3.0 * (1.0 - 2.0 * nu))
+
+    def kernel(sol, x, sg, jxw, vg):
+        F = torch.einsum("ai,qaj->qij", sol.reshape(-1, 3), sg) + torch.eye(3, dtype=sol.dtype, device=sol.device)
+        J = torch.linalg.det(F)
+        H = torch.linalg.inv(F).transpose(1, 2)
+        I1 = torch.einsum("qij,qij->q", F, F)
+        m = mu * J ** (-2.0 / 3.0)
+        P = m[:, None, None] * (F - (I1 / 3.0)[:, None, None] * H) + (kappa * J * (J - 1.0))[:, None, None] * H
+        return torch.einsum("qij,qaj->ai", P, vg[:, :, 0, :]).reshape(-1)
+
+    return kernel
+
+
+def cell_path_bench(pkg, device, n=30):
+    """Cost of the cell-kernel path: the Neo-Hookean twist on an n^3 HEX8
+    box with the weak form as a torch universal kernel (vmap of jacfwd, then
+    the CUDA scatter into a scalar CSR tangent), against the registered
+    NeoHookean CUDA kernel on the same box."""
+    m = pkg.box_mesh(n, n, n, 1.0, 1.0, 1.0)
+    mesh = pkg.Mesh(m.points, m.cells_dict["hexahedron"])
+
+    class Universal(pkg.Problem):
+        def get_universal_kernel(self):
+            return _nh_universal()
+
+    class Law(pkg.Problem):
+        def get_tensor_map(self):
+            return pkg.NeoHookean(10.0, 0.3)
+
+    out = {"workload": f"neo-hookean twist, {n}^3 HEX8 box, weak form as a torch universal kernel"}
+    for name, cls in (("cell_path", Universal), ("law_kernel", Law)):
+        prob = cls(mesh, vec=3, dim=3, dirichlet_bc_info=rotation_bc(0.0))
+        dv = prob.dev()
+        u = torch.zeros(dv.ndofs, dtype=torch.float64, device=device)
+        res = torch.empty_like(u)
+        A = dv.new_matrix(torch.float64)
+        t = time_kernel(lambda: prob.assemble(u, res=res, vals=A.vals), reps=5)
+        lin = {"bicgstab": {"precond": "jacobi", "rtol": "adaptive", "atol": 0.0, "maxiter": 20000}}
+        nh_solve(pkg, prob, "fp64", linear=lin)  # warm-up
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        _, infos = nh_solve(pkg, prob, "fp64", linear=lin)
+        e1.record()
+        torch.cuda.synchronize()
+        out[name] = {"dofs": dv.ndofs, "assembly_ms": round(t * 1e3, 3),
+                     "twist_solve_s": round(e0.elapsed_time(e1) * 1e-3, 4),
+                     "newton_iters": sum(i["newton_iters"] for i in infos),
+                     "krylov_iters": sum(sum(i["krylov_iters"]) for i in infos)}
+        del prob, dv, A
+        torch.cuda.empty_cache()
+    return out
+
+
 def j2_run(pkg, n=40, increments=10, precision="fp64", linear=None):
     """40^3 J2 cube with hardening: u_x(x=1) ramped to 0.02 over the increments,
     Newton to 1e-8 per increment, state committed after each."""
@@ -419,12 +478,16 @@ def run_ours(args, rank, world, device):
         e1.record()
         torch.cuda.synchronize()
         j2[arm] = {"s": round(e0.elapsed_time(e1) * 1e-3, 4), "newton": jn, "krylov": jk}
-    elements = None
+    elements = cell_path = None
     if not args.no_elements:
         try:
             elements = element_bench(pkg, device)
         except Exception as e:  # noqa: BLE001 - report, do not lose the headline line
             elements = {"error": str(e)[:300]}
+        try:
+            cell_path = cell_path_bench(pkg, device)
+        except Exception as e:  # noqa: BLE001 - report, do not lose the headline line
+            cell_path = {"error": str(e)[:300]}
     newton = {k: sum(i["newton_iters"] for i in v[1]) for k, v in results.items()}
     krylov = {k: sum(sum(i["krylov_iters"]) for i in v[1]) for k, v in results.items()}
     out = {
@@ -478,6 +541,7 @@ def run_ours(args, rank, world, device):
         "simp60_learned_warm_start": simp,
         "j2_40_10_increments": j2,
         "other_elements_neo_hookean_twist": elements,
+        "cell_kernel_path": cell_path,
         "e2e": {"value": round(t_e2e, 6), "unit": "s", "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": int(ndofs * 8)},
         "gpu_launches": int(launches),
@@ -703,7 +767,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--simp-samples", type=int, default=12)
     ap.add_argument("--no-elements", action="store_true", help="skip the TET4/TET10/HEX20/HEX27 measurements")
-    ap.add_argument("--elements-only", action="store_true", help="only the TET4/TET10/HEX20/HEX27 measurements")
+    ap.add_argument("--elements-only", action="store_true",
+                    help="only the TET4/TET10/HEX20/HEX27 and cell-kernel-path measurements")
     ap.add_argument("--profile", action="store_true", help="short kernel sequence for ncu captures")
     ap.add_argument("--profile-element", default="", choices=["", "TET4", "TET10", "HEX20", "HEX27"],
                     help="general-element assembly sequence for ncu captures")
@@ -742,7 +807,9 @@ def main():
         run_profile_element(args, device)
         return
     if args.elements_only:
-        print(json.dumps({"other_elements_neo_hookean_twist": element_bench(load_package(), device)}), flush=True)
+        pkg = load_package()
+        print(json.dumps({"other_elements_neo_hookean_twist": element_bench(pkg, device),
+                          "cell_kernel_path": cell_path_bench(pkg, device)}), flush=True)
         return
     if args.warmstart_train:
         run_warmstart_train(args, device)

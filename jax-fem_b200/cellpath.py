@@ -37,8 +37,10 @@ from torch.func import jacfwd, vmap
 
 from . import _native as nat
 
-# cells per batch: the batch's Jacobians take about this many doubles
-_BATCH_ENTRIES = 1 << 22
+# cells per batch: the batch's Jacobians take about this many doubles (the
+# forward-mode intermediates a few times more); larger batches launch fewer
+# kernels per cell
+_BATCH_ENTRIES = 1 << 25
 
 
 class CellSystem:
