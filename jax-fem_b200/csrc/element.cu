@@ -22,7 +22,10 @@
 //   phase 1  one thread per (cell, quadrature point of the chunk): J, det,
 //            J^-1, grad N, grad u and the constitutive update -> a per-quad
 //            record (shape gradients, law vectors, tangent coefficients and
-//            P*JxW) in shared memory
+//            P*JxW) in shared memory.  For HEX20 / HEX27 it is split: 1a per
+//            point forms J^-1, grad u and the law only; 1b, all threads, one
+//            (cell, point, node) item each, forms the node's shape gradient
+//            and law vectors
 //   phase 2  each thread adds the chunk into the node pairs a <= b it owns
 //            (FP64 registers, PPT pairs per thread); thread t < nen adds the
 //            residual of node t
@@ -59,28 +62,36 @@ struct ElemArgs {
   double p[4];
 };
 
-// Threads per cell, cells per block and quadrature points per chunk.
+// Threads per cell, cells per block, quadrature points per chunk, and
+// whether phase 1 is split (1a per point, 1b per (point, node)): measured on
+// B200, the split pays where a point's per-node work is long (20, 27 nodes:
+// 6 % faster) and costs where it is short (4 nodes: 13 % slower; 10: even).
 template <int NEN>
 struct ElemShape;
 template <>
 struct ElemShape<4> {
   static constexpr int TPC = 8, CPB = 16, QC = 4;
+  static constexpr bool SPLIT = false;
 };
 template <>
 struct ElemShape<8> {
   static constexpr int TPC = 16, CPB = 8, QC = 8;
+  static constexpr bool SPLIT = false;
 };
 template <>
 struct ElemShape<10> {
   static constexpr int TPC = 32, CPB = 4, QC = 4;
+  static constexpr bool SPLIT = false;
 };
 template <>
 struct ElemShape<20> {
   static constexpr int TPC = 128, CPB = 1, QC = 8;
+  static constexpr bool SPLIT = true;
 };
 template <>
-struct ElemShape<27> {  // 216 points at the default order: 8 chunks with 27 threads in phase 1
+struct ElemShape<27> {  // 216 points at the default order: 8 chunks with 27 threads in phase 1a
   static constexpr int TPC = 128, CPB = 1, QC = 27;
+  static constexpr bool SPLIT = true;
 };
 
 template <int LAW>
@@ -90,7 +101,9 @@ __host__ __device__ constexpr int law_vectors() {
 
 // Per-quad record (doubles): shape gradients g (nen x 3), law vectors
 // v1 = M1 g_b and v2 = M2 g_b per node (NH: F g_b, F^-T g_b; J2: s g_b),
-// four tangent coefficients * JxW, then P * JxW (VEC x 3).
+// four tangent coefficients * JxW, P * JxW (VEC x 3), then (split phase 1
+// only) J^-1 and the law's matrices M1, M2 (3 x 3 each), which phase 1b
+// turns into the per-node vectors.
 template <int NEN, int VEC, int LAW>
 struct ElemLayout {
   static constexpr int NV = law_vectors<LAW>();
@@ -99,7 +112,8 @@ struct ElemLayout {
   static constexpr int V2 = NEN * 6;
   static constexpr int C = NEN * 3 * (1 + NV);
   static constexpr int PO = C + 4;
-  static constexpr int QF = PO + VEC * 3;
+  static constexpr int SC = PO + VEC * 3;
+  static constexpr int QF = SC + (ElemShape<NEN>::SPLIT ? 9 * (1 + NV) : 0);
 };
 
 // Node record: X (3), u (VEC), d (VEC).
@@ -115,6 +129,25 @@ __host__ __device__ constexpr size_t elem_smem_bytes() {
   return sizeof(double) * (size_t(S::CPB) * S::QC * L::QF + size_t(S::CPB) * NEN * node_fields<VEC>() +
                            size_t(S::CPB) * NEN * VEC) +
          sizeof(int) * 2 * size_t(S::CPB) * NEN;
+}
+
+// J^-1 of a 3x3 matrix by cofactors; returns det J.
+__device__ __forceinline__ double invert3(const double J[3][3], double inv[3][3]) {
+  const double c00 = J[1][1] * J[2][2] - J[1][2] * J[2][1];
+  const double c01 = J[1][2] * J[2][0] - J[1][0] * J[2][2];
+  const double c02 = J[1][0] * J[2][1] - J[1][1] * J[2][0];
+  const double det = J[0][0] * c00 + J[0][1] * c01 + J[0][2] * c02;
+  const double id = 1.0 / det;
+  inv[0][0] = c00 * id;
+  inv[1][0] = c01 * id;
+  inv[2][0] = c02 * id;
+  inv[0][1] = (J[0][2] * J[2][1] - J[0][1] * J[2][2]) * id;
+  inv[1][1] = (J[0][0] * J[2][2] - J[0][2] * J[2][0]) * id;
+  inv[2][1] = (J[0][1] * J[2][0] - J[0][0] * J[2][1]) * id;
+  inv[0][2] = (J[0][1] * J[1][2] - J[0][2] * J[1][1]) * id;
+  inv[1][2] = (J[0][2] * J[1][0] - J[0][0] * J[1][2]) * id;
+  inv[2][2] = (J[0][0] * J[1][1] - J[0][1] * J[1][0]) * id;
+  return det;
 }
 
 // J at reference gradients gr (nen x 3) and node coordinates X (stride xs);
@@ -134,21 +167,7 @@ __device__ __forceinline__ double elem_jacobian(const double* __restrict__ gr, c
       J[i][2] = fma(x, d2, J[i][2]);
     }
   }
-  const double c00 = J[1][1] * J[2][2] - J[1][2] * J[2][1];
-  const double c01 = J[1][2] * J[2][0] - J[1][0] * J[2][2];
-  const double c02 = J[1][0] * J[2][1] - J[1][1] * J[2][0];
-  const double det = J[0][0] * c00 + J[0][1] * c01 + J[0][2] * c02;
-  const double id = 1.0 / det;
-  inv[0][0] = c00 * id;
-  inv[1][0] = c01 * id;
-  inv[2][0] = c02 * id;
-  inv[0][1] = (J[0][2] * J[2][1] - J[0][1] * J[2][2]) * id;
-  inv[1][1] = (J[0][0] * J[2][2] - J[0][2] * J[2][0]) * id;
-  inv[2][1] = (J[0][1] * J[2][0] - J[0][0] * J[2][1]) * id;
-  inv[0][2] = (J[0][1] * J[1][2] - J[0][2] * J[1][1]) * id;
-  inv[1][2] = (J[0][2] * J[1][0] - J[0][0] * J[1][2]) * id;
-  inv[2][2] = (J[0][0] * J[1][1] - J[0][1] * J[1][0]) * id;
-  return det;
+  return invert3(J, inv);
 }
 
 __device__ __forceinline__ void phys_grad(const double* __restrict__ gr, int a, const double inv[3][3],
@@ -326,7 +345,8 @@ __device__ __forceinline__ void elem_law(const ElemArgs& A, int64_t k, const dou
   }
 }
 
-// Phase 1: the record of quadrature point q of cell c (node record nd).
+// Phase 1 in one step (short per-node work): the record of quadrature point
+// q of cell c (node record nd).
 template <int NEN, int VEC, int LAW>
 __device__ __forceinline__ void quad_record(const ElemArgs& A, int64_t c, int q, const double* nd, double* qd) {
   using L = ElemLayout<NEN, VEC, LAW>;
@@ -362,6 +382,80 @@ __device__ __forceinline__ void quad_record(const ElemArgs& A, int64_t c, int q,
         qd[L::V1 + b * 3 + i] = M1[i][0] * g0 + M1[i][1] * g1 + M1[i][2] * g2;
         if constexpr (L::NV == 2) qd[L::V2 + b * 3 + i] = M2[i][0] * g0 + M2[i][1] * g1 + M2[i][2] * g2;
       }
+    }
+  }
+}
+
+// Split phase 1a, per quadrature point q of cell c (node record nd): J and the
+// reference gradient of u, sum_a u_a (x) dN_a/dxi, in one pass over the
+// nodes; J^-1, JxW; grad u = (sum_a u_a (x) dN_a/dxi) J^-1; the law.  J^-1
+// and the law's matrices go to the record's scratch for phase 1b.
+template <int NEN, int VEC, int LAW>
+__device__ __forceinline__ void quad_point(const ElemArgs& A, int64_t c, int q, const double* nd, double* qd) {
+  using L = ElemLayout<NEN, VEC, LAW>;
+  constexpr int NF = node_fields<VEC>();
+  const double* gr = A.gref + int64_t(q) * NEN * 3;
+  double J[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+  double ur[VEC][3];
+#pragma unroll
+  for (int i = 0; i < VEC; ++i) ur[i][0] = ur[i][1] = ur[i][2] = 0.0;
+#pragma unroll 4
+  for (int a = 0; a < NEN; ++a) {
+    const double d[3] = {__ldg(gr + a * 3), __ldg(gr + a * 3 + 1), __ldg(gr + a * 3 + 2)};
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+      const double x = nd[a * NF + i];
+#pragma unroll
+      for (int k = 0; k < 3; ++k) J[i][k] = fma(x, d[k], J[i][k]);
+    }
+#pragma unroll
+    for (int i = 0; i < VEC; ++i) {
+      const double ua = nd[a * NF + 3 + i];
+#pragma unroll
+      for (int k = 0; k < 3; ++k) ur[i][k] = fma(ua, d[k], ur[i][k]);
+    }
+  }
+  double inv[3][3];
+  const double det = invert3(J, inv);
+  const double jxw = det * __ldg(A.wq + q);
+  double ug[VEC][3];
+#pragma unroll
+  for (int i = 0; i < VEC; ++i)
+#pragma unroll
+    for (int k = 0; k < 3; ++k) ug[i][k] = ur[i][0] * inv[0][k] + ur[i][1] * inv[1][k] + ur[i][2] * inv[2][k];
+  double M1[3][3], M2[3][3];
+  elem_law<VEC, LAW>(A, c * A.nq + q, ug, jxw, qd + L::PO, qd + L::C, M1, M2);
+  double* sc = qd + L::SC;
+#pragma unroll
+  for (int i = 0; i < 3; ++i)
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      sc[i * 3 + k] = inv[i][k];
+      if constexpr (L::NV >= 1) sc[9 + i * 3 + k] = M1[i][k];
+      if constexpr (L::NV == 2) sc[18 + i * 3 + k] = M2[i][k];
+    }
+}
+
+// Phase 1b, per (quadrature point q, node a): g_a = J^-T dN_a/dxi and the
+// law vectors M1 g_a, M2 g_a, from the scratch phase 1a left in the record.
+template <int NEN, int VEC, int LAW>
+__device__ __forceinline__ void node_vectors(const ElemArgs& A, int q, int a, double* qd) {
+  using L = ElemLayout<NEN, VEC, LAW>;
+  const double* gr = A.gref + (int64_t(q) * NEN + a) * 3;
+  const double d0 = __ldg(gr), d1 = __ldg(gr + 1), d2 = __ldg(gr + 2);
+  const double* sc = qd + L::SC;
+  double g[3];
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    g[k] = d0 * sc[k] + d1 * sc[3 + k] + d2 * sc[6 + k];
+    qd[L::G + a * 3 + k] = g[k];
+  }
+  if constexpr (L::NV >= 1) {
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+      qd[L::V1 + a * 3 + i] = sc[9 + i * 3] * g[0] + sc[9 + i * 3 + 1] * g[1] + sc[9 + i * 3 + 2] * g[2];
+      if constexpr (L::NV == 2)
+        qd[L::V2 + a * 3 + i] = sc[18 + i * 3] * g[0] + sc[18 + i * 3 + 1] * g[1] + sc[18 + i * 3 + 2] * g[2];
     }
   }
 }
@@ -484,15 +578,33 @@ __global__ void __launch_bounds__(kElemThreads) elem_assemble_kernel(const ElemA
   __syncthreads();
 
   for (int q0 = 0; q0 < A.nq; q0 += S::QC) {
-    // ---- phase 1: one thread per (cell, quadrature point of the chunk) ----
+    // ---- phase 1 (1a): one thread per (cell, quadrature point of the chunk) ----
     if (threadIdx.x < S::CPB * S::QC) {
       const int wcl = threadIdx.x / S::QC;
       const int qi = threadIdx.x - wcl * S::QC;
       const int64_t wc = int64_t(blockIdx.x) * S::CPB + wcl;
-      if (wc < A.num_cells && q0 + qi < A.nq)
-        quad_record<NEN, VEC, LAW>(A, wc, q0 + qi, sn + wcl * NEN * NF, sq + (wcl * S::QC + qi) * L::QF);
+      if (wc < A.num_cells && q0 + qi < A.nq) {
+        if constexpr (S::SPLIT)
+          quad_point<NEN, VEC, LAW>(A, wc, q0 + qi, sn + wcl * NEN * NF, sq + (wcl * S::QC + qi) * L::QF);
+        else
+          quad_record<NEN, VEC, LAW>(A, wc, q0 + qi, sn + wcl * NEN * NF, sq + (wcl * S::QC + qi) * L::QF);
+      }
     }
     __syncthreads();
+    if constexpr (S::SPLIT) {
+      // ---- phase 1b: every thread, (cell, quadrature point, node) items ----
+#pragma unroll 1
+      for (int it = threadIdx.x; it < S::CPB * S::QC * NEN; it += kElemThreads) {
+        const int wcl = it / (S::QC * NEN);
+        const int rem = it - wcl * (S::QC * NEN);
+        const int qi = rem / NEN;
+        const int a = rem - qi * NEN;
+        const int64_t wc = int64_t(blockIdx.x) * S::CPB + wcl;
+        if (wc < A.num_cells && q0 + qi < A.nq)
+          node_vectors<NEN, VEC, LAW>(A, q0 + qi, a, sq + (wcl * S::QC + qi) * L::QF);
+      }
+      __syncthreads();
+    }
     // ---- phase 2: pairs and residual ----
     const int nqc = min(S::QC, A.nq - q0);
     if (valid) {
