@@ -242,3 +242,62 @@ def test_convergence_study_matches_oracle(pkg, cuda, ele, rates):
     l2_rate = np.log2(errs[0][0] / errs[1][0])
     h1_rate = np.log2(errs[0][1] / errs[1][1])
     assert abs(l2_rate - rates[0]) < 0.15 and abs(h1_rate - rates[1]) < 0.15, (l2_rate, h1_rate)
+
+
+def _twist_bc(deg):
+    import math
+    th = math.radians(deg)
+    c, s = math.cos(th), math.sin(th)
+    uy = lambda p: 0.5 + (p[1] - 0.5) * c - (p[2] - 0.5) * s - p[1]  # noqa: E731
+    uz = lambda p: 0.5 + (p[1] - 0.5) * s + (p[2] - 0.5) * c - p[2]  # noqa: E731
+    z = lambda p: 0.0 * p[0]  # noqa: E731
+    return [[face_fn(0, 0.0)] * 3 + [face_fn(0, 1.0)] * 3, [0, 1, 2] * 2, [z, z, z, z, uy, uz]]
+
+
+@pytest.mark.gpu
+def test_elem_arc_length_matches_oracle(pkg, cuda):
+    """Displacement-controlled arc-length continuation (solver.py:521-597)
+    of a 30-degree twist on TET10 cells: the load factor after every step
+    equals the oracle's (1e-8) and the polished end point its Newton
+    solution (1e-8)."""
+    mesh = element_box(pkg, "TET10", (2, 2, 2))
+    bc = _twist_bc(30.0)
+    prob = _problem(pkg, "TET10", None, pkg.NeoHookean(10.0, 0.3), [], bc=bc, mesh=mesh)
+    lin = {"cg": {"precond": "block_jacobi", "rtol": 1e-12, "atol": 0.0, "maxiter": 20000}}
+    (sol,), info = pkg.solver(prob, {"arc_length": {"control": "displacement", "Delta_l": 0.3, "psi": 1.0,
+                                                    "linear": lin, "return_info": True,
+                                                    "newton": {"rel_tol": 1e-10, "tol": 1e-14}}})
+    op = fo.OracleProblem(mesh.points, mesh.cells, 3, fo.Law("neo_hookean", E=10.0, nu=0.3), dirichlet_bc_info=bc,
+                          ele_type="TET10")
+    ref_u, ref_lams = fo.arc_length_disp(op, Delta_l=0.3, psi=1.0)
+    lams = [h["lam"] for h in info["history"]]
+    assert len(lams) == len(ref_lams) and info["polished"] and lams[-1] >= 1.0
+    np.testing.assert_allclose(lams, ref_lams, rtol=1e-8)
+    sol = sol.cpu().numpy().reshape(-1)
+    assert np.abs(sol - ref_u).max() <= 1e-8 * np.abs(ref_u).max()
+
+
+@pytest.mark.gpu
+def test_cell_path_dynamic_relax_matches_oracle(pkg, cuda):
+    """Dynamic relaxation (solver.py:837-1047) through the cell-kernel path:
+    a universal kernel restating the Neo-Hookean law on TET4 cells (scalar
+    CSR tangent, mass from its absolute row sums) takes the oracle's
+    iteration count (+-1) to the oracle's end point (1e-9)."""
+    import kernels as K
+    mesh = element_box(pkg, "TET4", (2, 2, 2))
+    bc = _twist_bc(20.0)
+
+    class Universal(pkg.Problem):
+        def get_universal_kernel(self):
+            return K.neo_hookean_universal(torch, 10.0, 0.3)
+
+    prob = Universal(mesh, vec=3, dim=3, ele_type="TET4", dirichlet_bc_info=bc)
+    assert prob.cell_path
+    (sol,) = pkg.solver(prob, {"dynamic_relax": {"tol": 1e-8, "nKMat": 1000, "info": False, "info_force": False}})
+    its = prob.last_solve_info["dr_iters"]
+    op = fo.OracleProblem(mesh.points, mesh.cells, 3, fo.Law("neo_hookean", E=10.0, nu=0.3), dirichlet_bc_info=bc,
+                          ele_type="TET4")
+    ref_u, ref_its = fo.dynamic_relax(op, tol=1e-8, nKMat=1000)
+    sol = sol.cpu().numpy().reshape(-1)
+    assert abs(its - ref_its) <= 1, (its, ref_its)
+    assert np.abs(sol - ref_u).max() <= 1e-9 * np.abs(ref_u).max()
