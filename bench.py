@@ -143,6 +143,19 @@ def element_bench(pkg, device):
         e1.record()
         torch.cuda.synchronize()
         hbm, _ = peaks()
+        gmg = None
+        if ele == "TET4":  # the lattice multigrid applies to TET4 boxes
+            lin_mg = {"cg": {"precond": "gmg", "rtol": "adaptive", "atol": 0.0, "mg_lag": 4}}
+            nh_solve(pkg, prob, "mixed", linear=lin_mg)
+            torch.cuda.synchronize()
+            e2, e3 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e2.record()
+            _, infos_mg = nh_solve(pkg, prob, "mixed", linear=lin_mg)
+            e3.record()
+            torch.cuda.synchronize()
+            gmg = {"twist_solve_s": round(e2.elapsed_time(e3) * 1e-3, 4),
+                   "newton_iters": sum(i["newton_iters"] for i in infos_mg),
+                   "krylov_iters": sum(sum(i["krylov_iters"]) for i in infos_mg)}
         out[ele] = {"cells": dv.num_cells, "dofs": nd, "nodes_per_cell": nen, "quad_points": nq, "nnzb": dv.nnzb,
                     "assembly_us": {"fp64": round(t64 * 1e6, 1), "fp32": round(t32 * 1e6, 1)},
                     "assembly_dofs_per_s": {"fp64": round(nd / t64), "fp32": round(nd / t32)},
@@ -150,6 +163,8 @@ def element_bench(pkg, device):
                     "twist_solve_s": round(e0.elapsed_time(e1) * 1e-3, 4),
                     "newton_iters": sum(i["newton_iters"] for i in infos),
                     "krylov_iters": sum(sum(i["krylov_iters"]) for i in infos)}
+        if gmg is not None:
+            out[ele]["multigrid_mixed"] = gmg
         del prob, dv
         torch.cuda.empty_cache()
     return out

@@ -2,8 +2,10 @@
 
 Stands in for the reference's optional AMGX path (solver.py:136-259) on the
 meshes ``box_mesh`` builds (generate_mesh.py:151-189): tensor lattices with
-node (i, j, k) = (i*ny + j)*nz + k.  Other meshes raise
-``NotImplementedError`` when ``precond='gmg'`` is asked for.
+node (i, j, k) = (i*ny + j)*nz + k, whose cells couple each node to lattice
+neighbours only (a 27-point stencil): HEX8 boxes, and the TET4 boxes of
+``box_mesh_gmsh`` (six tetrahedra per lattice cell, the same nodes).  Other
+meshes raise ``NotImplementedError`` when ``precond='gmg'`` is asked for.
 
 The hierarchy coarsens 2:1 per direction (a last odd interval stays one fine
 cell wide) down to a few nodes per direction.  Prolongation is trilinear
@@ -23,10 +25,11 @@ import torch
 from . import _native as nat
 
 
-def lattice_of(points, cells):
+def lattice_of(points, cells=None):
     """Nodes per direction (nx, ny, nz) and the coordinate of each lattice
-    line if the mesh is a box lattice numbered as box_mesh numbers it, else
-    None."""
+    line if the points form a box lattice numbered as box_mesh numbers it
+    (and, when ``cells`` are given, the cells are box_mesh's HEX8 cells),
+    else None."""
     pts = np.asarray(points, dtype=np.float64)
     axes = [np.unique(pts[:, d]) for d in range(3)]
     n = tuple(len(a) for a in axes)
@@ -36,7 +39,7 @@ def lattice_of(points, cells):
     expect = np.stack([axes[0][I], axes[1][J], axes[2][K]], axis=-1).reshape(-1, 3)
     if not np.array_equal(expect, pts):
         return None
-    if not np.array_equal(np.asarray(cells, dtype=np.int64), lattice_cells(n)):
+    if cells is not None and not np.array_equal(np.asarray(cells, dtype=np.int64), lattice_cells(n)):
         return None
     return n, axes
 
@@ -105,11 +108,16 @@ class Multigrid:
     one precision.  ``setup(A)`` forms the coarse operators of the FP64
     operator A; ``solve`` runs the V-cycle-preconditioned CG."""
 
-    def __init__(self, dv, mesh_points, mesh_cells, fp32=False, max_levels=10, dense_coarse=True, nu_fine=0):
+    def __init__(self, dv, mesh_points, mesh_cells=None, fp32=False, max_levels=10, dense_coarse=True, nu_fine=0):
         lat = lattice_of(mesh_points, mesh_cells)
         if lat is None:
             raise NotImplementedError("precond 'gmg' needs a box-lattice mesh numbered as box_mesh numbers it")
         n, axes = lat
+        try:  # the fine operator must couple lattice neighbours only
+            stencil_of(n, dv.row_ptr.cpu().numpy(), dv.col_idx.cpu().numpy())
+        except ValueError as e:
+            raise NotImplementedError(f"precond 'gmg': the mesh's cells couple nodes beyond lattice "
+                                      f"neighbours ({e})") from e
         self.vec, self.fp32 = dv.vec, fp32
         dev, dt = dv.device, (torch.float32 if fp32 else torch.float64)
         self._keep = []

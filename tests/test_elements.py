@@ -174,3 +174,28 @@ def test_oracle_convergence_rates(pkg, ele, rates):
     l2_rate = np.log2(errs[0][0] / errs[1][0])
     h1_rate = np.log2(errs[0][1] / errs[1][1])
     assert abs(l2_rate - rates[0]) < 0.15 and abs(h1_rate - rates[1]) < 0.15, (l2_rate, h1_rate)
+
+
+def test_multigrid_accepts_tet4_lattices_only(pkg):
+    """precond 'gmg' needs lattice nodes in box_mesh numbering and a fine
+    pattern inside the 27-point stencil: TET4 boxes qualify (each node
+    couples to at most 14 lattice neighbours), quadratic types do not."""
+    import ctypes
+    mg = importlib.import_module("jax_fem_b200.multigrid")
+    nat = pkg._native
+    m = element_box(pkg, "TET4", (3, 2, 4))
+    n, _ = mg.lattice_of(m.points)
+    assert n == (4, 3, 5) and mg.lattice_of(m.points, m.cells) is None  # not HEX8 cells
+    cells = np.ascontiguousarray(m.cells, dtype=np.int32)
+    N = len(m.points)
+    rp = np.zeros(N + 1, dtype=np.int32)
+    nnzb = nat.I64(0)
+    nat.check(nat.lib().fem_bsr_pattern_nen(cells.ctypes.data, len(cells), 4, N, rp.ctypes.data, ctypes.byref(nnzb),
+                                            None, 0, None, None), "count")
+    col = np.zeros(nnzb.value, dtype=np.int32)
+    nat.check(nat.lib().fem_bsr_pattern_nen(cells.ctypes.data, len(cells), 4, N, rp.ctypes.data, ctypes.byref(nnzb),
+                                            col.ctypes.data, col.size, None, None), "fill")
+    st = mg.stencil_of(n, rp, col)
+    assert (st >= 0).sum(axis=1).max() == 15 and (st[:, 13] >= 0).all()
+    for ele in ("TET10", "HEX20", "HEX27"):
+        assert mg.lattice_of(element_box(pkg, ele, (2, 2, 2)).points) is None

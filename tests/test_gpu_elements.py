@@ -301,3 +301,28 @@ def test_cell_path_dynamic_relax_matches_oracle(pkg, cuda):
     sol = sol.cpu().numpy().reshape(-1)
     assert abs(its - ref_its) <= 1, (its, ref_its)
     assert np.abs(sol - ref_u).max() <= 1e-9 * np.abs(ref_u).max()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_tet4_multigrid_matches_oracle(pkg, cuda, precision):
+    """The lattice multigrid preconditioner on a TET4 box (Galerkin coarse
+    operators from the TET4 tangent): Newton with gmg CG matches the oracle
+    (1e-8 plain, 1e-6 mixed) in far fewer CG iterations than block-Jacobi."""
+    mesh = element_box(pkg, "TET4", (8, 6, 6))
+    bc = _twist_bc(20.0)
+    prob = _problem(pkg, "TET4", None, pkg.NeoHookean(10.0, 0.3), [], bc=bc, mesh=mesh)
+    its = {}
+    for pc in ("gmg", "block_jacobi"):
+        lin = {"cg": {"precond": pc, "rtol": 1e-10, "atol": 0.0, "maxiter": 20000}}
+        opts = {"newton": {"rel_tol": 1e-10, "tol": 1e-14, "precision": precision, "linear": lin,
+                           "return_info": True}}
+        (sol,), info = pkg.solver(prob, opts)
+        its[pc] = sum(info["krylov_iters"])
+        if pc == "gmg":
+            got = sol.cpu().numpy().reshape(-1)
+    op = fo.OracleProblem(mesh.points, mesh.cells, 3, fo.Law("neo_hookean", E=10.0, nu=0.3), dirichlet_bc_info=bc,
+                          ele_type="TET4")
+    ref = fo.newton_solve(op, rel_tol=1e-12, tol=1e-14)
+    assert np.abs(got - ref).max() <= (1e-8 if precision == "fp64" else 1e-6) * np.abs(ref).max()
+    assert its["gmg"] * 4 < its["block_jacobi"], its
