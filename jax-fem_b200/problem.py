@@ -350,6 +350,11 @@ class Problem:
             fn = nat.lib().fem_assemble_elem_f32 if fp32 else nat.lib().fem_assemble_elem_f64
             nat.check(fn(law.law_id, pr, n, self.vec, dv.nen, wq.numel(), nat.ptr(gref), nat.ptr(wq), *tail),
                       "assemble_elem")
+        if vals is not None and self.fes[0].ele_type in ("TET10", "HEX20", "HEX27"):
+            # the state of this tangent, for p-multigrid's re-assembled coarse operator (pmultigrid.py)
+            if getattr(self, "_tangent_state", None) is None or self._tangent_state.numel() != dofs.numel():
+                self._tangent_state = torch.empty_like(dofs)
+            self._tangent_state.copy_(dofs)
 
     def _flat_dofs(self, sol_list):
         d = self.dev().device

@@ -327,3 +327,32 @@ def test_tet4_multigrid_matches_oracle(pkg, cuda, precision):
     ref = fo.newton_solve(op, rel_tol=1e-12, tol=1e-14)
     assert np.abs(got - ref).max() <= (1e-8 if precision == "fp64" else 1e-6) * np.abs(ref).max()
     assert its["gmg"] * 3 < its["block_jacobi"], its
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("ele,precision", [("TET10", "fp64"), ("HEX27", "fp64"), ("HEX20", "fp64"),
+                                           ("TET10", "mixed")])
+def test_quadratic_pmultigrid_matches_oracle(pkg, cuda, ele, precision):
+    """precond 'gmg' on quadratic cells runs p-multigrid (pmultigrid.py: the
+    linear element on the corner-node lattice, its lattice hierarchy,
+    Chebyshev / block-Jacobi smoothing on the fine level): Newton matches
+    the oracle (1e-8 plain, 1e-6 mixed) in under a third of block-Jacobi's
+    CG iterations (a CPU prototype of the same method: 15 / 19 / 29
+    iterations vs 186 / 278 / 376 for HEX27 / TET10 / HEX20 on 6x4x4 boxes)."""
+    mesh = element_box(pkg, ele, (6, 4, 4))
+    bc = _twist_bc(20.0)
+    prob = _problem(pkg, ele, None, pkg.NeoHookean(10.0, 0.3), [], bc=bc, mesh=mesh)
+    its = {}
+    for pc in ("gmg", "block_jacobi"):
+        lin = {"cg": {"precond": pc, "rtol": 1e-10, "atol": 0.0, "maxiter": 20000}}
+        opts = {"newton": {"rel_tol": 1e-10, "tol": 1e-14, "precision": precision, "linear": lin,
+                           "return_info": True}}
+        (sol,), info = pkg.solver(prob, opts)
+        its[pc] = sum(info["krylov_iters"])
+        if pc == "gmg":
+            got = sol.cpu().numpy().reshape(-1)
+    op = fo.OracleProblem(mesh.points, mesh.cells, 3, fo.Law("neo_hookean", E=10.0, nu=0.3), dirichlet_bc_info=bc,
+                          ele_type=ele)
+    ref = fo.newton_solve(op, rel_tol=1e-12, tol=1e-14)
+    assert np.abs(got - ref).max() <= (1e-8 if precision == "fp64" else 1e-6) * np.abs(ref).max()
+    assert its["gmg"] * 3 < its["block_jacobi"], its
