@@ -150,18 +150,20 @@ class PMultigrid:
         vec, n = self.vec, A.n_brows * self.vec
         blocks = A.vals.view(-1, vec, vec)[A.diag.long()]
         self.dinv = torch.linalg.inv(blocks).contiguous()
-        # largest eigenvalue of D^-1 A by power iteration (x 1.1)
-        g = torch.Generator(device=A.vals.device).manual_seed(0)
-        x = torch.rand(n, dtype=torch.float64, device=A.vals.device, generator=g)
-        y = torch.empty_like(x)
-        lam = 1.0
-        for _ in range(12):
-            x /= x.norm()
-            A.matvec(x, y)
-            z = self._jacobi(y)
-            lam = float(x.dot(z))
-            x = z
-        self.lmax = 1.1 * lam
+        if not fine_only or self.lmax is None:
+            # largest eigenvalue of D^-1 A by power iteration (x 1.1), at full
+            # setups; solves on kept coarse operators keep it too
+            g = torch.Generator(device=A.vals.device).manual_seed(0)
+            x = torch.rand(n, dtype=torch.float64, device=A.vals.device, generator=g)
+            y = torch.empty_like(x)
+            lam = torch.ones((), dtype=torch.float64, device=A.vals.device)
+            for _ in range(12):
+                x /= x.norm()
+                A.matvec(x, y)
+                z = self._jacobi(y)
+                lam = x.dot(z)
+                x = z
+            self.lmax = 1.1 * float(lam)
         if not fine_only:
             state = getattr(self.problem, "_tangent_state", None)
             if state is None:
@@ -177,15 +179,18 @@ class PMultigrid:
         return torch.bmm(self.dinv, r.view(-1, v, 1)).view(-1)
 
     # ---- preconditioner ------------------------------------------------------------
-    def _chebyshev(self, A, b, z, nu, ratio, tmp):
-        """nu Chebyshev steps for A z = b from z (in place)."""
+    def _chebyshev(self, A, b, z, nu, ratio, tmp, zero_start=False):
+        """nu Chebyshev steps for A z = b from z (in place; z = 0 when zero_start)."""
         lmax = self.lmax
         lmin = lmax / ratio
         theta, delta = 0.5 * (lmax + lmin), 0.5 * (lmax - lmin)
         sigma = theta / delta
         rho = 1.0 / sigma
-        A.matvec(z, tmp)
-        r = b - tmp
+        if zero_start:
+            r = b.clone()
+        else:
+            A.matvec(z, tmp)
+            r = b - tmp
         d = self._jacobi(r) / theta
         for k in range(nu):
             z += d
@@ -200,10 +205,10 @@ class PMultigrid:
 
     def apply(self, A, r, z, free, nu, coarse_steps, ratio, tmp):
         z.zero_()
-        self._chebyshev(A, r, z, nu, ratio, tmp)
+        self._chebyshev(A, r, z, nu, ratio, tmp, zero_start=True)
         A.matvec(z, tmp)
         r1 = (r - tmp) * free
-        rc = torch.empty(self.PT.n_brows * self.vec, dtype=torch.float64, device=r.device)
+        rc = self._rc
         self.PT.apply(r1, rc)
         rc *= self._free_c
         if self.fp32:
@@ -221,12 +226,14 @@ class PMultigrid:
         return z
 
     # ---- outer CG ----------------------------------------------------------------
-    def solve(self, A, b, x, rtol, atol=0.0, maxiter=1000, nu=2, coarse_steps=8, ratio=25.0, check_every=1):
-        """Preconditioned CG on A x = b (x: initial guess, in place).  Returns
-        (iterations, relative residual)."""
+    def solve(self, A, b, x, rtol, atol=0.0, maxiter=1000, nu=2, coarse_steps=8, ratio=25.0, check_every=4):
+        """Preconditioned CG on A x = b (x: initial guess, in place).  The
+        scalars stay on the device; the residual is read every
+        ``check_every`` iterations.  Returns (iterations, relative residual)."""
         mask, _ = self.problem.dirichlet_device()
         free = (~mask.bool()).to(torch.float64)
         self._free_c = free[self.corner_dofs].contiguous()
+        self._rc = torch.empty(self.PT.n_brows * self.vec, dtype=torch.float64, device=b.device)
         tmp = torch.empty_like(b)
         A.matvec(x, tmp)
         r = b - tmp
@@ -238,21 +245,25 @@ class PMultigrid:
         z = torch.empty_like(b)
         self.apply(A, r, z, free, nu, coarse_steps, ratio, tmp)
         p = z.clone()
-        rz = float(r.dot(z))
+        rz = r.dot(z)
         q = torch.empty_like(b)
+        pq_min = torch.full((), math.inf, dtype=torch.float64, device=b.device)
         for it in range(1, maxiter + 1):
             A.matvec(p, q)
-            pq = float(p.dot(q))
-            if not (pq > 0.0) or not math.isfinite(pq):
-                raise nat.FEMNativeError(nat.FEM_ERR_BREAKDOWN, f"p-multigrid CG breakdown (p.Ap = {pq})")
+            pq = p.dot(q)
+            torch.minimum(pq_min, pq, out=pq_min)
             alpha = rz / pq
-            x += alpha * p
-            r -= alpha * q
-            rn = float(r.norm())
-            if rn <= target:
-                return it, rn / bn if bn > 0 else rn
+            x.add_(alpha * p)
+            r.sub_(alpha * q)
+            if it % check_every == 0 or it == maxiter:
+                rn = float(r.norm())
+                pqm = float(pq_min)
+                if not (pqm > 0.0) or not math.isfinite(rn):
+                    raise nat.FEMNativeError(nat.FEM_ERR_BREAKDOWN, f"p-multigrid CG breakdown (min p.Ap = {pqm})")
+                if rn <= target:
+                    return it, rn / bn if bn > 0 else rn
             self.apply(A, r, z, free, nu, coarse_steps, ratio, tmp)
-            rz_new = float(r.dot(z))
+            rz_new = r.dot(z)
             p.mul_(rz_new / rz).add_(z)
             rz = rz_new
         raise nat.FEMNativeError(nat.FEM_ERR_NOT_CONVERGED,
