@@ -22,7 +22,7 @@ import math
 import numpy as np
 import pytest
 
-from helpers import element_box, mms_bc, mms_errors, mms_mass_map
+from helpers import element_box, face_fn, mms_bc, mms_errors, mms_mass_map
 from oracle import fem_oracle as fo
 
 TYPES = ["HEX8", "TET4", "TET10", "HEX20", "HEX27"]
@@ -199,3 +199,111 @@ def test_multigrid_accepts_tet4_lattices_only(pkg):
     assert (st >= 0).sum(axis=1).max() == 15 and (st[:, 13] >= 0).all()
     for ele in ("TET10", "HEX20", "HEX27"):
         assert mg.lattice_of(element_box(pkg, ele, (2, 2, 2)).points) is None
+
+
+@pytest.mark.parametrize("ele", ["TET10", "HEX20", "HEX27"])
+def test_pmultigrid_prolongation(pkg, ele):
+    """p-multigrid's prolongation (pmultigrid.coarse_space) reproduces every
+    linear field on all nodes from its corner values, its rows sum to one,
+    and the corner nodes of box meshes form a lattice."""
+    pm = importlib.import_module("jax_fem_b200.pmultigrid")
+    mg = importlib.import_module("jax_fem_b200.multigrid")
+    import scipy.sparse as sp
+    m = element_box(pkg, ele, (3, 2, 2), amp=0.0)
+    corners, cc, (r, c, w) = pm.coarse_space(ele, m.points, np.asarray(m.cells, dtype=np.int64))
+    P = sp.csr_matrix((w, (r, c)), shape=(len(m.points), len(corners)))
+    f = lambda X: 1.0 + 2.0 * X[:, 0] - X[:, 1] + 0.5 * X[:, 2]  # noqa: E731
+    np.testing.assert_allclose(P @ f(m.points[corners]), f(m.points), atol=1e-14)
+    np.testing.assert_allclose(np.asarray(P.sum(axis=1)).ravel(), 1.0, atol=1e-14)
+    assert mg.lattice_of(m.points[corners]) is not None
+    assert cc.shape == (len(m.cells), 4 if ele == "TET10" else 8)
+
+
+@pytest.mark.parametrize("ele", ["TET10", "HEX27"])
+def test_pmultigrid_method_on_oracle_tangents(pkg, ele):
+    """The p-multigrid method of pmultigrid.py -- Chebyshev smoothing in the
+    3x3 block-Jacobi-scaled operator (degree 2, [lmax/25, lmax]), the
+    prolongation of coarse_space, the linear element re-discretised on the
+    corner nodes (an exact coarse solve here), Dirichlet dofs projected out
+    -- restated with scipy on the oracle's eliminated linear-elastic
+    tangent: PCG reaches 1e-10 in under a fifth of block-Jacobi PCG's
+    iterations, with the same solution."""
+    import scipy.sparse as sp
+    import scipy.sparse.linalg as spla
+    pm = importlib.import_module("jax_fem_b200.pmultigrid")
+    m = element_box(pkg, ele, (4, 3, 3))
+    bc = [[face_fn(0, 0.0)] * 3, [0, 1, 2], [lambda p: 0.0] * 3]
+    law = fo.Law("linear", E=70e3, nu=0.3)
+    op = fo.OracleProblem(m.points, m.cells, 3, law, dirichlet_bc_info=bc, ele_type=ele)
+    op.newton_update(np.zeros(op.ndofs))
+    K = op.assemble_global().tocsr()
+    free = np.ones(op.ndofs)
+    free[op.bc_rows()] = 0.0
+    A = (sp.diags(free) @ K @ sp.diags(free) + sp.diags(1.0 - free)).tocsr()
+    corners, cc, (r, c, w) = pm.coarse_space(ele, m.points, np.asarray(m.cells, dtype=np.int64))
+    lin = "TET4" if ele == "TET10" else "HEX8"
+    opc = fo.OracleProblem(m.points[corners], cc, 3, law, ele_type=lin)
+    opc.newton_update(np.zeros(opc.ndofs))
+    cd = (corners[:, None] * 3 + np.arange(3)).reshape(-1)
+    fc = free[cd]
+    Ac = (sp.diags(fc) @ opc.assemble_global() @ sp.diags(fc) + sp.diags(1.0 - fc)).tocsc()
+    P = sp.kron(sp.csr_matrix((w, (r, c)), shape=(len(m.points), len(corners))), sp.eye(3)).tocsr()
+    n = op.ndofs
+    D = np.stack([A[3 * i:3 * i + 3, 3 * i:3 * i + 3].toarray() for i in range(n // 3)])
+    Dinv = np.linalg.inv(D)
+    jac = lambda v: np.einsum("nij,nj->ni", Dinv, v.reshape(-1, 3)).reshape(-1)  # noqa: E731
+    x = np.random.default_rng(0).random(n)
+    for _ in range(12):
+        x /= np.linalg.norm(x)
+        z = jac(A @ x)
+        lam, x = x @ z, z
+    lmax, ratio, nu = 1.1 * lam, 25.0, 2
+
+    def cheb(b, z):
+        lmin = lmax / ratio
+        th, de = 0.5 * (lmax + lmin), 0.5 * (lmax - lmin)
+        sig = th / de
+        rho = 1.0 / sig
+        rr = b - A @ z
+        d = jac(rr) / th
+        for k in range(nu):
+            z = z + d
+            if k == nu - 1:
+                break
+            rr = rr - A @ d
+            rn = 1.0 / (2.0 * sig - rho)
+            d = rn * rho * d + 2.0 * rn / de * jac(rr)
+            rho = rn
+        return z
+
+    lu = spla.splu(Ac)
+
+    def pmg(rv):
+        z = cheb(rv, np.zeros(n))
+        zc = lu.solve((P.T @ ((rv - A @ z) * free)) * fc) * fc
+        z = z + (P @ zc) * free
+        return cheb(rv, z) * free
+
+    def pcg(M, b):
+        x = np.zeros(n)
+        rv = b.copy()
+        z = M(rv)
+        p = z.copy()
+        rz = rv @ z
+        for it in range(1, 5000):
+            q = A @ p
+            a = rz / (p @ q)
+            x += a * p
+            rv -= a * q
+            if np.linalg.norm(rv) <= 1e-10 * np.linalg.norm(b):
+                return x, it
+            z = M(rv)
+            rz, rz_old = rv @ z, rz
+            p = z + rz / rz_old * p
+        raise AssertionError("no convergence")
+
+    b = np.random.default_rng(1).normal(size=n) * free
+    x1, it_pmg = pcg(pmg, b)
+    x2, it_bj = pcg(lambda v: jac(v) * free + v * (1.0 - free), b)
+    assert it_pmg * 5 < it_bj, (it_pmg, it_bj)
+    np.testing.assert_allclose(x1, x2, rtol=0, atol=1e-8 * np.abs(x2).max())
