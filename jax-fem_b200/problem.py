@@ -262,8 +262,11 @@ class Problem:
         key = tuple(fe.bc_version for fe in self.fes)
         if self._bc_cache is None or self._bc_cache[0] != key:
             arrays = [fe.dirichlet_arrays() for fe in self.fes]
-            mask = np.concatenate([a[0] for a in arrays])
-            vals = np.concatenate([a[1] for a in arrays])
+            if len(arrays) == 1:  # one variable: no host copy
+                mask, vals = arrays[0]
+            else:
+                mask = np.concatenate([a[0] for a in arrays])
+                vals = np.concatenate([a[1] for a in arrays])
             d = self.dev().device
             self._bc_cache = (key, torch.from_numpy(mask).to(d), torch.from_numpy(vals).to(d))
         return self._bc_cache[1], self._bc_cache[2]
