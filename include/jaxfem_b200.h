@@ -275,7 +275,9 @@ FEM_API int fem_param_vjp_f64(int law, const double* h_params, int n_params, int
                       void* stream);
 
 /* ---- block-CSR operators ------------------------------------------------
- * Replace the BCOO mat-vec inside jax.scipy bicgstab (solver.py:63-92). */
+ * Replace the BCOO mat-vec inside jax.scipy bicgstab (solver.py:63-92).
+ * y (n_brows*vec) = A x; x is read only at the column indices, so A may be
+ * rectangular (p-multigrid's transfers between node sets). */
 FEM_API int fem_bsr_spmv_f64(int vec, int64_t n_brows, const int32_t* d_row_ptr, const int32_t* d_col_idx,
                      const double* d_vals, const double* d_x, double* d_y, void* stream);
 FEM_API int fem_bsr_spmv_f32(int vec, int64_t n_brows, const int32_t* d_row_ptr, const int32_t* d_col_idx,
