@@ -307,3 +307,68 @@ def test_pmultigrid_method_on_oracle_tangents(pkg, ele):
     x2, it_bj = pcg(lambda v: jac(v) * free + v * (1.0 - free), b)
     assert it_pmg * 5 < it_bj, (it_pmg, it_bj)
     np.testing.assert_allclose(x1, x2, rtol=0, atol=1e-8 * np.abs(x2).max())
+
+
+def test_pmultigrid_solver_code_on_cpu(pkg):
+    """PMultigrid's own code -- setup (block-Jacobi inverse, power
+    iteration), the Chebyshev smoother, the two-level apply with Dirichlet
+    projection and the device-scalar CG -- run on CPU tensors with stand-ins
+    for its library calls (operator and transfer products through scipy, an
+    exact coarse solve for the V-cycle): on the oracle's eliminated TET10
+    linear-elastic tangent it converges to the direct solution (1e-8) in
+    under a fifth of block-Jacobi PCG's iterations (counted by scipy)."""
+    import types
+
+    import scipy.sparse as sp
+    import scipy.sparse.linalg as spla
+    import torch
+    pm = importlib.import_module("jax_fem_b200.pmultigrid")
+    ele = "TET10"
+    m = element_box(pkg, ele, (4, 3, 3))
+    bc = [[face_fn(0, 0.0)] * 3, [0, 1, 2], [lambda p: 0.0] * 3]
+    law = fo.Law("linear", E=70e3, nu=0.3)
+    op = fo.OracleProblem(m.points, m.cells, 3, law, dirichlet_bc_info=bc, ele_type=ele)
+    op.newton_update(np.zeros(op.ndofs))
+    free = np.ones(op.ndofs)
+    free[op.bc_rows()] = 0.0
+    A = (sp.diags(free) @ op.assemble_global() @ sp.diags(free) + sp.diags(1.0 - free)).tocsr()
+    corners, cc, (r, c, w) = pm.coarse_space(ele, m.points, np.asarray(m.cells, dtype=np.int64))
+    opc = fo.OracleProblem(m.points[corners], cc, 3, law, ele_type="TET4")
+    opc.newton_update(np.zeros(opc.ndofs))
+    cd = (corners[:, None] * 3 + np.arange(3)).reshape(-1)
+    fc = free[cd]
+    lu = spla.splu((sp.diags(fc) @ opc.assemble_global() @ sp.diags(fc) + sp.diags(1.0 - fc)).tocsc())
+    P = sp.kron(sp.csr_matrix((w, (r, c)), shape=(len(m.points), len(corners))), sp.eye(3)).tocsr()
+    n = op.ndofs
+    Ab = A.tobsr(blocksize=(3, 3))
+    Ab.sort_indices()
+    diag = np.array([Ab.indptr[i] + np.searchsorted(Ab.indices[Ab.indptr[i]:Ab.indptr[i + 1]], i)
+                     for i in range(n // 3)])
+
+    def product(M):
+        return lambda x, y: y.copy_(torch.from_numpy(M @ x.numpy()))
+
+    Aop = types.SimpleNamespace(vals=torch.from_numpy(Ab.data.reshape(-1).copy()), diag=torch.from_numpy(diag),
+                                n_brows=n // 3, vec=3, matvec=product(A))
+    g = pm.PMultigrid.__new__(pm.PMultigrid)
+    g.vec, g.fp32, g.lmax, g.dinv = 3, False, None, None
+    g.corner_dofs = torch.from_numpy(cd)
+    g.P = types.SimpleNamespace(n_brows=len(m.points), apply=product(P))
+    g.PT = types.SimpleNamespace(n_brows=len(corners), apply=product(P.T.tocsr()))
+    g.mg = types.SimpleNamespace(vcycle=lambda rhs, z, **kw: z.copy_(torch.from_numpy(lu.solve(rhs.numpy()))))
+    mask = torch.from_numpy((1.0 - free).astype(np.uint8))
+    g.problem = types.SimpleNamespace(dirichlet_device=lambda: (mask, torch.zeros(n, dtype=torch.float64)))
+    g.setup(Aop, fine_only=True)
+    b = np.random.default_rng(1).normal(size=n) * free
+    x = torch.zeros(n, dtype=torch.float64)
+    its, rel = g.solve(Aop, torch.from_numpy(b), x, rtol=1e-10, maxiter=500)
+    ref = spla.spsolve(A.tocsc(), b)
+    assert rel <= 1e-10
+    np.testing.assert_allclose(x.numpy(), ref, rtol=0, atol=1e-8 * np.abs(ref).max())
+    bj = []
+    D = np.stack([A[3 * i:3 * i + 3, 3 * i:3 * i + 3].toarray() for i in range(n // 3)])
+    Dinv = np.linalg.inv(D)
+    spla.cg(A, b, rtol=1e-10, atol=0.0, maxiter=20000,
+            M=spla.LinearOperator((n, n), lambda v: np.einsum("nij,nj->ni", Dinv, v.reshape(-1, 3)).reshape(-1)),
+            callback=lambda xk: bj.append(1))
+    assert its * 5 < len(bj), (its, len(bj))
