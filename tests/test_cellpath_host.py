@@ -169,3 +169,21 @@ def test_param_vjp_matches_complex_step_on_cpu(pkg):
         r = oracle.cell_kernel(c, dofs[idx[c]].astype(np.complex128), [cs])
         ref[c] = -np.imag(r) @ lam[idx[c]] / 1e-30
     np.testing.assert_allclose(g.numpy(), ref, rtol=0, atol=1e-12 * np.abs(ref).max())
+
+
+def test_ad_wrapper_rejects_differentiable_surface_variables(pkg):
+    """Gradients flow through internal_vars only: a set_params that puts
+    parameter-dependent tensors into internal_vars_surfaces is refused
+    before any solve, instead of returning a silently partial gradient."""
+    import torch
+    m10, m4 = thermo_meshes(pkg)
+    p, _, _, _ = thermo_problem(pkg, m10, m4)
+
+    def set_params(params):
+        p.internal_vars = [params]
+        p.internal_vars_surfaces = [[params[:2] * 1.0]]
+
+    p.set_params = set_params
+    fwd = pkg.ad_wrapper(p, {}, {})
+    with pytest.raises(NotImplementedError):
+        fwd(torch.ones(p.num_cells, dtype=torch.float64, requires_grad=True))
