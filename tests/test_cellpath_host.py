@@ -187,3 +187,25 @@ def test_ad_wrapper_rejects_differentiable_surface_variables(pkg):
     fwd = pkg.ad_wrapper(p, {}, {})
     with pytest.raises(NotImplementedError):
         fwd(torch.ones(p.num_cells, dtype=torch.float64, requires_grad=True))
+
+
+def test_registered_law_on_the_cell_path_is_refused(pkg):
+    """A registered law (a descriptor of the CUDA kernels) cannot serve as the
+    tensor map of a cell-kernel problem; the error says so."""
+    import importlib
+
+    import torch
+    cp = importlib.import_module("jax_fem_b200.cellpath")
+    mesh = perturbed_box(pkg, (1, 1, 1))
+
+    class Mixed(pkg.Problem):
+        def get_tensor_map(self):
+            return pkg.NeoHookean(10.0, 0.3)
+
+        def get_universal_kernel(self):
+            return lambda *a: 0.0
+
+    prob = Mixed(mesh, vec=3, dim=3)
+    assert prob.cell_path
+    with pytest.raises(NotImplementedError, match="registered law"):
+        cp.CellPath(prob, torch.device("cpu"))._kernels()
