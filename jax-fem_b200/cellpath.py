@@ -145,10 +145,8 @@ class CellPath:
         sv0 = fe0.shape_vals_t
         tm = p.get_tensor_map() if hasattr(p, "get_tensor_map") else None
         from .laws import Law
-        if isinstance(tm, Law):
-            raise NotImplementedError(
-                f"{type(tm).__name__} is a registered law for the CUDA cell kernels (one variable, no universal "
-                "kernel); on the cell-kernel path the tensor map is a torch function of (u_grad, *internal_vars)")
+        if isinstance(tm, Law):  # a registered law: its torch form (J2 has none)
+            tm = tm.torch_map()
         mm = p.get_mass_map() if hasattr(p, "get_mass_map") else None
         uk = p.get_universal_kernel() if hasattr(p, "get_universal_kernel") else None
         pad = nd - n0 * v0

@@ -31,11 +31,21 @@ class Law:
     def params(self):
         return []
 
+    def torch_map(self):
+        """The law as a torch tensor map ``P(u_grad, *ivars at a point)`` for
+        the cell-kernel path (problem.py:189-214 form), where the CUDA
+        kernels do not apply (several variables, universal kernels,
+        u-dependent loads)."""
+        raise NotImplementedError(f"{type(self).__name__} has no torch form for the cell-kernel path")
+
 
 class Laplace(Law):
     """Tensor map P = grad u (the linear Poisson test, test_linear_poisson.py:15-17)."""
     law_id = nat.LAW_LAPLACE
     vec = None  # any vec
+
+    def torch_map(self):
+        return lambda u_grad, *ivars: u_grad
 
 
 class LinearElastic(Law):
@@ -48,6 +58,23 @@ class LinearElastic(Law):
     def params(self):
         return [self.E, self.nu]
 
+    def torch_map(self):
+        return _elastic_map(self.E, self.nu)
+
+
+def _elastic_map(E, nu):
+    mu = E / (2.0 * (1.0 + nu))
+    lm = E * nu / ((1.0 + nu) * (1.0 - 2.0 * nu))
+
+    def stress(u_grad, scale=None):
+        import torch
+        eps = 0.5 * (u_grad + u_grad.transpose(-1, -2))
+        sig = lm * torch.diagonal(eps, dim1=-2, dim2=-1).sum(-1)[..., None, None] * torch.eye(
+            3, dtype=u_grad.dtype, device=u_grad.device) + 2.0 * mu * eps
+        return sig if scale is None else scale * sig
+
+    return stress
+
 
 class SIMPElastic(Law):
     """SIMP-penalised linear elasticity (top_opt/fem_model.py:67-80 in the reference)."""
@@ -58,6 +85,15 @@ class SIMPElastic(Law):
 
     def params(self):
         return [self.E0, self.Emin, self.nu, self.penal]
+
+    def torch_map(self):
+        unit = _elastic_map(1.0, self.nu)
+        E0, Emin, p = self.E0, self.Emin, self.penal
+
+        def stress(u_grad, theta):
+            return unit(u_grad, (Emin + (E0 - Emin) * theta.reshape(()) ** p))
+
+        return stress
 
 
 class NeoHookean(Law):
@@ -70,6 +106,26 @@ class NeoHookean(Law):
 
     def params(self):
         return [self.E, self.nu]
+
+    def torch_map(self):
+        mu = self.E / (2.0 * (1.0 + self.nu))
+        kappa = self.E / (3.0 * (1.0 - 2.0 * self.nu))
+
+        def stress(u_grad, scale=None):
+            import torch
+            F = u_grad + torch.eye(3, dtype=u_grad.dtype, device=u_grad.device)
+            # cofactor matrix (J F^-T) and J by cofactor expansion
+            c0 = torch.linalg.cross(F[1], F[2])
+            c1 = torch.linalg.cross(F[2], F[0])
+            c2 = torch.linalg.cross(F[0], F[1])
+            cof = torch.stack([c0, c1, c2])
+            J = (F[0] * c0).sum()
+            H = cof / J
+            I1 = (F * F).sum()
+            P = mu * J ** (-2.0 / 3.0) * (F - I1 / 3.0 * H) + kappa * J * (J - 1.0) * H
+            return P if scale is None else scale.reshape(()) * P
+
+        return stress
 
 
 class J2Plasticity(Law):

@@ -189,23 +189,45 @@ def test_ad_wrapper_rejects_differentiable_surface_variables(pkg):
         fwd(torch.ones(p.num_cells, dtype=torch.float64, requires_grad=True))
 
 
-def test_registered_law_on_the_cell_path_is_refused(pkg):
-    """A registered law (a descriptor of the CUDA kernels) cannot serve as the
-    tensor map of a cell-kernel problem; the error says so."""
+def test_registered_laws_on_the_cell_path(pkg):
+    """On the cell-kernel path a registered law runs as its torch form
+    (Law.torch_map): Neo-Hookean with a u-dependent load and SIMP with theta
+    per point give the oracle's per-cell residuals and complex-step
+    Jacobians (1e-12, CPU tensors); J2 has no torch form and is refused."""
     import importlib
 
     import torch
     cp = importlib.import_module("jax_fem_b200.cellpath")
-    mesh = perturbed_box(pkg, (1, 1, 1))
-
-    class Mixed(pkg.Problem):
-        def get_tensor_map(self):
-            return pkg.NeoHookean(10.0, 0.3)
-
-        def get_universal_kernel(self):
-            return lambda *a: 0.0
-
-    prob = Mixed(mesh, vec=3, dim=3)
-    assert prob.cell_path
-    with pytest.raises(NotImplementedError, match="registered law"):
-        cp.CellPath(prob, torch.device("cpu"))._kernels()
+    mesh = perturbed_box(pkg, (2, 2, 1), seed=3)
+    C = len(mesh.cells)
+    rng = np.random.default_rng(9)
+    theta = rng.uniform(0.2, 1.0, size=(C, 8))
+    cases = [
+        (pkg.NeoHookean(10.0, 0.3), "get_mass_map", lambda u, x: 0.5 * u ** 3,
+         lambda ug: fo.stress_neo_hookean(ug, 10.0, 0.3), None, 0.05),
+        (pkg.SIMPElastic(70e3, 70.0, 0.3, 3.0), "get_universal_kernel", lambda *a: 0.0,
+         lambda ug, th: fo.stress_simp(ug, th, 70e3, 70.0, 0.3, 3.0), theta, 2e-3),
+    ]
+    for law, hook, extra, np_map, iv, scale in cases:
+        hooks = {"get_tensor_map": (lambda law: lambda self: law)(law),
+                 hook: (lambda e: lambda self: e)(extra)}
+        prob = type("P", (pkg.Problem,), hooks)(mesh, vec=3, dim=3)
+        assert prob.cell_path
+        ivs = [torch.tensor(iv)] if iv is not None else []
+        path = cp.CellPath(prob, torch.device("cpu"))
+        dofs = rng.normal(0, scale, size=prob.num_total_dofs_all_vars)
+        idx = path.sys.cell_dofs_long
+        jac, r = path._kernels()[2](torch.tensor(dofs)[idx], path.x, path.shape_grads, path.JxW,
+                                    path.v_grads_JxW, *ivs)
+        kp = fo.KernelProblem([dict(points=mesh.points, cells=mesh.cells, vec=3)], tensor_map=np_map,
+                              mass_map=extra if hook == "get_mass_map" else None,
+                              internal_vars=[iv] if iv is not None else [])
+        for c, (oidx, k) in enumerate(kp._items()):
+            ref = k(dofs[oidx])
+            np.testing.assert_allclose(r[c].numpy(), ref, rtol=0, atol=1e-12 * max(1.0, np.abs(ref).max()))
+            up = dofs[oidx].astype(np.complex128)
+            up[5] += 1e-30j
+            col = np.imag(k(up)) / 1e-30
+            np.testing.assert_allclose(jac[c][:, 5].numpy(), col, rtol=0, atol=1e-10 * max(1.0, np.abs(col).max()))
+    with pytest.raises(NotImplementedError, match="torch form"):
+        pkg.J2Plasticity(70e3, 0.3, 250.0).torch_map()
