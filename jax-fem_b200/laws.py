@@ -139,6 +139,33 @@ class J2Plasticity(Law):
     def params(self):
         return [self.E, self.nu, self.sigma_y, self.H]
 
+    def torch_map(self):
+        """The radial return as a torch tensor map of (u_grad, sigma_old,
+        eps_old, alpha_old): the plastic branch chosen with torch.where, the
+        deviatoric norm's square root guarded at zero, so that forward-mode
+        derivatives stay finite on both branches."""
+        E, nu, sy0, Hh = self.E, self.nu, self.sigma_y, self.H
+        mu = E / (2.0 * (1.0 + nu))
+        lm = E * nu / ((1.0 + nu) * (1.0 - 2.0 * nu))
+
+        def stress(u_grad, sigma_old, eps_old, alpha_old=None):
+            import torch
+            I = torch.eye(3, dtype=u_grad.dtype, device=u_grad.device)  # noqa: E741
+            eps = 0.5 * (u_grad + u_grad.T)
+            de = eps - eps_old.reshape(3, 3)
+            st = lm * torch.trace(de) * I + 2.0 * mu * de + sigma_old.reshape(3, 3)
+            s = st - torch.trace(st) / 3.0 * I
+            ss = 1.5 * (s * s).sum()
+            pos = ss > 0.0
+            q = torch.where(pos, torch.sqrt(torch.where(pos, ss, torch.ones_like(ss))), torch.zeros_like(ss))
+            a = alpha_old.reshape(()) if alpha_old is not None else torch.zeros_like(ss)
+            f = q - (sy0 + Hh * a)
+            dg = torch.where(f > 0.0, f, torch.zeros_like(f)) / (3.0 * mu + Hh)
+            qs = torch.where(pos, q, torch.ones_like(q))
+            return st - torch.where(pos, 3.0 * mu * dg / qs, torch.zeros_like(q)) * s
+
+        return stress
+
 
 def _probe(fn, vec, dim, rng):
     x = rng.standard_normal((vec, dim))

@@ -192,8 +192,8 @@ def test_ad_wrapper_rejects_differentiable_surface_variables(pkg):
 def test_registered_laws_on_the_cell_path(pkg):
     """On the cell-kernel path a registered law runs as its torch form
     (Law.torch_map): Neo-Hookean with a u-dependent load and SIMP with theta
-    per point give the oracle's per-cell residuals and complex-step
-    Jacobians (1e-12, CPU tensors); J2 has no torch form and is refused."""
+    per point, and J2 with hardening from a yielding prior state, give the
+    oracle's per-cell residuals and complex-step Jacobians (CPU tensors)."""
     import importlib
 
     import torch
@@ -229,5 +229,29 @@ def test_registered_laws_on_the_cell_path(pkg):
             up[5] += 1e-30j
             col = np.imag(k(up)) / 1e-30
             np.testing.assert_allclose(jac[c][:, 5].numpy(), col, rtol=0, atol=1e-10 * max(1.0, np.abs(col).max()))
+    # J2 with hardening: a random prior state with most points yielding
+    so = rng.normal(0, 150.0, size=(C, 8, 3, 3))
+    so = 0.5 * (so + np.swapaxes(so, -1, -2))
+    eo = rng.normal(0, 2e-3, size=(C, 8, 3, 3))
+    eo = 0.5 * (eo + np.swapaxes(eo, -1, -2))
+    ao = rng.uniform(0, 0.01, size=(C, 8))
+    law = pkg.J2Plasticity(70e3, 0.3, 250.0, 700.0)
+    prob = type("P", (pkg.Problem,), {"get_tensor_map": lambda self: law,
+                                      "get_universal_kernel": lambda self: (lambda *a: 0.0)})(mesh, vec=3, dim=3)
+    path = cp.CellPath(prob, torch.device("cpu"))
+    dofs = rng.normal(0, 6e-4, size=prob.num_total_dofs_all_vars)
+    idx = path.sys.cell_dofs_long
+    jac, r = path._kernels()[2](torch.tensor(dofs)[idx], path.x, path.shape_grads, path.JxW, path.v_grads_JxW,
+                                torch.tensor(so), torch.tensor(eo), torch.tensor(ao))
+    np_j2 = lambda ug, s_, e_, a_: fo.j2_return_map(ug, s_, e_, a_, 70e3, 0.3, 250.0, 700.0)[0]  # noqa: E731
+    kp = fo.KernelProblem([dict(points=mesh.points, cells=mesh.cells, vec=3)], tensor_map=np_j2,
+                          internal_vars=[so, eo, ao])
+    for c, (oidx, k) in enumerate(kp._items()):
+        ref = k(dofs[oidx])
+        np.testing.assert_allclose(r[c].numpy(), ref, rtol=0, atol=1e-11 * np.abs(ref).max())
+        up = dofs[oidx].astype(np.complex128)
+        up[7] += 1e-30j
+        col = np.imag(k(up)) / 1e-30
+        np.testing.assert_allclose(jac[c][:, 7].numpy(), col, rtol=0, atol=1e-9 * max(1.0, np.abs(col).max()))
     with pytest.raises(NotImplementedError, match="torch form"):
-        pkg.J2Plasticity(70e3, 0.3, 250.0).torch_map()
+        pkg.laws.Law().torch_map()
