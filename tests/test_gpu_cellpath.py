@@ -146,3 +146,29 @@ def test_cell_path_adjoint_matches_finite_differences(pkg, cuda):
             vals.append(objective(fwd(torch.tensor(cc, device=cuda))).item())
         fd = (vals[0] - vals[1]) / (2 * h)
         assert abs(fd - g[k]) <= 1e-6 * max(abs(g).max(), 1e-12), (k, fd, g[k])
+
+
+@pytest.mark.gpu
+def test_registered_law_with_u_dependent_load_matches_oracle(pkg, cuda):
+    """A registered law with a u-dependent body load goes to the cell-kernel
+    path as its torch form: Newton on a jittered HEX8 box vs the oracle's
+    KernelProblem with the oracle's Neo-Hookean stress (1e-9)."""
+    mesh = perturbed_box(pkg, (3, 2, 2), seed=11)
+    bc = [[face_fn(0, 0.0)] * 3 + [face_fn(0, 1.0)], [0, 1, 2, 0], [lambda p: 0.0] * 3 + [lambda p: 0.05]]
+
+    class NHReaction(pkg.Problem):
+        def get_tensor_map(self):
+            return pkg.NeoHookean(10.0, 0.3)
+
+        def get_mass_map(self):
+            return lambda u, x: 2.0 * u ** 3
+
+    prob = NHReaction(mesh, vec=3, dim=3, dirichlet_bc_info=bc)
+    assert prob.cell_path
+    sol = pkg.solver(prob, {"newton": {"rel_tol": 1e-11, "tol": 1e-14, "linear": LIN_BICG}})[0]
+    kp = fo.KernelProblem([dict(points=mesh.points, cells=mesh.cells, vec=3, dirichlet=bc)],
+                          tensor_map=lambda ug: fo.stress_neo_hookean(ug, 10.0, 0.3),
+                          mass_map=lambda u, x: 2.0 * u ** 3)
+    ref = kp.newton()
+    got = sol.cpu().numpy().reshape(-1)
+    assert np.abs(got - ref).max() <= 1e-9 * np.abs(ref).max()
