@@ -61,6 +61,14 @@ def box_mesh(Nx, Ny, Nz, domain_x, domain_y, domain_z):
     return _BoxMesh(points, cells)
 
 
+def check_mesh_TET4(points, cells):  # noqa: N802 - the reference's name
+    """Orientation measure of TET4 cells (generate_mesh.py:58-80): the triple
+    product (p1 - p0) x (p2 - p0) . (p3 - p0), positive for the node order
+    the element tables assume."""
+    X = np.asarray(points, dtype=np.float64)[np.asarray(cells)[:, :4]]
+    return np.einsum("ci,ci->c", np.cross(X[:, 1] - X[:, 0], X[:, 2] - X[:, 0]), X[:, 3] - X[:, 0])
+
+
 def get_meshio_cell_type(ele_type):
     """meshio cell type of an element type (generate_mesh.py:83-117)."""
     return MESHIO_CELL_TYPE[check_ele_type(ele_type)]

@@ -371,3 +371,78 @@ def read_mesh(path, ele_type=None):
     if ext == ".inp":
         return read_abaqus(path, ele_type)
     raise NotImplementedError(f"mesh file type '{ext}' (read .vtu, .msh or .inp)")
+
+
+# ---- the reference's small helpers (utils.py:60-180) ---------------------------------
+
+def modify_vtu_file(input_file_path, output_file_path):
+    """Copy a VTU file, declaring VTK XML version 1.0 where it says 2.2 (the
+    form dolfinx writes; utils.py:60-80)."""
+    with open(input_file_path) as f:
+        text = f.read()
+    text = text.replace('<VTKFile type="UnstructuredGrid" version="2.2">',
+                        '<VTKFile type="UnstructuredGrid" version="1.0">')
+    d = os.path.dirname(os.path.abspath(output_file_path))
+    os.makedirs(d, exist_ok=True)
+    with open(output_file_path, "w") as f:
+        f.write(text)
+
+
+def read_abaqus_and_write_vtk(abaqus_file, vtk_file):
+    """Convert an Abaqus .inp mesh to a .vtu file for viewing (utils.py:83-94)."""
+    mesh = read_abaqus(abaqus_file)
+    write_vtu(vtk_file, mesh.points, mesh.cells, ele_type=mesh.ele_type)
+
+
+def json_parse(json_filepath):
+    """Read a JSON configuration file, print it indented and return it (utils.py:97-114)."""
+    import json
+    with open(json_filepath) as f:
+        args = json.load(f)
+    print(json.dumps(args, indent=4))
+    return args
+
+
+def timeit(func):
+    """Decorator that logs how long each call of ``func`` took (utils.py:141-163)."""
+    import functools
+    import logging
+    import time
+
+    @functools.wraps(func)
+    def wrapper(*args, **kwargs):
+        t0 = time.perf_counter()
+        out = func(*args, **kwargs)
+        logging.getLogger("jax_fem_b200").debug(f"Function {func.__name__} took {time.perf_counter() - t0:.4f} seconds")
+        return out
+
+    return wrapper
+
+
+def walltime(txt_dir=None, filename=None):
+    """Decorator factory that logs a call's wall time and, with ``txt_dir``,
+    writes it to ``{txt_dir}/{filename or 'walltime'}_{platform}.txt``
+    (utils.py:166-200); the platform is "cuda" when a device is present."""
+    import functools
+    import logging
+    import time
+
+    def decorate(func):
+        @functools.wraps(func)
+        def wrapper(*args, **kwargs):
+            t0 = time.time()
+            out = func(*args, **kwargs)
+            elapsed = time.time() - t0
+            import torch
+            platform = "cuda" if torch.cuda.is_available() else "cpu"
+            logging.getLogger("jax_fem_b200").info(
+                f"Time elapsed {elapsed} of function {func.__name__} on platform {platform}")
+            if txt_dir is not None:
+                os.makedirs(txt_dir, exist_ok=True)
+                with open(os.path.join(txt_dir, f"{filename or 'walltime'}_{platform}.txt"), "w") as f:
+                    f.write(f"{elapsed}\n")
+            return out
+
+        return wrapper
+
+    return decorate

@@ -12,6 +12,7 @@
   and Abaqus cells come back in VTK order, checked by geometry: every
   edge / face / centre node sits where the cell's corners put it."""
 import base64
+import os
 import struct
 import zlib
 
@@ -259,3 +260,36 @@ def test_abaqus_tet10_and_hex20(io, tmp_path):
         assert got.ele_type == ele
         np.testing.assert_array_equal(got.points[got.cells], m.points[m.cells])
         assert _isoparametric_ok(pkg, got)
+
+
+def test_small_helpers(io, tmp_path, capsys):
+    """modify_vtu_file, read_abaqus_and_write_vtk, json_parse, walltime and
+    check_mesh_TET4 (the reference's utils.py:60-200, generate_mesh.py:58-80)."""
+    import importlib
+    import json
+    pkg, ut = io
+    gm = importlib.import_module("jax_fem_b200.generate_mesh")
+    src = tmp_path / "in.vtu"
+    src.write_text('<?xml version="1.0"?>\n<VTKFile type="UnstructuredGrid" version="2.2">\n</VTKFile>\n')
+    ut.modify_vtu_file(str(src), str(tmp_path / "out" / "o.vtu"))
+    assert 'version="1.0"' in (tmp_path / "out" / "o.vtu").read_text()
+    from helpers import element_box
+    m = element_box(pkg, "TET10", (1, 1, 1))
+    lines = ["*NODE"] + [f"{i + 1}, {float(x)!r}, {float(y)!r}, {float(z)!r}" for i, (x, y, z) in enumerate(m.points)]
+    lines.append("*ELEMENT, TYPE=C3D10")
+    lines += [", ".join(str(v) for v in [k + 1] + [int(c) + 1 for c in cell]) for k, cell in enumerate(m.cells)]
+    (tmp_path / "a.inp").write_text("\n".join(lines) + "\n")
+    ut.read_abaqus_and_write_vtk(str(tmp_path / "a.inp"), str(tmp_path / "a.vtu"))
+    got = ut.read_mesh(str(tmp_path / "a.vtu"))
+    assert got.ele_type == "TET10" and np.array_equal(got.points[got.cells], m.points[m.cells])
+    (tmp_path / "c.json").write_text(json.dumps({"E": 70e3, "nu": 0.3}))
+    assert ut.json_parse(str(tmp_path / "c.json")) == {"E": 70e3, "nu": 0.3}
+    assert '"nu": 0.3' in capsys.readouterr().out
+    timed = ut.walltime(str(tmp_path / "t"), "run")(lambda a: a + 1)
+    assert timed(1) == 2 and any(f.startswith("run_") for f in os.listdir(tmp_path / "t"))
+    assert ut.timeit(lambda: 3)() == 3
+    m4 = element_box(pkg, "TET4", (2, 1, 1))
+    q = gm.check_mesh_TET4(m4.points, m4.cells)
+    assert q.shape == (len(m4.cells),) and (q > 0).all()
+    flipped = m4.cells[:, [0, 2, 1, 3]]
+    assert (gm.check_mesh_TET4(m4.points, flipped) < 0).all()
