@@ -11,13 +11,14 @@ name ``jax_fem_b200`` by ``load_package()`` in the repository root's
 ``__graft_entry__.py`` (a hyphen cannot appear in an import statement).
 """
 from . import _native
-from .generate_mesh import Mesh, box_mesh, box_mesh_gmsh, check_mesh_TET4, get_meshio_cell_type
+from .generate_mesh import Mesh, box_mesh, box_mesh_gmsh, check_mesh_TET4, get_meshio_cell_type, rectangle_mesh
 from .laws import J2Plasticity, Laplace, LinearElastic, NeoHookean, SIMPElastic
 from .problem import BSRMatrix, Problem, compliance
 from .solver import J2YieldSensitivity, ad_wrapper, get_A, get_q_vec, j2_reaction, solver, stress_divergence
 from .utils import read_mesh, save_sol
 
-__all__ = ["Mesh", "box_mesh", "box_mesh_gmsh", "check_mesh_TET4", "get_meshio_cell_type", "Problem", "solver", "ad_wrapper", "get_A",
+__all__ = ["Mesh", "box_mesh", "box_mesh_gmsh", "check_mesh_TET4", "get_meshio_cell_type", "rectangle_mesh",
+           "Problem", "solver", "ad_wrapper", "get_A",
            "BSRMatrix", "compliance", "Laplace", "LinearElastic", "SIMPElastic", "NeoHookean",
            "J2Plasticity", "J2YieldSensitivity", "j2_reaction", "stress_divergence", "save_sol", "read_mesh",
            "get_q_vec",

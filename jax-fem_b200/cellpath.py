@@ -15,16 +15,20 @@ Newton, the Krylov solvers and the outer loops are those of the law path.
 
 Kernel signatures are the reference's, with torch tensors:
 
-- universal kernel (per cell): ``(cell_sol_flat (nd,), x (nq, 3),
-  cell_shape_grads (nq, sum nen, 3), cell_JxW (num_vars, nq),
-  cell_v_grads_JxW (nq, sum nen, 1, 3), *cell_internal_vars) -> (nd,)``;
+- universal kernel (per cell): ``(cell_sol_flat (nd,), x (nq, dim),
+  cell_shape_grads (nq, sum nen, dim), cell_JxW (num_vars, nq),
+  cell_v_grads_JxW (nq, sum nen, 1, dim), *cell_internal_vars) -> (nd,)``;
 - surface universal kernel (per selected face): ``(cell_sol_flat,
-  x (nfq, 3), face_shape_vals (nfq, sum nen), face_shape_grads
-  (nfq, sum nen, 3), face_nanson_scale (num_vars, nfq),
+  x (nfq, dim), face_shape_vals (nfq, sum nen), face_shape_grads
+  (nfq, sum nen, dim), face_nanson_scale (num_vars, nfq),
   *cell_internal_vars_surface) -> (nd,)``;
-- ``tensor_map(u_grad (vec, 3), *ivars)``, ``mass_map(u (vec,), x (3,),
+- ``tensor_map(u_grad (vec, dim), *ivars)``, ``mass_map(u (vec,), x (dim,),
   *ivars)``, ``surface_map(u, x, *ivars_surface)`` per quadrature point,
   on the first variable (problem.py:189-259).
+
+dim is 3, or 2 for the 2D element types (QUAD4, QUAD8, TRI3, TRI6), which
+always run here.  A registered law on a 2D problem is its plane-strain
+form (``laws.plane_strain``).
 
 Inside torch kernels the element tables are ``fe.shape_vals_t`` and
 ``fe.face_shape_vals_t`` (torch copies of ``shape_vals`` and
@@ -82,7 +86,7 @@ class CellSystem:
 
 
 def _geometry(fe, points=None):
-    """Physical shape gradients (C,Q,nen,3) and JxW (C,Q) (fe.py:112-141)."""
+    """Physical shape gradients (C,Q,nen,dim) and JxW (C,Q) (fe.py:112-141)."""
     X = (fe.points if points is None else points)[fe.cells]
     J = np.einsum("cai,qaj->cqij", X, fe.shape_grads_ref)
     g = np.einsum("qaj,cqjk->cqak", fe.shape_grads_ref, np.linalg.inv(J))
@@ -110,10 +114,10 @@ class CellPath:
         t = lambda a: torch.as_tensor(np.ascontiguousarray(a), dtype=torch.float64, device=device)  # noqa: E731
         # initialize_geometric_quantities (problem.py:130-190)
         grads, jxws = zip(*[_geometry(fe) for fe in fes])
-        self.shape_grads = t(np.concatenate(grads, axis=2))                      # (C,Q,sum nen,3)
+        self.shape_grads = t(np.concatenate(grads, axis=2))                      # (C,Q,sum nen,dim)
         self.JxW = t(np.stack(jxws, axis=1))                                      # (C,V,Q)
         self.v_grads_JxW = t(np.concatenate([g[:, :, :, None, :] * w[:, :, None, None, None]
-                                              for g, w in zip(grads, jxws)], axis=2))  # (C,Q,sum nen,1,3)
+                                              for g, w in zip(grads, jxws)], axis=2))  # (C,Q,sum nen,1,dim)
         self.x = t(np.einsum("qa,cai->cqi", fes[0].shape_vals, fes[0].points[fes[0].cells]))
         for fe in fes:
             fe.shape_vals_t = t(fe.shape_vals)
@@ -144,9 +148,13 @@ class CellPath:
         n0, v0, nd = fe0.num_nodes, fe0.vec, self.nd
         sv0 = fe0.shape_vals_t
         tm = p.get_tensor_map() if hasattr(p, "get_tensor_map") else None
-        from .laws import Law
-        if isinstance(tm, Law):  # a registered law: its torch form (J2 has none)
-            tm = tm.torch_map()
+        from .laws import Laplace, Law, plane_strain
+        if isinstance(tm, Law):  # a registered law: its torch form
+            if tm.vec is not None and v0 != p.dim:
+                raise NotImplementedError(f"{type(tm).__name__} needs vec={p.dim} on a {p.dim}D problem, got {v0}")
+            law, tm = tm, tm.torch_map()
+            if p.dim == 2 and not isinstance(law, Laplace):
+                tm = plane_strain(tm)
         mm = p.get_mass_map() if hasattr(p, "get_mass_map") else None
         uk = p.get_universal_kernel() if hasattr(p, "get_universal_kernel") else None
         pad = nd - n0 * v0
@@ -260,6 +268,26 @@ class CellPath:
             fn = nat.lib().fem_bsr_bc_diag_f32 if fp32 else nat.lib().fem_bsr_bc_diag_f64
             nat.check(fn(1, sys_.num_nodes, nat.ptr(mask), nat.ptr(sys_.diag), nat.ptr(vals), nat.stream_ptr()),
                       "bc_diag")
+
+    # ---- J2 state commit (test_plasticity.py:67-78) ------------------------------------
+    def j2_commit(self, dofs, law, ivars):
+        """The state a converged increment commits, at every quadrature point:
+        [sigma (C,Q,3,3), eps (C,Q,3,3), alpha (C,Q)] from the radial return
+        of ``law`` (J2Plasticity) at the first variable's gradient (2D
+        gradients embedded as plane strain)."""
+        fe0 = self.p.fes[0]
+        n0, v0, d = fe0.num_nodes, fe0.vec, self.p.dim
+        C, Q = self.sys.num_cells, fe0.num_quads
+        iv = self._ivars(ivars, C)
+        if len(iv) < 2:
+            raise ValueError("J2Plasticity needs internal_vars = [sigma_old, eps_old(, alpha_old)]")
+        u = dofs.reshape(-1)[self.sys.cell_dofs_long[:, : n0 * v0]].reshape(C, n0, v0)
+        ug = torch.einsum("cai,cqaj->cqij", u, self.shape_grads[:, :, :n0, :])
+        ug = torch.nn.functional.pad(ug, (0, 3 - d, 0, 3 - v0))
+        so, eo = iv[0].reshape(C, Q, 3, 3), iv[1].reshape(C, Q, 3, 3)
+        ao = iv[2].reshape(C, Q) if len(iv) > 2 else torch.zeros(C, Q, dtype=torch.float64, device=self.device)
+        sn, en, an = vmap(vmap(law.torch_state()))(ug, so, eo, ao)
+        return [sn, en, an]
 
     # ---- adjoint (solver.py:1340-1378) ---------------------------------------------
     def param_vjp(self, dofs, ivars, lam):

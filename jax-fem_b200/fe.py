@@ -138,14 +138,16 @@ def _location_flags(fn, points):
 
 
 class FiniteElement:
-    """One field on a mesh of one 3D element type (fe.py:20-110).  Holds the
-    element tables (basis.py) and Dirichlet data as host arrays."""
+    """One field on a mesh of one element type (fe.py:20-110), 3D or 2D.
+    Holds the element tables (basis.py) and Dirichlet data as host arrays."""
 
     def __init__(self, mesh, vec, dim, ele_type="HEX8", quadrature_rule=None, quadrature_order=None,
                  dirichlet_bc_info=None):
         basis.check_ele_type(ele_type)
-        if dim != 3:
-            raise NotImplementedError("only dim=3 is supported")
+        if dim != basis.ELEMENT_DIM[ele_type]:
+            raise ValueError(f"{ele_type} is a {basis.ELEMENT_DIM[ele_type]}D element, the problem has dim={dim}")
+        if mesh.points.shape[1] != dim:
+            raise ValueError(f"dim={dim} needs points of {dim} coordinates, the mesh has {mesh.points.shape[1]}")
         if quadrature_rule not in (None, "default"):
             raise NotImplementedError("only basix's default quadrature rule is supported")
         if mesh.cells.shape[1] != basis.NODES_PER_CELL[ele_type]:
@@ -237,14 +239,14 @@ class FiniteElement:
         return out
 
     def get_face_shape_grads(self, boundary_inds):
-        """Physical face shape gradients (F,fq,nen,3) and Nanson scale (F,fq) (fe.py:143-183)."""
+        """Physical face shape gradients (F,fq,nen,dim) and Nanson scale (F,fq) (fe.py:143-183)."""
         binds = np.asarray(boundary_inds).reshape(-1, 2)
         F = len(binds)
-        gref = self.face_shape_grads_ref[binds[:, 1]]  # (F,fq,nen,3)
-        X = self.points[self.cells[binds[:, 0]]] if F else np.zeros((0, self.num_nodes, 3))
-        J = np.einsum("fai,fqaj->fqij", X, gref)
         if F == 0:
-            return np.zeros((0, self.num_face_quads, self.num_nodes, 3)), np.zeros((0, self.num_face_quads))
+            return np.zeros((0, self.num_face_quads, self.num_nodes, self.dim)), np.zeros((0, self.num_face_quads))
+        gref = self.face_shape_grads_ref[binds[:, 1]]  # (F,fq,nen,dim)
+        X = self.points[self.cells[binds[:, 0]]]
+        J = np.einsum("fai,fqaj->fqij", X, gref)
         Jinv = np.linalg.inv(J)
         grads = np.einsum("fqaj,fqjk->fqak", gref, Jinv)
         nJ = np.einsum("fi,fqij->fqj", self.face_normals[binds[:, 1]], Jinv)
@@ -279,10 +281,10 @@ class FiniteElement:
 
     def body_load(self, mass_map):
         """int mass_map(u, x) . v dx as a (ndofs,) vector."""
-        X = self.points[self.cells]  # (C,nen,3)
+        X = self.points[self.cells]  # (C,nen,dim)
         J = np.einsum("cai,qaj->cqij", X, self.shape_grads_ref)
         jxw = np.linalg.det(J) * self.quad_weights[None]
-        xq = np.einsum("qa,cai->cqi", self.shape_vals, X).reshape(-1, 3)
+        xq = np.einsum("qa,cai->cqi", self.shape_vals, X).reshape(-1, self.dim)
         self._check_u_independent(mass_map, xq)
         u0 = np.zeros((len(xq), self.vec))
         val = _batched_or_pointwise(mass_map, (u0, xq), (self.vec,)).reshape(self.num_cells, self.num_quads,
@@ -301,7 +303,7 @@ class FiniteElement:
         _, scale = self.get_face_shape_grads(binds)
         fv = self.face_shape_vals_at(binds[:, 1])  # (F,fq,nen)
         X = self.points[self.cells[binds[:, 0]]]
-        xq = np.einsum("fqa,fai->fqi", fv, X).reshape(-1, 3)
+        xq = np.einsum("fqa,fai->fqi", fv, X).reshape(-1, self.dim)
         self._check_u_independent(surface_map, xq)
         u0 = np.zeros((len(xq), self.vec))
         val = _batched_or_pointwise(surface_map, (u0, xq), (self.vec,)).reshape(len(binds), self.num_face_quads,

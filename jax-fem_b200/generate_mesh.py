@@ -5,6 +5,9 @@ Mirrors ``Mesh`` (generate_mesh.py:13-27 in the reference) and ``box_mesh``
 index (i*(Ny+1) + j)*(Nz+1) + k and cells list their nodes in VTK HEX8 order,
 so meshes, solutions and per-cell data line up with the reference's.
 
+``rectangle_mesh`` (generate_mesh.py:120-148) is the 2D counterpart: node
+(i, j) of an (Nx+1, Ny+1) grid has index i*(Ny+1) + j.
+
 ``box_mesh_gmsh`` (generate_mesh.py:192-260) meshes the same box with gmsh,
 which is not available here; this version builds the structured mesh of
 the requested element type directly: HEX8 as ``box_mesh``, TET4 by
@@ -16,23 +19,29 @@ numbering of ``box_mesh``; added nodes follow them.
 """
 import numpy as np
 
-from .basis import HEX_EDGES, HEX_FACE_CORNERS, MESHIO_CELL_TYPE, NODES_PER_CELL, TET_EDGES, check_ele_type
+from .basis import (ELEMENT_DIM, HEX_EDGES, HEX_FACE_CORNERS, MESHIO_CELL_TYPE, NODES_PER_CELL, QUAD_EDGES,
+                    TET_EDGES, TRI_EDGES, check_ele_type)
 
-_ELE_OF_NEN = {n: e for e, n in NODES_PER_CELL.items()}
+# element type of (dim, nodes per cell)
+_ELE_OF_NEN = {(ELEMENT_DIM[e], n): e for e, n in NODES_PER_CELL.items()}
 
 
 class Mesh:
     """points (num_nodes, dim) float64 and cells (num_cells, nen) int32.
 
-    ``ele_type`` defaults to the element type with ``nen`` nodes."""
+    ``ele_type`` defaults to the element type of the points' dimension
+    with ``nen`` nodes."""
 
     def __init__(self, points, cells, ele_type=None):
         self.points = np.ascontiguousarray(np.asarray(points, dtype=np.float64))
         self.cells = np.ascontiguousarray(np.asarray(cells, dtype=np.int32))
-        if self.cells.ndim != 2 or self.cells.shape[1] not in _ELE_OF_NEN:
-            raise NotImplementedError("cells must be (num_cells, nen) with nen in 4, 8, 10, 20, 27 "
-                                      "(TET4, HEX8, TET10, HEX20, HEX27)")
-        self.ele_type = _ELE_OF_NEN[self.cells.shape[1]] if ele_type is None else check_ele_type(ele_type)
+        key = (self.points.shape[1] if self.points.ndim == 2 else 0,
+               self.cells.shape[1] if self.cells.ndim == 2 else 0)
+        if ele_type is None and key not in _ELE_OF_NEN:
+            raise NotImplementedError("cells must be (num_cells, nen) with nen in 4, 8, 10, 20, 27 for 3D points "
+                                      "(TET4, HEX8, TET10, HEX20, HEX27) or 3, 4, 6, 8 for 2D points "
+                                      "(TRI3, QUAD4, TRI6, QUAD8)")
+        self.ele_type = _ELE_OF_NEN[key] if ele_type is None else check_ele_type(ele_type)
         if NODES_PER_CELL[self.ele_type] != self.cells.shape[1]:
             raise ValueError(f"{self.ele_type} cells have {NODES_PER_CELL[self.ele_type]} nodes, "
                              f"got {self.cells.shape[1]}")
@@ -44,6 +53,36 @@ class _BoxMesh:
     def __init__(self, points, cells):
         self.points = points
         self.cells_dict = {"hexahedron": cells}
+
+
+def rectangle_mesh(Nx, Ny, domain_x, domain_y, ele_type="QUAD4"):
+    """Structured mesh of [0,Lx]x[0,Ly] with Nx*Ny squares
+    (generate_mesh.py:120-148): node (i, j) of the (Nx+1, Ny+1) grid has
+    index i*(Ny+1) + j, QUAD4 cells list (i,j) (i+1,j) (i+1,j+1) (i,j+1).
+    Other 2D types (an extension): TRI3 splits every square along its
+    (i,j)-(i+1,j+1) diagonal into two counter-clockwise triangles; QUAD8
+    and TRI6 add one node per edge, numbered after the grid's."""
+    check_ele_type(ele_type)
+    if ELEMENT_DIM[ele_type] != 2:
+        raise ValueError(f"rectangle_mesh makes 2D cells, not {ele_type}")
+    ix, iy = np.meshgrid(np.arange(Nx + 1), np.arange(Ny + 1), indexing="ij")
+    points = np.stack([np.linspace(0, domain_x, Nx + 1)[ix], np.linspace(0, domain_y, Ny + 1)[iy]],
+                      axis=-1).reshape(-1, 2)
+    i, j = np.meshgrid(np.arange(Nx), np.arange(Ny), indexing="ij")
+    base = (i * (Ny + 1) + j).reshape(-1)
+    quads = (base[:, None] + np.array([0, Ny + 1, Ny + 2, 1])[None, :]).astype(np.int32)
+    if ele_type.startswith("TRI"):
+        cells = quads[:, [[0, 1, 2], [0, 2, 3]]].reshape(-1, 3)
+        edges = TRI_EDGES
+    else:
+        cells = quads
+        edges = QUAD_EDGES
+    if ele_type in ("QUAD8", "TRI6"):
+        points, mid = _add_entity_nodes(points, cells, cells[:, edges])
+        cells = np.hstack([cells, mid])
+    out = _BoxMesh(np.ascontiguousarray(points), np.ascontiguousarray(cells, dtype=np.int32))
+    out.cells_dict = {get_meshio_cell_type(ele_type): out.cells_dict.pop("hexahedron")}
+    return out
 
 
 def box_mesh(Nx, Ny, Nz, domain_x, domain_y, domain_z):
@@ -111,6 +150,8 @@ def box_mesh_gmsh(Nx, Ny, Nz, domain_x, domain_y, domain_z, data_dir=None, ele_t
     ``data_dir`` is accepted for the reference's signature; nothing is
     written."""
     check_ele_type(ele_type)
+    if ELEMENT_DIM[ele_type] != 3:
+        raise ValueError(f"box_mesh_gmsh makes 3D cells; use rectangle_mesh for {ele_type}")
     hexmesh = box_mesh(Nx, Ny, Nz, domain_x, domain_y, domain_z)
     points, hexes = hexmesh.points, hexmesh.cells_dict["hexahedron"]
     if ele_type.startswith("TET"):

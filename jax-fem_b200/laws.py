@@ -18,6 +18,10 @@ J2Plasticity      radial return + linear iso. hardening       [sigma_old, eps_ol
 ``as_law`` also accepts a plain callable when it is recognisably the
 identity (the Poisson test's ``lambda x: x``) or a linear isotropic elastic
 stress; anything else raises ``NotImplementedError``.
+
+Each law also has a torch form (``torch_map``) for the cell-kernel path;
+on 2D problems the elastic and inelastic laws act in plane strain through
+``plane_strain``.
 """
 import numpy as np
 
@@ -139,16 +143,17 @@ class J2Plasticity(Law):
     def params(self):
         return [self.E, self.nu, self.sigma_y, self.H]
 
-    def torch_map(self):
-        """The radial return as a torch tensor map of (u_grad, sigma_old,
-        eps_old, alpha_old): the plastic branch chosen with torch.where, the
-        deviatoric norm's square root guarded at zero, so that forward-mode
-        derivatives stay finite on both branches."""
+    def torch_state(self):
+        """The radial return in torch form: (u_grad (3,3), sigma_old,
+        eps_old, alpha_old) at one point -> (sigma, eps, alpha), the state a
+        converged increment commits.  The plastic branch is chosen with
+        torch.where and the deviatoric norm's square root is guarded at
+        zero, so forward-mode derivatives stay finite on both branches."""
         E, nu, sy0, Hh = self.E, self.nu, self.sigma_y, self.H
         mu = E / (2.0 * (1.0 + nu))
         lm = E * nu / ((1.0 + nu) * (1.0 - 2.0 * nu))
 
-        def stress(u_grad, sigma_old, eps_old, alpha_old=None):
+        def state(u_grad, sigma_old, eps_old, alpha_old=None):
             import torch
             I = torch.eye(3, dtype=u_grad.dtype, device=u_grad.device)  # noqa: E741
             eps = 0.5 * (u_grad + u_grad.T)
@@ -162,9 +167,35 @@ class J2Plasticity(Law):
             f = q - (sy0 + Hh * a)
             dg = torch.where(f > 0.0, f, torch.zeros_like(f)) / (3.0 * mu + Hh)
             qs = torch.where(pos, q, torch.ones_like(q))
-            return st - torch.where(pos, 3.0 * mu * dg / qs, torch.zeros_like(q)) * s
+            sigma = st - torch.where(pos, 3.0 * mu * dg / qs, torch.zeros_like(q)) * s
+            return sigma, eps, a + dg
+
+        return state
+
+    def torch_map(self):
+        """The stress of ``torch_state`` as a tensor map of (u_grad,
+        sigma_old, eps_old, alpha_old)."""
+        state = self.torch_state()
+
+        def stress(u_grad, sigma_old, eps_old, alpha_old=None):
+            return state(u_grad, sigma_old, eps_old, alpha_old)[0]
 
         return stress
+
+
+def plane_strain(tensor_map):
+    """A 3D tensor map on a 2D problem: the in-plane gradient (vec, 2) is
+    the upper-left block of a 3x3 gradient (no out-of-plane displacement or
+    variation) and the in-plane block of the 3D stress is returned, so the
+    2D weak form is the 3D one restricted to in-plane fields."""
+    import torch
+
+    def tm2(u_grad, *ivars):
+        v, d = u_grad.shape[-2:]
+        g = torch.nn.functional.pad(u_grad, (0, 3 - d, 0, 3 - v))
+        return tensor_map(g, *ivars)[..., :v, :d]
+
+    return tm2
 
 
 def _probe(fn, vec, dim, rng):

@@ -111,8 +111,8 @@ def _to_dev(x, device, dtype=torch.float64):
 
 @dataclass
 class Problem:
-    """One field on a mesh of one 3D element type; see the module docstring.
-    Fields as the reference's."""
+    """Fields on meshes of one or several element types (3D, or 2D on the
+    cell-kernel path); see the module docstring.  Fields as the reference's."""
     mesh: Mesh
     vec: int
     dim: int
@@ -183,10 +183,11 @@ class Problem:
     def cell_path(self):
         """True when the weak form is user code run by the cell-kernel path
         (cellpath.py): a universal kernel, several variables, a tensor map
-        that is not a registered law, no tensor map, or mass / surface maps
-        that depend on u.  False: the registered-law kernels."""
+        that is not a registered law, no tensor map, mass / surface maps
+        that depend on u, or a 2D problem (the registered-law CUDA kernels
+        are 3D).  False: the registered-law kernels."""
         if self._cell_path is None:
-            cp = (self.num_vars > 1 or hasattr(self, "get_universal_kernel")
+            cp = (self.num_vars > 1 or self.dim == 2 or hasattr(self, "get_universal_kernel")
                   or hasattr(self, "get_universal_kernels_surface") or not hasattr(self, "get_tensor_map"))
             if not cp:
                 try:
@@ -384,6 +385,13 @@ class Problem:
     # ---- J2 state commit (test_plasticity.py:67-78) -----------------------------
     def update_j2_state(self, sol):
         """Commit the return map at the converged ``sol``: internal_vars <- new state."""
+        if self.cell_path:  # the torch radial return at every quadrature point
+            law = self.get_tensor_map() if hasattr(self, "get_tensor_map") else None
+            if not isinstance(law, J2Plasticity):
+                raise TypeError("update_j2_state needs a J2Plasticity law")
+            self.dev()
+            self.internal_vars = self._cells.j2_commit(self._flat_dofs(sol), law, self.internal_vars)
+            return self.internal_vars
         law = self.law
         if not isinstance(law, J2Plasticity):
             raise TypeError("update_j2_state needs a J2Plasticity law")

@@ -5,15 +5,17 @@ solution and optional point/cell fields of a finite element to a VTK XML
 UnstructuredGrid (.vtu) through meshio, and gives the reading side the
 reference gets from ``meshio.read``: VTU files (ASCII, base64 binary, zlib
 compressed; what dolfinx and meshio write), Gmsh ``.msh`` (ASCII, formats 2.2
-and 4.1) and Abaqus ``.inp`` meshes, returning the cells of one 3D element
-type (TET4, TET10, HEX8, HEX20, HEX27) as a ``Mesh``.
+and 4.1) and Abaqus ``.inp`` meshes, returning the cells of one element
+type (TET4, TET10, HEX8, HEX20, HEX27; the 2D TRI3, QUAD4, TRI6, QUAD8 with
+(N, 2) points) as a ``Mesh``.
 
 File formats followed: the VTK XML file format (UnstructuredGrid, inline
 DataArrays, ``header_type`` UInt32/UInt64, ``vtkZLibDataCompressor`` block
-layout; cell types 10, 24, 12, 25, 29 and the order-1 Lagrange cells 71, 72),
-the Gmsh MSH 2.2 / 4.1 ASCII formats (element types 4, 11, 5, 17, 12) and the
-Abaqus input format (``*NODE``, ``*ELEMENT, TYPE=C3D4 / C3D10 / C3D8 /
-C3D20`` and their R/I/M/H variants).  ``Mesh`` uses the VTK (= meshio) node
+layout; cell types 10, 24, 12, 25, 29, 5, 9, 22, 23 and the order-1 Lagrange
+cells 71, 72, 69, 70), the Gmsh MSH 2.2 / 4.1 ASCII formats (element types
+4, 11, 5, 17, 12, 2, 3, 9, 16) and the Abaqus input format (``*NODE``,
+``*ELEMENT, TYPE=C3D4 / C3D10 / C3D8 / C3D20`` and their R/I/M/H variants,
+the 2D CPS / CPE / CAX 3, 4, 6, 8).  ``Mesh`` uses the VTK (= meshio) node
 order; Abaqus lists the same order, Gmsh numbers the edge (and face) nodes of
 its quadratic cells differently and is permuted on reading (Gmsh node
 ordering: edges in the order of their corner pairs listed below).
@@ -31,10 +33,12 @@ from . import basis
 from .generate_mesh import Mesh
 
 # VTK cell type of each element type, and the types read back: the order-1
-# Lagrange cells of dolfinx (71 tetrahedron, 72 hexahedron) list the same
-# nodes in the same order as 10 and 12.
-_VTK_CELL = {"TET4": 10, "TET10": 24, "HEX8": 12, "HEX20": 25, "HEX27": 29}
-_VTK_READ = {10: "TET4", 24: "TET10", 12: "HEX8", 25: "HEX20", 29: "HEX27", 71: "TET4", 72: "HEX8"}
+# Lagrange cells of dolfinx (71 tetrahedron, 72 hexahedron, 69 triangle,
+# 70 quadrilateral) list the same nodes in the same order as 10, 12, 5, 9.
+_VTK_CELL = {"TET4": 10, "TET10": 24, "HEX8": 12, "HEX20": 25, "HEX27": 29,
+             "TRI3": 5, "QUAD4": 9, "TRI6": 22, "QUAD8": 23}
+_VTK_READ = {10: "TET4", 24: "TET10", 12: "HEX8", 25: "HEX20", 29: "HEX27", 71: "TET4", 72: "HEX8",
+             5: "TRI3", 9: "QUAD4", 22: "TRI6", 23: "QUAD8", 69: "TRI3", 70: "QUAD4"}
 _VTK_TYPES = {"Float32": np.float32, "Float64": np.float64, "Int8": np.int8, "UInt8": np.uint8,
               "Int16": np.int16, "UInt16": np.uint16, "Int32": np.int32, "UInt32": np.uint32,
               "Int64": np.int64, "UInt64": np.uint64}
@@ -62,18 +66,19 @@ def _data_array(arr, name=None, ncomp=None, fmt="binary"):
 def write_vtu(path, points, cells, point_data=None, cell_data=None, fmt="binary", ele_type=None):
     """Write a mesh of one element type with point and cell fields as a .vtu file.
 
-    points (N, 3); cells (C, nen) in VTK node order (the element type follows
-    from nen unless given); point_data / cell_data: dicts name -> array with
-    N (or C) rows.  ``fmt`` is "binary" (inline base64, UInt64 headers) or
-    "ascii"."""
+    points (N, 3) or (N, 2) (written with z = 0); cells (C, nen) in VTK node
+    order (the element type follows from nen and the points' dimension
+    unless given); point_data / cell_data: dicts name -> array with N (or C)
+    rows.  ``fmt`` is "binary" (inline base64, UInt64 headers) or "ascii"."""
     points = np.asarray(points, dtype=np.float64)
-    if points.shape[1] == 2:
+    dim = points.shape[1]
+    if dim == 2:
         points = np.hstack([points, np.zeros((len(points), 1))])
     cells = np.asarray(cells, dtype=np.int64)
     if ele_type is None:
-        by_nen = {n: e for e, n in basis.NODES_PER_CELL.items()}
+        by_nen = {n: e for e, n in basis.NODES_PER_CELL.items() if basis.ELEMENT_DIM[e] == dim}
         if cells.shape[1] not in by_nen:
-            raise NotImplementedError(f"cells of {cells.shape[1]} nodes: no 3D element type has that many")
+            raise NotImplementedError(f"cells of {cells.shape[1]} nodes: no {dim}D element type has that many")
         ele_type = by_nen[cells.shape[1]]
     vtk_type = _VTK_CELL[basis.check_ele_type(ele_type)]
     root = ET.Element("VTKFile", {"type": "UnstructuredGrid", "version": "1.0", "byte_order": "LittleEndian",
@@ -183,7 +188,8 @@ def read_vtu(path, with_type=False):
     """Read a .vtu file: returns (points (N,3) float64, cells (C,nen) int32,
     point_data dict, cell_data dict), and the element type when
     ``with_type``.  All cells must be of one supported type (VTK 10, 24, 12,
-    25, 29, or 71 / 72 of order 1); others raise NotImplementedError."""
+    25, 29, 5, 9, 22, 23, or 71 / 72 / 69 / 70 of order 1); others raise
+    NotImplementedError."""
     root = ET.parse(path).getroot()
     if root.get("type") != "UnstructuredGrid":
         raise NotImplementedError("only VTK UnstructuredGrid files are read")
@@ -199,8 +205,9 @@ def read_vtu(path, with_type=False):
     eles = {_VTK_READ.get(int(t)) for t in np.unique(types)}
     ele = eles.pop() if len(eles) == 1 else None
     if ele is None or not np.all(sizes == basis.NODES_PER_CELL[ele]):
-        raise NotImplementedError("the cells must be of one type: TET4, TET10, HEX8, HEX20 or HEX27 "
-                                  "(VTK 10, 24, 12, 25, 29; 71/72 of order 1)")
+        raise NotImplementedError("the cells must be of one type: TET4, TET10, HEX8, HEX20, HEX27, TRI3, "
+                                  "QUAD4, TRI6 or QUAD8 (VTK 10, 24, 12, 25, 29, 5, 9, 22, 23; "
+                                  "71/72/69/70 of order 1)")
     cells = conn.reshape(-1, basis.NODES_PER_CELL[ele]).astype(np.int32)
     fields = []
     for tag in ("PointData", "CellData"):
@@ -215,8 +222,10 @@ def read_vtu(path, with_type=False):
 
 # Gmsh element type -> element; Gmsh's corner pairs of the edge nodes of the
 # quadratic tetrahedron and hexahedron, and the corner sets of the
-# hexahedron's face nodes (Gmsh node ordering).
-_GMSH_TYPES = {4: "TET4", 11: "TET10", 5: "HEX8", 17: "HEX20", 12: "HEX27"}
+# hexahedron's face nodes (Gmsh node ordering).  Gmsh's 2D cells list their
+# nodes in VTK order (corners, then edges (0,1), (1,2), ... in turn).
+_GMSH_TYPES = {4: "TET4", 11: "TET10", 5: "HEX8", 17: "HEX20", 12: "HEX27",
+               2: "TRI3", 3: "QUAD4", 9: "TRI6", 16: "QUAD8"}
 _GMSH_TET_EDGES = [(0, 1), (1, 2), (2, 0), (3, 0), (3, 2), (3, 1)]
 _GMSH_HEX_EDGES = [(0, 1), (0, 3), (0, 4), (1, 2), (1, 5), (2, 3), (2, 6), (3, 7), (4, 5), (4, 7), (5, 6), (6, 7)]
 _GMSH_HEX_FACES = [(0, 1, 2, 3), (0, 1, 4, 5), (0, 3, 4, 7), (1, 2, 5, 6), (2, 3, 6, 7), (4, 5, 6, 7)]
@@ -224,6 +233,8 @@ _GMSH_HEX_FACES = [(0, 1, 2, 3), (0, 1, 4, 5), (0, 3, 4, 7), (1, 2, 5, 6), (2, 3
 
 def _gmsh_to_vtk(ele):
     """perm with vtk_cell = gmsh_cell[perm]."""
+    if basis.ELEMENT_DIM[ele] == 2:
+        return np.arange(basis.NODES_PER_CELL[ele])
     tet = ele.startswith("TET")
     nc = 4 if tet else 8
     perm = list(range(nc))
@@ -239,31 +250,45 @@ def _gmsh_to_vtk(ele):
 
 
 def _pick(found, ele_type, path, what):
-    """The cells of the requested element type, or of the single one found."""
+    """The cells of the requested element type, or of the single one of the
+    highest dimension found (a 3D mesh's boundary triangles and quadrangles
+    are not cells of it)."""
     if ele_type is not None:
         if ele_type not in found:
             raise ValueError(f"{path}: no {ele_type} {what}")
         return ele_type
-    if len(found) != 1:
-        raise ValueError(f"{path}: {'no' if not found else 'several'} 3D element types "
-                         f"({sorted(found)}); pass ele_type")
-    return next(iter(found))
+    top = max((basis.ELEMENT_DIM[e] for e in found), default=3)
+    cand = sorted(e for e in found if basis.ELEMENT_DIM[e] == top)
+    if len(cand) != 1:
+        raise ValueError(f"{path}: {'no' if not cand else 'several'} {top}D element types "
+                         f"({cand}); pass ele_type")
+    return cand[0]
 
 
-def _compact(points, node_ids, cells_ids, ele):
+def _planar(points, ele, path):
+    """Points of a 2D element type as (N, 2): z dropped, which must be 0."""
+    if basis.ELEMENT_DIM[ele] == 3 or points.shape[1] == 2:
+        return points
+    if len(points) and np.abs(points[:, 2]).max() > 0.0:
+        raise ValueError(f"{path}: {ele} cells off the z = 0 plane")
+    return np.ascontiguousarray(points[:, :2])
+
+
+def _compact(points, node_ids, cells_ids, ele, path=""):
     """Mesh from node ids and cells of ids: the points the cells use, in the
     order of the node table (unused nodes, e.g. geometry points, dropped)."""
     nen = basis.NODES_PER_CELL[ele]
     index = {int(t): i for i, t in enumerate(node_ids)}
     cells = np.array([[index[int(t)] for t in c] for c in cells_ids], dtype=np.int64).reshape(-1, nen)
     used, inv = np.unique(cells.reshape(-1), return_inverse=True)
-    return Mesh(points[used], inv.reshape(-1, nen).astype(np.int32), ele)
+    return Mesh(_planar(points[used], ele, path), inv.reshape(-1, nen).astype(np.int32), ele)
 
 
 def read_gmsh(path, ele_type=None):
     """Mesh from a Gmsh ASCII .msh file (format 2.2 or 4.1): the cells of
-    one 3D element type (``ele_type``, or the only one in the file), in VTK
-    node order; nodes not used by them dropped."""
+    one element type (``ele_type``, or the only one of the highest
+    dimension in the file), in VTK node order; nodes not used by them
+    dropped; 2D cells get (N, 2) points."""
     with open(path) as f:
         lines = [ln.strip() for ln in f]
     sec = {}
@@ -310,21 +335,26 @@ def read_gmsh(path, ele_type=None):
             if v[1] in _GMSH_TYPES:
                 nen = basis.NODES_PER_CELL[_GMSH_TYPES[v[1]]]
                 found.setdefault(_GMSH_TYPES[v[1]], []).append(v[3 + v[2]:3 + v[2] + nen])
-    ele = _pick(found, ele_type, path, "cells (Gmsh element types 4, 11, 5, 17, 12)")
+    ele = _pick(found, ele_type, path, "cells (Gmsh element types 4, 11, 5, 17, 12, 2, 3, 9, 16)")
     cells = np.array(found[ele], dtype=np.int64)[:, _gmsh_to_vtk(ele)]
-    return _compact(np.array(xyz, dtype=np.float64), ids, cells, ele)
+    return _compact(np.array(xyz, dtype=np.float64), ids, cells, ele, path)
 
 
 _ABAQUS_TYPES = {"C3D4": "TET4", "C3D4H": "TET4", "C3D10": "TET10", "C3D10H": "TET10", "C3D10M": "TET10",
                  "C3D10MH": "TET10", "C3D8": "HEX8", "C3D8R": "HEX8", "C3D8I": "HEX8", "C3D8H": "HEX8",
                  "C3D20": "HEX20", "C3D20R": "HEX20", "C3D20H": "HEX20", "C3D20RH": "HEX20"}
+# plane stress / plane strain / axisymmetric continuum cells
+for _fam in ("CPS", "CPE", "CAX"):
+    _ABAQUS_TYPES.update({_fam + "3": "TRI3", _fam + "4": "QUAD4", _fam + "4R": "QUAD4", _fam + "4I": "QUAD4",
+                          _fam + "6": "TRI6", _fam + "6M": "TRI6", _fam + "8": "QUAD8", _fam + "8R": "QUAD8"})
 
 
 def read_abaqus(path, ele_type=None):
     """Mesh from an Abaqus .inp file: the *NODE table and the *ELEMENT
-    blocks of one 3D element type (C3D4, C3D10, C3D8, C3D20 and their
-    R/I/M/H variants; ``ele_type`` or the only one in the file).  Abaqus
-    lists the nodes of these cells in VTK order."""
+    blocks of one element type (C3D4, C3D10, C3D8, C3D20 and their R/I/M/H
+    variants; the 2D CPS/CPE/CAX 3, 4, 6, 8; ``ele_type`` or the only one
+    of the highest dimension in the file).  Abaqus lists the nodes of these
+    cells in VTK order; 2D cells get (N, 2) points."""
     ids, xyz, found = [], [], {}
     mode, pending = None, []
     with open(path) as f:
@@ -353,19 +383,19 @@ def read_abaqus(path, ele_type=None):
                 if len(pending) >= nen + 1:
                     found.setdefault(mode, []).append(pending[1:nen + 1])
                     pending = []
-    ele = _pick(found, ele_type, path, "elements (C3D4, C3D10, C3D8, C3D20)")
-    return _compact(np.array(xyz, dtype=np.float64), ids, found[ele], ele)
+    ele = _pick(found, ele_type, path, "elements (C3D4, C3D10, C3D8, C3D20, CPS/CPE/CAX 3, 4, 6, 8)")
+    return _compact(np.array(xyz, dtype=np.float64), ids, found[ele], ele, path)
 
 
 def read_mesh(path, ele_type=None):
-    """``Mesh`` of the cells of one 3D element type in a .vtu, .msh or .inp
-    file (by extension)."""
+    """``Mesh`` of the cells of one element type in a .vtu, .msh or .inp
+    file (by extension); 2D cells get (N, 2) points."""
     ext = os.path.splitext(path)[1].lower()
     if ext == ".vtu":
         points, cells, _, _, ele = read_vtu(path, with_type=True)
         if ele_type is not None and ele_type != ele:
             raise ValueError(f"{path}: holds {ele} cells, not {ele_type}")
-        return Mesh(points, cells, ele)
+        return Mesh(_planar(points, ele, path), cells, ele)
     if ext == ".msh":
         return read_gmsh(path, ele_type)
     if ext == ".inp":

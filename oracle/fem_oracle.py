@@ -1,5 +1,6 @@
 """FP64 numpy restatement of the reference's assemble-and-solve path (HEX8,
-and the TET4, TET10, HEX20 and HEX27 element types).
+and the TET4, TET10, HEX20, HEX27 and 2D QUAD4, QUAD8, TRI3, TRI6 element
+types).
 
 TEST INFRASTRUCTURE ONLY: the parity checker and the CPU baseline.  The
 product (``jax-fem_b200``) never imports this module.
@@ -18,6 +19,8 @@ basix 0.10.0 (HEX8 Lagrange tabulation, Gauss-Jacobi quadrature; see
 ``hex8_tables``) and PETSc 3.25.1 COO summation / ``zeroRows`` (see
 ``assemble_global``).
 """
+import itertools
+
 import numpy as np
 import scipy.sparse as sp
 import scipy.sparse.linalg as spla
@@ -120,30 +123,47 @@ BASIX_TET_NORMALS = np.array([[1, 1, 1], [-1, 0, 0], [0, -1, 0], [0, 0, -1]], dt
 BASIX_TET_NORMALS[0] /= np.sqrt(3.0)
 BASIX_HEX_EDGES = np.array([[0, 1], [0, 2], [0, 4], [1, 3], [1, 5], [2, 3], [2, 6], [3, 7],
                             [4, 5], [4, 6], [5, 7], [6, 7]])
-# re_order of basis.py:53-76 (mesh position -> basix dof)
+# basix quadrilateral / triangle: vertices, edges (= facets) and the
+# facets' outward normals.
+BASIX_QUAD_VERTICES = np.array([[0, 0], [1, 0], [0, 1], [1, 1]], dtype=np.float64)
+BASIX_QUAD_EDGES = np.array([[0, 1], [0, 2], [1, 3], [2, 3]])
+BASIX_QUAD_NORMALS = np.array([[0, -1], [-1, 0], [1, 0], [0, 1]], dtype=np.float64)
+BASIX_TRI_VERTICES = np.array([[0, 0], [1, 0], [0, 1]], dtype=np.float64)
+BASIX_TRI_EDGES = np.array([[1, 2], [0, 2], [0, 1]])
+BASIX_TRI_NORMALS = np.array([[1, 1], [-1, 0], [0, -1]], dtype=np.float64) / np.array([[np.sqrt(2.0)], [1], [1]])
+# re_order of basis.py:53-107 (mesh position -> basix dof)
 RE_ORDER = {
     "HEX8": [0, 1, 3, 2, 4, 5, 7, 6],
     "HEX27": [0, 1, 3, 2, 4, 5, 7, 6, 8, 11, 13, 9, 16, 18, 19, 17, 10, 12, 15, 14, 22, 23, 21, 24, 20, 25, 26],
     "HEX20": [0, 1, 3, 2, 4, 5, 7, 6, 8, 11, 13, 9, 16, 18, 19, 17, 10, 12, 15, 14],
     "TET4": [0, 1, 2, 3],
     "TET10": [0, 1, 2, 3, 9, 6, 8, 7, 5, 4],
+    "QUAD4": [0, 1, 3, 2],
+    "QUAD8": [0, 1, 3, 2, 4, 6, 7, 5],
+    "TRI3": [0, 1, 2],
+    "TRI6": [0, 1, 2, 5, 3, 4],
 }
-DEFAULT_QUADRATURE_ORDER = {"HEX8": 2, "HEX27": 10, "HEX20": 2, "TET4": 0, "TET10": 2}
+DEFAULT_QUADRATURE_ORDER = {"HEX8": 2, "HEX27": 10, "HEX20": 2, "TET4": 0, "TET10": 2,
+                            "QUAD4": 2, "QUAD8": 2, "TRI3": 0, "TRI6": 2}
+
+
+def element_dim(ele_type):
+    return 2 if ele_type[:3] in ("QUA", "TRI") else 3
 
 
 def _monomial_table(pts, exps):
-    """Values (n, m) and gradients (n, m, 3) of monomials x^e at points."""
+    """Values (n, m) and gradients (n, m, dim) of monomials x^e at points."""
     pts = np.atleast_2d(pts)
-    n, m = len(pts), len(exps)
+    n, m, dim = len(pts), len(exps), pts.shape[1]
     vals = np.ones((n, m))
-    grads = np.zeros((n, m, 3))
+    grads = np.zeros((n, m, dim))
     for k, e in enumerate(exps):
-        vals[:, k] = np.prod([pts[:, d] ** e[d] for d in range(3)], axis=0)
-        for d in range(3):
+        vals[:, k] = np.prod([pts[:, d] ** e[d] for d in range(dim)], axis=0)
+        for d in range(dim):
             if e[d] == 0:
                 continue
             g = e[d] * pts[:, d] ** (e[d] - 1)
-            for o in range(3):
+            for o in range(dim):
                 if o != d:
                     g = g * pts[:, o] ** e[o]
             grads[:, k, d] = g
@@ -152,27 +172,33 @@ def _monomial_table(pts, exps):
 
 def _element_space(ele_type):
     """Monomial exponents of the element's polynomial space."""
-    if ele_type == "TET4":
-        return [e for e in np.ndindex(2, 2, 2) if sum(e) <= 1]
-    if ele_type == "TET10":
-        return [e for e in np.ndindex(3, 3, 3) if sum(e) <= 2]
-    if ele_type == "HEX27":
+    d = element_dim(ele_type)
+    if ele_type in ("TET4", "TRI3"):
+        return [e for e in np.ndindex(*(2,) * d) if sum(e) <= 1]
+    if ele_type in ("TET10", "TRI6"):
+        return [e for e in np.ndindex(*(3,) * d) if sum(e) <= 2]
+    if ele_type in ("HEX27",):
         return list(np.ndindex(3, 3, 3))
-    if ele_type == "HEX20":  # superlinear degree (degree minus linearly entering variables) <= 2
-        return [e for e in np.ndindex(4, 4, 4) if sum(e) - sum(x == 1 for x in e) <= 2]
+    if ele_type == "QUAD4":
+        return list(np.ndindex(2, 2))
+    if ele_type in ("HEX20", "QUAD8"):  # superlinear degree (degree minus linearly entering variables) <= 2
+        return [e for e in np.ndindex(*(4,) * d) if sum(e) - sum(x == 1 for x in e) <= 2]
     raise ValueError(ele_type)
+
+
+def _basix_vertices_edges(ele_type):
+    return {"TET": (BASIX_TET_VERTICES, BASIX_TET_EDGES), "HEX": (BASIX_HEX_VERTICES, BASIX_HEX_EDGES),
+            "QUA": (BASIX_QUAD_VERTICES, BASIX_QUAD_EDGES), "TRI": (BASIX_TRI_VERTICES, BASIX_TRI_EDGES)}[ele_type[:3]]
 
 
 def _basix_dof_functionals(ele_type):
     """The element's dofs in basix order, each (points, weights): a point
     value is one point with weight 1; an edge mean is a Gauss rule on the edge."""
-    tet = ele_type.startswith("TET")
-    V = BASIX_TET_VERTICES if tet else BASIX_HEX_VERTICES
-    E = BASIX_TET_EDGES if tet else BASIX_HEX_EDGES
+    V, E = _basix_vertices_edges(ele_type)
     dofs = [(V[i][None], np.ones(1)) for i in range(len(V))]
-    if ele_type in ("TET10", "HEX27"):
+    if ele_type in ("TET10", "HEX27", "TRI6"):
         dofs += [(0.5 * (V[a] + V[b])[None], np.ones(1)) for a, b in E]
-    if ele_type == "HEX20":
+    if ele_type in ("HEX20", "QUAD8"):
         t, w = gauss_jacobi_01(3)
         dofs += [(V[a][None] + t[:, None] * (V[b] - V[a])[None], w) for a, b in E]
     if ele_type == "HEX27":
@@ -211,23 +237,42 @@ def simplex_quadrature(dim, order):
 
 
 def element_tables(ele_type, quadrature_order=None):
-    """shape_vals (Q,nen), shape_grads_ref (Q,nen,3), weights (Q,) (basis.py:141-175)."""
+    """shape_vals (Q,nen), shape_grads_ref (Q,nen,dim), weights (Q,) (basis.py:141-175)."""
     order = DEFAULT_QUADRATURE_ORDER[ele_type] if quadrature_order is None else quadrature_order
-    if ele_type.startswith("TET"):
-        pts, wts = simplex_quadrature(3, order)
+    dim = element_dim(ele_type)
+    if ele_type[:3] in ("TET", "TRI"):
+        pts, wts = simplex_quadrature(dim, order)
     else:
         m = (order + 2) // 2
         p, w = gauss_jacobi_01(m)
-        pts = np.array([[a, b, c] for a in p for b in p for c in p])
-        wts = np.array([wa * wb * wc for wa in w for wb in w for wc in w])
+        pts = np.array(list(itertools.product(p, repeat=dim)))
+        wts = np.array([np.prod(c) for c in itertools.product(w, repeat=dim)])
     vals, grads = element_shape(ele_type, pts)
     return vals, grads, wts
 
 
+def _edge_face_tables(ele_type, order):
+    """2D cells: facets are edges, the Gauss-Jacobi rule of the order on
+    each, weights times the edge length (basis.py:225-233)."""
+    p, w = gauss_jacobi_01((order + 2) // 2)
+    V, E = _basix_vertices_edges(ele_type)
+    normals = BASIX_TRI_NORMALS if ele_type.startswith("TRI") else BASIX_QUAD_NORMALS
+    ro = np.array(RE_ORDER[ele_type])
+    fpts = np.stack([np.outer(1 - p, V[a]) + np.outer(p, V[b]) for a, b in E])
+    fw = np.stack([w * np.linalg.norm(V[b] - V[a]) for a, b in E])
+    finds = np.array([[int(np.argwhere(ro == i)[0, 0]) for i in e] for e in E])
+    nf, nq = fpts.shape[:2]
+    vals, grads = element_shape(ele_type, fpts.reshape(-1, 2))
+    nen = vals.shape[1]
+    return vals.reshape(nf, nq, nen), grads.reshape(nf, nq, nen, 2), fw, normals.copy(), finds
+
+
 def element_face_tables(ele_type, quadrature_order=None):
     """Face tables (basis.py:178-250) for any element type: vals (nf,F,nen),
-    grads (nf,F,nen,3), weights (nf,F), normals (nf,3), face_inds (nf,nfv)."""
+    grads (nf,F,nen,dim), weights (nf,F), normals (nf,dim), face_inds (nf,nfv)."""
     order = DEFAULT_QUADRATURE_ORDER[ele_type] if quadrature_order is None else quadrature_order
+    if element_dim(ele_type) == 2:
+        return _edge_face_tables(ele_type, order)
     if ele_type.startswith("TET"):
         qp, qw = simplex_quadrature(2, order)
         s, t = qp[:, 0], qp[:, 1]

@@ -74,6 +74,19 @@ def element_box(pkg, ele_type, N, L=(1.0, 1.0, 1.0), amp=0.0, seed=0):
     return pkg.Mesh(pts, m.cells_dict[gm.get_meshio_cell_type(ele_type)], ele_type)
 
 
+def planar_box(pkg, ele_type, N, L=(1.0, 1.0), amp=0.0, seed=0):
+    """Structured rectangle mesh of one 2D element type; with amp > 0 every
+    node off the boundary moves by up to amp * h (curved, general cells)."""
+    m = pkg.rectangle_mesh(N[0], N[1], L[0], L[1], ele_type=ele_type)
+    pts = m.points.copy()
+    if amp > 0:
+        rng = np.random.default_rng(seed)
+        h = np.array(L) / np.array(N)
+        inner = np.all((pts > 1e-9) & (pts < np.array(L) - 1e-9), axis=1)
+        pts[inner] += amp * h * rng.uniform(-1, 1, size=(inner.sum(), 2))
+    return pkg.Mesh(pts, m.cells_dict[pkg.get_meshio_cell_type(ele_type)], ele_type)
+
+
 def face_fn(axis, value):
     """Location function of the plane x[axis] = value."""
     return lambda p: np.isclose(p[axis], value, atol=1e-5)

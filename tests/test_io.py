@@ -10,7 +10,10 @@
 - TET4, TET10, HEX20 and HEX27 meshes and solutions round-trip through VTU
   with their VTK cell types; their Gmsh (edge and face nodes renumbered)
   and Abaqus cells come back in VTK order, checked by geometry: every
-  edge / face / centre node sits where the cell's corners put it."""
+  edge / face / centre node sits where the cell's corners put it;
+- QUAD4, QUAD8, TRI3 and TRI6 meshes round-trip through VTU (z = 0 written,
+  (N, 2) points read back), Gmsh and Abaqus CPS / CPE cells; a 3D file's
+  boundary triangles do not shadow its tetrahedra."""
 import base64
 import os
 import struct
@@ -293,3 +296,56 @@ def test_small_helpers(io, tmp_path, capsys):
     assert q.shape == (len(m4.cells),) and (q > 0).all()
     flipped = m4.cells[:, [0, 2, 1, 3]]
     assert (gm.check_mesh_TET4(m4.points, flipped) < 0).all()
+
+
+@pytest.mark.parametrize("ele", ["QUAD4", "QUAD8", "TRI3", "TRI6"])
+def test_planar_types_round_trip(io, tmp_path, ele):
+    """2D meshes: VTU round trip (points written with z = 0, read back as
+    (N, 2)), Gmsh cells (node order = VTK's for these types) and Abaqus
+    CPS / CPE cells."""
+    pkg, ut = io
+    from helpers import planar_box
+    m = planar_box(pkg, ele, (2, 3), amp=0.1, seed=1)
+    fe = pkg.fe.FiniteElement(m, 2, 2, ele_type=ele)
+    sol = np.random.default_rng(3).normal(size=(len(m.points), 2))
+    path = str(tmp_path / f"{ele}.vtu")
+    ut.save_sol(fe, sol, path)
+    pts, cells, pd, _, got = ut.read_vtu(path, with_type=True)
+    assert got == ele and pts.shape == (len(m.points), 3) and not pts[:, 2].any()
+    np.testing.assert_array_equal(cells, m.cells)
+    np.testing.assert_array_equal(pd["sol"], sol.astype(np.float32))
+    mm = ut.read_mesh(path)
+    assert mm.ele_type == ele and mm.points.shape == m.points.shape
+    np.testing.assert_array_equal(mm.points, m.points)
+    # Gmsh 2.2 with line elements beside the cells, Abaqus with 2D node lines
+    gtype = {"TRI3": 2, "QUAD4": 3, "TRI6": 9, "QUAD8": 16}[ele]
+    node_lines = "\n".join(f"{i + 1} {float(x)!r} {float(y)!r} 0" for i, (x, y) in enumerate(m.points))
+    els = [f"1 1 2 0 1 {m.cells[0, 0] + 1} {m.cells[0, 1] + 1}"]
+    els += [f"{k + 2} {gtype} 2 0 1 " + " ".join(str(int(v) + 1) for v in c) for k, c in enumerate(m.cells)]
+    (tmp_path / "p.msh").write_text(f"$MeshFormat\n2.2 0 8\n$EndMeshFormat\n$Nodes\n{len(m.points)}\n{node_lines}\n"
+                                    f"$EndNodes\n$Elements\n{len(els)}\n" + "\n".join(els) + "\n$EndElements\n")
+    typ = {"TRI3": "CPS3", "QUAD4": "CPE4R", "TRI6": "CPS6M", "QUAD8": "CPE8"}[ele]
+    lines = ["*NODE"] + [f"{i + 1}, {float(x)!r}, {float(y)!r}" for i, (x, y) in enumerate(m.points)]
+    lines += [f"*ELEMENT, TYPE={typ}"] + [", ".join([str(k + 1)] + [str(int(v) + 1) for v in c])
+                                           for k, c in enumerate(m.cells)]
+    (tmp_path / "p.inp").write_text("\n".join(lines) + "\n")
+    for name in ("p.msh", "p.inp"):
+        g = ut.read_mesh(str(tmp_path / name))
+        assert g.ele_type == ele and g.points.shape[1] == 2, name
+        np.testing.assert_array_equal(g.points[g.cells], m.points[m.cells])
+
+
+def test_boundary_cells_do_not_shadow_volume_cells(io, tmp_path):
+    """A 3D Gmsh mesh with its boundary triangles gives the tetrahedra unless
+    TRI3 is asked for; 2D cells off the z = 0 plane are refused."""
+    pkg, ut = io
+    nodes = "1 0 0 0\n2 1 0 0\n3 0 1 0\n4 0 0 1"
+    text = ("$MeshFormat\n2.2 0 8\n$EndMeshFormat\n$Nodes\n4\n" + nodes + "\n$EndNodes\n"
+            "$Elements\n3\n1 2 2 0 1 1 2 3\n2 4 2 0 1 1 2 3 4\n3 2 2 0 1 2 3 4\n$EndElements\n")
+    (tmp_path / "t.msh").write_text(text)
+    assert ut.read_mesh(str(tmp_path / "t.msh")).ele_type == "TET4"
+    with pytest.raises(ValueError, match="off the z = 0 plane"):
+        ut.read_mesh(str(tmp_path / "t.msh"), ele_type="TRI3")
+    (tmp_path / "u.msh").write_text(text.replace("3 2 2 0 1 2 3 4\n", "").replace("$Elements\n3", "$Elements\n2"))
+    tri = ut.read_mesh(str(tmp_path / "u.msh"), ele_type="TRI3")
+    assert tri.ele_type == "TRI3" and tri.points.shape == (3, 2)
