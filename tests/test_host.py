@@ -227,8 +227,17 @@ def test_solver_option_resolution(pkg):
     assert lc.method == pkg._native.KRYLOV_CG and lc.precond == pkg._native.PRECOND_JACOBI
     with pytest.raises(ValueError):
         s._resolve_solver_options({"newton": {}, "arc_length": {}})
-    with pytest.raises(NotImplementedError):
-        s.resolve_linear({"amgx_solver": {}})
+    # the reference's AMGX key: CG with the smoothed-aggregation AMG to an
+    # absolute residual of 1e-10 (its built-in configuration's tolerance)
+    lc = s.resolve_linear({"amgx_solver": {}})
+    assert lc.method == pkg._native.KRYLOV_CG and lc.gmg and lc.mg["amg"] and lc.atol == 1e-10 and lc.rtol == 0.0
+    with pytest.warns(UserWarning, match="configuration files"):
+        s.resolve_linear({"amgx_solver": {"cfg_path": "amgx.json"}})
+    lc = s.resolve_linear({"cg": {"precond": "amg", "mg_nu": 3}})
+    assert lc.gmg and lc.mg["amg"] and lc.mg["nu"] == 3 and lc.with_rtol(1e-6).mg["amg"]
+    assert not s.resolve_linear({"cg": {"precond": "gmg"}}).mg["amg"]
+    with pytest.raises(ValueError, match="'cg' only"):
+        s.resolve_linear({"bicgstab": {"precond": "amg"}})
     lc = s.resolve_linear({"cg": {"precond": "gmg", "rtol": "adaptive", "mg_lag": 4, "mg_nu_fine": 2, "mg_nu": 3}})
     assert lc.gmg and lc.adaptive and lc.eta_max == 1e-3
     assert lc.mg["lag"] == 4 and lc.mg["nu_fine"] == 2 and lc.mg["nu"] == 3 and lc.mg["coarse_steps"] == 8
