@@ -24,6 +24,7 @@ def _renumbered_tet10(pkg):
 
 
 @pytest.mark.gpu
+@pytest.mark.late
 @pytest.mark.parametrize("kind", ["linear", "neo_hookean"])
 def test_amg_newton_on_renumbered_tet10(pkg, cuda, kind):
     mesh = _renumbered_tet10(pkg)
@@ -56,6 +57,7 @@ def test_amg_newton_on_renumbered_tet10(pkg, cuda, kind):
 
 
 @pytest.mark.gpu
+@pytest.mark.late
 def test_amg_on_tri6_poisson(pkg, cuda):
     mesh = planar_box(pkg, "TRI6", (10, 8), amp=0.05, seed=4)
     bnd = lambda p: np.isclose(p[0], 0.0) | np.isclose(p[0], 1.0)  # noqa: E731

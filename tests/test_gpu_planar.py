@@ -35,6 +35,7 @@ def _boundary(p):
 
 
 @pytest.mark.gpu
+@pytest.mark.late
 @pytest.mark.parametrize("ele", ["TRI6", "QUAD4"])
 def test_planar_poisson_matches_oracle(pkg, cuda, ele):
     mesh = planar_box(pkg, ele, (6, 5), amp=0.1, seed=1)
@@ -59,6 +60,7 @@ def test_planar_poisson_matches_oracle(pkg, cuda, ele):
 
 
 @pytest.mark.gpu
+@pytest.mark.late
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
 def test_planar_neo_hookean_traction_matches_oracle(pkg, cuda, precision):
     mesh = planar_box(pkg, "QUAD8", (4, 2), L=(2.0, 1.0), amp=0.1, seed=2)
@@ -92,6 +94,7 @@ def test_planar_neo_hookean_traction_matches_oracle(pkg, cuda, precision):
 
 
 @pytest.mark.gpu
+@pytest.mark.late
 def test_planar_simp_adjoint_matches_finite_differences(pkg, cuda):
     mesh = planar_box(pkg, "QUAD4", (6, 3), L=(2.0, 1.0))
     C, Q = len(mesh.cells), 4
