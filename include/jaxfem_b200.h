@@ -484,6 +484,8 @@ FEM_API int fem_mg_pcg_solve_mixed(int vec, int64_t n_brows, const int32_t* d_ro
  *  - All calls share it: calls whose kernels overlap on the GPU race.
  *  - The first call on a device looks up the array's address
  *    (cudaGetSymbolAddress); make it before any stream capture.
+ *  - `stream` must belong to the current device; a stream of another device
+ *    returns FEM_ERR_ARG.
  * ------------------------------------------------------------------------ */
 FEM_API int fem_dot_f64_noalloc(int64_t n, const double* d_x, const double* d_y, double* d_out,
                                 void* stream);

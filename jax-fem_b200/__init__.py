@@ -14,12 +14,13 @@ from . import _native
 from .generate_mesh import Mesh, box_mesh, box_mesh_gmsh, check_mesh_TET4, get_meshio_cell_type, rectangle_mesh
 from .laws import J2Plasticity, Laplace, LinearElastic, NeoHookean, SIMPElastic
 from .problem import BSRMatrix, Problem, compliance
-from .solver import J2YieldSensitivity, ad_wrapper, get_A, get_q_vec, j2_reaction, solver, stress_divergence
+from .solver import (J2YieldSensitivity, ad_wrapper, get_A, get_q_vec, j2_reaction, reset_multigrid, solver,
+                     stress_divergence)
 from .utils import read_mesh, save_sol
 
 __all__ = ["Mesh", "box_mesh", "box_mesh_gmsh", "check_mesh_TET4", "get_meshio_cell_type", "rectangle_mesh",
            "Problem", "solver", "ad_wrapper", "get_A",
            "BSRMatrix", "compliance", "Laplace", "LinearElastic", "SIMPElastic", "NeoHookean",
            "J2Plasticity", "J2YieldSensitivity", "j2_reaction", "stress_divergence", "save_sol", "read_mesh",
-           "get_q_vec",
+           "get_q_vec", "reset_multigrid",
            "_native"]

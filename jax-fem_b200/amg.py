@@ -176,13 +176,14 @@ class AMG:
     """Smoothed-aggregation AMG preconditioned CG for one problem (see the
     module docstring).  Interface of the multigrid objects of solver.mg_solve."""
 
-    def __init__(self, problem, max_levels=10, coarse_size=500, theta=0.08):
+    def __init__(self, problem, max_levels=10, coarse_size=500, theta=0.08, nu_fine=0):
         if problem.num_vars != 1:
             raise NotImplementedError("precond 'amg' needs a problem of one variable")
         self.problem = problem
         fe = problem.fes[0]
         self.node_vec, self.points = fe.vec, fe.points
         self.max_levels, self.coarse_size, self.theta = int(max_levels), int(coarse_size), float(theta)
+        self.nu_fine = int(nu_fine)  # smoothing steps on the finest level (0: nu, as on the others)
         self.device = problem.dev().device
         self.T = None
         self.lmax = None
@@ -304,51 +305,85 @@ class AMG:
             Al, dinv, lmax = self.levels[level - 1]
             matvec = lambda v: Al.apply(v.contiguous(), torch.empty(Al.n_brows, dtype=v.dtype,  # noqa: E731
                                                                     device=v.device))
+        nu_l = self.nu_fine if (level == 0 and self.nu_fine > 0) else nu
         z = torch.zeros_like(b)
-        self._chebyshev(matvec, dinv, lmax, b, z, nu, ratio, zero_start=True)
+        self._chebyshev(matvec, dinv, lmax, b, z, nu_l, ratio, zero_start=True)
         r = (b - matvec(z)).contiguous()
         R, P = self.R[level], self.P[level]
         rc = R.apply(r, torch.empty(R.n_brows, dtype=b.dtype, device=b.device))
         zc = self._vcycle(level + 1, A, rc, nu, ratio).contiguous()
         z += P.apply(zc, torch.empty(P.n_brows, dtype=b.dtype, device=b.device))
-        return self._chebyshev(matvec, dinv, lmax, b, z, nu, ratio)
+        return self._chebyshev(matvec, dinv, lmax, b, z, nu_l, ratio)
 
     def apply(self, A, r, nu=2, ratio=30.0):
         return self._vcycle(0, A, r.contiguous(), nu, ratio)
 
     # ---- outer CG ----------------------------------------------------------------
-    def solve(self, A, b, x, rtol, atol=0.0, maxiter=1000, nu=2, coarse_steps=None, ratio=30.0, check_every=4):
-        """Preconditioned CG on A x = b (x: initial guess, in place); the
-        scalars stay on the device and the residual is read every
-        ``check_every`` iterations.  Returns (iterations, relative residual)."""
-        tmp = torch.empty_like(b)
-        A.matvec(x, tmp)
-        r = b - tmp
+    def solve(self, A, b, x, rtol, atol=0.0, maxiter=1000, nu=2, coarse_steps=None, ratio=30.0, check_every=4,
+              max_restarts=3, strict=True):
+        """Preconditioned CG on A x = b (x: initial guess, in place).
+
+        The scalars stay on the device; the recursive residual is read every
+        ``check_every`` iterations.  When it meets max(rtol ||b||, atol) the
+        true residual b - A x is formed, and when that misses the target CG
+        restarts from it (at most ``max_restarts`` times), as the native CG
+        of krylov.cu does.  A step whose curvature p.Ap is not positive
+        leaves x and r unchanged and ends the solve with FEM_ERR_BREAKDOWN at
+        the next check (the operator is not positive definite: the Newton
+        loop then retries with BiCGSTAB); ``maxiter`` iterations without
+        convergence end it with FEM_ERR_NOT_CONVERGED, unless ``strict`` is
+        False: the reference's AMGX call returns its last iterate whatever
+        the residual (solver.py:200-209), and so does this solve then.
+        Returns (iterations, relative true residual)."""
         bn = float(b.norm())
         target = max(rtol * bn, atol)
-        rn = float(r.norm())
-        if rn <= target:
-            return 0, rn / bn if bn > 0 else rn
-        z = self.apply(A, r, nu, ratio)
-        p = z.clone()
-        rz = r.dot(z)
-        q = torch.empty_like(b)
-        pq_min = torch.full((), math.inf, dtype=torch.float64, device=b.device)
-        for it in range(1, maxiter + 1):
-            A.matvec(p, q)
-            pq = p.dot(q)
-            torch.minimum(pq_min, pq, out=pq_min)
-            alpha = rz / pq
-            x.add_(alpha * p)
-            r.sub_(alpha * q)
-            if it % check_every == 0 or it == maxiter:
-                rn = float(r.norm())
-                if not float(pq_min) > 0.0:
-                    raise FloatingPointError("AMG-CG: the operator is not positive definite")
-                if rn <= target:
-                    return it, rn / bn if bn > 0 else rn
+        r, q = torch.empty_like(b), torch.empty_like(b)
+        zero = torch.zeros((), dtype=b.dtype, device=b.device)
+        total = 0
+        for restart in range(max_restarts + 1):
+            A.matvec(x, q)
+            torch.sub(b, q, out=r)
+            rn = float(r.norm())
+            if not math.isfinite(rn):
+                raise nat.FEMNativeError(nat.FEM_ERR_NONFINITE, "AMG-CG: non-finite residual")
+            if rn <= target:
+                return total, rn / bn if bn > 0 else rn
+            if restart == max_restarts or total >= maxiter:
+                break
             z = self.apply(A, r, nu, ratio)
-            rz_new = r.dot(z)
-            p.mul_(rz_new / rz).add_(z)
-            rz = rz_new
-        return maxiter, float(r.norm()) / bn if bn > 0 else float(r.norm())
+            p = z.clone()
+            rz = r.dot(z)
+            bad = torch.zeros((), dtype=torch.bool, device=b.device)
+            met = False
+            while total < maxiter:
+                total += 1
+                A.matvec(p, q)
+                pq = p.dot(q)
+                ok = pq > 0
+                bad |= ~ok
+                alpha = torch.where(ok, rz / torch.where(ok, pq, 1.0), zero)
+                x.add_(alpha * p)
+                r.sub_(alpha * q)
+                if total % check_every == 0 or total == maxiter:
+                    if bool(bad):
+                        raise nat.FEMNativeError(nat.FEM_ERR_BREAKDOWN,
+                                                 "AMG-CG: the operator is not positive definite")
+                    rn = float(r.norm())
+                    if not math.isfinite(rn):
+                        raise nat.FEMNativeError(nat.FEM_ERR_NONFINITE, "AMG-CG: non-finite residual")
+                    if rn <= target:
+                        met = True
+                        break
+                z = self.apply(A, r, nu, ratio)
+                rz_new = r.dot(z)
+                p.mul_(rz_new / rz).add_(z)
+                rz = rz_new
+            if not met:
+                break
+        if not strict:
+            A.matvec(x, q)
+            rn = float((b - q).norm())
+            return total, rn / bn if bn > 0 else rn
+        raise nat.FEMNativeError(nat.FEM_ERR_NOT_CONVERGED,
+                                 f"AMG-CG: relative residual {rn / bn if bn > 0 else rn:.3e} after {total} iterations "
+                                 f"(target {target / bn if bn > 0 else target:.3e})")

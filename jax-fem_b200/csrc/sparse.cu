@@ -224,6 +224,9 @@ extern "C" int fem_newton_rhs(int64_t ndofs, const double* d_res, const double* 
 //  - The first call on a device resolves the array's device address with
 //    cudaGetSymbolAddress (once per device, that device current).  Make that
 //    first call before any stream capture.
+//  - `stream` must belong to the device that is current on the calling
+//    thread (the address is that device's); a stream of another device is
+//    rejected with FEM_ERR_ARG.
 //  - The result is written to the caller's device double *d_out; the call is
 //    asynchronous on `stream` (no host synchronisation, no pinned buffer).
 // ---------------------------------------------------------------------------
@@ -265,10 +268,17 @@ extern "C" int fem_dot_f64_noalloc(int64_t n, const double* d_x, const double* d
                 (long long)n, (long long)fem::kNoAllocMaxN);
   FEM_CHECK_ARG(d_out != nullptr && (n == 0 || (d_x != nullptr && d_y != nullptr)),
                 "NULL pointer argument");
+  auto st = as_stream(stream);
+  if (st != nullptr) {
+    int cur = 0, sdev = 0;
+    FEM_CUDA_TRY(cudaGetDevice(&cur));
+    FEM_CUDA_TRY(cudaStreamGetDevice(st, &sdev));
+    FEM_CHECK_ARG(sdev == cur, "fem_dot_f64_noalloc: the stream belongs to device %d, not the current device %d",
+                  sdev, cur);
+  }
   double* scratch = nullptr;
   int rc = fem::noalloc_scratch(&scratch);
   if (rc != FEM_OK) return rc;
-  auto st = as_stream(stream);
   unsigned int* counter = reinterpret_cast<unsigned int*>(scratch);
   double* result = scratch + 8;
   double* partials = scratch + 16;

@@ -12,7 +12,10 @@ writes one ``<case>.npz`` per test with the arrays the parity tests need:
 - case-specific scalars (``traction``, ``surface_area``, ``disps``,
   ``avg_stresses``).
 
-Usage: python tests/golden/make_fixtures.py [reference_root]
+Usage: python tests/golden/make_fixtures.py REFERENCE_ROOT
+
+REFERENCE_ROOT is the root of a checkout of the reference project (the
+directory that holds its ``tests/benchmarks``).
 """
 import os
 import re
@@ -71,4 +74,6 @@ def main(ref_root):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        sys.exit("usage: python tests/golden/make_fixtures.py REFERENCE_ROOT")
+    main(sys.argv[1])

@@ -79,8 +79,8 @@ def test_aggregation_and_tentative_prolongator(pkg, amg):
     assert T2[:30].nnz == 0
 
 
-def _run_amg(amg, monkeypatch, A, free, points, vec, block, min_transfers=2):
-    """AMG's solve on CPU tensors; returns (iterations, solution, rhs)."""
+def _amg_on_cpu(amg, monkeypatch, A, free, points, vec, block):
+    """(AMG set up on CPU tensors, its operator stand-in)."""
     n = A.shape[0]
 
     def csr_apply(self, x, y):
@@ -105,6 +105,13 @@ def _run_amg(amg, monkeypatch, A, free, points, vec, block, min_transfers=2):
                                     dev=lambda: types.SimpleNamespace(device=torch.device("cpu")))
     g = amg.AMG(problem, coarse_size=60)
     g.setup(Aop)
+    return g, Aop
+
+
+def _run_amg(amg, monkeypatch, A, free, points, vec, block, min_transfers=2):
+    """AMG's solve on CPU tensors; returns (iterations, solution, rhs)."""
+    n = A.shape[0]
+    g, Aop = _amg_on_cpu(amg, monkeypatch, A, free, points, vec, block)
     assert len(g.T) >= min_transfers
     b = np.random.default_rng(1).normal(size=n) * free
     x = torch.zeros(n, dtype=torch.float64)
@@ -175,3 +182,38 @@ def test_amg_cg_on_quad8_poisson(pkg, amg, monkeypatch):
         counts.append((its, _pcg_iterations(A, b, 1)))
     (a0, j0), (a1, j1) = counts
     assert a1 <= 1.3 * a0 and j1 >= 1.9 * j0 and 5 * a1 < j1, counts
+
+
+def test_amg_cg_failures_are_reported(pkg, amg, monkeypatch):
+    """A failed AMG-CG solve raises the native error codes the Newton loop
+    acts on: FEM_ERR_BREAKDOWN on an indefinite operator (Newton then
+    retries with BiCGSTAB), FEM_ERR_NOT_CONVERGED at maxiter; with
+    strict=False (the reference's AMGX call, which returns its last iterate)
+    the solve returns its true residual instead."""
+    nat = importlib.import_module("jax_fem_b200._native")
+    points, cells = _renumbered_tet10(pkg)
+    bc = [[face_fn(0, 0.0)] * 3, [0, 1, 2], [lambda p: 0.0] * 3]
+    A, free = _eliminated(fo.OracleProblem(points, cells, 3, fo.Law("linear", E=70e3, nu=0.3),
+                                           dirichlet_bc_info=bc, ele_type="TET10"))
+    n = A.shape[0]
+    b = torch.from_numpy(np.random.default_rng(1).normal(size=n) * free)
+    g, Aop = _amg_on_cpu(amg, monkeypatch, A, free, points, 3, 3)
+    x = torch.zeros(n, dtype=torch.float64)
+    with pytest.raises(nat.FEMNativeError) as e:
+        g.solve(Aop, b, x, rtol=1e-10, maxiter=3)
+    assert e.value.status == nat.FEM_ERR_NOT_CONVERGED
+    x.zero_()
+    its, rel = g.solve(Aop, b, x, rtol=1e-10, maxiter=3, strict=False)
+    assert its == 3 and 1e-10 < rel < 1.0
+    r = b.numpy() - A @ x.numpy()
+    assert abs(np.linalg.norm(r) / np.linalg.norm(b.numpy()) - rel) <= 1e-12
+    # shift the free block by minus its median eigenvalue: indefinite
+    lam = np.sort(np.linalg.eigvalsh(A.toarray()[np.ix_(free > 0, free > 0)]))
+    shift = lam[len(lam) // 2]
+    A2 = (A - shift * sp.diags(free)).tocsr()
+    g2, Aop2 = _amg_on_cpu(amg, monkeypatch, A2, free, points, 3, 3)
+    x = torch.zeros(n, dtype=torch.float64)
+    with pytest.raises(nat.FEMNativeError) as e:
+        g2.solve(Aop2, b, x, rtol=1e-10, maxiter=200)
+    assert e.value.status == nat.FEM_ERR_BREAKDOWN
+    assert torch.isfinite(x).all()

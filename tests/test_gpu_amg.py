@@ -5,7 +5,12 @@ on meshes the geometric multigrid cannot take:
 - linear elasticity and Neo-Hookean Newton on a TET10 box whose nodes are
   randomly renumbered (no lattice numbering): the solution equals the
   oracle's (1e-8), with fewer CG iterations than block-Jacobi; the
-  reference's ``amgx_solver`` key solves the same linear problem;
+  reference's ``amgx_solver`` key solves the same linear problem.  Newton
+  stops at rel.res 1e-9: the residual at u = 0 is dominated by the
+  Dirichlet rows (a mismatch of 0.05), while the free rows are forces of
+  order E = 70e3 times the strains, so the assembled FP64 residual has a
+  round-off floor near eps * 70e3 / 0.05 ~ 2e-11 of it (a 1e-11 request
+  stalled there, at 1.97e-11); each linear solve still goes to 1e-11;
 - Poisson on curved TRI6 cells (a 2D problem on the cell-kernel path):
   the solution equals the oracle's (1e-9)."""
 import numpy as np
@@ -40,9 +45,10 @@ def test_amg_newton_on_renumbered_tet10(pkg, cuda, kind):
     iters = {}
     for precond in ("amg", "block_jacobi"):
         prob = P(mesh, vec=3, dim=3, ele_type="TET10", dirichlet_bc_info=bc)
-        opts = {"newton": {"rel_tol": 1e-11, "tol": 1e-14, "return_info": True,
+        opts = {"newton": {"rel_tol": 1e-9, "tol": 1e-14, "return_info": True,
                            "linear": {"cg": {"precond": precond, "rtol": 1e-11, "atol": 0.0, "maxiter": 20000}}}}
         sol, info = pkg.solver(prob, opts)
+        assert info["rel_res"] <= 1e-9, info["res_hist"]
         iters[precond] = sum(info["krylov_iters"])
         if precond == "amg":
             got = sol[0].cpu().numpy().reshape(-1)
@@ -52,7 +58,7 @@ def test_amg_newton_on_renumbered_tet10(pkg, cuda, kind):
     assert iters["amg"] < iters["block_jacobi"], iters
     if kind == "linear":
         prob = P(mesh, vec=3, dim=3, ele_type="TET10", dirichlet_bc_info=bc)
-        sol = pkg.solver(prob, {"newton": {"rel_tol": 1e-11, "tol": 1e-14, "linear": {"amgx_solver": {}}}})[0]
+        sol = pkg.solver(prob, {"newton": {"rel_tol": 1e-9, "tol": 1e-14, "linear": {"amgx_solver": {}}}})[0]
         assert np.abs(sol.cpu().numpy().reshape(-1) - ref).max() <= 1e-8 * np.abs(ref).max()
 
 

@@ -75,6 +75,30 @@ def test_config_neo_hookean_50(pkg, cuda):
 
 
 @pytest.mark.gpu
+def test_config_neo_hookean_50_headline_path(pkg, cuda):
+    """The exact path bench.py times as its headline value (mixed precision,
+    FP64 CG over an FP32 multigrid V-cycle, Eisenstat-Walker forcing, coarse
+    operators kept for up to 4 Newton solves): the oracle's residual of its
+    solution is <= 1e-8 of the residual at u = 0, and it agrees with the
+    plain FP64 path (tight block-Jacobi CG) to 1e-6.  Run twice, so that the
+    second solve starts with the hierarchy the first left behind."""
+    import bench
+    prob = bench.nh_problem(pkg, 50)
+    sol_p, _ = bench.nh_solve(pkg, prob, "fp64")
+    up = sol_p.cpu().numpy().reshape(-1)
+    bc = bench.rotation_bc(math.radians(30.0))
+    op = fo.OracleProblem(prob.mesh.points, prob.mesh.cells, 3, fo.Law("neo_hookean", E=10.0, nu=0.3),
+                          dirichlet_bc_info=bc)
+    zero = np.zeros(op.ndofs)
+    for _ in range(2):
+        sol_h, infos = bench.nh_solve(pkg, prob, bench.HEADLINE_PRECISION, linear=bench.HEADLINE_LINEAR)
+        uh = sol_h.cpu().numpy().reshape(-1)
+        assert all(i["rel_res"] <= 1e-8 for i in infos)
+        assert np.abs(uh - up).max() <= 1e-6 * np.abs(up).max()
+        assert _rel_residual(op, uh, zero) <= 1e-8
+
+
+@pytest.mark.gpu
 def test_config_simp_adjoint_vs_fd(pkg, cuda):
     ws = importlib.import_module("jax_fem_b200.warmstart")
     prob = ws.cantilever_problem(z0=0.0)
@@ -126,7 +150,7 @@ def test_config_simp_adjoint_vs_fd(pkg, cuda):
     assert abs(fd - ad) <= 1e-4 * abs(ad), (fd, ad)
 
 
-def _j2_history(pkg, cuda, mesh, sy, with_sens, rel_tol=1e-8):
+def _j2_history(pkg, cuda, mesh, sy, with_sens, rel_tol=1e-8, precision="fp64", linear=None):
     """10 increments of u_x(x=1) up to 0.02 on the J2 cube; returns the
     problem, the last solution, the state before the last commit, the last
     start, the bc list, the end reaction F and (with_sens) dF/dsigma_y."""
@@ -143,8 +167,9 @@ def _j2_history(pkg, cuda, mesh, sy, with_sens, rel_tol=1e-8):
     prob = J2(mesh, vec=3, dim=3, dirichlet_bc_info=bc)
     prob.internal_vars = [z(C, 8, 3, 3), z(C, 8, 3, 3), z(C, 8)]
     sens = pkg.J2YieldSensitivity(prob) if with_sens else None
-    opts = {"newton": {"rel_tol": rel_tol, "tol": 1e-14,
-                       "linear": {"cg": {"precond": "block_jacobi", "rtol": 1e-10, "atol": 0.0, "maxiter": 20000}}}}
+    opts = {"newton": {"rel_tol": rel_tol, "tol": 1e-14, "precision": precision,
+                       "linear": linear or {"cg": {"precond": "block_jacobi", "rtol": 1e-10, "atol": 0.0,
+                                                   "maxiter": 20000}}}}
     sol = None
     for k in range(1, 11):
         bc[2][-1] = (lambda v: (lambda p: v + 0.0 * p[0]))(0.02 * k / 10)
@@ -184,3 +209,29 @@ def test_config_j2_40(pkg, cuda):
     fd = (Fp - Fm) / (2 * h)
     print(f"J2 40^3: reaction {F:.10g}, dF/dsigma_y {dF:.10g}, central difference {fd:.10g}")
     assert abs(dF - fd) <= 1e-5 * abs(fd), (dF, fd)
+
+
+@pytest.mark.gpu
+def test_config_j2_40_mixed_gmg(pkg, cuda):
+    """The J2 40^3 history on the mixed multigrid path bench.py times
+    (mixed precision, FP64 CG over an FP32 V-cycle, adaptive forcing): after
+    the last increment the oracle's residual is <= 1e-8 of its value at the
+    increment's start, the committed state equals the oracle's return map
+    (1e-8), and the solution agrees with the plain FP64 history to 1e-6."""
+    n = 40
+    m = pkg.box_mesh(n, n, n, 1.0, 1.0, 1.0)
+    mesh = pkg.Mesh(m.points, m.cells_dict["hexahedron"])
+    gmg = {"cg": {"precond": "gmg", "rtol": "adaptive", "atol": 0.0, "maxiter": 20000}}
+    prob, sol, prev_state, start, bc, F, _ = _j2_history(pkg, cuda, mesh, 250.0, False, precision="mixed",
+                                                         linear=gmg)
+    u = sol.cpu().numpy().reshape(-1)
+    op = fo.OracleProblem(mesh.points, mesh.cells, 3, fo.Law("j2", E=70e3, nu=0.3, sig0=250.0, H=700.0),
+                          dirichlet_bc_info=bc, internal_vars=[prev_state[0], prev_state[1], prev_state[2]])
+    assert _rel_residual(op, u, start) <= 1e-8
+    fo.j2_commit(op, u)
+    sig = prob.internal_vars[0].cpu().numpy()
+    assert np.abs(sig - op.internal_vars[0]).max() <= 1e-8 * np.abs(op.internal_vars[0]).max()
+    _, sol_p, _, _, _, F_p, _ = _j2_history(pkg, cuda, mesh, 250.0, False)
+    up = sol_p.cpu().numpy().reshape(-1)
+    assert np.abs(u - up).max() <= 1e-6 * np.abs(up).max()
+    assert abs(F - F_p) <= 1e-6 * abs(F_p)
