@@ -6,8 +6,9 @@ TEST INFRASTRUCTURE ONLY: the timed CPU baseline of ``bench.py`` (its
 check it against the numpy oracle.  The product (``jax-fem_b200``) never
 imports, links or runs it.
 
-``build()`` compiles ``oracle/lib/libfem_cpu.so`` with g++ (x86-64-v3: AVX2
-and FMA, so the library built here runs on any current x86 host).
+``build()`` compiles ``oracle/lib/libfem_cpu.so`` with the recipe in
+``oracle/Makefile`` (g++, x86-64-v3: AVX2 and FMA, so a library built on one
+x86 host runs on any current one).
 """
 import ctypes as _c
 import os
@@ -18,7 +19,6 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 SRC = os.path.join(HERE, "fem_cpu.cpp")
 LIB = os.path.join(HERE, "lib", "libfem_cpu.so")
-FLAGS = ["-O3", "-march=x86-64-v3", "-fopenmp", "-fPIC", "-shared", "-std=c++17"]
 
 LAW_LINEAR, LAW_NEO_HOOKEAN = 0, 1
 METHOD_BICGSTAB, METHOD_CG = 0, 1  # jax_solve's BiCGSTAB + Jacobi; PETSc CG + Jacobi
@@ -30,8 +30,7 @@ def build(force=False):
     """Compile the library (when the source is newer than it, or ``force``)."""
     if not force and os.path.exists(LIB) and os.path.getmtime(LIB) >= os.path.getmtime(SRC):
         return LIB
-    os.makedirs(os.path.dirname(LIB), exist_ok=True)
-    subprocess.run(["g++", *FLAGS, "-o", LIB, SRC], check=True, capture_output=True, text=True)
+    subprocess.run(["make", "-B" if force else "-s", "-C", HERE], check=True, capture_output=True, text=True)
     return LIB
 
 
