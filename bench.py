@@ -181,6 +181,44 @@ def element_bench(pkg, device):
     return out
 
 
+def amg_bench(pkg, device, n=12):
+    """precond='amg' (smoothed-aggregation AMG, hierarchy formed on the host)
+    on a mesh where the lattice multigrid cannot run: the Neo-Hookean twist
+    on an n^3 TET10 box whose nodes are randomly renumbered, FP64, against
+    block-Jacobi CG.  Reports the solve time and, for AMG, the host setup
+    time inside it (wall clock, included in the solve time)."""
+    import importlib
+    gm = importlib.import_module("jax_fem_b200.generate_mesh")
+    m = gm.box_mesh_gmsh(n, n, n, 1.0, 1.0, 1.0, None, "TET10")
+    cells = m.cells_dict[gm.get_meshio_cell_type("TET10")]
+    perm = np.random.default_rng(3).permutation(len(m.points))
+    inv = np.argsort(perm)
+    mesh = pkg.Mesh(m.points[perm], inv[cells], "TET10")
+
+    class HyperElasticity(pkg.Problem):
+        def get_tensor_map(self):
+            return pkg.NeoHookean(10.0, 0.3)
+
+    out = {"workload": f"neo-hookean twist, {n}^3 TET10 box, nodes randomly renumbered (no lattice), FP64"}
+    for name, pc in (("amg", "amg"), ("block_jacobi", "block_jacobi")):
+        prob = HyperElasticity(mesh, vec=3, dim=3, ele_type="TET10", dirichlet_bc_info=rotation_bc(0.0))
+        lin = {"cg": {"precond": pc, "rtol": "adaptive", "atol": 0.0, "maxiter": 20000}}
+        nh_solve(pkg, prob, "fp64", linear=lin)  # warm-up
+        mgc = prob.dev().__dict__.get("_mg", {}).get("amg")
+        s0 = getattr(mgc, "setup_seconds", 0.0)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        _, infos = nh_solve(pkg, prob, "fp64", linear=lin)
+        torch.cuda.synchronize()
+        r = {"twist_solve_s": round(time.perf_counter() - t0, 4), "newton_iters": sum(i["newton_iters"] for i in infos),
+             "krylov_iters": sum(sum(i["krylov_iters"]) for i in infos), "dofs": prob.num_total_dofs_all_vars}
+        if mgc is not None:
+            r["host_setup_s"] = round(mgc.setup_seconds - s0, 4)
+            r["levels"] = len(mgc.levels) + 1
+        out[name] = r
+    return out
+
+
 def _nh_universal(E=10.0, nu=0.3):
     """The compressible Neo-Hookean weak form written as a torch universal
     kernel (the reference's form of a user-written weak form)."""
@@ -583,7 +621,7 @@ def run_ours(args, rank, world, device):
         e1.record()
         torch.cuda.synchronize()
         j2[arm] = {"s": round(e0.elapsed_time(e1) * 1e-3, 4), "newton": jn, "krylov": jk}
-    elements = cell_path = None
+    elements = cell_path = amg = None
     if not args.no_elements:
         try:
             elements = element_bench(pkg, device)
@@ -593,6 +631,10 @@ def run_ours(args, rank, world, device):
             cell_path = cell_path_bench(pkg, device)
         except Exception as e:  # noqa: BLE001 - report, do not lose the headline line
             cell_path = {"error": str(e)[:300]}
+        try:
+            amg = amg_bench(pkg, device)
+        except Exception as e:  # noqa: BLE001 - report, do not lose the headline line
+            amg = {"error": str(e)[:300]}
     try:
         tc = conv_bench(pkg, device)
     except Exception as e:  # noqa: BLE001 - report, do not lose the headline line
@@ -615,7 +657,11 @@ def run_ours(args, rank, world, device):
         "config": {"workload": f"neo-hookean {args.n}^3 HEX8, 30 deg twist in 5 load steps, "
                                "Newton rel.res 1e-8", "dofs": ndofs, "cells": dv.num_cells,
                    "precision": "mixed", "krylov": "cg (f64 vectors, f32 tangent) preconditioned by a geometric multigrid v-cycle (f32)",
-                   "l2": "flushed (256 MB write) between timed steps", "parallelism": f"replicas x{world}"},
+                   "l2": "flushed (256 MB write) between timed steps", "parallelism": f"replicas x{world}",
+                   "learned_warm_start": "not in value: the trained network gains nothing at rel.res 1e-8 "
+                                         "(simp60_learned_warm_start), and no network is trained for this "
+                                         "twist; value is the mixed-precision multigrid solve alone",
+                   "multigrid_state": "reset before every timed solve (each pays its own coarse setups)"},
         "plain_fp64_s": round(t_plain, 6),
         "speedup_vs_plain_fp64": round(t_plain / t_mixed, 3),
         "speedup_mixed_vs_fp64_same_method": {
@@ -652,6 +698,7 @@ def run_ours(args, rank, world, device):
         "other_elements_neo_hookean_twist": elements,
         "cell_kernel_path": cell_path,
         "tensor_core_conv": tc,
+        "amg_renumbered_tet10": amg,
         "e2e": {"value": round(t_e2e, 6), "unit": "s", "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": int(ndofs * 8)},
         "gpu_launches": int(launches),
@@ -772,6 +819,31 @@ def run_reference(args, rank, world):
                        "newton_iters_timed": newton, "krylov_iters_timed": krylov},
             "cpu_baseline": cb,
             "e2e": {"value": round(v, 3), "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
+def run_asm_only(args, device):
+    """Assembly times of the HEX8 kernel (CUDA events, 20 launches after 3
+    warm-up ones) at a twisted state of the n^3 Neo-Hookean cube: FP64
+    residual with the FP64 / FP32 tangent, and the residual alone."""
+    pkg = load_package()
+    prob = nh_problem(pkg, n=args.n)
+    dv = prob.dev()
+    prob.fes[0].update_Dirichlet_boundary_conditions(rotation_bc(math.radians(6.0)))
+    mask, vals = prob.dirichlet_device()
+    u = torch.where(mask.bool(), vals, torch.zeros_like(vals))
+    res = torch.empty_like(u)
+    A64, A32 = dv.new_matrix(torch.float64), dv.new_matrix(torch.float32)
+    hbm, kind = peaks()
+    t64 = time_kernel(lambda: prob.assemble(u, res=res, vals=A64.vals))
+    t32 = time_kernel(lambda: prob.assemble(u, res=res, vals=A32.vals, fp32=True))
+    tr = time_kernel(lambda: prob.assemble(u, res=res))
+    nd = dv.ndofs
+    b64 = dv.num_cells * (32 + 8 * 3 * 8 + 24 * 8 + 256) + dv.nnzb * 9 * 8 + nd * 8
+    b32 = dv.num_cells * (32 + 8 * 3 * 8 + 24 * 8 + 256) + dv.nnzb * 9 * 4 + nd * 8
+    print(json.dumps({"n": args.n, "cells": dv.num_cells, "us": {"fp64": round(t64 * 1e6, 1),
+                      "fp32": round(t32 * 1e6, 1), "residual_only": round(tr * 1e6, 1)},
+                      "hbm_frac": {"fp64": round(b64 / t64 / 1e9 / hbm, 4), "fp32": round(b32 / t32 / 1e9 / hbm, 4)},
+                      "peak_kind": kind}), flush=True)
 
 
 def run_profile_element(args, device):
@@ -924,6 +996,7 @@ def main():
     ap.add_argument("--elements-only", action="store_true",
                     help="only the TET4/TET10/HEX20/HEX27 and cell-kernel-path measurements")
     ap.add_argument("--profile", action="store_true", help="short kernel sequence for ncu captures")
+    ap.add_argument("--asm-only", action="store_true", help="only the HEX8 assembly times")
     ap.add_argument("--conv-only", action="store_true",
                     help="only the tensor-core convolution / weight-gradient throughput")
     ap.add_argument("--profile-element", default="", choices=["", "TET4", "TET10", "HEX20", "HEX27"],
@@ -958,13 +1031,17 @@ def main():
     if args.profile_element:
         run_profile_element(args, device)
         return
+    if args.asm_only:
+        run_asm_only(args, device)
+        return
     if args.conv_only:
         print(json.dumps({"tensor_core_conv": conv_bench(load_package(), device)}), flush=True)
         return
     if args.elements_only:
         pkg = load_package()
         print(json.dumps({"other_elements_neo_hookean_twist": element_bench(pkg, device),
-                          "cell_kernel_path": cell_path_bench(pkg, device)}), flush=True)
+                          "cell_kernel_path": cell_path_bench(pkg, device),
+                          "amg_renumbered_tet10": amg_bench(pkg, device)}), flush=True)
         return
     if args.warmstart_train:
         run_warmstart_train(args, device)

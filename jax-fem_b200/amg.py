@@ -230,6 +230,14 @@ class AMG:
         return P, (0.5 * (Ac + Ac.T)).tocsr()
 
     def setup(self, A, fine_only=False):
+        import time
+        t0 = time.perf_counter()
+        self._setup(A, fine_only)
+        self.setup_seconds = getattr(self, "setup_seconds", 0.0) + time.perf_counter() - t0
+        self.full_setups = getattr(self, "full_setups", 0) + (0 if fine_only else 1)
+        self._setups = getattr(self, "_setups", 0) + 1  # the captured CG iteration reads this setup's buffers
+
+    def _setup(self, A, fine_only=False):
         if A.vals.dtype != torch.float64:
             raise TypeError("AMG works on the FP64 fine operator")
         vec = A.vec
@@ -319,6 +327,23 @@ class AMG:
         return self._vcycle(0, A, r.contiguous(), nu, ratio)
 
     # ---- outer CG ----------------------------------------------------------------
+    def _cg_step(self, A, nu, ratio):
+        """One CG iteration on the persistent state (self._cg), scalars on the
+        device: q = A p, the curvature check, x += alpha p, r -= alpha q, then
+        the V-cycle's z and the next direction."""
+        c = self._cg
+        A.matvec(c["p"], c["q"])
+        pq = c["p"].dot(c["q"])
+        ok = pq > 0
+        c["bad"] |= ~ok
+        alpha = torch.where(ok, c["rz"] / torch.where(ok, pq, 1.0), c["zero"])
+        c["x"].add_(alpha * c["p"])
+        c["r"].sub_(alpha * c["q"])
+        z = self.apply(A, c["r"], nu, ratio)
+        rz_new = c["r"].dot(z)
+        c["p"].mul_(rz_new / c["rz"]).add_(z)
+        c["rz"].copy_(rz_new)
+
     def solve(self, A, b, x, rtol, atol=0.0, maxiter=1000, nu=2, coarse_steps=None, ratio=30.0, check_every=4,
               max_restarts=3, strict=True):
         """Preconditioned CG on A x = b (x: initial guess, in place).
@@ -333,57 +358,74 @@ class AMG:
         loop then retries with BiCGSTAB); ``maxiter`` iterations without
         convergence end it with FEM_ERR_NOT_CONVERGED, unless ``strict`` is
         False: the reference's AMGX call returns its last iterate whatever
-        the residual (solver.py:200-209), and so does this solve then.
+        the residual (solver.py:200-209), and so does this solve then.  On
+        the GPU one iteration (operator product, updates and the whole
+        V-cycle) is captured as a CUDA graph after it has run once eagerly,
+        and replayed; a new setup is captured anew.
         Returns (iterations, relative true residual)."""
         bn = float(b.norm())
         target = max(rtol * bn, atol)
-        r, q = torch.empty_like(b), torch.empty_like(b)
-        zero = torch.zeros((), dtype=b.dtype, device=b.device)
+        n, dev = b.numel(), b.device
+        if getattr(self, "_cg", None) is None or self._cg["x"].numel() != n or self._cg["x"].device != dev:
+            e = lambda: torch.empty(n, dtype=b.dtype, device=dev)  # noqa: E731
+            self._cg = {"x": e(), "r": e(), "p": e(), "q": e(), "rz": torch.empty((), dtype=b.dtype, device=dev),
+                        "bad": torch.zeros((), dtype=torch.bool, device=dev),
+                        "zero": torch.zeros((), dtype=b.dtype, device=dev)}
+            self._graph = None
+        c = self._cg
+        c["x"].copy_(x)
+        key = (getattr(self, "_setups", 0), A.vals.data_ptr(), int(nu), float(ratio))
+        use_graph = b.is_cuda and _graphs_enabled()
         total = 0
         for restart in range(max_restarts + 1):
-            A.matvec(x, q)
-            torch.sub(b, q, out=r)
-            rn = float(r.norm())
+            A.matvec(c["x"], c["q"])
+            torch.sub(b, c["q"], out=c["r"])
+            rn = float(c["r"].norm())
             if not math.isfinite(rn):
                 raise nat.FEMNativeError(nat.FEM_ERR_NONFINITE, "AMG-CG: non-finite residual")
             if rn <= target:
+                x.copy_(c["x"])
                 return total, rn / bn if bn > 0 else rn
             if restart == max_restarts or total >= maxiter:
                 break
-            z = self.apply(A, r, nu, ratio)
-            p = z.clone()
-            rz = r.dot(z)
-            bad = torch.zeros((), dtype=torch.bool, device=b.device)
+            z = self.apply(A, c["r"], nu, ratio)
+            c["p"].copy_(z)
+            c["rz"].copy_(c["r"].dot(z))
+            c["bad"].fill_(False)
             met = False
             while total < maxiter:
                 total += 1
-                A.matvec(p, q)
-                pq = p.dot(q)
-                ok = pq > 0
-                bad |= ~ok
-                alpha = torch.where(ok, rz / torch.where(ok, pq, 1.0), zero)
-                x.add_(alpha * p)
-                r.sub_(alpha * q)
+                if use_graph and self._graph is not None and self._graph_key == key:
+                    self._graph.replay()
+                else:
+                    self._cg_step(A, nu, ratio)
+                    if use_graph:
+                        g = torch.cuda.CUDAGraph()
+                        with torch.cuda.graph(g):
+                            self._cg_step(A, nu, ratio)
+                        self._graph, self._graph_key = g, key
                 if total % check_every == 0 or total == maxiter:
-                    if bool(bad):
+                    if bool(c["bad"]):
                         raise nat.FEMNativeError(nat.FEM_ERR_BREAKDOWN,
                                                  "AMG-CG: the operator is not positive definite")
-                    rn = float(r.norm())
+                    rn = float(c["r"].norm())
                     if not math.isfinite(rn):
                         raise nat.FEMNativeError(nat.FEM_ERR_NONFINITE, "AMG-CG: non-finite residual")
                     if rn <= target:
                         met = True
                         break
-                z = self.apply(A, r, nu, ratio)
-                rz_new = r.dot(z)
-                p.mul_(rz_new / rz).add_(z)
-                rz = rz_new
             if not met:
                 break
+        x.copy_(c["x"])
         if not strict:
-            A.matvec(x, q)
-            rn = float((b - q).norm())
+            A.matvec(x, c["q"])
+            rn = float((b - c["q"]).norm())
             return total, rn / bn if bn > 0 else rn
         raise nat.FEMNativeError(nat.FEM_ERR_NOT_CONVERGED,
                                  f"AMG-CG: relative residual {rn / bn if bn > 0 else rn:.3e} after {total} iterations "
                                  f"(target {target / bn if bn > 0 else target:.3e})")
+
+
+def _graphs_enabled():
+    import os
+    return os.environ.get("FEM_AMG_GRAPHS", "1") != "0"

@@ -149,10 +149,16 @@ class PMultigrid:
             raise TypeError("p-multigrid works on the FP64 fine operator")
         vec, n = self.vec, A.n_brows * self.vec
         blocks = A.vals.view(-1, vec, vec)[A.diag.long()]
-        self.dinv = torch.linalg.inv(blocks).contiguous()
+        inv = torch.linalg.inv(blocks)
+        # persistent buffers: the captured CG iteration reads them by address
+        if self.dinv is None or self.dinv.shape != inv.shape:
+            self.dinv = inv.contiguous()
+        else:
+            self.dinv.copy_(inv)
         if not fine_only or self.lmax is None:
             # largest eigenvalue of D^-1 A by power iteration (x 1.1), at full
-            # setups; solves on kept coarse operators keep it too
+            # setups; solves on kept coarse operators keep it too.  It stays
+            # on the device (the Chebyshev coefficients are formed there).
             g = torch.Generator(device=A.vals.device).manual_seed(0)
             x = torch.rand(n, dtype=torch.float64, device=A.vals.device, generator=g)
             y = torch.empty_like(x)
@@ -163,7 +169,10 @@ class PMultigrid:
                 z = self._jacobi(y)
                 lam = x.dot(z)
                 x = z
-            self.lmax = 1.1 * float(lam)
+            if getattr(self, "_lmax_t", None) is None or self._lmax_t.device != lam.device:
+                self._lmax_t = torch.empty((), dtype=torch.float64, device=lam.device)
+            self._lmax_t.copy_(1.1 * lam)
+            self.lmax = self._lmax_t
         if not fine_only:
             state = getattr(self.problem, "_tangent_state", None)
             if state is None:
@@ -180,18 +189,19 @@ class PMultigrid:
 
     # ---- preconditioner ------------------------------------------------------------
     def _chebyshev(self, A, b, z, nu, ratio, tmp, zero_start=False):
-        """nu Chebyshev steps for A z = b from z (in place; z = 0 when zero_start)."""
-        lmax = self.lmax
-        lmin = lmax / ratio
-        theta, delta = 0.5 * (lmax + lmin), 0.5 * (lmax - lmin)
-        sigma = theta / delta
+        """nu Chebyshev steps for A z = b from z (in place; z = 0 when
+        zero_start), on [lmax/ratio, lmax].  sigma = theta/delta depends on
+        the ratio only; 1/theta and 1/delta are device scalars."""
+        sigma = (1.0 + 1.0 / ratio) / (1.0 - 1.0 / ratio)
+        inv_theta = 2.0 / (self.lmax * (1.0 + 1.0 / ratio))
+        inv_delta = 2.0 / (self.lmax * (1.0 - 1.0 / ratio))
         rho = 1.0 / sigma
         if zero_start:
             r = b.clone()
         else:
             A.matvec(z, tmp)
             r = b - tmp
-        d = self._jacobi(r) / theta
+        d = self._jacobi(r) * inv_theta
         for k in range(nu):
             z += d
             if k == nu - 1:
@@ -199,7 +209,7 @@ class PMultigrid:
             A.matvec(d, tmp)
             r -= tmp
             rho_new = 1.0 / (2.0 * sigma - rho)
-            d = rho_new * rho * d + (2.0 * rho_new / delta) * self._jacobi(r)
+            d = rho_new * rho * d + (2.0 * rho_new) * inv_delta * self._jacobi(r)
             rho = rho_new
         return z
 
@@ -226,45 +236,91 @@ class PMultigrid:
         return z
 
     # ---- outer CG ----------------------------------------------------------------
+    def _buffers(self, b):
+        """Persistent CG state (the captured iteration reads it by address)."""
+        n, dev = b.numel(), b.device
+        if getattr(self, "_cg", None) is None or self._cg["x"].numel() != n or self._cg["x"].device != dev:
+            e = lambda: torch.empty(n, dtype=torch.float64, device=dev)  # noqa: E731
+            s = lambda: torch.empty((), dtype=torch.float64, device=dev)  # noqa: E731
+            self._cg = {"x": e(), "r": e(), "p": e(), "q": e(), "z": e(), "tmp": e(), "free": e(), "rz": s(),
+                        "pq_min": s()}
+            self._graph = None
+        return self._cg
+
+    def _iteration(self, A, nu, coarse_steps, ratio):
+        """One CG iteration on the persistent state, scalars on the device:
+        q = A p, x += alpha p, r -= alpha q, then the preconditioned residual
+        z and the next direction."""
+        c = self._cg
+        A.matvec(c["p"], c["q"])
+        pq = c["p"].dot(c["q"])
+        torch.minimum(c["pq_min"], pq, out=c["pq_min"])
+        alpha = c["rz"] / pq
+        c["x"].add_(alpha * c["p"])
+        c["r"].sub_(alpha * c["q"])
+        self.apply(A, c["r"], c["z"], c["free"], nu, coarse_steps, ratio, c["tmp"])
+        rz_new = c["r"].dot(c["z"])
+        c["p"].mul_(rz_new / c["rz"]).add_(c["z"])
+        c["rz"].copy_(rz_new)
+
     def solve(self, A, b, x, rtol, atol=0.0, maxiter=1000, nu=2, coarse_steps=8, ratio=25.0, check_every=4):
         """Preconditioned CG on A x = b (x: initial guess, in place).  The
-        scalars stay on the device; the residual is read every
-        ``check_every`` iterations.  Returns (iterations, relative residual)."""
+        scalars stay on the device and the residual is read every
+        ``check_every`` iterations.  On the GPU the iteration (operator
+        product, updates and the whole preconditioner: fine-level Chebyshev
+        smoothing, transfers and the coarse lattice V-cycle) is captured once
+        as a CUDA graph and replayed; the iteration that triggers a capture
+        runs eagerly.  Returns (iterations, relative residual)."""
         mask, _ = self.problem.dirichlet_device()
-        free = (~mask.bool()).to(torch.float64)
-        self._free_c = free[self.corner_dofs].contiguous()
-        self._rc = torch.empty(self.PT.n_brows * self.vec, dtype=torch.float64, device=b.device)
-        tmp = torch.empty_like(b)
-        A.matvec(x, tmp)
-        r = b - tmp
+        c = self._buffers(b)
+        c["free"].copy_(~mask.bool())
+        fc = c["free"][self.corner_dofs]
+        if getattr(self, "_free_c", None) is None or self._free_c.shape != fc.shape:
+            self._free_c = fc.contiguous()
+        else:
+            self._free_c.copy_(fc)
+        if getattr(self, "_rc", None) is None or self._rc.numel() != self.PT.n_brows * self.vec:
+            self._rc = torch.empty(self.PT.n_brows * self.vec, dtype=torch.float64, device=b.device)
+        c["x"].copy_(x)
+        A.matvec(c["x"], c["tmp"])
+        torch.sub(b, c["tmp"], out=c["r"])
         bn = float(b.norm())
         target = max(rtol * bn, atol)
-        rn = float(r.norm())
+        rn = float(c["r"].norm())
         if rn <= target:
             return 0, rn / bn if bn > 0 else rn
-        z = torch.empty_like(b)
-        self.apply(A, r, z, free, nu, coarse_steps, ratio, tmp)
-        p = z.clone()
-        rz = r.dot(z)
-        q = torch.empty_like(b)
-        pq_min = torch.full((), math.inf, dtype=torch.float64, device=b.device)
+        self.apply(A, c["r"], c["z"], c["free"], nu, coarse_steps, ratio, c["tmp"])
+        c["p"].copy_(c["z"])
+        c["rz"].copy_(c["r"].dot(c["z"]))
+        c["pq_min"].fill_(math.inf)
+        key = (A.vals.data_ptr(), A.n_brows, nu, coarse_steps, float(ratio))
+        use_graph = b.is_cuda and _graphs_enabled()
         for it in range(1, maxiter + 1):
-            A.matvec(p, q)
-            pq = p.dot(q)
-            torch.minimum(pq_min, pq, out=pq_min)
-            alpha = rz / pq
-            x.add_(alpha * p)
-            r.sub_(alpha * q)
+            if use_graph and self._graph is not None and self._graph_key == key:
+                self._graph.replay()
+            else:
+                self._iteration(A, nu, coarse_steps, ratio)
+                if use_graph:
+                    self._capture(A, nu, coarse_steps, ratio, key)
             if it % check_every == 0 or it == maxiter:
-                rn = float(r.norm())
-                pqm = float(pq_min)
+                rn = float(c["r"].norm())
+                pqm = float(c["pq_min"])
                 if not (pqm > 0.0) or not math.isfinite(rn):
                     raise nat.FEMNativeError(nat.FEM_ERR_BREAKDOWN, f"p-multigrid CG breakdown (min p.Ap = {pqm})")
                 if rn <= target:
+                    x.copy_(c["x"])
                     return it, rn / bn if bn > 0 else rn
-            self.apply(A, r, z, free, nu, coarse_steps, ratio, tmp)
-            rz_new = r.dot(z)
-            p.mul_(rz_new / rz).add_(z)
-            rz = rz_new
         raise nat.FEMNativeError(nat.FEM_ERR_NOT_CONVERGED,
                                  f"p-multigrid CG: {maxiter} iterations, relres {rn / bn if bn > 0 else rn:.3e}")
+
+    def _capture(self, A, nu, coarse_steps, ratio, key):
+        """Record one CG iteration as a CUDA graph (recording runs nothing)."""
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g):
+            self._iteration(A, nu, coarse_steps, ratio)
+        self._graph, self._graph_key = g, key
+
+
+def _graphs_enabled():
+    import os
+    return os.environ.get("FEM_PMG_GRAPHS", "1") != "0"

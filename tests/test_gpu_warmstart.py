@@ -66,21 +66,27 @@ def test_network_trains_and_predicts(pkg, cuda):
 
 
 @pytest.mark.gpu
-def test_trained_network_gain_on_heldout(pkg, cuda):
-    """What the committed trained network gains over the zero start on
-    held-out SIMP cantilevers (seeds disjoint from training).
+def test_trained_network_effect_on_heldout(pkg, cuda):
+    """What the committed trained network does on held-out SIMP cantilevers
+    (seeds disjoint from training), measured against the zero start.
 
-    Asserted:
+    Asserted, from measurements of this network:
     - the raw prediction's relative displacement error ||u* - d|| / ||u*||
-      is below 0.1 (the zero start's is 1);
+      is below 0.1 (the zero start's is 1): the network has learned the
+      displacement field to a few per cent;
     - the Galerkin-scaled start's energy-norm error ||u* - u0||_K / ||u*||_K
-      is below 1 (the zero start's is 1).
-    Recorded: Krylov iterations from both starts to the same absolute
-    residual (1e-8 of the zero-start residual) on the FP64 path and on the
-    mixed path with FP32 CG inside FP64 refinement.  The raw prediction's
-    strain is noisy (its energy-norm error is above 1), so the Galerkin
-    factor shrinks it, and CG, which resolves the smooth error no later than
-    the rest, gains about nothing at 1e-8."""
+      is below 1 (the zero start's is 1);
+    - to the same absolute residual (1e-8 of the zero-start residual) the
+      learned start takes at most 5 % more Krylov iterations than the zero
+      start, on the FP64 path and on the mixed path (FP32 CG inside FP64
+      refinement).
+    Not asserted, because it does not hold: a gain at rel.res 1e-8.  The
+    raw prediction's strain is noisy (its energy-norm error is above 1), so
+    the Galerkin factor shrinks it to an energy-norm error of about 0.9,
+    and CG, which removes the smooth error no later than the rest, gains
+    about nothing at 1e-8 (measured 1110 vs 1108 iterations on the FP64
+    path).  This is the measured ceiling of a coarse-grid (2h) prediction
+    of this high-contrast field."""
     import os
     ws = _ws()
     path = os.path.join(os.path.dirname(ws.__file__), "weights", "warmstart_simp60.pt")
@@ -112,3 +118,5 @@ def test_trained_network_gain_on_heldout(pkg, cuda):
           f"krylov {iters}")
     assert max(l2) < 0.1
     assert max(energy) < 1.0
+    for prec in ("fp64", "mixed"):
+        assert sum(iters[f"{prec}_learned"]) <= 1.05 * sum(iters[f"{prec}_zero"]), iters
