@@ -6,12 +6,29 @@
 // (problem.py:426-437) and the PETSc COO insertion + zeroRows of get_A
 // (solver.py:485-491).  The reference differentiates the kernel with 24
 // forward-mode JVPs per cell; here every law supplies its exact tangent in a
-// rank-structured form (law_quad / pair_row below), so one evaluation per
-// quadrature point yields residual and tangent together.
+// rank-structured form (see law_quad below), so one evaluation per quadrature
+// point yields residual and tangent together.
 //
 // Precision: geometry, the constitutive update and the residual are FP64 in
-// every variant; the tangent (its per-quad factors and node vectors in shared
-// memory, the row products and the stored values) is FP64 or FP32.
+// every variant; the tangent (its per-quad factors in shared memory, the
+// node-pair products and the stored values) is FP64 or FP32.
+//
+// Work split: 12 threads per cell, 8 cells (96 threads) per block.
+//  phase 0  thread t < 8 loads node t of its cell (coords, u, Dirichlet data)
+//  phase 1  thread t < 8 = quadrature point q: geometry (J, det, grad N),
+//           grad u, the constitutive update; P*JxW (FP64) and the tangent
+//           factors -> smem
+//  phase 2  residual: thread t < 8 = node a, r_a = sum_q P_q g_a,q in FP64;
+//           tangent: every element matrix here is symmetric, so only the 36
+//           node pairs a <= b are formed, three per thread.  Each pair goes
+//           to the block of the global upper triangle (row node < column
+//           node), transposed when the local order is reversed, through the
+//           precomputed cell->block map (no sort, no search), with Dirichlet
+//           row/column elimination.  The lift K d of the eliminated columns
+//           gathers per cell in shared memory.
+//  mirror   a second kernel writes each lower block as the transpose of its
+//           upper partner, so the stored matrix stays the full block CSR.
+// A cell's threads span warps, so phases are separated by __syncthreads.
 #include "common.cuh"
 #include "tangent.cuh"
 
@@ -35,86 +52,69 @@ struct AsmArgs {
   double p[4];
 };
 
-// ---- work split --------------------------------------------------------------
-// Each warp owns groups of kGroupCells = 4 consecutive cells and loops over
-// them (grid-stride); warps share nothing, so only __syncwarp orders the
-// phases.  For one group:
-//  phase 0  lane = (cell, node): connectivity, coordinates, u, the prescribed
-//           increment d and the Dirichlet bits of one node -> warp smem
-//  phase 1  lane = (cell, quadrature point), all 32 lanes busy: FP64
-//           geometry, grad u and the constitutive update; the per-node law
-//           vectors and the tangent coefficients (type T) -> warp smem; the
-//           residual contributions of the 8 nodes are summed over the cell's
-//           8 lanes by a transposed shuffle reduction (each round halves the
-//           values a lane holds, 21 FP64 shuffles), after which lane q holds
-//           node q's residual and adds it to R with 3 atomics
-//  phase 2  lane = element-matrix row (node a, component i); for VEC = 3 one
-//           cell per pass (24 lanes), for VEC = 1 four cells per pass.  Every
-//           element matrix here is symmetric, so of the 64 node blocks only
-//           36 are formed: row a takes the blocks (a, a + j mod 8), j = 0..3,
-//           and j = 4 for a < 4 (each unordered pair once; 5 or 4 blocks per
-//           lane).  The lane keeps its own node's vectors in registers and
-//           reads node b's from the record; as the lanes of a warp read one
-//           record at 8 distinct nodes, whose rows are laid out bank-disjoint,
-//           a 16-byte load is a single shared-memory wavefront.  The blocks go
-//           to the global upper triangle (row node < column node), transposed
-//           when the local order is reversed, through the cell -> block map,
-//           with Dirichlet rows and columns left out; the lift K d of the
-//           eliminated columns is gathered per cell in warp smem.
-//  mirror   finish_tangent writes each lower block as the transpose of its
-//           upper partner, and the unit diagonal at Dirichlet dofs.
-constexpr int kGroupCells = 4;
-constexpr int kAsmWarps = 4;
-constexpr int kAsmThreads = 32 * kAsmWarps;
+constexpr int kCellsPerBlock = 8;
+constexpr int kThreadsPerCell = 12;
+constexpr int kAsmThreads = kCellsPerBlock * kThreadsPerCell;
 
-// Per-node vectors a law stores per quadrature point: g (physical shape
-// gradient) for all; NH adds f = F g and h = F^-T g; J2 adds s g (deviatoric
-// trial stress applied to g).
 template <int LAW>
 struct LawTraits {
-  static constexpr int NV = (LAW == FEM_LAW_NEO_HOOKEAN) ? 3 : ((LAW == FEM_LAW_J2) ? 2 : 1);
+  static constexpr int NV = (LAW == FEM_LAW_NEO_HOOKEAN) ? 2 : ((LAW == FEM_LAW_J2) ? 1 : 0);
 };
 
-// Record of one (cell, quadrature point) in warp smem, in units of T:
-//   [0, 4)              tangent coefficients * JxW
-//   [4 + b NS, ...)     node b's vectors g, (f, h | s), padded to NS
-// NS keeps every node row 16-byte aligned and the 8 rows of a record in
-// disjoint banks (float: 4 or 12 words; double: 6 or 10 doubles).
-template <int LAW, typename T>
-struct Rec {
+// Per-quad record in shared memory (type T, the tangent's type):
+//   [0,24)            g_b  (physical shape gradients of the 8 nodes)
+//   [24, 24+24 NV)    law vectors per node (NH: F g_b, F^-T g_b; J2: s g_b)
+//   then 4            tangent coefficients * JxW
+// The stress P * JxW (and, with an FP32 record, the shape gradients) go to a
+// separate FP64 area, so the residual is FP64 whatever T is.
+template <int VEC, int LAW>
+struct QuadLayout {
   static constexpr int NV = LawTraits<LAW>::NV;
-  static constexpr int NS = sizeof(T) == 4 ? (NV == 1 ? 4 : 12) : (NV == 3 ? 10 : 6);
-  static constexpr int SIZE = 4 + 8 * NS;
+  static constexpr int G = 0;
+  static constexpr int V1 = 24;
+  static constexpr int V2 = 48;
+  static constexpr int C = 24 + 24 * NV;
+  static constexpr int QF = C + 4;
 };
 
-// Per-node data of the group's 32 nodes (FP64): x, u, d.
+// Words per cell padded so that consecutive cells start 8 banks apart.
+template <typename T>
+__host__ __device__ constexpr int padded_cell_elems(int n) {
+  // elements -> 4-byte words: n * sizeof(T)/4; want words % 32 == 8
+  return (sizeof(T) == 8) ? (n + ((4 - n % 16) + 16) % 16) : (n + ((8 - n % 32) + 32) % 32);
+}
+
 template <int VEC>
-struct NodeRec {
-  static constexpr int X = 0;
+struct NodeLayout {
   static constexpr int U = 3;
   static constexpr int D = 3 + VEC;
   static constexpr int NF = 3 + 2 * VEC;
 };
 
-template <int VEC, int LAW, typename T>
-__host__ __device__ constexpr size_t warp_smem_bytes() {
-  return size_t(kGroupCells) * 8 * Rec<LAW, T>::SIZE * sizeof(T) +     // records
-         size_t(kGroupCells) * 8 * NodeRec<VEC>::NF * sizeof(double) +  // node data
-         size_t(kGroupCells) * 8 * VEC * sizeof(double) +               // lift accumulators
-         size_t(kGroupCells) * 8 * 2 * sizeof(int);                     // Dirichlet bits, node ids
+// FP64 copies of the shape gradients for the residual, kept only when the
+// tangent record is FP32 (an FP64 record already holds them).
+template <typename T>
+__host__ __device__ constexpr int residual_g_elems() {
+  return sizeof(T) == 8 ? 0 : 24;
 }
 
-// Phase 1 law update at one quadrature point (FP64): P*JxW and the record.
+template <int VEC, int LAW, typename T>
+__host__ __device__ constexpr size_t asm_smem_bytes() {
+  return size_t(kCellsPerBlock) * padded_cell_elems<T>(8 * QuadLayout<VEC, LAW>::QF) * sizeof(T) +
+         size_t(kCellsPerBlock) * 8 * (VEC * 3 + residual_g_elems<T>()) * sizeof(double) +  // P*JxW, g (FP64)
+         size_t(kCellsPerBlock) * 8 * NodeLayout<VEC>::NF * sizeof(double) +              // node data
+         size_t(kCellsPerBlock) * 8 * VEC * sizeof(double) +                              // lift accumulators
+         size_t(kCellsPerBlock) * 8 * 2 * sizeof(int);                                    // BC bits, node ids
+}
+
+// Phase 1: constitutive update at one quadrature point, in FP64.
+// ug = grad u (VEC x 3), g = physical shape gradients; returns P*JxW in P and
+// writes the tangent coefficients*JxW and per-node law vectors (as T).
 template <int VEC, int LAW, typename T>
 __device__ __forceinline__ void law_quad(const AsmArgs& A, int64_t c, int q, const double ug[VEC][3],
-                                         const double g[8][3], double jxw, T* rec, double P[VEC * 3]) {
-  using R = Rec<LAW, T>;
-  T* cf = rec;
-  T* nd = rec + 4;
-#pragma unroll
-  for (int b = 0; b < 8; ++b)
-#pragma unroll
-    for (int j = 0; j < 3; ++j) nd[b * R::NS + j] = T(g[b][j]);
+                                         const double g[8][3], double jxw, T* qd, double* P) {
+  using L = QuadLayout<VEC, LAW>;
+  T* cf = qd + L::C;
   if constexpr (LAW == FEM_LAW_LAPLACE) {
 #pragma unroll
     for (int i = 0; i < VEC; ++i)
@@ -135,12 +135,16 @@ __device__ __forceinline__ void law_quad(const AsmArgs& A, int64_t c, int q, con
     }
     const double mu = E / (2.0 * (1.0 + nu));
     const double lm = E * nu / ((1.0 + nu) * (1.0 - 2.0 * nu));
-    const double tr = ug[0][0] + ug[1][1] + ug[2][2];
+    double eps[3][3];
 #pragma unroll
     for (int i = 0; i < 3; ++i)
 #pragma unroll
-      for (int j = 0; j < 3; ++j) P[i * 3 + j] = jxw * (mu * (ug[i][j] + ug[j][i]) + (i == j ? lm * tr : 0.0));
-    // K_ab = lm g_a (x) g_b + mu g_b (x) g_a + mu (g_a . g_b) I
+      for (int j = 0; j < 3; ++j) eps[i][j] = 0.5 * (ug[i][j] + ug[j][i]);
+    const double tr = eps[0][0] + eps[1][1] + eps[2][2];
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+      for (int j = 0; j < 3; ++j) P[i * 3 + j] = jxw * (2.0 * mu * eps[i][j] + (i == j ? lm * tr : 0.0));
     cf[0] = T(lm * jxw);
     cf[1] = T(mu * jxw);
     cf[2] = cf[3] = T(0);
@@ -189,13 +193,16 @@ __device__ __forceinline__ void law_quad(const AsmArgs& A, int64_t c, int q, con
     cf[1] = T(scale * (-2.0 / 3.0) * m);
     cf[2] = T(scale * (2.0 / 9.0 * m * I1 + kappa * (2.0 * J - 1.0) * J));
     cf[3] = T(scale * (m * I1 / 3.0 - kJ1));
+    T* v1 = qd + L::V1;
+    T* v2 = qd + L::V2;
 #pragma unroll
-    for (int b = 0; b < 8; ++b)
+    for (int b = 0; b < 8; ++b) {
 #pragma unroll
       for (int i = 0; i < 3; ++i) {
-        nd[b * R::NS + 3 + i] = T(F[i][0] * g[b][0] + F[i][1] * g[b][1] + F[i][2] * g[b][2]);
-        nd[b * R::NS + 6 + i] = T(H[i][0] * g[b][0] + H[i][1] * g[b][1] + H[i][2] * g[b][2]);
+        v1[b * 3 + i] = T(F[i][0] * g[b][0] + F[i][1] * g[b][1] + F[i][2] * g[b][2]);
+        v2[b * 3 + i] = T(H[i][0] * g[b][0] + H[i][1] * g[b][1] + H[i][2] * g[b][2]);
       }
+    }
   } else if constexpr (LAW == FEM_LAW_J2) {
     const double E = A.p[0], nu = A.p[1], sy0 = A.p[2], Hh = A.p[3];
     const double mu = E / (2.0 * (1.0 + nu));
@@ -241,340 +248,297 @@ __device__ __forceinline__ void law_quad(const AsmArgs& A, int64_t c, int q, con
     cf[1] = T(jxw * mu * (1.0 - beta));
     cf[2] = T(jxw * gam2);
     cf[3] = T(0);
+    T* v1 = qd + L::V1;
 #pragma unroll
     for (int b = 0; b < 8; ++b)
 #pragma unroll
-      for (int i = 0; i < 3; ++i)
-        nd[b * R::NS + 3 + i] = T(s[i][0] * g[b][0] + s[i][1] * g[b][1] + s[i][2] * g[b][2]);
+      for (int i = 0; i < 3; ++i) v1[b * 3 + i] = T(s[i][0] * g[b][0] + s[i][1] * g[b][1] + s[i][2] * g[b][2]);
   }
 }
 
-// Select v[i] for a lane-dependent i in {0, 1, 2} without local memory.
-template <typename T>
-__device__ __forceinline__ T pick3(const T v[3], int i) {
-  return i == 0 ? v[0] : (i == 1 ? v[1] : v[2]);
-}
-
-// Phase 2 update of one row (a, i) against node b at one quadrature point:
-// K[k] += K_ab[i][k] except the (g_a . g_b) I term, whose coefficient times
-// the dot product is returned (added to K[i] once, after the quadrature loop).
-// ar: the lane's own node vectors premultiplied as each law needs (own_row);
-// br: node b's vectors; cf: the record's coefficients.
-template <int LAW, typename T>
-__device__ __forceinline__ T pair_row(const T* ar, const T* br, const T* cf, int i, T K[3]) {
-  const T dot = ar[0] * br[0] + ar[1] * br[1] + ar[2] * br[2];
+template <int VEC, int LAW, typename T>
+__device__ __forceinline__ void pair_block(const T* qd, int a, int b, T K[VEC][VEC]) {
+  using L = QuadLayout<VEC, LAW>;
+  const T* g = qd + L::G;
+  const T* cf = qd + L::C;
+  const T ga0 = g[a * 3], ga1 = g[a * 3 + 1], ga2 = g[a * 3 + 2];
+  const T gb0 = g[b * 3], gb1 = g[b * 3 + 1], gb2 = g[b * 3 + 2];
+  const T dot = ga0 * gb0 + ga1 * gb1 + ga2 * gb2;
   if constexpr (LAW == FEM_LAW_LAPLACE) {
-    return cf[0] * dot;
-  } else if constexpr (LAW == FEM_LAW_LINEAR || LAW == FEM_LAW_SIMP) {
-    // ar[3] = lm g_a[i];  K[k] += lm ga_i gb_k + mu gb_i ga_k
-    const T y = cf[1] * pick3(br, i);
+    const T s = cf[0] * dot;
 #pragma unroll
-    for (int k = 0; k < 3; ++k) K[k] += ar[3] * br[k] + y * ar[k];
-    return cf[1] * dot;
-  } else if constexpr (LAW == FEM_LAW_NEO_HOOKEAN) {
-    // ar[3] = c2 f_a[i] + c4 h_a[i], ar[4] = c2 h_a[i], ar[5..8) = h_a
-    // K[k] += ar3 hb_k + ar4 fb_k + c5 hb_i ha_k
-    const T* fb = br + 3;
-    const T* hb = br + 6;
-    const T y = cf[3] * pick3(hb, i);
-#pragma unroll
-    for (int k = 0; k < 3; ++k) K[k] += ar[3] * hb[k] + ar[4] * fb[k] + y * ar[5 + k];
-    return cf[0] * dot;
-  } else {  // J2
-    // ar[3] = cII g_a[i], ar[4] = -gam2 (s g)_a[i]
-    // K[k] += cII ga_i gb_k + ch gb_i ga_k - gam2 sa_i sb_k
-    const T* sb = br + 3;
-    const T y = cf[1] * pick3(br, i);
-#pragma unroll
-    for (int k = 0; k < 3; ++k) K[k] += ar[3] * br[k] + y * ar[k] + ar[4] * sb[k];
-    return cf[1] * dot;
-  }
-}
-
-// The lane's own node vectors for pair_row (see there).
-template <int LAW, typename T>
-__device__ __forceinline__ void own_row(const T* na, const T* cf, int i, T ar[8]) {
-  ar[0] = na[0], ar[1] = na[1], ar[2] = na[2];
-  if constexpr (LAW == FEM_LAW_LINEAR || LAW == FEM_LAW_SIMP) {
-    ar[3] = cf[0] * pick3(na, i);
-  } else if constexpr (LAW == FEM_LAW_NEO_HOOKEAN) {
-    const T fi = pick3(na + 3, i), hi = pick3(na + 6, i);
-    ar[3] = cf[1] * fi + cf[2] * hi;
-    ar[4] = cf[1] * hi;
-    ar[5] = na[6], ar[6] = na[7], ar[7] = na[8];
-  } else if constexpr (LAW == FEM_LAW_J2) {
-    ar[3] = cf[0] * pick3(na, i);
-    ar[4] = -cf[2] * pick3(na + 3, i);
-  }
-}
-
-// Load a record node row (NV vectors of 3) into registers with 16-byte loads.
-template <int LAW, typename T>
-__device__ __forceinline__ void load_row(const T* src, T* dst) {
-  constexpr int N = 3 * LawTraits<LAW>::NV;
-  if constexpr (sizeof(T) == 4) {
-    const float4* s4 = reinterpret_cast<const float4*>(src);
-    float tmp[4 * ((N + 3) / 4)];
-#pragma unroll
-    for (int v = 0; v < (N + 3) / 4; ++v) {
-      const float4 x = s4[v];
-      tmp[4 * v] = x.x, tmp[4 * v + 1] = x.y, tmp[4 * v + 2] = x.z, tmp[4 * v + 3] = x.w;
-    }
-#pragma unroll
-    for (int v = 0; v < N; ++v) dst[v] = tmp[v];
+    for (int i = 0; i < VEC; ++i) K[i][i] += s;
   } else {
-    const double2* s2 = reinterpret_cast<const double2*>(src);
+    const T ga[3] = {ga0, ga1, ga2};
+    const T gb[3] = {gb0, gb1, gb2};
+    if constexpr (LAW == FEM_LAW_LINEAR || LAW == FEM_LAW_SIMP) {
+      const T lm = cf[0], mu = cf[1];
 #pragma unroll
-    for (int v = 0; v < (N + 1) / 2; ++v) {
-      const double2 x = s2[v];
-      dst[2 * v] = x.x;
-      if (2 * v + 1 < N) dst[2 * v + 1] = x.y;
+      for (int i = 0; i < 3; ++i) {
+#pragma unroll
+        for (int k = 0; k < 3; ++k) K[i][k] += lm * ga[i] * gb[k] + mu * gb[i] * ga[k];
+        K[i][i] += mu * dot;
+      }
+    } else if constexpr (LAW == FEM_LAW_NEO_HOOKEAN) {
+      const T* f = qd + L::V1;
+      const T* h = qd + L::V2;
+      const T m = cf[0], c2 = cf[1], c4 = cf[2], c5 = cf[3];
+      T fa[3], ha[3], fb[3], hb[3];
+#pragma unroll
+      for (int i = 0; i < 3; ++i) {
+        fa[i] = f[a * 3 + i];
+        ha[i] = h[a * 3 + i];
+        fb[i] = f[b * 3 + i];
+        hb[i] = h[b * 3 + i];
+      }
+#pragma unroll
+      for (int i = 0; i < 3; ++i) {
+        const T ua = c2 * fa[i] + c4 * ha[i];
+        const T va = c2 * ha[i];
+#pragma unroll
+        for (int k = 0; k < 3; ++k) K[i][k] += ua * hb[k] + va * fb[k] + c5 * hb[i] * ha[k];
+        K[i][i] += m * dot;
+      }
+    } else if constexpr (LAW == FEM_LAW_J2) {
+      const T* sg = qd + L::V1;
+      const T cII = cf[0], ch = cf[1], g2 = cf[2];
+      T sa[3], sb[3];
+#pragma unroll
+      for (int i = 0; i < 3; ++i) {
+        sa[i] = sg[a * 3 + i];
+        sb[i] = sg[b * 3 + i];
+      }
+#pragma unroll
+      for (int i = 0; i < 3; ++i) {
+#pragma unroll
+        for (int k = 0; k < 3; ++k) K[i][k] += cII * ga[i] * gb[k] + ch * gb[i] * ga[k] - g2 * sa[i] * sb[k];
+        K[i][i] += ch * dot;
+      }
     }
   }
 }
 
-// Resident blocks per SM the register budget is held to: shared memory allows
-// about 3 (FP32 records) and 2 (FP64 records) for the Neo-Hookean law.
-template <int VEC, int LAW, typename T, bool WANT_K>
-__global__ void __launch_bounds__(kAsmThreads, sizeof(T) == 4 ? 3 : 2) assemble_kernel(const AsmArgs A) {
-  using R = Rec<LAW, T>;
-  using N = NodeRec<VEC>;
-  constexpr int NCV = 3 * LawTraits<LAW>::NV;
-  extern __shared__ __align__(16) unsigned char smem[];
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  unsigned char* ws = smem + size_t(warp) * warp_smem_bytes<VEC, LAW, T>();
-  T* srec = reinterpret_cast<T*>(ws);
-  double* snode = reinterpret_cast<double*>(srec + kGroupCells * 8 * R::SIZE);
-  double* slift = snode + kGroupCells * 8 * N::NF;
-  int* sbits = reinterpret_cast<int*>(slift + kGroupCells * 8 * VEC);
-  int* sid = sbits + kGroupCells * 8;
-  T* vals = reinterpret_cast<T*>(A.vals);
-  const bool want_k = WANT_K && (A.vals != nullptr || A.lift != nullptr);
+// Local node pairs (a, b), a <= b, in row-major order of the upper triangle.
+__constant__ unsigned char kPairA[36] = {0, 0, 0, 0, 0, 0, 0, 0, 1, 1, 1, 1, 1, 1, 1, 2, 2, 2,
+                                         2, 2, 2, 3, 3, 3, 3, 3, 4, 4, 4, 4, 5, 5, 5, 6, 6, 7};
+__constant__ unsigned char kPairB[36] = {0, 1, 2, 3, 4, 5, 6, 7, 1, 2, 3, 4, 5, 6, 7, 2, 3, 4,
+                                         5, 6, 7, 3, 4, 5, 6, 7, 4, 5, 6, 7, 5, 6, 7, 6, 7, 7};
 
-  const int64_t groups = (A.num_cells + kGroupCells - 1) / kGroupCells;
-  const int64_t wstride = int64_t(gridDim.x) * kAsmWarps;
-  for (int64_t grp = int64_t(blockIdx.x) * kAsmWarps + warp; grp < groups; grp += wstride) {
-    const int64_t c0 = grp * kGroupCells;
-    // ---- phase 0: lane = (cell cl, node t) ----
-    {
-      const int cl = lane >> 3, t = lane & 7;
-      const int64_t c = c0 + cl;
-      const bool valid = c < A.num_cells;
-      const int node = valid ? A.cells[c * 8 + t] : 0;
-      double* nd = snode + lane * N::NF;
-      if (valid) {
-        nd[N::X + 0] = A.points[int64_t(node) * 3 + 0];
-        nd[N::X + 1] = A.points[int64_t(node) * 3 + 1];
-        nd[N::X + 2] = A.points[int64_t(node) * 3 + 2];
-      } else {  // unit cube keeps the tail math finite; its outputs are dropped
-        nd[N::X + 0] = vtk_xbit(t);
-        nd[N::X + 1] = vtk_ybit(t);
-        nd[N::X + 2] = vtk_zbit(t);
-      }
-      int bits = 0;
+template <int VEC, int LAW, typename T, bool WANT_K>
+#ifndef FEM_ASM_MIN_BLOCKS_F32
+#define FEM_ASM_MIN_BLOCKS_F32 5
+#endif
+#ifndef FEM_ASM_MIN_BLOCKS_F64
+#define FEM_ASM_MIN_BLOCKS_F64 4
+#endif
+// Resident blocks per SM: shared memory allows about 5 (FP32 records) and 4
+// (FP64 records); the register budget is held to match.
+__global__ void __launch_bounds__(kAsmThreads, sizeof(T) == 4 ? FEM_ASM_MIN_BLOCKS_F32 : FEM_ASM_MIN_BLOCKS_F64)
+    assemble_kernel(const AsmArgs A) {
+  using L = QuadLayout<VEC, LAW>;
+  using N = NodeLayout<VEC>;
+  constexpr int CELLF = padded_cell_elems<T>(8 * L::QF);
+  extern __shared__ __align__(16) unsigned char smem[];
+  T* sq = reinterpret_cast<T*>(smem);
+  constexpr int QD = VEC * 3 + residual_g_elems<T>();  // per-quad FP64 residual data: P*JxW, then g
+  double* sP = reinterpret_cast<double*>(smem + size_t(kCellsPerBlock) * CELLF * sizeof(T));
+  double* sn = sP + kCellsPerBlock * 8 * QD;
+  double* slift = sn + kCellsPerBlock * 8 * N::NF;
+  int* sbc = reinterpret_cast<int*>(slift + kCellsPerBlock * 8 * VEC);
+  int* snode = sbc + kCellsPerBlock * 8;
+
+  const int cl = threadIdx.x / kThreadsPerCell;
+  const int t = threadIdx.x - cl * kThreadsPerCell;
+  const int64_t c = int64_t(blockIdx.x) * kCellsPerBlock + cl;
+  const bool valid = c < A.num_cells;
+
+  // ---- phase 0: node data ----
+  if (t < 8) {
+    const int node = valid ? A.cells[c * 8 + t] : 0;
+    double* nd = sn + (cl * 8 + t) * N::NF;
+    if (valid) {
+      nd[0] = A.points[int64_t(node) * 3 + 0];
+      nd[1] = A.points[int64_t(node) * 3 + 1];
+      nd[2] = A.points[int64_t(node) * 3 + 2];
+    } else {  // unit cube keeps the tail math finite; its outputs are dropped
+      nd[0] = vtk_xbit(t);
+      nd[1] = vtk_ybit(t);
+      nd[2] = vtk_zbit(t);
+    }
+    int bits = 0;
+#pragma unroll
+    for (int i = 0; i < VEC; ++i) {
+      const int64_t dof = int64_t(node) * VEC + i;
+      nd[N::U + i] = valid ? A.u[dof] : 0.0;
+      nd[N::D + i] = (valid && A.dvec != nullptr) ? A.dvec[dof] : 0.0;
+      if (valid && A.bc != nullptr && A.bc[dof]) bits |= 1 << i;
+      if (nd[N::D + i] != 0.0) bits |= kLiftBit;
+      slift[(cl * 8 + t) * VEC + i] = 0.0;
+    }
+    sbc[cl * 8 + t] = bits;
+    snode[cl * 8 + t] = node;
+  }
+  __syncthreads();
+
+  // ---- phase 1: quadrature point q = t ----
+  T* cq = sq + cl * CELLF;
+  const double* nb = sn + cl * 8 * N::NF;
+  if (t < 8) {
+    const int q = t;
+    double X[8][3], g[8][3];
+#pragma unroll
+    for (int b = 0; b < 8; ++b)
+#pragma unroll
+      for (int i = 0; i < 3; ++i) X[b][i] = nb[b * N::NF + i];
+    double jxw;
+    hex8_geometry(q, X, g, &jxw);
+    double ug[VEC][3];
+#pragma unroll
+    for (int i = 0; i < VEC; ++i)
+#pragma unroll
+      for (int j = 0; j < 3; ++j) ug[i][j] = 0.0;
+#pragma unroll
+    for (int b = 0; b < 8; ++b)
 #pragma unroll
       for (int i = 0; i < VEC; ++i) {
-        const int64_t dof = int64_t(node) * VEC + i;
-        nd[N::U + i] = valid ? A.u[dof] : 0.0;
-        const double d = (valid && A.dvec != nullptr) ? A.dvec[dof] : 0.0;
-        nd[N::D + i] = d;
-        if (valid && A.bc != nullptr && A.bc[dof]) bits |= 1 << i;
-        if (d != 0.0) bits |= kLiftBit;
-        slift[lane * VEC + i] = 0.0;
+        const double ub = nb[b * N::NF + N::U + i];
+#pragma unroll
+        for (int j = 0; j < 3; ++j) ug[i][j] = fma(ub, g[b][j], ug[i][j]);
       }
-      sbits[lane] = bits;
-      sid[lane] = node;
-    }
-    __syncwarp();
-    // ---- phase 1: lane = (cell cl, quadrature point q) ----
-    {
-      const int cl = lane >> 3, q = lane & 7;
-      const int64_t c = c0 + cl;
-      const bool valid = c < A.num_cells;
-      const double* nb = snode + cl * 8 * N::NF;
-      double X[8][3], g[8][3];
+    T* qd = cq + q * L::QF;
+#pragma unroll
+    for (int b = 0; b < 8; ++b)
+#pragma unroll
+      for (int j = 0; j < 3; ++j) qd[L::G + b * 3 + j] = T(g[b][j]);
+    double* pq = sP + (cl * 8 + q) * QD;
+    law_quad<VEC, LAW, T>(A, valid ? c : 0, q, ug, g, jxw, qd, pq);
+    if constexpr (residual_g_elems<T>() > 0) {
 #pragma unroll
       for (int b = 0; b < 8; ++b)
 #pragma unroll
-        for (int i = 0; i < 3; ++i) X[b][i] = nb[b * N::NF + N::X + i];
-      double jxw;
-      hex8_geometry(q, X, g, &jxw);
-      double ug[VEC][3];
-#pragma unroll
-      for (int i = 0; i < VEC; ++i)
-#pragma unroll
-        for (int j = 0; j < 3; ++j) ug[i][j] = 0.0;
-#pragma unroll
-      for (int b = 0; b < 8; ++b)
-#pragma unroll
-        for (int i = 0; i < VEC; ++i) {
-          const double ub = nb[b * N::NF + N::U + i];
-#pragma unroll
-          for (int j = 0; j < 3; ++j) ug[i][j] = fma(ub, g[b][j], ug[i][j]);
-        }
-      double P[VEC * 3];
-      law_quad<VEC, LAW, T>(A, valid ? c : c0, q, ug, g, jxw, srec + lane * R::SIZE, P);
-      if (A.res != nullptr) {
-        // r_b = P g_b for the 8 nodes, summed over the cell's 8 lanes: round
-        // r keeps the half of the nodes selected by bit (2 - r) of q.
-        double r[8 * VEC];
-#pragma unroll
-        for (int b = 0; b < 8; ++b)
-#pragma unroll
-          for (int i = 0; i < VEC; ++i)
-            r[b * VEC + i] = P[i * 3] * g[b][0] + P[i * 3 + 1] * g[b][1] + P[i * 3 + 2] * g[b][2];
-        const bool h4 = q & 4, h2 = q & 2, h1 = q & 1;
-#pragma unroll
-        for (int v = 0; v < 4 * VEC; ++v) {
-          const double send = h4 ? r[v] : r[4 * VEC + v];
-          const double keep = h4 ? r[4 * VEC + v] : r[v];
-          r[v] = keep + __shfl_xor_sync(0xffffffffu, send, 4);
-        }
-#pragma unroll
-        for (int v = 0; v < 2 * VEC; ++v) {
-          const double send = h2 ? r[v] : r[2 * VEC + v];
-          const double keep = h2 ? r[2 * VEC + v] : r[v];
-          r[v] = keep + __shfl_xor_sync(0xffffffffu, send, 2);
-        }
-#pragma unroll
-        for (int v = 0; v < VEC; ++v) {
-          const double send = h1 ? r[v] : r[VEC + v];
-          const double keep = h1 ? r[VEC + v] : r[v];
-          r[v] = keep + __shfl_xor_sync(0xffffffffu, send, 1);
-        }
-        if (valid) {
-          const int64_t node = sid[lane];  // lane (cl, q) now holds node q of cell cl
-#pragma unroll
-          for (int i = 0; i < VEC; ++i) atomicAdd(A.res + node * VEC + i, r[i]);
-        }
-      }
+        for (int j = 0; j < 3; ++j) pq[VEC * 3 + b * 3 + j] = g[b][j];
     }
-    __syncwarp();
-    if (!want_k) continue;
-    // ---- phase 2: lane = row (node a, component i) ----
-    constexpr int ROWS = 8 * VEC;                    // rows per cell
-    constexpr int CPP = VEC == 1 ? kGroupCells : 1;  // cells per pass
-    for (int pass = 0; pass < kGroupCells / CPP; ++pass) {
-      const int cl = VEC == 1 ? (lane >> 3) : pass;
-      const int rl = VEC == 1 ? (lane & 7) : lane;
-      const int64_t c = c0 + cl;
-      const bool active = rl < ROWS && c < A.num_cells;
-      const int a = rl / VEC, i = rl - (rl / VEC) * VEC;
-      const T* rec0 = srec + (cl * 8) * R::SIZE;
-      const int nblk = a < 4 ? 5 : 4;
-      T K[5][3];
-      T Kd[5];
-#pragma unroll
-      for (int j = 0; j < 5; ++j) {
-        Kd[j] = T(0);
-#pragma unroll
-        for (int k = 0; k < 3; ++k) K[j][k] = T(0);
-      }
-      if (active) {
-#pragma unroll 1
-        for (int q = 0; q < 8; ++q) {
-          const T* rec = rec0 + q * R::SIZE;
-          const T cf[4] = {rec[0], rec[1], rec[2], rec[3]};
-          T na[NCV], ar[8];
-          load_row<LAW, T>(rec + 4 + a * R::NS, na);
-          own_row<LAW, T>(na, cf, i, ar);
-#pragma unroll
-          for (int j = 0; j < 5; ++j) {
-            if (j < nblk) {
-              const int b = (a + j) & 7;
-              T br[NCV];
-              load_row<LAW, T>(rec + 4 + b * R::NS, br);
-              Kd[j] += pair_row<LAW, T>(ar, br, cf, i, K[j]);
-            }
-          }
-        }
-      }
-      // the (g_a . g_b) I term on the row's own component
-#pragma unroll
-      for (int j = 0; j < 5; ++j) {
-        if constexpr (VEC == 1) {
-          K[j][0] += Kd[j];
-        } else {
-          K[j][0] += i == 0 ? Kd[j] : T(0);
-          K[j][1] += i == 1 ? Kd[j] : T(0);
-          K[j][2] += i == 2 ? Kd[j] : T(0);
-        }
-      }
-      const int ca = cl * 8;  // the cell's first node slot
-      const bool lift_cell =
-          A.lift != nullptr && (__reduce_or_sync(0xffffffffu, active ? (sbits[ca + a] & kLiftBit) : 0) != 0);
-      if (active) {
-        const int abits = sbits[ca + a];
-        const int na_id = sid[ca + a];
-        const bool arow_bc = (abits >> i) & 1;
-        double lrow = 0.0;
-#pragma unroll
-        for (int j = 0; j < 5; ++j) {
-          if (j >= nblk) continue;
-          const int b = (a + j) & 7;
-          const int bbits = sbits[ca + b];
-          if (lift_cell) {
-            // row (a, i): K_ab[i][:] d_b; row (b, k): K_ab[i][k] d_a[i]
-            const double* db = snode + (ca + b) * N::NF + N::D;
-            if (bbits & kLiftBit)
-#pragma unroll
-              for (int k = 0; k < VEC; ++k) lrow += double(K[j][k]) * db[k];
-            if (b != a && (abits & kLiftBit)) {
-              const double dai = snode[(ca + a) * N::NF + N::D + i];
-#pragma unroll
-              for (int k = 0; k < VEC; ++k) atomicAdd(slift + (ca + b) * VEC + k, double(K[j][k]) * dai);
-            }
-          }
-          if (vals != nullptr && !arow_bc) {
-            const int nb_id = sid[ca + b];
-            const int* smap = A.scatter + c * 64;
-            if (a == b || na_id < nb_id) {
-              T* blk = vals + int64_t(smap[a * 8 + b]) * (VEC * VEC) + i * VEC;
-#pragma unroll
-              for (int k = 0; k < VEC; ++k)
-                if (!((bbits >> k) & 1)) atomicAdd(blk + k, K[j][k]);
-            } else {
-              T* blk = vals + int64_t(smap[b * 8 + a]) * (VEC * VEC) + i;
-#pragma unroll
-              for (int k = 0; k < VEC; ++k)
-                if (!((bbits >> k) & 1)) atomicAdd(blk + k * VEC, K[j][k]);
-            }
-          }
-        }
-        if (lift_cell) atomicAdd(slift + (ca + a) * VEC + i, lrow);
-      }
-      if (lift_cell) {
-        __syncwarp();
-        if (active && !((sbits[ca + a] >> i) & 1))
-          atomicAdd(A.lift + int64_t(sid[ca + a]) * VEC + i, slift[(ca + a) * VEC + i]);
-      }
-    }
-    __syncwarp();
   }
-}
+  __syncthreads();
 
-template <int VEC, int LAW, typename T, bool WANT_K>
-int launch_variant(const AsmArgs& A, cudaStream_t st) {
-  auto k = assemble_kernel<VEC, LAW, T, WANT_K>;
-  const size_t sm = size_t(kAsmWarps) * warp_smem_bytes<VEC, LAW, T>();
-  static int blocks_per_sm = 0;
-  if (blocks_per_sm == 0) {
-    FEM_CUDA_TRY(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sm)));
-    FEM_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, k, kAsmThreads, sm));
-    if (blocks_per_sm < 1) blocks_per_sm = 1;
+  // ---- phase 2a: residual of node a = t, r_a = sum_q P_q g_a,q (FP64) ----
+  if (valid && t < 8 && A.res != nullptr) {
+    const int a = t;
+    double r[VEC];
+#pragma unroll
+    for (int i = 0; i < VEC; ++i) r[i] = 0.0;
+#pragma unroll 1
+    for (int q = 0; q < 8; ++q) {
+      const double* pq = sP + (cl * 8 + q) * QD;
+      double ga[3];
+#pragma unroll
+      for (int j = 0; j < 3; ++j)
+        ga[j] = residual_g_elems<T>() > 0 ? pq[VEC * 3 + a * 3 + j] : double(cq[q * L::QF + L::G + a * 3 + j]);
+#pragma unroll
+      for (int i = 0; i < VEC; ++i) r[i] += pq[i * 3] * ga[0] + pq[i * 3 + 1] * ga[1] + pq[i * 3 + 2] * ga[2];
+    }
+    const int64_t node = snode[cl * 8 + a];
+#pragma unroll
+    for (int i = 0; i < VEC; ++i) atomicAdd(A.res + node * VEC + i, r[i]);
   }
-  const int64_t groups = (A.num_cells + kGroupCells - 1) / kGroupCells;
-  const int64_t need = (groups + kAsmWarps - 1) / kAsmWarps;
-  const int64_t cap = int64_t(num_sms()) * blocks_per_sm;
-  const unsigned grid = unsigned(need < cap ? need : cap);
-  k<<<grid, kAsmThreads, sm, st>>>(A);
-  FEM_LAUNCH_CHECK();
-  return FEM_OK;
+  if constexpr (WANT_K) {
+    if (A.vals == nullptr && A.lift == nullptr) return;  // uniform over the block
+    T* vals = reinterpret_cast<T*>(A.vals);
+    // ---- phase 2b: node pairs p = t, t+12, t+24 ----
+    if (valid) {
+#pragma unroll 1
+      for (int p = t; p < 36; p += kThreadsPerCell) {
+        const int a = kPairA[p], b = kPairB[p];
+        T K[VEC][VEC];
+#pragma unroll
+        for (int i = 0; i < VEC; ++i)
+#pragma unroll
+          for (int k = 0; k < VEC; ++k) K[i][k] = T(0);
+#pragma unroll 2
+        for (int q = 0; q < 8; ++q) pair_block<VEC, LAW, T>(cq + q * L::QF, a, b, K);
+        const int abits = sbc[cl * 8 + a], bbits = sbc[cl * 8 + b];
+        if (A.lift != nullptr && (bbits & kLiftBit)) {
+          // row a: K_ab d_b (only a node with non-zero d contributes)
+#pragma unroll
+          for (int i = 0; i < VEC; ++i) {
+            double la = 0.0;
+#pragma unroll
+            for (int k = 0; k < VEC; ++k) la += double(K[i][k]) * nb[b * N::NF + N::D + k];
+            atomicAdd(slift + (cl * 8 + a) * VEC + i, la);
+          }
+        }
+        if (A.lift != nullptr && a != b && (abits & kLiftBit)) {
+          // row b: K_ab^T d_a
+#pragma unroll
+          for (int k = 0; k < VEC; ++k) {
+            double lb = 0.0;
+#pragma unroll
+            for (int i = 0; i < VEC; ++i) lb += double(K[i][k]) * nb[a * N::NF + N::D + i];
+            atomicAdd(slift + (cl * 8 + b) * VEC + k, lb);
+          }
+        }
+        if (vals != nullptr) {
+          const int na = snode[cl * 8 + a], nbn = snode[cl * 8 + b];
+          const int* smap = A.scatter + c * 64;
+          if (a == b || na < nbn) {
+            T* blk = vals + int64_t(smap[a * 8 + b]) * (VEC * VEC);
+#pragma unroll
+            for (int i = 0; i < VEC; ++i)
+#pragma unroll
+              for (int k = 0; k < VEC; ++k)
+                if (!(((abits >> i) | (bbits >> k)) & 1)) atomicAdd(blk + i * VEC + k, K[i][k]);
+          }
+          if (a != b && na >= nbn) {  // (na == nbn only in a degenerate cell: both orientations)
+            T* blk = vals + int64_t(smap[b * 8 + a]) * (VEC * VEC);
+#pragma unroll
+            for (int k = 0; k < VEC; ++k)
+#pragma unroll
+              for (int i = 0; i < VEC; ++i)
+                if (!(((bbits >> k) | (abits >> i)) & 1)) atomicAdd(blk + k * VEC + i, K[i][k]);
+          }
+        }
+      }
+    }
+    if (A.lift != nullptr) {
+      __syncthreads();
+      // the cell's lift is non-zero only if one of its nodes has non-zero d
+      int any = 0;
+#pragma unroll
+      for (int b = 0; b < 8; ++b) any |= sbc[cl * 8 + b];
+      if (valid && t < 8 && (any & kLiftBit)) {
+        const int abits = sbc[cl * 8 + t];
+        const int64_t node = snode[cl * 8 + t];
+#pragma unroll
+        for (int i = 0; i < VEC; ++i)
+          if (!((abits >> i) & 1)) atomicAdd(A.lift + node * VEC + i, slift[(cl * 8 + t) * VEC + i]);
+      }
+    }
+  }
 }
 
 template <int VEC, int LAW, typename T>
 int launch_law(const AsmArgs& A, bool want_k, cudaStream_t st) {
-  return want_k ? launch_variant<VEC, LAW, T, true>(A, st) : launch_variant<VEC, LAW, T, false>(A, st);
+  const unsigned grid = unsigned((A.num_cells + kCellsPerBlock - 1) / kCellsPerBlock);
+  const size_t sm = asm_smem_bytes<VEC, LAW, T>();
+  if (want_k) {
+    auto k = assemble_kernel<VEC, LAW, T, true>;
+    static bool attr = false;
+    if (!attr) {
+      FEM_CUDA_TRY(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sm)));
+      attr = true;
+    }
+    k<<<grid, kAsmThreads, sm, st>>>(A);
+  } else {
+    auto k = assemble_kernel<VEC, LAW, T, false>;
+    static bool attr = false;
+    if (!attr) {
+      FEM_CUDA_TRY(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sm)));
+      attr = true;
+    }
+    k<<<grid, kAsmThreads, sm, st>>>(A);
+  }
+  FEM_LAUNCH_CHECK();
+  return FEM_OK;
 }
 
 template <typename T>
