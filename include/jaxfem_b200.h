@@ -428,6 +428,11 @@ typedef struct FemMGLevel {
                              written by setup; the V-cycle then solves that level exactly */
   int32_t nu;             /* smoothing steps on this level; 0: the call's nu */
   int32_t reserved;
+  void* vals_lo;          /* FP32 hierarchies only, or NULL: device, 16-byte aligned, nnzb*vec*vec FP16
+                             values, written by setup as the level's values times a power of two s
+                             (max |a| s < 2^14); the V-cycle's smoothing and residual products on this
+                             level then read them (half the bytes of FP32) */
+  double* lo_scale;       /* with vals_lo: device, 2 doubles; setup writes 1/s to [0] ([1] is its scratch) */
 } FemMGLevel;
 #define FEM_MG_DENSE_MAX 128
 

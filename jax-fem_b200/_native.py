@@ -35,7 +35,7 @@ class FemMGLevel(ctypes.Structure):
                 ("b", ctypes.c_void_p), ("r", ctypes.c_void_p), ("d0", ctypes.c_void_p), ("d1", ctypes.c_void_p),
                 ("cpos", ctypes.c_void_p), ("ilo", ctypes.c_void_p), ("whi", ctypes.c_void_p),
                 ("lmax", ctypes.c_void_p), ("cinv", ctypes.c_void_p), ("nu", ctypes.c_int32),
-                ("reserved", ctypes.c_int32)]
+                ("reserved", ctypes.c_int32), ("vals_lo", ctypes.c_void_p), ("lo_scale", ctypes.c_void_p)]
 
 FEM_MG_DENSE_MAX = 128  # largest coarsest level (n_brows * vec) solved by a dense inverse
 

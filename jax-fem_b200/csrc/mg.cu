@@ -340,20 +340,24 @@ __global__ void cheb_first_kernel(int64_t n, const T* __restrict__ dinv, const T
   }
 }
 
+// Value types of the row kernels: the level's own (VT = T), or for a level of
+// an FP32 hierarchy an FP16 copy of its values scaled by a power of two s
+// (VT = __half; the row sums are multiplied by vinv[0] = 1/s).
 // q = A d_old; r -= q; d_new = a d_old + c D^-1 r; x += d_new (x += d_old + d_new with fold)
-template <int VEC, typename T>
+template <int VEC, typename VT, typename T>
 __global__ void __launch_bounds__(kRowThreads, kRowBlocksPerSM)
-    cheb_step_kernel(int64_t n_brows, const int32_t* rp, const int32_t* ci, const T* vals, const T* __restrict__ dold,
+    cheb_step_kernel(int64_t n_brows, const int32_t* rp, const int32_t* ci, const VT* vals, const T* __restrict__ dold,
                      T* dnew, T* r, T* x, const T* __restrict__ dinv, const void* lmax, double ratio, int step,
-                     int fold) {
+                     int fold, const double* vinv) {
   pdl_wait();
   const ChebCoef cf = cheb_coef(lmax, ratio, step);
   const double a = cf.a, c = cf.c;
-  bsr_rows<VEC, T, T>(
+  const double vs = vinv != nullptr ? vinv[0] : 1.0;
+  bsr_rows<VEC, VT, T>(
       n_brows, rp, ci, vals, [&](int64_t i) { return dold[i]; },
       [&](int64_t row, int comp, T q) {
         const int64_t i = row * VEC + comp;
-        const double rn = double(r[i]) - double(q);
+        const double rn = double(r[i]) - double(q) * vs;
         r[i] = T(rn);
         const T dn = T(a * double(dold[i]) + c * double(dinv[i]) * rn);
         dnew[i] = dn;
@@ -363,16 +367,17 @@ __global__ void __launch_bounds__(kRowThreads, kRowBlocksPerSM)
 }
 
 // r -= A d
-template <int VEC, typename T>
+template <int VEC, typename VT, typename T>
 __global__ void __launch_bounds__(kRowThreads, kRowBlocksPerSM)
-    cheb_resid_kernel(int64_t n_brows, const int32_t* rp, const int32_t* ci, const T* vals, const T* __restrict__ d,
-                      T* r) {
+    cheb_resid_kernel(int64_t n_brows, const int32_t* rp, const int32_t* ci, const VT* vals, const T* __restrict__ d,
+                      T* r, const double* vinv) {
   pdl_wait();
-  bsr_rows<VEC, T, T>(
+  const double vs = vinv != nullptr ? vinv[0] : 1.0;
+  bsr_rows<VEC, VT, T>(
       n_brows, rp, ci, vals, [&](int64_t i) { return d[i]; },
       [&](int64_t row, int comp, T q) {
         const int64_t i = row * VEC + comp;
-        r[i] = T(double(r[i]) - double(q));
+        r[i] = T(double(r[i]) - double(q) * vs);
       });
 }
 
@@ -380,8 +385,10 @@ __global__ void __launch_bounds__(kRowThreads, kRowBlocksPerSM)
 template <int VEC, typename VT, typename T>
 __global__ void __launch_bounds__(kRowThreads, kRowBlocksPerSM)
     mg_residual_kernel(int64_t n_brows, const int32_t* rp, const int32_t* ci, const VT* vals, const T* __restrict__ x,
-                       const T* b, T* r, const T* __restrict__ dinv, T* d0, const void* lmax, double ratio) {
+                       const T* b, T* r, const T* __restrict__ dinv, T* d0, const void* lmax, double ratio,
+                       const double* vinv) {
   pdl_wait();
+  const double vs = vinv != nullptr ? vinv[0] : 1.0;
   // with d0 given: also the first Chebyshev step's d0 = D^-1 r / theta (its
   // x += d0 is folded into the next step)
   const double inv_theta = d0 != nullptr ? cheb_coef(lmax, ratio, 0).inv_theta : 0.0;
@@ -389,7 +396,7 @@ __global__ void __launch_bounds__(kRowThreads, kRowBlocksPerSM)
       n_brows, rp, ci, vals, [&](int64_t i) { return x[i]; },
       [&](int64_t row, int comp, T q) {
         const int64_t i = row * VEC + comp;
-        const T ri = T(double(b[i]) - double(q));
+        const T ri = T(double(b[i]) - double(q) * vs);
         r[i] = ri;
         if (d0 != nullptr) d0[i] = T(double(dinv[i]) * double(ri) * inv_theta);
       });
@@ -483,6 +490,9 @@ int check_levels(int nlevels, const FemMGLevel* L) {
                   "level %d: NULL pattern, values, bound slot or work vector", l);
     FEM_CHECK_ARG(bsr_aligned(v.vals, v.col_idx), "level %d: vals and col_idx must be 16-byte aligned", l);
     FEM_CHECK_ARG(v.nu >= 0 && v.nu <= 16, "level %d: nu must be in [0, 16]", l);
+    FEM_CHECK_ARG(v.vals_lo == nullptr || (sizeof(T) == 4 && v.lo_scale != nullptr &&
+                                           (reinterpret_cast<uintptr_t>(v.vals_lo) & 15u) == 0),
+                  "level %d: an FP16 value copy needs an FP32 hierarchy, 16-byte alignment and lo_scale", l);
     FEM_CHECK_ARG(v.cinv == nullptr || (l == nlevels - 1 && v.n_brows * VEC <= FEM_MG_DENSE_MAX),
                   "level %d: a dense inverse is for a coarsest level of at most %d unknowns", l, FEM_MG_DENSE_MAX);
     if (l >= 1) {
@@ -497,10 +507,39 @@ int check_levels(int nlevels, const FemMGLevel* L) {
 template <int VEC, typename T>
 int ensure_attrs() {
   int rc;
-  if ((rc = ensure_smem_attr(cheb_step_kernel<VEC, T>)) != FEM_OK) return rc;
-  if ((rc = ensure_smem_attr(cheb_resid_kernel<VEC, T>)) != FEM_OK) return rc;
+  if ((rc = ensure_smem_attr(cheb_step_kernel<VEC, T, T>)) != FEM_OK) return rc;
+  if ((rc = ensure_smem_attr(cheb_resid_kernel<VEC, T, T>)) != FEM_OK) return rc;
   if ((rc = ensure_smem_attr(mg_residual_kernel<VEC, T, T>)) != FEM_OK) return rc;
+  if constexpr (sizeof(T) == 4) {
+    if ((rc = ensure_smem_attr(cheb_step_kernel<VEC, __half, T>)) != FEM_OK) return rc;
+    if ((rc = ensure_smem_attr(cheb_resid_kernel<VEC, __half, T>)) != FEM_OK) return rc;
+    if ((rc = ensure_smem_attr(mg_residual_kernel<VEC, __half, T>)) != FEM_OK) return rc;
+  }
   return FEM_OK;
+}
+
+// ---- FP16 copy of a level's values (FP32 hierarchies) ---------------------------
+// max |a| over the values (non-negative floats order like their bit patterns)
+__global__ void absmax_kernel(const int32_t* rp, int64_t n_brows, int vv, const float* __restrict__ a,
+                              unsigned* maxbits) {
+  const int64_t n = int64_t(rp[n_brows]) * vv;
+  float m = 0.0f;
+  for (int64_t k = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; k < n; k += int64_t(gridDim.x) * blockDim.x)
+    m = fmaxf(m, fabsf(a[k]));
+  for (int o = 16; o >= 1; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+  if ((threadIdx.x & 31) == 0) atomicMax(maxbits, __float_as_uint(m));
+}
+// a16 = round(a s) with s = 2^e the largest power of two with max|a| s <=
+// 2^14 (well inside FP16's range); scale[0] = 1/s for the row kernels.
+__global__ void half_vals_kernel(const int32_t* rp, int64_t n_brows, int vv, const float* __restrict__ a,
+                                 const unsigned* maxbits, __half* a16, double* scale) {
+  const float m = __uint_as_float(*maxbits);
+  const int e = m > 0.0f ? 14 - ilogbf(m) - 1 : 0;
+  const float s = ldexpf(1.0f, e);
+  if (blockIdx.x == 0 && threadIdx.x == 0) scale[0] = ldexp(1.0, -e);
+  const int64_t n = int64_t(rp[n_brows]) * vv;
+  for (int64_t k = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; k < n; k += int64_t(gridDim.x) * blockDim.x)
+    a16[k] = __float2half_rn(a[k] * s);
 }
 
 size_t setup_scratch_bytes(int vec, int64_t fine_n_brows, size_t elem) {
@@ -533,6 +572,19 @@ int setup_impl(int nlevels, const FemMGLevel* L, const double* fine64, void* scr
       ptap_kernel<VEC, T><<<vgrid(L[l].n_brows * 27), 256, 0, st>>>(F, C, L[l].stencil, B, static_cast<T*>(L[l].vals),
                                                                    L[l].cpos, L[l].ilo, L[l].whi);
       FEM_LAUNCH_CHECK();
+    }
+    if constexpr (sizeof(T) == 4) {
+      if (L[l].vals_lo != nullptr) {
+        unsigned* maxbits = reinterpret_cast<unsigned*>(L[l].lo_scale + 1);
+        FEM_CUDA_TRY(cudaMemsetAsync(maxbits, 0, sizeof(unsigned), st));
+        absmax_kernel<<<unsigned(num_sms()) * 8, 256, 0, st>>>(L[l].row_ptr, L[l].n_brows, VV,
+                                                               static_cast<const float*>(L[l].vals), maxbits);
+        FEM_LAUNCH_CHECK();
+        half_vals_kernel<<<unsigned(num_sms()) * 8, 256, 0, st>>>(L[l].row_ptr, L[l].n_brows, VV,
+                                                                  static_cast<const float*>(L[l].vals), maxbits,
+                                                                  static_cast<__half*>(L[l].vals_lo), L[l].lo_scale);
+        FEM_LAUNCH_CHECK();
+      }
     }
     FEM_CUDA_TRY(cudaMemsetAsync(L[l].lmax, 0, sizeof(unsigned long long), st));
     jacobi_setup_kernel<VEC, T><<<vgrid(L[l].n_brows * VEC), 256, 0, st>>>(
@@ -570,17 +622,29 @@ int smooth(const FemMGLevel& L, const T* b, T* x, int m, double ratio, bool zero
                             zero_start ? 1 : 0));
     FEM_LAUNCH_CHECK();
   }
+  const bool lo = sizeof(T) == 4 && L.vals_lo != nullptr;  // the level's FP16 value copy
+  const __half* v16 = static_cast<const __half*>(L.vals_lo);
+  const double* vinv = lo ? L.lo_scale : nullptr;
   int cur = 0;
   for (int k = 1; k < m; ++k) {
-    FEM_CUDA_TRY(launch_pdl(cheb_step_kernel<VEC, T>, rg, kRowThreads, bsr_rows_smem(), st, L.n_brows, L.row_ptr,
-                            L.col_idx, vals, static_cast<const T*>(d[cur]), d[cur ^ 1], r, x, dinv, L.lmax, ratio, k,
-                            (fold && k == 1) ? 1 : 0));
+    if (lo)
+      FEM_CUDA_TRY(launch_pdl(cheb_step_kernel<VEC, __half, T>, rg, kRowThreads, bsr_rows_smem(), st, L.n_brows,
+                              L.row_ptr, L.col_idx, v16, static_cast<const T*>(d[cur]), d[cur ^ 1], r, x, dinv,
+                              L.lmax, ratio, k, (fold && k == 1) ? 1 : 0, vinv));
+    else
+      FEM_CUDA_TRY(launch_pdl(cheb_step_kernel<VEC, T, T>, rg, kRowThreads, bsr_rows_smem(), st, L.n_brows,
+                              L.row_ptr, L.col_idx, vals, static_cast<const T*>(d[cur]), d[cur ^ 1], r, x, dinv,
+                              L.lmax, ratio, k, (fold && k == 1) ? 1 : 0, vinv));
     FEM_LAUNCH_CHECK();
     cur ^= 1;
   }
   if (want_residual) {
-    FEM_CUDA_TRY(launch_pdl(cheb_resid_kernel<VEC, T>, rg, kRowThreads, bsr_rows_smem(), st, L.n_brows, L.row_ptr,
-                            L.col_idx, vals, d[cur], r));
+    if (lo)
+      FEM_CUDA_TRY(launch_pdl(cheb_resid_kernel<VEC, __half, T>, rg, kRowThreads, bsr_rows_smem(), st, L.n_brows,
+                              L.row_ptr, L.col_idx, v16, static_cast<const T*>(d[cur]), r, vinv));
+    else
+      FEM_CUDA_TRY(launch_pdl(cheb_resid_kernel<VEC, T, T>, rg, kRowThreads, bsr_rows_smem(), st, L.n_brows,
+                              L.row_ptr, L.col_idx, vals, static_cast<const T*>(d[cur]), r, vinv));
     FEM_LAUNCH_CHECK();
   }
   return FEM_OK;
@@ -623,11 +687,18 @@ int vcycle_level(int l, int nlevels, const FemMGLevel* L, int nu, int coarse_ste
   // post-smoothing with two or more steps: the residual kernel forms the
   // first step's d0 and the second step adds its x += d0
   const bool fuse_post = nul >= 2;
-  FEM_CUDA_TRY(launch_pdl(mg_residual_kernel<VEC, T, T>, row_grid<T>(L[l].n_brows), kRowThreads, bsr_rows_smem(), st,
-                          L[l].n_brows, L[l].row_ptr, L[l].col_idx, static_cast<const T*>(L[l].vals),
-                          static_cast<const T*>(x), b, static_cast<T*>(L[l].r),
-                          static_cast<const T*>(L[l].dinv), fuse_post ? static_cast<T*>(L[l].d0) : static_cast<T*>(nullptr),
-                          static_cast<const void*>(L[l].lmax), ratio));
+  T* d0p = fuse_post ? static_cast<T*>(L[l].d0) : static_cast<T*>(nullptr);
+  if (sizeof(T) == 4 && L[l].vals_lo != nullptr)
+    FEM_CUDA_TRY(launch_pdl(mg_residual_kernel<VEC, __half, T>, row_grid<T>(L[l].n_brows), kRowThreads,
+                            bsr_rows_smem(), st, L[l].n_brows, L[l].row_ptr, L[l].col_idx,
+                            static_cast<const __half*>(L[l].vals_lo), static_cast<const T*>(x), b,
+                            static_cast<T*>(L[l].r), static_cast<const T*>(L[l].dinv), d0p,
+                            static_cast<const void*>(L[l].lmax), ratio, static_cast<const double*>(L[l].lo_scale)));
+  else
+    FEM_CUDA_TRY(launch_pdl(mg_residual_kernel<VEC, T, T>, row_grid<T>(L[l].n_brows), kRowThreads, bsr_rows_smem(),
+                            st, L[l].n_brows, L[l].row_ptr, L[l].col_idx, static_cast<const T*>(L[l].vals),
+                            static_cast<const T*>(x), b, static_cast<T*>(L[l].r), static_cast<const T*>(L[l].dinv),
+                            d0p, static_cast<const void*>(L[l].lmax), ratio, static_cast<const double*>(nullptr)));
   FEM_LAUNCH_CHECK();
   return smooth<VEC, T>(L[l], b, x, nul, ratio, false, false, st, fuse_post, fuse_post);
 }
@@ -899,7 +970,8 @@ int pcg_impl(int64_t n_brows, const int32_t* rp, const int32_t* ci, const VT* va
   float* z32 = fp32 ? static_cast<float*>(L[0].x) : nullptr;
   // r = b - A x, the reductions and status
   mg_residual_kernel<VEC, VT, double><<<rg, kRowThreads, bsr_rows_smem(), st>>>(
-      n_brows, rp, ci, vals, x, b, r, static_cast<const double*>(nullptr), static_cast<double*>(nullptr), nullptr, 0.0);
+      n_brows, rp, ci, vals, x, b, r, static_cast<const double*>(nullptr), static_cast<double*>(nullptr), nullptr, 0.0,
+      static_cast<const double*>(nullptr));
   FEM_LAUNCH_CHECK();
   pcg_init_kernel<VEC><<<vg, 256, 0, st>>>(n, r, b, partials, counter, S, rtol, atol);
   FEM_LAUNCH_CHECK();
@@ -998,7 +1070,8 @@ int pcg_impl(int64_t n_brows, const int32_t* rp, const int32_t* ci, const VT* va
   const double bb = hs->bb;
   // report the true residual ||b - A x||
   mg_residual_kernel<VEC, VT, double><<<rg, kRowThreads, bsr_rows_smem(), st>>>(
-      n_brows, rp, ci, vals, x, b, q, static_cast<const double*>(nullptr), static_cast<double*>(nullptr), nullptr, 0.0);
+      n_brows, rp, ci, vals, x, b, q, static_cast<const double*>(nullptr), static_cast<double*>(nullptr), nullptr, 0.0,
+      static_cast<const double*>(nullptr));
   FEM_LAUNCH_CHECK();
   FEM_CUDA_TRY(cudaMemsetAsync(counter, 0, sizeof(unsigned), st));
   pcg_init_kernel<VEC><<<vg, 256, 0, st>>>(n, q, b, partials, counter, S, rtol, atol);

@@ -1,5 +1,7 @@
 // Block-CSR row kernels shared by the SpMV entry points and the Krylov solvers.
 #pragma once
+#include <cuda_fp16.h>
+
 #include "common.cuh"
 
 namespace fem {
@@ -31,7 +33,7 @@ constexpr int kRowBlocksPerSM = FEM_ROW_BLOCKS_PER_SM;  // resident blocks per S
 // ~1 % faster per multigrid CG iteration than 2 on the 50^3 tangent).
 template <typename VT, typename AT = VT>
 __host__ __device__ constexpr int rows_per_warp() {
-  return (sizeof(VT) == 4 && sizeof(AT) == 4) ? FEM_ROW_GROUP_F32
+  return (sizeof(VT) <= 4 && sizeof(AT) == 4) ? FEM_ROW_GROUP_F32  // FP32 or FP16 values, FP32 sums
          : (sizeof(VT) == 4)                      ? FEM_ROW_GROUP_MIXED
                                                   : FEM_ROW_GROUP_F64;
 }

@@ -15,7 +15,8 @@ coarse operators are Galerkin products P^T A P formed on the device
 (``fem_mg_vcycle_*``) and solves a small coarsest level exactly (a dense
 inverse formed by setup), and ``fem_mg_pcg_solve`` runs CG in FP64 with one
 V-cycle per iteration.  The V-cycle is in FP64 or, for the mixed-precision
-path, in FP32 on a rounded copy of the hierarchy.
+path, in FP32 on a rounded copy of the hierarchy, whose finest level smooths
+with an FP16 copy of its values.
 """
 import ctypes
 
@@ -103,6 +104,11 @@ def _pattern(cells, N):
     return rp, col
 
 
+def _half_fine_enabled():
+    import os
+    return os.environ.get("FEM_MG_HALF", "1") != "0"
+
+
 class Multigrid:
     """Lattice hierarchy of one mesh (``DeviceMesh``) with device buffers for
     one precision.  ``setup(A)`` forms the coarse operators of the FP64
@@ -170,6 +176,16 @@ class Multigrid:
                         torch.from_numpy(np.concatenate([q[3] for q in parts]).astype(np.float64)).to(dev))
         # smoothing steps on the finest level (0: the V-cycle's nu)
         self.levels[0].nu = int(nu_fine)
+        # An FP32 hierarchy smooths its finest level with an FP16 copy of the
+        # values (scaled by a power of two, written by every setup): the
+        # V-cycle's two finest-level products then read half the bytes.  The
+        # CG operator keeps the FP32 values.  FEM_MG_HALF=0 turns it off.
+        self.half_fine = bool(fp32) and _half_fine_enabled()
+        if self.half_fine:
+            self._vals16 = torch.empty(dv.nnzb * self.vec * self.vec, dtype=torch.float16, device=dev)
+            self._scale16 = torch.zeros(2, dtype=torch.float64, device=dev)
+            self.levels[0].vals_lo = self._vals16.data_ptr()
+            self.levels[0].lo_scale = self._scale16.data_ptr()
         # a coarsest level of at most FEM_MG_DENSE_MAX unknowns is solved
         # exactly with a dense inverse (formed by setup) instead of smoothed
         last = self.levels[self.nlevels - 1]
