@@ -391,7 +391,7 @@ __global__ void __launch_bounds__(kAsmThreads, sizeof(T) == 4 ? FEM_ASM_MIN_BLOC
 #pragma unroll
       for (int i = 0; i < 3; ++i) X[b][i] = nb[b * N::NF + i];
     double jxw;
-    hex8_geometry(q, X, g, &jxw);
+    if (!hex8_box_geometry(q, X, g, &jxw)) hex8_geometry(q, X, g, &jxw);
     double ug[VEC][3];
 #pragma unroll
     for (int i = 0; i < VEC; ++i)

@@ -161,6 +161,42 @@ __device__ __forceinline__ double hex8_geometry(int q, const double X[8][3], dou
   return det;
 }
 
+// The same for a cell that is an axis-aligned box (as every cell of a
+// box_mesh lattice is): J = diag(h), so grad N_a = dN_a/dxi / h and
+// JxW = hx hy hz w.  The test is exact: along each axis every node takes the
+// coordinate of node 0 or of the node one step along that axis (VTK nodes 1,
+// 3, 4), as its reference bit says.  Returns false (nothing written) for any
+// other cell.
+__device__ __forceinline__ bool hex8_box_geometry(int q, const double X[8][3], double g[8][3], double* jxw) {
+  const int corner[3] = {1, 3, 4};
+  double h[3];
+  bool box = true;
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    const double lo = X[0][d], hi = X[corner[d]][d];
+    h[d] = hi - lo;
+#pragma unroll
+    for (int a = 0; a < 8; ++a) {
+      const int bit = d == 0 ? vtk_xbit(a) : (d == 1 ? vtk_ybit(a) : vtk_zbit(a));
+      box = box && (X[a][d] == (bit ? hi : lo));
+    }
+  }
+  box = box && h[0] != 0.0 && h[1] != 0.0 && h[2] != 0.0;
+  if (!box) return false;
+  double xi[3];
+  quad_point(q, xi);
+  const double ih[3] = {1.0 / h[0], 1.0 / h[1], 1.0 / h[2]};
+#pragma unroll
+  for (int a = 0; a < 8; ++a) {
+    double dn[3];
+    shape_grad_ref(a, xi, dn);
+#pragma unroll
+    for (int k = 0; k < 3; ++k) g[a][k] = dn[k] * ih[k];
+  }
+  *jxw = h[0] * h[1] * h[2] * kQuadWeight;
+  return true;
+}
+
 // ---- reductions ----------------------------------------------------------------
 template <typename T>
 __device__ __forceinline__ T warp_sum(T v) {

@@ -1,6 +1,8 @@
 """Cell-kernel parity: GPU residual / BC-eliminated tangent / Dirichlet lift
 against the FP64 oracle (complex-step cell Jacobians, PETSc-style COO sum),
-on jittered meshes so every cell is a general trilinear hexahedron.
+on jittered meshes so every cell is a general trilinear hexahedron, and on
+graded box lattices (every cell an axis-aligned box of its own size, the
+kernel's box-cell geometry).
 
 Tolerances: FP64 path 1e-11 relative (round-off of two differently ordered
 FP64 computations); FP32 tangent 2e-5 relative to the matrix norm."""
@@ -14,9 +16,24 @@ from oracle import fem_oracle as fo
 LAWS = ["laplace", "linear", "simp", "neo_hookean", "neo_hookean_scaled", "j2"]
 
 
-def _setup(pkg, kind, N=(3, 4, 5), seed=0):
+def graded_lattice(pkg, N, seed=0):
+    """Box lattice with randomly graded spacing per direction: every cell is
+    an axis-aligned box, each of its own size (the kernel's box-cell
+    geometry path)."""
     rng = np.random.default_rng(seed)
-    mesh = perturbed_box(pkg, N, seed=seed)
+    axes = [np.concatenate([[0.0], np.cumsum(rng.uniform(0.5, 1.5, n))]) for n in N]
+    axes = [a / a[-1] for a in axes]
+    m = pkg.box_mesh(N[0], N[1], N[2], 1.0, 1.0, 1.0)
+    n1 = [n + 1 for n in N]
+    idx = np.arange(np.prod(n1))
+    i, j, k = idx // (n1[1] * n1[2]), (idx // n1[2]) % n1[1], idx % n1[2]
+    pts = np.stack([axes[0][i], axes[1][j], axes[2][k]], axis=1)
+    return pkg.Mesh(pts, m.cells_dict["hexahedron"])
+
+
+def _setup(pkg, kind, N=(3, 4, 5), seed=0, cells="jittered"):
+    rng = np.random.default_rng(seed)
+    mesh = perturbed_box(pkg, N, seed=seed) if cells == "jittered" else graded_lattice(pkg, N, seed=seed)
     C = len(mesh.cells)
     law, olaw, iv, oiv = law_pair(pkg, kind, C, rng)
     left = lambda p: np.isclose(p[0], 0.0, atol=1e-5)  # noqa: E731
@@ -41,9 +58,10 @@ def _eliminate(A, rows):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("cells", ["jittered", "boxes"])
 @pytest.mark.parametrize("kind", LAWS)
-def test_residual_tangent_lift_f64(pkg, cuda, kind):
-    prob, oprob, u = _setup(pkg, kind)
+def test_residual_tangent_lift_f64(pkg, cuda, kind, cells):
+    prob, oprob, u = _setup(pkg, kind, cells=cells)
     n = prob.num_total_dofs_all_vars
     ud = torch.tensor(u, device=cuda)
     mask, ubc = prob.dirichlet_device()
@@ -77,11 +95,12 @@ def test_residual_tangent_lift_f64(pkg, cuda, kind):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("cells", ["jittered", "boxes"])
 @pytest.mark.parametrize("kind", ["linear", "neo_hookean", "j2"])
-def test_tangent_f32(pkg, cuda, kind):
+def test_tangent_f32(pkg, cuda, kind, cells):
     """The FP32-tangent pass: tangent within FP32 rounding of the FP64 one,
     residual FP64 (as the FP64 pass gives it), lift from the FP32 tangent."""
-    prob, oprob, u = _setup(pkg, kind, seed=1)
+    prob, oprob, u = _setup(pkg, kind, seed=1, cells=cells)
     ud = torch.tensor(u, device=cuda)
     n = ud.numel()
     mask, _ = prob.dirichlet_device()
