@@ -30,6 +30,7 @@ import torch
 from . import _native as nat
 from . import basis
 from .multigrid import Multigrid, lattice_of
+from .problem import BSRMatrix
 
 _COARSE_ELEMENT = {"TET10": "TET4", "HEX20": "HEX8", "HEX27": "HEX8"}
 
@@ -155,6 +156,18 @@ class PMultigrid:
             self.dinv = inv.contiguous()
         else:
             self.dinv.copy_(inv)
+        if self.fp32 and A.vals.is_cuda:
+            # the mixed path smooths the fine level in FP32: FP32 copies of the
+            # operator values and of the block-Jacobi inverse (the CG operator
+            # product stays FP64)
+            if getattr(self, "_A32", None) is None or self._A32.vals.numel() != A.vals.numel():
+                self._A32 = BSRMatrix(A.vec, A.row_ptr, A.col_idx, A.diag, A.vals.float())
+                self._dinv32 = self.dinv.float()
+            else:
+                self._A32.vals.copy_(A.vals)
+                self._dinv32.copy_(self.dinv)
+        else:
+            self._A32 = None
         if not fine_only or self.lmax is None:
             # largest eigenvalue of D^-1 A by power iteration (x 1.1), at full
             # setups; solves on kept coarse operators keep it too.  It stays
@@ -185,7 +198,8 @@ class PMultigrid:
 
     def _jacobi(self, r):
         v = self.vec
-        return torch.bmm(self.dinv, r.view(-1, v, 1)).view(-1)
+        dinv = self.dinv if r.dtype == torch.float64 else self._dinv32
+        return torch.bmm(dinv, r.view(-1, v, 1)).view(-1)
 
     # ---- preconditioner ------------------------------------------------------------
     def _chebyshev(self, A, b, z, nu, ratio, tmp, zero_start=False):
@@ -214,6 +228,8 @@ class PMultigrid:
         return z
 
     def apply(self, A, r, z, free, nu, coarse_steps, ratio, tmp):
+        if getattr(self, "_A32", None) is not None:
+            return self._apply32(r, z, free, nu, coarse_steps, ratio)
         z.zero_()
         self._chebyshev(A, r, z, nu, ratio, tmp, zero_start=True)
         A.matvec(z, tmp)
@@ -233,6 +249,32 @@ class PMultigrid:
         z += tmp * free
         self._chebyshev(A, r, z, nu, ratio, tmp)
         z *= free
+        return z
+
+    def _apply32(self, r, z, free, nu, coarse_steps, ratio):
+        """The same V-cycle with the fine-level smoothing and residual in FP32
+        (FP32 operator copy and block-Jacobi inverse; transfers in FP64, the
+        coarse lattice V-cycle in FP32); z (FP64) = the result."""
+        A32 = self._A32
+        r32 = r.float()
+        f32 = free.float()
+        z32 = torch.zeros_like(r32)
+        t32 = torch.empty_like(r32)
+        self._chebyshev(A32, r32, z32, nu, ratio, t32, zero_start=True)
+        A32.matvec(z32, t32)
+        r1 = ((r32 - t32) * f32).double()
+        rc = self._rc
+        self.PT.apply(r1, rc)
+        rc *= self._free_c
+        zc32 = torch.zeros_like(rc, dtype=torch.float32)
+        self.mg.vcycle(rc.float(), zc32, nu=nu, coarse_steps=coarse_steps, ratio=ratio)
+        zc = zc32.double() * self._free_c
+        tmp = torch.empty_like(r)
+        self.P.apply(zc, tmp)
+        z32 += tmp.float() * f32
+        self._chebyshev(A32, r32, z32, nu, ratio, t32)
+        torch.mul(z32, f32, out=t32)
+        z.copy_(t32)
         return z
 
     # ---- outer CG ----------------------------------------------------------------
