@@ -280,11 +280,14 @@ __global__ void prolong_add_kernel(Lat F, Lat C, const int32_t* ilo, const doubl
 }
 
 // ---- Jacobi scaling and the Gershgorin bound of D^-1 A ----------------------
+// With absmax_bits given it also finds max |a| over the values (the scale of
+// the level's FP16 copy; non-negative floats order like their bit patterns).
 template <int VEC, typename T>
 __global__ void jacobi_setup_kernel(int64_t n_brows, const int32_t* __restrict__ st, const T* __restrict__ vals,
-                                    T* dinv, unsigned long long* lmax_bits) {
+                                    T* dinv, unsigned long long* lmax_bits, unsigned* absmax_bits) {
   constexpr int VV = VEC * VEC;
   double local = 0.0;
+  float amax = 0.0f;
   for (int64_t dof = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; dof < n_brows * VEC;
        dof += int64_t(gridDim.x) * blockDim.x) {
     const int64_t row = dof / VEC;
@@ -296,7 +299,11 @@ __global__ void jacobi_setup_kernel(int64_t n_brows, const int32_t* __restrict__
       const int32_t blk = st[row * 27 + o];
       if (blk < 0) continue;
 #pragma unroll
-      for (int k = 0; k < VEC; ++k) rs += fabs(double(vals[int64_t(blk) * VV + c * VEC + k]));
+      for (int k = 0; k < VEC; ++k) {
+        const double a = fabs(double(vals[int64_t(blk) * VV + c * VEC + k]));
+        rs += a;
+        amax = fmaxf(amax, float(a));
+      }
     }
     const double ad = fabs(aii);
     dinv[dof] = T(ad > 0.0 ? 1.0 / aii : 0.0);
@@ -309,6 +316,10 @@ __global__ void jacobi_setup_kernel(int64_t n_brows, const int32_t* __restrict__
   local = fmax(local, __shfl_xor_sync(0xffffffffu, local, 1));
   // non-negative doubles order like their bit patterns
   if ((threadIdx.x & 31) == 0) atomicMax(lmax_bits, static_cast<unsigned long long>(__double_as_longlong(local)));
+  if (absmax_bits != nullptr) {
+    for (int o = 16; o >= 1; o >>= 1) amax = fmaxf(amax, __shfl_xor_sync(0xffffffffu, amax, o));
+    if ((threadIdx.x & 31) == 0) atomicMax(absmax_bits, __float_as_uint(amax));
+  }
 }
 
 template <typename T>
@@ -407,7 +418,7 @@ __global__ void __launch_bounds__(kRowThreads, kRowBlocksPerSM)
 // operator of an SPD operator is SPD, so every pivot is positive).  A pivot
 // that is not positive leaves the Jacobi inverse instead.
 constexpr int kDenseThreads = 1024;
-inline size_t dense_inverse_smem(int n) { return (size_t(n) * n + n) * sizeof(double); }
+inline size_t dense_inverse_smem(int n) { return (size_t(n) * n + 2 * n) * sizeof(double); }
 
 template <int VEC, typename T>
 __global__ void __launch_bounds__(kDenseThreads)
@@ -425,20 +436,39 @@ __global__ void __launch_bounds__(kDenseThreads)
       for (int e = 0; e < VV; ++e)
         M[(br * VEC + e / VEC) * n + ci[k] * VEC + e % VEC] = double(vals[int64_t(k) * VV + e]);
   __syncthreads();
+  // Gauss-Jordan in place, two barriers per pivot: phase A copies column k
+  // (f) and the unscaled pivot row (prow); phase B forms every entry from
+  // them, the pivot row as prow / piv and the others as
+  // M_ij - M_ik prow_j / piv (column k: -M_ik / piv; the pivot: 1 / piv).
+  // Each thread keeps the (i, j) of its entries (at most 16 for n <= 128).
+  double* prow = f + n;
+  constexpr int kMaxPer = (FEM_MG_DENSE_MAX * FEM_MG_DENSE_MAX + kDenseThreads - 1) / kDenseThreads;
+  int mi[kMaxPer], mj[kMaxPer];
+#pragma unroll
+  for (int e = 0; e < kMaxPer; ++e) {
+    const int idx = tid + e * nt;
+    mi[e] = idx < n * n ? idx / n : -1;
+    mj[e] = idx < n * n ? idx - (idx / n) * n : 0;
+  }
   bool ok = true;
   for (int k = 0; k < n; ++k) {
-    const double piv = M[k * n + k];
+    for (int i = tid; i < n; i += nt) {
+      f[i] = M[i * n + k];
+      prow[i] = M[k * n + i];
+    }
+    __syncthreads();
+    const double piv = prow[k];
     if (!(piv > 0.0) || !isfinite(piv)) {  // same value in every thread: uniform exit
       ok = false;
       break;
     }
-    __syncthreads();  // every thread holds piv before row k changes
-    for (int j = tid; j < n; j += nt) M[k * n + j] = (j == k ? 1.0 : M[k * n + j]) / piv;
-    for (int i = tid; i < n; i += nt) f[i] = i == k ? 0.0 : M[i * n + k];
-    __syncthreads();
-    for (int idx = tid; idx < n * n; idx += nt) {
-      const int i = idx / n, j = idx - i * n;
-      if (i != k) M[idx] = (j == k ? 0.0 : M[idx]) - f[i] * M[k * n + j];
+    const double ip = 1.0 / piv;
+#pragma unroll
+    for (int e = 0; e < kMaxPer; ++e) {
+      const int i = mi[e], j = mj[e];
+      if (i < 0) continue;
+      const double pj = j == k ? 1.0 : prow[j];
+      M[i * n + j] = i == k ? pj * ip : (j == k ? 0.0 : M[i * n + j]) - f[i] * pj * ip;
     }
     __syncthreads();
   }
@@ -519,16 +549,6 @@ int ensure_attrs() {
 }
 
 // ---- FP16 copy of a level's values (FP32 hierarchies) ---------------------------
-// max |a| over the values (non-negative floats order like their bit patterns)
-__global__ void absmax_kernel(const int32_t* rp, int64_t n_brows, int vv, const float* __restrict__ a,
-                              unsigned* maxbits) {
-  const int64_t n = int64_t(rp[n_brows]) * vv;
-  float m = 0.0f;
-  for (int64_t k = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; k < n; k += int64_t(gridDim.x) * blockDim.x)
-    m = fmaxf(m, fabsf(a[k]));
-  for (int o = 16; o >= 1; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
-  if ((threadIdx.x & 31) == 0) atomicMax(maxbits, __float_as_uint(m));
-}
 // a16 = round(a s) with s = 2^e the largest power of two with max|a| s <=
 // 2^14 (well inside FP16's range); scale[0] = 1/s for the row kernels.
 __global__ void half_vals_kernel(const int32_t* rp, int64_t n_brows, int vv, const float* __restrict__ a,
@@ -573,24 +593,22 @@ int setup_impl(int nlevels, const FemMGLevel* L, const double* fine64, void* scr
                                                                    L[l].cpos, L[l].ilo, L[l].whi);
       FEM_LAUNCH_CHECK();
     }
-    if constexpr (sizeof(T) == 4) {
-      if (L[l].vals_lo != nullptr) {
-        unsigned* maxbits = reinterpret_cast<unsigned*>(L[l].lo_scale + 1);
-        FEM_CUDA_TRY(cudaMemsetAsync(maxbits, 0, sizeof(unsigned), st));
-        absmax_kernel<<<unsigned(num_sms()) * 8, 256, 0, st>>>(L[l].row_ptr, L[l].n_brows, VV,
-                                                               static_cast<const float*>(L[l].vals), maxbits);
-        FEM_LAUNCH_CHECK();
-        half_vals_kernel<<<unsigned(num_sms()) * 8, 256, 0, st>>>(L[l].row_ptr, L[l].n_brows, VV,
-                                                                  static_cast<const float*>(L[l].vals), maxbits,
-                                                                  static_cast<__half*>(L[l].vals_lo), L[l].lo_scale);
-        FEM_LAUNCH_CHECK();
-      }
-    }
+    // the level's FP16 copy (FP32 hierarchies): its scale comes from the
+    // max |a| the Jacobi setup finds
+    const bool lo = sizeof(T) == 4 && L[l].vals_lo != nullptr;
+    unsigned* maxbits = lo ? reinterpret_cast<unsigned*>(L[l].lo_scale + 1) : nullptr;
+    if (lo) FEM_CUDA_TRY(cudaMemsetAsync(maxbits, 0, sizeof(unsigned), st));
     FEM_CUDA_TRY(cudaMemsetAsync(L[l].lmax, 0, sizeof(unsigned long long), st));
     jacobi_setup_kernel<VEC, T><<<vgrid(L[l].n_brows * VEC), 256, 0, st>>>(
         L[l].n_brows, L[l].stencil, static_cast<const T*>(L[l].vals), static_cast<T*>(L[l].dinv),
-        static_cast<unsigned long long*>(L[l].lmax));
+        static_cast<unsigned long long*>(L[l].lmax), maxbits);
     FEM_LAUNCH_CHECK();
+    if (lo) {
+      half_vals_kernel<<<unsigned(num_sms()) * 8, 256, 0, st>>>(L[l].row_ptr, L[l].n_brows, VV,
+                                                                reinterpret_cast<const float*>(L[l].vals), maxbits,
+                                                                static_cast<__half*>(L[l].vals_lo), L[l].lo_scale);
+      FEM_LAUNCH_CHECK();
+    }
     if (L[l].cinv != nullptr) {
       const int n = int(L[l].n_brows) * VEC;
       const size_t sm = dense_inverse_smem(n);
