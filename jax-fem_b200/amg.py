@@ -46,9 +46,17 @@ from . import _native as nat
 
 
 class _CSR:
-    """A scalar CSR matrix on the device (y = M x)."""
+    """A scalar CSR matrix on the device (y = M x), from a scipy matrix or a
+    torch sparse CSR tensor."""
 
     def __init__(self, M, device):
+        if isinstance(M, torch.Tensor):
+            self.shape = tuple(M.shape)
+            self.n_brows = M.shape[0]
+            self.row_ptr = M.crow_indices().to(device=device, dtype=torch.int32).contiguous()
+            self.col_idx = M.col_indices().to(device=device, dtype=torch.int32).contiguous()
+            self.vals = M.values().to(device=device, dtype=torch.float64).contiguous()
+            return
         M = sp.csr_matrix(M)
         M.sort_indices()
         self.shape = M.shape
@@ -172,6 +180,69 @@ def spectral_radius(A, dinv, iters=15, seed=0):
     return lam
 
 
+def _t_csr(M, device):
+    """scipy CSR -> torch sparse CSR (FP64, int64 indices) on device."""
+    M = sp.csr_matrix(M)
+    M.sort_indices()
+    return torch.sparse_csr_tensor(torch.from_numpy(M.indptr.astype(np.int64)),
+                                   torch.from_numpy(M.indices.astype(np.int64)),
+                                   torch.from_numpy(M.data.astype(np.float64)), size=M.shape).to(device)
+
+
+def _t_scipy(M):
+    """torch sparse CSR -> scipy CSR (host copy)."""
+    return sp.csr_matrix((M.values().cpu().numpy(), M.col_indices().cpu().numpy(), M.crow_indices().cpu().numpy()),
+                         shape=tuple(M.shape))
+
+
+def _t_diag(M):
+    """Diagonal of a square torch sparse CSR matrix (dense vector)."""
+    crow, col, val = M.crow_indices(), M.col_indices(), M.values()
+    rows = torch.repeat_interleave(torch.arange(M.shape[0], device=val.device), crow[1:] - crow[:-1])
+    d = torch.zeros(M.shape[0], dtype=val.dtype, device=val.device)
+    on = rows == col
+    d.index_add_(0, rows[on], val[on])
+    return d
+
+
+def _t_scale_rows(M, s):
+    """diag(s) M for a torch sparse CSR matrix (same pattern)."""
+    crow, col, val = M.crow_indices(), M.col_indices(), M.values()
+    rows = torch.repeat_interleave(torch.arange(M.shape[0], device=val.device), crow[1:] - crow[:-1])
+    return torch.sparse_csr_tensor(crow, col, val * s[rows], size=M.shape)
+
+
+def _t_transpose(M):
+    return M.t().to_sparse_csr()
+
+
+def _t_spectral_radius(A, dinv, iters=15, seed=0):
+    """Largest eigenvalue of D^-1 A by power iteration (A torch sparse CSR)."""
+    g = torch.Generator(device=dinv.device).manual_seed(seed)
+    x = torch.rand(A.shape[0], 1, dtype=torch.float64, device=dinv.device, generator=g)
+    lam = torch.ones((), dtype=torch.float64, device=dinv.device)
+    for _ in range(iters):
+        x = x / x.norm()
+        y = dinv[:, None] * (A @ x)
+        lam = (x * y).sum()
+        x = y
+    return float(lam)
+
+
+def galerkin_t(A, T):
+    """(P, P^T A P) with P = (I - omega D^-1 A) T, omega = 4 / (3 rho(D^-1 A)),
+    as sparse products on the operators' device (torch sparse CSR, FP64);
+    the coarse operator symmetrised."""
+    d = _t_diag(A)
+    dinv = torch.where(d != 0, 1.0 / torch.where(d != 0, d, torch.ones_like(d)), torch.zeros_like(d))
+    omega = 4.0 / (3.0 * _t_spectral_radius(A, dinv))
+    AT = torch.sparse.mm(A, T)
+    P = torch.add(T, _t_scale_rows(AT, omega * dinv), alpha=-1.0)
+    Ac = torch.sparse.mm(_t_transpose(P), torch.sparse.mm(A, P))
+    Ac = torch.add(Ac, _t_transpose(Ac)) * 0.5
+    return P, Ac
+
+
 class AMG:
     """Smoothed-aggregation AMG preconditioned CG for one problem (see the
     module docstring).  Interface of the multigrid objects of solver.mg_solve."""
@@ -192,42 +263,66 @@ class AMG:
         self.setup_for = None
 
     # ---- setup -------------------------------------------------------------------
-    def _hierarchy(self, A):
+    def _fine_csr(self, A):
+        """The fine operator as a torch sparse CSR matrix on its device: the
+        block-CSR values gathered into scalar CSR order (the gather index is
+        built once from the pattern)."""
+        vec = A.vec
+        if getattr(self, "_fine_map", None) is None:
+            rp = A.row_ptr.cpu().numpy().astype(np.int64)
+            ci = A.col_idx.cpu().numpy().astype(np.int64)
+            nb = len(rp) - 1
+            cnt = np.diff(rp)
+            # entries in the order (block row b, component i, block k, component c):
+            # scalar row r = vec b + i holds blocks k of block row b, columns vec ci[k] + c
+            per_row = np.repeat(cnt, vec)  # blocks per scalar row
+            crow = np.zeros(nb * vec + 1, dtype=np.int64)
+            crow[1:] = np.cumsum(per_row * vec)
+            r_k = np.repeat(np.arange(nb * vec), per_row)
+            starts = np.concatenate([[0], np.cumsum(per_row)[:-1]]).astype(np.int64)
+            t = np.arange(len(r_k)) - np.repeat(starts, per_row)
+            b_of, i_of = r_k // vec, r_k % vec
+            k = rp[b_of] + t
+            k_rep, i_rep = np.repeat(k, vec), np.repeat(i_of, vec)
+            c_rep = np.tile(np.arange(vec), len(k))
+            col = ci[k_rep] * vec + c_rep
+            gather = k_rep * vec * vec + i_rep * vec + c_rep
+            dev = A.vals.device
+            self._fine_map = (torch.from_numpy(crow).to(dev), torch.from_numpy(col).to(dev),
+                              torch.from_numpy(gather).to(dev), (nb * vec, nb * vec))
+        crow, col, gather, shape = self._fine_map
+        return torch.sparse_csr_tensor(crow, col, A.vals.to(torch.float64)[gather], size=shape)
+
+    def _hierarchy(self, A, Ah):
         """Aggregates and tentative prolongators of every level (first
-        setup); returns the (P, coarse operator) pairs it formed."""
+        setup), with the Galerkin products of each level (needed for the
+        next level's strength of connection) on A's device; returns the
+        (P, coarse operator) torch pairs it formed.  Ah: host copy of A."""
         mask, _ = self.problem.dirichlet_device()
         free = (mask.cpu().numpy() == 0).astype(np.float64)
         vec = self.node_vec
-        dof_node = np.where(free > 0, np.arange(A.shape[0]) // vec, -1)
-        n_nodes = A.shape[0] // vec
+        dof_node = np.where(free > 0, np.arange(Ah.shape[0]) // vec, -1)
+        n_nodes = Ah.shape[0] // vec
         B = near_null_space(self.points, vec, free)
-        self.T, self.free = [], free
-        Al = A
+        self.T, self._Td, self.free = [], [], free
+        Al, Al_h = A, Ah
         formed = []
         for _ in range(self.max_levels - 1):
-            if Al.shape[0] <= self.coarse_size:
+            if Al_h.shape[0] <= self.coarse_size:
                 break
-            agg, na = aggregate(strength(Al, dof_node, n_nodes, self.theta))
+            agg, na = aggregate(strength(Al_h, dof_node, n_nodes, self.theta))
             if na == 0:
                 break
             T, B, owner = tentative(agg, na, dof_node, B)
-            if T.shape[1] >= Al.shape[0]:
+            if T.shape[1] >= Al_h.shape[0]:
                 break
             self.T.append(T)
-            formed.append(self._galerkin(Al, T))
+            self._Td.append(_t_csr(T, A.values().device))
+            formed.append(galerkin_t(Al, self._Td[-1]))
             Al = formed[-1][1]
+            Al_h = _t_scipy(Al)
             dof_node, n_nodes = owner, na
         return formed
-
-    @staticmethod
-    def _galerkin(A, T):
-        """(P, P^T A P) with P = (I - omega D^-1 A) T."""
-        d = A.diagonal()
-        dinv = np.where(d != 0, 1.0 / np.where(d != 0, d, 1.0), 0.0)
-        omega = 4.0 / (3.0 * spectral_radius(A, dinv))
-        P = (T - sp.diags(omega * dinv) @ (A @ T)).tocsr()
-        Ac = (P.T @ A @ P).tocsr()
-        return P, (0.5 * (Ac + Ac.T)).tocsr()
 
     def setup(self, A, fine_only=False):
         import time
@@ -246,25 +341,25 @@ class AMG:
         if not fine_only or self.lmax is None:
             self.lmax = 1.1 * self._power(A)
         if not fine_only or self.T is None:
-            Ah = sp.csr_matrix(A.to_scipy())
-            formed = self._hierarchy(Ah) if self.T is None else None
+            Ad = self._fine_csr(A)
+            formed = self._hierarchy(Ad, sp.csr_matrix(A.to_scipy())) if self.T is None else None
             self.levels = []  # (A_l on the device, D_l^-1, lmax_l) for l >= 1
             self.P, self.R = [], []
-            Al = Ah
-            for k, T in enumerate(self.T):
-                P, Al = formed[k] if formed is not None else self._galerkin(Al, T)
+            Al = Ad
+            for k, Td in enumerate(self._Td):
+                P, Al = formed[k] if formed is not None else galerkin_t(Al, Td)
                 self.P.append(_CSR(P, self.device))
-                self.R.append(_CSR(P.T.tocsr(), self.device))
-                d = Al.diagonal()
-                dinv = np.where(d != 0, 1.0 / np.where(d != 0, d, 1.0), 0.0)
-                self.levels.append((_CSR(Al, self.device), torch.from_numpy(dinv).to(self.device),
-                                    1.1 * spectral_radius(Al, dinv)))
-            Ad = Al.toarray()
+                self.R.append(_CSR(_t_transpose(P), self.device))
+                d = _t_diag(Al)
+                dinv = torch.where(d != 0, 1.0 / torch.where(d != 0, d, torch.ones_like(d)), torch.zeros_like(d))
+                self.levels.append((_CSR(Al, self.device), dinv.to(self.device),
+                                    1.1 * _t_spectral_radius(Al, dinv)))
+            Ad_dense = Al.to_dense()
             try:
-                inv = np.linalg.inv(Ad)
-            except np.linalg.LinAlgError:
-                inv = np.linalg.pinv(Ad)
-            self.coarse_inv = torch.from_numpy(inv).to(self.device)
+                inv = torch.linalg.inv(Ad_dense)
+            except RuntimeError:
+                inv = torch.linalg.pinv(Ad_dense)
+            self.coarse_inv = inv.to(self.device).contiguous()
             self.solves_on_coarse = 0
         self.setup_for = A
 

@@ -98,6 +98,8 @@ def _amg_on_cpu(amg, monkeypatch, A, free, points, vec, block):
         return y if out is None else out.copy_(y)
 
     Aop = types.SimpleNamespace(vals=torch.from_numpy(Ab.data.reshape(-1).copy()), diag=torch.from_numpy(diag),
+                                row_ptr=torch.from_numpy(Ab.indptr.astype(np.int32)),
+                                col_idx=torch.from_numpy(Ab.indices.astype(np.int32)),
                                 n_brows=n // block, vec=block, matvec=matvec, to_scipy=lambda: A)
     mask = torch.from_numpy((1.0 - free).astype(np.uint8))
     fe = types.SimpleNamespace(vec=vec, points=points)
@@ -217,3 +219,36 @@ def test_amg_cg_failures_are_reported(pkg, amg, monkeypatch):
         g2.solve(Aop2, b, x, rtol=1e-10, maxiter=200)
     assert e.value.status == nat.FEM_ERR_BREAKDOWN
     assert torch.isfinite(x).all()
+
+
+def test_device_galerkin_matches_scipy(pkg, amg):
+    """The Galerkin products as torch sparse products (the form setup runs on
+    the operator's device) equal scipy's: P = (I - omega D^-1 A) T and
+    P^T A P (symmetrised), 1e-12 relative; the fine operator gathered from
+    block-CSR values into scalar CSR equals the block matrix."""
+    points, cells = _renumbered_tet10(pkg)
+    A = fo.OracleProblem(points, cells, 3, fo.Law("linear", E=70e3, nu=0.3), ele_type="TET10")
+    A.newton_update(np.zeros(A.ndofs))
+    K = A.assemble_global().tocsr()
+    Kb = K.tobsr(blocksize=(3, 3))
+    Kb.sort_indices()
+    Aop = types.SimpleNamespace(vals=torch.from_numpy(Kb.data.reshape(-1).copy()),
+                                row_ptr=torch.from_numpy(Kb.indptr.astype(np.int32)),
+                                col_idx=torch.from_numpy(Kb.indices.astype(np.int32)), vec=3)
+    g = amg.AMG.__new__(amg.AMG)
+    Kt = g._fine_csr(Aop)
+    assert abs(amg._t_scipy(Kt) - K).max() == 0.0
+    n_nodes = len(points)
+    free = np.ones(3 * n_nodes)
+    dof_node = np.arange(3 * n_nodes) // 3
+    agg, na = amg.aggregate(amg.strength(K, dof_node, n_nodes, 0.08))
+    T, _, _ = amg.tentative(agg, na, dof_node, amg.near_null_space(points, 3, free))
+    P_t, Ac_t = amg.galerkin_t(Kt, amg._t_csr(T, "cpu"))
+    d = K.diagonal()
+    dinv = 1.0 / d
+    omega = 4.0 / (3.0 * amg._t_spectral_radius(Kt, torch.from_numpy(dinv)))
+    P = (T - sp.diags(omega * dinv) @ (K @ T)).tocsr()
+    Ac = P.T @ K @ P
+    Ac = 0.5 * (Ac + Ac.T)
+    assert abs(amg._t_scipy(P_t) - P).max() <= 1e-12 * abs(P).max()
+    assert abs(amg._t_scipy(Ac_t) - Ac).max() <= 1e-12 * abs(Ac).max()
