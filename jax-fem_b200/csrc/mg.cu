@@ -24,6 +24,7 @@
 #include <cstring>
 #include <map>
 #include <mutex>
+#include <set>
 #include <string>
 #include <vector>
 
@@ -431,10 +432,15 @@ __global__ void __launch_bounds__(kDenseThreads)
   const int tid = threadIdx.x, nt = blockDim.x;
   for (int i = tid; i < n * n; i += nt) M[i] = 0.0;
   __syncthreads();
-  for (int br = tid; br < n_brows; br += nt)
-    for (int k = rp[br]; k < rp[br + 1]; ++k)
-      for (int e = 0; e < VV; ++e)
-        M[(br * VEC + e / VEC) * n + ci[k] * VEC + e % VEC] = double(vals[int64_t(k) * VV + e]);
+  // one thread per stored value (its block row by a scan of the <= 43 row
+  // pointers), so the loads are issued together
+  const int nvals = rp[n_brows] * VV;
+  for (int idx = tid; idx < nvals; idx += nt) {
+    const int k = idx / VV, e = idx - (idx / VV) * VV;
+    int br = 0;
+    while (br + 1 < n_brows && rp[br + 1] <= k) ++br;
+    M[(br * VEC + e / VEC) * n + ci[k] * VEC + e % VEC] = double(vals[int64_t(k) * VV + e]);
+  }
   __syncthreads();
   // Gauss-Jordan in place, two barriers per pivot: phase A copies column k
   // (f) and the unscaled pivot row (prow); phase B forms every entry from
@@ -612,8 +618,19 @@ int setup_impl(int nlevels, const FemMGLevel* L, const double* fine64, void* scr
     if (L[l].cinv != nullptr) {
       const int n = int(L[l].n_brows) * VEC;
       const size_t sm = dense_inverse_smem(n);
-      FEM_CUDA_TRY(cudaFuncSetAttribute(dense_inverse_kernel<VEC, T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                        int(dense_inverse_smem(FEM_MG_DENSE_MAX))));
+      static std::mutex attr_mu;  // per instantiation, once per device
+      static std::set<int> attr_done;
+      int dev = 0;
+      FEM_CUDA_TRY(cudaGetDevice(&dev));
+      {
+        std::lock_guard<std::mutex> lock(attr_mu);
+        if (!attr_done.count(dev)) {
+          FEM_CUDA_TRY(cudaFuncSetAttribute(dense_inverse_kernel<VEC, T>,
+                                            cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                            int(dense_inverse_smem(FEM_MG_DENSE_MAX))));
+          attr_done.insert(dev);
+        }
+      }
       dense_inverse_kernel<VEC, T><<<1, kDenseThreads, sm, st>>>(int(L[l].n_brows), L[l].row_ptr, L[l].col_idx,
                                                                  static_cast<const T*>(L[l].vals), L[l].cinv);
       FEM_LAUNCH_CHECK();
