@@ -846,6 +846,31 @@ def run_asm_only(args, device):
                       "peak_kind": kind}), flush=True)
 
 
+def run_mg_only(args, device):
+    """Multigrid times on the n^3 Neo-Hookean tangent at a twisted state
+    (CUDA events, 20 calls after 3 warm-up ones): a full setup of the FP32
+    hierarchy from the FP32 tangent, a fine-only setup, one V-cycle."""
+    import importlib
+    pkg = load_package()
+    mgm = importlib.import_module("jax_fem_b200.multigrid")
+    prob = nh_problem(pkg, n=args.n)
+    dv = prob.dev()
+    prob.fes[0].update_Dirichlet_boundary_conditions(rotation_bc(math.radians(6.0)))
+    mask, vals = prob.dirichlet_device()
+    u = torch.where(mask.bool(), vals, torch.zeros_like(vals))
+    A32 = dv.new_matrix(torch.float32)
+    prob.assemble(u, res=torch.empty_like(u), vals=A32.vals, fp32=True)
+    M = mgm.Multigrid(dv, prob.mesh.points, prob.mesh.cells, fp32=True, nu_fine=1)
+    t_full = time_kernel(lambda: M.setup(A32))
+    t_fine = time_kernel(lambda: M.setup(A32, fine_only=True))
+    r = torch.randn(dv.ndofs, device=device)
+    z = torch.empty_like(r)
+    t_v = time_kernel(lambda: M.vcycle(r, z, nu=2, coarse_steps=8, ratio=25.0))
+    print(json.dumps({"n": args.n, "levels": M.nlevels, "us": {"full_setup": round(t_full * 1e6, 1),
+                      "fine_setup": round(t_fine * 1e6, 1), "vcycle": round(t_v * 1e6, 1)},
+                      "half_fine": M.half_fine}), flush=True)
+
+
 def run_profile_element(args, device):
     """For ncu: the general-element kernel on one element type at its bench
     size (ELEMENT_BOXES), Neo-Hookean at a twisted state: FP64 assembly x2,
@@ -997,6 +1022,7 @@ def main():
                     help="only the TET4/TET10/HEX20/HEX27 and cell-kernel-path measurements")
     ap.add_argument("--profile", action="store_true", help="short kernel sequence for ncu captures")
     ap.add_argument("--asm-only", action="store_true", help="only the HEX8 assembly times")
+    ap.add_argument("--mg-only", action="store_true", help="only the multigrid setup and V-cycle times")
     ap.add_argument("--conv-only", action="store_true",
                     help="only the tensor-core convolution / weight-gradient throughput")
     ap.add_argument("--profile-element", default="", choices=["", "TET4", "TET10", "HEX20", "HEX27"],
@@ -1033,6 +1059,9 @@ def main():
         return
     if args.asm_only:
         run_asm_only(args, device)
+        return
+    if args.mg_only:
+        run_mg_only(args, device)
         return
     if args.conv_only:
         print(json.dumps({"tensor_core_conv": conv_bench(load_package(), device)}), flush=True)

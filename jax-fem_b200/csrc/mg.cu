@@ -70,7 +70,10 @@ __global__ void __launch_bounds__(kApWarps * 32) ap_kernel(Lat F, const int32_t*
                                                            const T* __restrict__ fv, Lat C, const int32_t* ilo,
                                                            const double* whi, T* B) {
   constexpr int VV = VEC * VEC;
-  __shared__ T sA[kApWarps][27][VV];
+  // each staged block padded to a 16-byte multiple, read back with 16-byte loads
+  constexpr int PER16 = 16 / int(sizeof(T));
+  constexpr int VVP = ((VV + PER16 - 1) / PER16) * PER16;
+  __shared__ __align__(16) T sA[kApWarps][27][VVP];
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   const int32_t* il[3] = {ilo, ilo + F.n[0], ilo + F.n[0] + F.n[1]};
   const double* wh[3] = {whi, whi + F.n[0], whi + F.n[0] + F.n[1]};
@@ -104,8 +107,12 @@ __global__ void __launch_bounds__(kApWarps * 32) ap_kernel(Lat F, const int32_t*
     for (int o = 0; o < 27; ++o) {
       const double ww = w[0][o / 9] * w[1][(o / 3) % 3] * w[2][o % 3];
       if (ww == 0.0) continue;
+      T blk[VVP];
+      const uint4* src = reinterpret_cast<const uint4*>(&sA[wid][o][0]);
 #pragma unroll
-      for (int e = 0; e < VV; ++e) acc[e] = fma(ww, double(sA[wid][o][e]), acc[e]);
+      for (int v = 0; v < VVP / PER16; ++v) reinterpret_cast<uint4*>(blk)[v] = src[v];
+#pragma unroll
+      for (int e = 0; e < VV; ++e) acc[e] = fma(ww, double(blk[e]), acc[e]);
     }
 #pragma unroll
     for (int e = 0; e < VV; ++e) B[(i * 27 + lane) * VV + e] = T(acc[e]);

@@ -15,21 +15,20 @@ constexpr int kLiftBit = 8;
 // Lower-triangle blocks as transposes of their upper partners: block k of
 // row i, column j < i, takes block tmap[k] = (j, i) transposed.  In the
 // row-sorted layout tmap[k] < k holds exactly for those blocks.  One thread
-// per block: its VEC*VEC loads from the partner block are independent and in
-// flight together, and consecutive threads store consecutive blocks.
+// per value word: consecutive threads store consecutive words (coalesced),
+// and the VEC*VEC threads of a block read one partner block.
 template <int VEC, typename T>
 __global__ void mirror_lower_kernel(int64_t nnzb, const int32_t* __restrict__ tmap, T* vals) {
   constexpr int VV = VEC * VEC;
-  for (int64_t k = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; k < nnzb; k += int64_t(gridDim.x) * blockDim.x) {
+  const int64_t nwords = nnzb * VV;
+  for (int64_t w = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; w < nwords;
+       w += int64_t(gridDim.x) * blockDim.x) {
+    const int64_t k = w / VV;
+    const int e = int(w - k * VV);
     const int64_t p = tmap[k];
     if (p >= k) continue;
-    T v[VV];
-#pragma unroll
-    for (int e = 0; e < VV; ++e) v[e] = vals[p * VV + e];
-#pragma unroll
-    for (int r = 0; r < VEC; ++r)
-#pragma unroll
-      for (int c = 0; c < VEC; ++c) vals[k * VV + r * VEC + c] = v[c * VEC + r];
+    const int r = e / VEC, c = e - (e / VEC) * VEC;
+    vals[w] = vals[p * VV + c * VEC + r];
   }
 }
 
@@ -48,7 +47,7 @@ __global__ void bc_diag_kernel(int vec, int64_t ndofs, const uint8_t* bc, const 
 template <typename T>
 int finish_tangent(int vec, int64_t nnzb, int64_t ndofs, const int32_t* d_transpose,
                    const uint8_t* d_bc, const int32_t* d_diag, T* d_vals, cudaStream_t st) {
-  const int64_t blocks = (nnzb + 255) / 256;
+  const int64_t blocks = (nnzb * vec * vec + 255) / 256;
   const unsigned grid = unsigned(blocks < int64_t(num_sms()) * 16 ? blocks : int64_t(num_sms()) * 16);
   if (grid > 0) {
     if (vec == 3)
