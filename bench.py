@@ -849,7 +849,8 @@ def run_asm_only(args, device):
 def run_mg_only(args, device):
     """Multigrid times on the n^3 Neo-Hookean tangent at a twisted state
     (CUDA events, 20 calls after 3 warm-up ones): a full setup of the FP32
-    hierarchy from the FP32 tangent, a fine-only setup, one V-cycle."""
+    hierarchy from the FP32 tangent, a fine-only setup, one V-cycle launched
+    directly and replayed from a CUDA graph."""
     import importlib
     pkg = load_package()
     mgm = importlib.import_module("jax_fem_b200.multigrid")
@@ -866,8 +867,19 @@ def run_mg_only(args, device):
     r = torch.randn(dv.ndofs, device=device)
     z = torch.empty_like(r)
     t_v = time_kernel(lambda: M.vcycle(r, z, nu=2, coarse_steps=8, ratio=25.0))
+    # the same V-cycle replayed from a CUDA graph (as inside the solve graph)
+    s = torch.cuda.Stream(device=device)
+    s.wait_stream(torch.cuda.current_stream(device))
+    with torch.cuda.stream(s):
+        M.vcycle(r, z, nu=2, coarse_steps=8, ratio=25.0)
+    torch.cuda.current_stream(device).wait_stream(s)
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g):
+        M.vcycle(r, z, nu=2, coarse_steps=8, ratio=25.0)
+    t_g = time_kernel(g.replay)
     print(json.dumps({"n": args.n, "levels": M.nlevels, "us": {"full_setup": round(t_full * 1e6, 1),
-                      "fine_setup": round(t_fine * 1e6, 1), "vcycle": round(t_v * 1e6, 1)},
+                      "fine_setup": round(t_fine * 1e6, 1), "vcycle": round(t_v * 1e6, 1),
+                      "vcycle_graph": round(t_g * 1e6, 1)},
                       "half_fine": M.half_fine}), flush=True)
 
 

@@ -450,11 +450,11 @@ __global__ void __launch_bounds__(kDenseThreads)
   }
   __syncthreads();
   // Gauss-Jordan in place, two barriers per pivot: phase A copies column k
-  // (f) and the unscaled pivot row (prow); phase B forms every entry from
-  // them, the pivot row as prow / piv and the others as
-  // M_ij - M_ik prow_j / piv (column k: -M_ik / piv; the pivot: 1 / piv).
-  // Each thread keeps the (i, j) of its entries (at most 16 for n <= 128).
-  double* prow = f + n;
+  // (f) and forms the scaled pivot row q_j = M_kj / piv (q_k = 1 / piv), n
+  // divisions; phase B forms every entry with one FMA: the pivot row as q_j
+  // and the others as M_ij - M_ik q_j (column k: -M_ik q_k).  Each thread
+  // keeps the (i, j) of its entries (at most 16 for n <= 128).
+  double* q = f + n;
   constexpr int kMaxPer = (FEM_MG_DENSE_MAX * FEM_MG_DENSE_MAX + kDenseThreads - 1) / kDenseThreads;
   int mi[kMaxPer], mj[kMaxPer];
 #pragma unroll
@@ -465,23 +465,22 @@ __global__ void __launch_bounds__(kDenseThreads)
   }
   bool ok = true;
   for (int k = 0; k < n; ++k) {
-    for (int i = tid; i < n; i += nt) {
-      f[i] = M[i * n + k];
-      prow[i] = M[k * n + i];
-    }
-    __syncthreads();
-    const double piv = prow[k];
-    if (!(piv > 0.0) || !isfinite(piv)) {  // same value in every thread: uniform exit
+    const double piv = M[k * n + k];  // same value in every thread
+    if (!(piv > 0.0) || !isfinite(piv)) {  // uniform exit
       ok = false;
       break;
     }
-    const double ip = 1.0 / piv;
+    for (int i = tid; i < n; i += nt) {
+      f[i] = M[i * n + k];
+      q[i] = (i == k ? 1.0 : M[k * n + i]) / piv;
+    }
+    __syncthreads();
 #pragma unroll
     for (int e = 0; e < kMaxPer; ++e) {
       const int i = mi[e], j = mj[e];
       if (i < 0) continue;
-      const double pj = j == k ? 1.0 : prow[j];
-      M[i * n + j] = i == k ? pj * ip : (j == k ? 0.0 : M[i * n + j]) - f[i] * pj * ip;
+      const double qj = q[j];
+      M[i * n + j] = i == k ? qj : fma(-f[i], qj, j == k ? 0.0 : M[i * n + j]);
     }
     __syncthreads();
   }

@@ -258,18 +258,41 @@ class Problem:
             k += fe.num_nodes * fe.vec
         return out
 
+    def _dirichlet_compact(self):
+        """Constrained global dofs (sorted) and their values; where conditions
+        overlap the later one wins, as in FiniteElement.dirichlet_arrays."""
+        dofs, vals, off = [], [], 0
+        for fe in self.fes:
+            for nodes, v, val in zip(fe.node_inds_list, fe.vec_inds_list, fe.vals_list):
+                dofs.append(off + np.asarray(nodes, dtype=np.int64) * fe.vec + v)
+                vals.append(np.broadcast_to(np.asarray(val, dtype=np.float64), np.shape(nodes)))
+            off += fe.num_total_dofs
+        if not dofs:
+            return np.zeros(0, dtype=np.int64), np.zeros(0, dtype=np.float64)
+        d, x = np.concatenate(dofs), np.concatenate(vals)
+        u, last = np.unique(d[::-1], return_index=True)  # first in reverse = last in order
+        return u, x[::-1][last]
+
     def dirichlet_device(self):
-        """(mask uint8, values f64) over all dofs on the device, refreshed after BC updates."""
+        """(mask uint8, values f64) over all dofs on the device, refreshed after
+        BC updates.  A refresh copies only the constrained dofs' values and
+        scatters them on the device; the mask (and the index copy) is reused
+        while the constrained dofs stay the same (load stepping)."""
         key = tuple(fe.bc_version for fe in self.fes)
         if self._bc_cache is None or self._bc_cache[0] != key:
-            arrays = [fe.dirichlet_arrays() for fe in self.fes]
-            if len(arrays) == 1:  # one variable: no host copy
-                mask, vals = arrays[0]
-            else:
-                mask = np.concatenate([a[0] for a in arrays])
-                vals = np.concatenate([a[1] for a in arrays])
             d = self.dev().device
-            self._bc_cache = (key, torch.from_numpy(mask).to(d), torch.from_numpy(vals).to(d))
+            n = self.num_total_dofs_all_vars
+            dofs, vals = self._dirichlet_compact()
+            prev = self._bc_cache
+            if prev is not None and np.array_equal(prev[3], dofs):
+                mask, idx = prev[1], prev[4]
+            else:
+                idx = torch.from_numpy(dofs).to(d)
+                mask = torch.zeros(n, dtype=torch.uint8, device=d)
+                mask[idx] = 1
+            ubc = torch.zeros(n, dtype=torch.float64, device=d)
+            ubc[idx] = torch.from_numpy(np.ascontiguousarray(vals)).to(d)
+            self._bc_cache = (key, mask, ubc, dofs, idx)
         return self._bc_cache[1], self._bc_cache[2]
 
     def surface_load_vectors(self):

@@ -122,6 +122,29 @@ def test_dirichlet_discovery_batched_and_pointwise(pkg):
         np.testing.assert_allclose(a, b, rtol=0, atol=0)
 
 
+def test_dirichlet_compact_matches_full_arrays(pkg):
+    """The compact form a Dirichlet refresh copies to the device (constrained
+    dofs and their values) equals the full-length mask and values, with the
+    later condition winning where conditions overlap."""
+    m = pkg.box_mesh(4, 3, 3, 1.0, 1.0, 1.0)
+    left = lambda p: np.isclose(p[0], 0.0)  # noqa: E731
+    low = lambda p: p[1] < 0.5  # overlaps the left face  # noqa: E731
+    bc = [[left, left, low, left], [0, 1, 0, 2],
+          [lambda p: 1.0 + p[1], lambda p: 0.0 * p[0], lambda p: -2.0 + 0.0 * p[0], lambda p: 3.0 * p[2]]]
+
+    class P(pkg.Problem):
+        def get_tensor_map(self):
+            return pkg.LinearElastic(1.0, 0.3)
+
+    p = P(pkg.Mesh(m.points, m.cells_dict["hexahedron"]), vec=3, dim=3, dirichlet_bc_info=bc)
+    dofs, vals = p._dirichlet_compact()
+    mask, full = p.fes[0].dirichlet_arrays()
+    np.testing.assert_array_equal(dofs, np.flatnonzero(mask))
+    np.testing.assert_array_equal(vals, full[dofs])
+    assert np.all(np.diff(dofs) > 0)
+    assert np.any(np.isclose(vals, -2.0))  # the later condition where it overlaps the left face
+
+
 _XCUT = 2.0
 
 
