@@ -422,10 +422,16 @@ __global__ void __launch_bounds__(kRowThreads, kRowBlocksPerSM)
 }
 
 // ---- exact solve of a small coarsest level -------------------------------------
-// Gauss-Jordan inversion in FP64 shared memory (no pivoting: the Galerkin
-// operator of an SPD operator is SPD, so every pivot is positive).  A pivot
-// that is not positive leaves the Jacobi inverse instead.
+// Gauss-Jordan inversion in FP64 (no pivoting: the Galerkin operator of an
+// SPD operator is SPD, so every pivot is positive).  A pivot that is not
+// positive leaves the Jacobi inverse instead.  One CTA of 1024 threads; the
+// matrix is gathered into shared memory, then held in registers: thread
+// (ty, tx) = (tid / 128, tid % 128) owns column j = tx, rows ty + 8 r
+// (r < 16), so with n <= FEM_MG_DENSE_MAX = 128 every entry has an owner.
 constexpr int kDenseThreads = 1024;
+constexpr int kDenseCols = 128, kDenseRowStep = kDenseThreads / kDenseCols, kDenseRows = 16;
+static_assert(FEM_MG_DENSE_MAX <= kDenseCols && FEM_MG_DENSE_MAX <= kDenseRowStep * kDenseRows,
+              "dense inverse: one owner per entry");
 inline size_t dense_inverse_smem(int n) { return (size_t(n) * n + 2 * n) * sizeof(double); }
 
 template <int VEC, typename T>
@@ -435,7 +441,8 @@ __global__ void __launch_bounds__(kDenseThreads)
   extern __shared__ __align__(16) double dsm[];
   const int n = n_brows * VEC;
   double* M = dsm;
-  double* f = dsm + n * n;
+  double* col = dsm + n * n;  // column k of the current pivot
+  double* prow = col + n;     // row k
   const int tid = threadIdx.x, nt = blockDim.x;
   for (int i = tid; i < n * n; i += nt) M[i] = 0.0;
   __syncthreads();
@@ -449,43 +456,54 @@ __global__ void __launch_bounds__(kDenseThreads)
     M[(br * VEC + e / VEC) * n + ci[k] * VEC + e % VEC] = double(vals[int64_t(k) * VV + e]);
   }
   __syncthreads();
-  // Gauss-Jordan in place, two barriers per pivot: phase A copies column k
-  // (f) and forms the scaled pivot row q_j = M_kj / piv (q_k = 1 / piv), n
-  // divisions; phase B forms every entry with one FMA: the pivot row as q_j
-  // and the others as M_ij - M_ik q_j (column k: -M_ik q_k).  Each thread
-  // keeps the (i, j) of its entries (at most 16 for n <= 128).
-  double* q = f + n;
-  constexpr int kMaxPer = (FEM_MG_DENSE_MAX * FEM_MG_DENSE_MAX + kDenseThreads - 1) / kDenseThreads;
-  int mi[kMaxPer], mj[kMaxPer];
+  const int j = tid % kDenseCols, ty = tid / kDenseCols;
+  const bool own = j < n;
+  double m[kDenseRows];
 #pragma unroll
-  for (int e = 0; e < kMaxPer; ++e) {
-    const int idx = tid + e * nt;
-    mi[e] = idx < n * n ? idx / n : -1;
-    mj[e] = idx < n * n ? idx - (idx / n) * n : 0;
+  for (int r = 0; r < kDenseRows; ++r) {
+    const int i = ty + kDenseRowStep * r;
+    m[r] = own && i < n ? M[i * n + j] : 0.0;
   }
+  // Per pivot k: the owners of row k and column k publish them (barrier);
+  // with q_j = M_kj / piv (q_k = 1 / piv), row k becomes q_j and every other
+  // row M_ij - M_ik q_j: one broadcast load and one FMA per entry (barrier
+  // before the next pivot's row and column overwrite these).
   bool ok = true;
   for (int k = 0; k < n; ++k) {
-    const double piv = M[k * n + k];  // same value in every thread
+    if (own) {
+#pragma unroll
+      for (int r = 0; r < kDenseRows; ++r) {
+        const int i = ty + kDenseRowStep * r;
+        if (i == k) prow[j] = m[r];
+        if (j == k && i < n) col[i] = m[r];
+      }
+    }
+    __syncthreads();
+    const double piv = prow[k];  // same value in every thread
     if (!(piv > 0.0) || !isfinite(piv)) {  // uniform exit
       ok = false;
       break;
     }
-    for (int i = tid; i < n; i += nt) {
-      f[i] = M[i * n + k];
-      q[i] = (i == k ? 1.0 : M[k * n + i]) / piv;
-    }
-    __syncthreads();
+    if (own) {
+      const double ip = __drcp_rn(piv);  // 1 / piv, correctly rounded
+      const double qj = j == k ? ip : prow[j] * ip;
+      const bool jk = j == k;
 #pragma unroll
-    for (int e = 0; e < kMaxPer; ++e) {
-      const int i = mi[e], j = mj[e];
-      if (i < 0) continue;
-      const double qj = q[j];
-      M[i * n + j] = i == k ? qj : fma(-f[i], qj, j == k ? 0.0 : M[i * n + j]);
+      for (int r = 0; r < kDenseRows; ++r) {
+        const int i = ty + kDenseRowStep * r;
+        if (i < n) m[r] = i == k ? qj : fma(-col[i], qj, jk ? 0.0 : m[r]);
+      }
     }
     __syncthreads();
   }
   if (ok) {
-    for (int idx = tid; idx < n * n; idx += nt) inv[idx] = M[idx];
+    if (own) {
+#pragma unroll
+      for (int r = 0; r < kDenseRows; ++r) {
+        const int i = ty + kDenseRowStep * r;
+        if (i < n) inv[i * n + j] = m[r];
+      }
+    }
   } else {
     for (int idx = tid; idx < n * n; idx += nt) inv[idx] = 0.0;
     __syncthreads();

@@ -260,18 +260,28 @@ class Problem:
 
     def _dirichlet_compact(self):
         """Constrained global dofs (sorted) and their values; where conditions
-        overlap the later one wins, as in FiniteElement.dirichlet_arrays."""
-        dofs, vals, off = [], [], 0
+        overlap the later one wins, as in FiniteElement.dirichlet_arrays.  The
+        selection is kept while the conditions' nodes and components stay the
+        same (load stepping changes values only)."""
+        struct, vals, off = [], [], 0
         for fe in self.fes:
             for nodes, v, val in zip(fe.node_inds_list, fe.vec_inds_list, fe.vals_list):
-                dofs.append(off + np.asarray(nodes, dtype=np.int64) * fe.vec + v)
+                struct.append((off, fe.vec, nodes, v))
                 vals.append(np.broadcast_to(np.asarray(val, dtype=np.float64), np.shape(nodes)))
             off += fe.num_total_dofs
-        if not dofs:
+        if not struct:
             return np.zeros(0, dtype=np.int64), np.zeros(0, dtype=np.float64)
-        d, x = np.concatenate(dofs), np.concatenate(vals)
+        x = np.concatenate(vals)
+        cache = self.__dict__.get("_bc_compact")
+        if cache is not None and len(cache[0]) == len(struct) and all(
+                a[0] == b[0] and a[1] == b[1] and np.array_equal(a[2], b[2]) and np.array_equal(a[3], b[3])
+                for a, b in zip(cache[0], struct)):
+            return cache[1], x[cache[2]]
+        d = np.concatenate([o + np.asarray(nodes, dtype=np.int64) * vec + v for o, vec, nodes, v in struct])
         u, last = np.unique(d[::-1], return_index=True)  # first in reverse = last in order
-        return u, x[::-1][last]
+        sel = len(d) - 1 - last
+        self._bc_compact = ([(o, vec, np.array(nodes), np.array(v)) for o, vec, nodes, v in struct], u, sel)
+        return u, x[sel]
 
     def dirichlet_device(self):
         """(mask uint8, values f64) over all dofs on the device, refreshed after

@@ -145,6 +145,27 @@ def test_dirichlet_compact_matches_full_arrays(pkg):
     assert np.any(np.isclose(vals, -2.0))  # the later condition where it overlaps the left face
 
 
+def test_batched_confirmation_by_code(pkg):
+    """A value function rebuilt with new closure numbers (one per load step)
+    reuses its code's batched confirmation with a two-point check; a closure
+    value under which batching is wrong still ends in point-wise values."""
+    fe_mod = pkg.fe
+    pts = np.random.default_rng(1).uniform(size=(50, 3))
+
+    def make(c, k=0):
+        def f(p):
+            return c * p[1] + (p[0].sum() if k else 0.0)  # k: sums over every point when batched
+        return f
+
+    first = fe_mod._batched_or_pointwise(make(0.5), (pts,), ())
+    np.testing.assert_array_equal(first, 0.5 * pts[:, 1])
+    assert any(key[0] is make(0.0).__code__ for key in fe_mod._BATCHED_CODE)
+    again = fe_mod._batched_or_pointwise(make(-2.0), (pts,), ())
+    np.testing.assert_array_equal(again, -2.0 * pts[:, 1])
+    wrong = fe_mod._batched_or_pointwise(make(1.0, 1), (pts,), ())
+    np.testing.assert_allclose(wrong, pts[:, 1] + pts[:, 0], rtol=1e-15)
+
+
 _XCUT = 2.0
 
 
