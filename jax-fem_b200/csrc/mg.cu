@@ -61,36 +61,55 @@ __device__ __forceinline__ void fine_range(const int32_t* cpos, int64_t I, int64
 __device__ __forceinline__ int64_t col_base(const int32_t* ilo, int64_t i) { return ilo[i > 0 ? i - 1 : 0]; }
 
 // B[i][t] = sum_j A_ij w(j, J_t), J_t = base(i) + (t/9, t/3%3, t%3): one warp
-// per fine row.  Lane o stages the row's block of neighbour offset o in shared
-// memory (the row's blocks are contiguous); lane t then forms window slot t
-// from the 27 staged blocks.
+// per fine row.  Lane o stages the row's block of neighbour offset
+// o = (a, b, c) in shared memory (the row's blocks are contiguous).  P is a
+// tensor product, w(j, J) = wx wy wz, so the 27 x 27 block products factor
+// into three contractions of 27 outputs by 3 terms, one direction each, lane
+// l forming output l of each:
+//   T1[a,b,tz] = sum_c A[a,b,c] wz[c][tz],  T2[a,ty,tz] = sum_b T1[a,b,tz] wy[b][ty],
+//   B[tx,ty,tz] = sum_a T2[a,ty,tz] wx[a][tx]   (FP64 sums).
 constexpr int kApWarps = 8;
+template <int VEC, typename T>
+struct ApStage {
+  static constexpr int VV = VEC * VEC;
+  // staged blocks padded to a 16-byte multiple, read back with 16-byte loads
+  static constexpr int PER16 = 16 / int(sizeof(T));
+  static constexpr int VVP = ((VV + PER16 - 1) / PER16) * PER16;
+  static constexpr int kA = 27 * VVP * int(sizeof(T));  // the row's blocks
+  static constexpr int kT = 27 * VV * 8;                 // one FP64 intermediate
+  static constexpr int kX = kA > kT ? kA : kT;            // A, then T2
+  // both parts start on 16-byte boundaries in every warp's stage (A is read
+  // back with 16-byte loads)
+  static constexpr int kXr = ((kX + 15) / 16) * 16;
+  static constexpr int kWarp = kXr + ((kT + 15) / 16) * 16;
+  static_assert(kWarp % 16 == 0 && (VVP * int(sizeof(T))) % 16 == 0, "ap stage alignment");
+};
 template <int VEC, typename T>
 __global__ void __launch_bounds__(kApWarps * 32) ap_kernel(Lat F, const int32_t* __restrict__ fst,
                                                            const T* __restrict__ fv, Lat C, const int32_t* ilo,
                                                            const double* whi, T* B) {
-  constexpr int VV = VEC * VEC;
-  // each staged block padded to a 16-byte multiple, read back with 16-byte loads
-  constexpr int PER16 = 16 / int(sizeof(T));
-  constexpr int VVP = ((VV + PER16 - 1) / PER16) * PER16;
-  __shared__ __align__(16) T sA[kApWarps][27][VVP];
+  using S = ApStage<VEC, T>;
+  constexpr int VV = S::VV, VVP = S::VVP, PER16 = S::PER16;
+  __shared__ __align__(16) unsigned char stage[kApWarps * S::kWarp];
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  T (*sA)[VVP] = reinterpret_cast<T (*)[VVP]>(stage + wid * S::kWarp);
+  double (*sT2)[VV] = reinterpret_cast<double (*)[VV]>(stage + wid * S::kWarp);
+  double (*sT1)[VV] = reinterpret_cast<double (*)[VV]>(stage + wid * S::kWarp + S::kXr);
   const int32_t* il[3] = {ilo, ilo + F.n[0], ilo + F.n[0] + F.n[1]};
   const double* wh[3] = {whi, whi + F.n[0], whi + F.n[0] + F.n[1]};
   const int64_t Nf = F.n[0] * F.n[1] * F.n[2];
   const int64_t w0 = int64_t(blockIdx.x) * kApWarps + wid, nw = int64_t(gridDim.x) * kApWarps;
+  const int l = lane < 27 ? lane : 26;  // lanes 27-31 mirror lane 26's work and store nothing
+  const int td[3] = {l / 9, (l / 3) % 3, l % 3};
   for (int64_t i = w0; i < Nf; i += nw) {
-    __syncwarp();  // the previous row's stage is no longer read
+    __syncwarp();  // the previous row's stages are no longer read
     if (lane < 27) {
       const int32_t blk = fst[i * 27 + lane];
 #pragma unroll
-      for (int e = 0; e < VV; ++e) sA[wid][lane][e] = blk >= 0 ? fv[int64_t(blk) * VV + e] : T(0);
+      for (int e = 0; e < VV; ++e) sA[lane][e] = blk >= 0 ? fv[int64_t(blk) * VV + e] : T(0);
     }
-    __syncwarp();
-    if (lane >= 27) continue;
     const int64_t ii[3] = {i / (F.n[1] * F.n[2]), (i / F.n[2]) % F.n[1], i % F.n[2]};
-    const int td[3] = {lane / 9, (lane / 3) % 3, lane % 3};
-    double w[3][3];  // w[d][k]: weight of column J_d at fine index ii[d] + k - 1
+    double w[3][3];  // w[d][k]: weight of column J_d = base + td[d] at fine index ii[d] + k - 1
 #pragma unroll
     for (int d = 0; d < 3; ++d) {
       const int64_t J = col_base(il[d], ii[d]) + td[d];
@@ -100,22 +119,53 @@ __global__ void __launch_bounds__(kApWarps * 32) ap_kernel(Lat F, const int32_t*
         w[d][k] = (J < C.n[d] && j >= 0 && j < F.n[d]) ? w1(il[d], wh[d], j, J) : 0.0;
       }
     }
+    __syncwarp();
     double acc[VV];
+    // z: T1[l = (a, b, tz)] from A[(a, b, c)], c = 0..2
 #pragma unroll
     for (int e = 0; e < VV; ++e) acc[e] = 0.0;
 #pragma unroll
-    for (int o = 0; o < 27; ++o) {
-      const double ww = w[0][o / 9] * w[1][(o / 3) % 3] * w[2][o % 3];
-      if (ww == 0.0) continue;
+    for (int c = 0; c < 3; ++c) {
+      if (w[2][c] == 0.0) continue;
       T blk[VVP];
-      const uint4* src = reinterpret_cast<const uint4*>(&sA[wid][o][0]);
+      const uint4* src = reinterpret_cast<const uint4*>(&sA[(l / 3) * 3 + c][0]);
 #pragma unroll
       for (int v = 0; v < VVP / PER16; ++v) reinterpret_cast<uint4*>(blk)[v] = src[v];
 #pragma unroll
-      for (int e = 0; e < VV; ++e) acc[e] = fma(ww, double(blk[e]), acc[e]);
+      for (int e = 0; e < VV; ++e) acc[e] = fma(w[2][c], double(blk[e]), acc[e]);
     }
+    if (lane < 27)
 #pragma unroll
-    for (int e = 0; e < VV; ++e) B[(i * 27 + lane) * VV + e] = T(acc[e]);
+      for (int e = 0; e < VV; ++e) sT1[l][e] = acc[e];
+    __syncwarp();
+    // y: T2[l = (a, ty, tz)] from T1[(a, b, tz)], b = 0..2 (T2 over A's stage)
+#pragma unroll
+    for (int e = 0; e < VV; ++e) acc[e] = 0.0;
+#pragma unroll
+    for (int b = 0; b < 3; ++b) {
+      if (w[1][b] == 0.0) continue;
+      const double* src = sT1[(l / 9) * 9 + b * 3 + l % 3];
+#pragma unroll
+      for (int e = 0; e < VV; ++e) acc[e] = fma(w[1][b], src[e], acc[e]);
+    }
+    __syncwarp();  // every lane has read its A blocks before T2 overwrites them
+    if (lane < 27)
+#pragma unroll
+      for (int e = 0; e < VV; ++e) sT2[l][e] = acc[e];
+    __syncwarp();
+    // x: B[l = (tx, ty, tz)] from T2[(a, ty, tz)], a = 0..2
+#pragma unroll
+    for (int e = 0; e < VV; ++e) acc[e] = 0.0;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      if (w[0][a] == 0.0) continue;
+      const double* src = sT2[a * 9 + l % 9];
+#pragma unroll
+      for (int e = 0; e < VV; ++e) acc[e] = fma(w[0][a], src[e], acc[e]);
+    }
+    if (lane < 27)
+#pragma unroll
+      for (int e = 0; e < VV; ++e) B[(i * 27 + lane) * VV + e] = T(acc[e]);
   }
 }
 
