@@ -59,6 +59,15 @@ inline cudaStream_t as_stream(void* s) { return reinterpret_cast<cudaStream_t>(s
 // launch pdl_wait() returns at once.  FEM_PDL=0 in the environment launches
 // normally.
 __device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+// Lets the next kernel in the stream (launched with launch_pdl) be scheduled
+// once every CTA of this one has called it or exited, instead of at its end.
+// Called only after this kernel's own pdl_wait(), so the kernel before it
+// has completed and the successor overlaps this kernel alone.  pdl_wait()
+// in the successor orders this kernel's writes before its reads, but an L1
+// line that this kernel's CTAs loaded on the successor's SM after the
+// successor started is not refreshed: the successor reads what this kernel
+// writes through L2 (ld.global.cg).
+__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
 
 bool pdl_enabled();
 

@@ -19,6 +19,7 @@
 // updates fused into the row epilogue.  Pre- and
 // post-smoothing apply the same polynomial, the coarsest level a longer one,
 // so a V-cycle is a fixed symmetric positive operator (a CG preconditioner).
+#include <algorithm>
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
@@ -242,11 +243,9 @@ __device__ __forceinline__ ChebCoef cheb_coef(const void* lmax_bits, double rati
 // step from a zero start (as cheb_first_kernel: r = b, d0 = D^-1 b / theta,
 // x = d0), node by node, so that step needs no launch of its own.
 template <int VEC, typename T>
-__global__ void restrict_kernel(Lat F, Lat C, const int32_t* cpos, const int32_t* ilo, const double* whi,
-                                const T* __restrict__ rf, T* bc, const T* __restrict__ dinvc, T* rc, T* d0c, T* xc,
-                                const void* lmaxc, double ratio) {
-  pdl_wait();
-  const double inv_theta = dinvc != nullptr ? cheb_coef(lmaxc, ratio, 0).inv_theta : 0.0;
+__device__ __forceinline__ void restrict_body(Lat F, Lat C, const int32_t* cpos, const int32_t* ilo,
+                                              const double* whi, const T* rf, T* bc, const T* __restrict__ dinvc,
+                                              T* rc, T* d0c, T* xc, double inv_theta) {
   const int nc[3] = {int(C.n[0]), int(C.n[1]), int(C.n[2])};
   const int nf[3] = {int(F.n[0]), int(F.n[1]), int(F.n[2])};
   const int32_t* cp[3] = {cpos, cpos + nc[0], cpos + nc[0] + nc[1]};
@@ -301,11 +300,22 @@ __global__ void restrict_kernel(Lat F, Lat C, const int32_t* cpos, const int32_t
   }
 }
 
+template <int VEC, typename T>
+__global__ void restrict_kernel(Lat F, Lat C, const int32_t* cpos, const int32_t* ilo, const double* whi,
+                                const T* __restrict__ rf, T* bc, const T* __restrict__ dinvc, T* rc, T* d0c, T* xc,
+                                const void* lmaxc, double ratio, int early) {
+  pdl_wait();
+  // early: the next kernel is coarse_tail_kernel, which reads what this one
+  // writes through L2 and may start (and copy its constant data) right away
+  if (early) pdl_trigger();
+  restrict_body<VEC, T>(F, C, cpos, ilo, whi, rf, bc, dinvc, rc, d0c, xc,
+                        dinvc != nullptr ? cheb_coef(lmaxc, ratio, 0).inv_theta : 0.0);
+}
+
 // xf[i] += sum_J w_iJ ec[J]   (P, one thread per fine node)
 template <int VEC, typename T>
-__global__ void prolong_add_kernel(Lat F, Lat C, const int32_t* ilo, const double* whi, const T* __restrict__ ec,
-                                   T* xf) {
-  pdl_wait();
+__device__ __forceinline__ void prolong_add_body(Lat F, Lat C, const int32_t* ilo, const double* whi, const T* ec,
+                                                 T* xf) {
   const int nf[3] = {int(F.n[0]), int(F.n[1]), int(F.n[2])};
   const int nc1 = int(C.n[1]), nc2 = int(C.n[2]);
   const int32_t* il[3] = {ilo, ilo + nf[0], ilo + nf[0] + nf[1]};
@@ -335,6 +345,13 @@ __global__ void prolong_add_kernel(Lat F, Lat C, const int32_t* ilo, const doubl
 #pragma unroll
     for (int c = 0; c < VEC; ++c) xf[int64_t(i) * VEC + c] = T(double(xf[int64_t(i) * VEC + c]) + acc[c]);
   }
+}
+
+template <int VEC, typename T>
+__global__ void prolong_add_kernel(Lat F, Lat C, const int32_t* ilo, const double* whi, const T* __restrict__ ec,
+                                   T* xf) {
+  pdl_wait();
+  prolong_add_body<VEC, T>(F, C, ilo, whi, ec, xf);
 }
 
 // ---- Jacobi scaling and the Gershgorin bound of D^-1 A ----------------------
@@ -569,8 +586,7 @@ __global__ void __launch_bounds__(kDenseThreads)
 
 // x = inv b (one warp per row)
 template <typename T>
-__global__ void dense_apply_kernel(int n, const double* __restrict__ inv, const T* __restrict__ b, T* x) {
-  pdl_wait();
+__device__ __forceinline__ void dense_apply_body(int n, const double* __restrict__ inv, const T* b, T* x) {
   const int lane = threadIdx.x & 31;
   for (int row = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; row < n; row += (gridDim.x * blockDim.x) >> 5) {
     double acc = 0.0;
@@ -579,6 +595,286 @@ __global__ void dense_apply_kernel(int n, const double* __restrict__ inv, const 
     for (int o = 16; o >= 1; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
     if (lane == 0) x[row] = T(acc);
   }
+}
+
+template <typename T>
+__global__ void dense_apply_kernel(int n, const double* __restrict__ inv, const T* __restrict__ b, T* x) {
+  pdl_wait();
+  dense_apply_body<T>(n, inv, b, x);
+}
+
+// ---- the coarse end of a V-cycle in one CTA ------------------------------------
+// The last levels of a hierarchy are small (the 50^3 lattice ends with 5^3
+// and 3^3 nodes) and each of their steps as a launch costs its completion
+// and the next launch's dependent loads, 3-5 us, for a few thousand FMAs.
+// When their patterns, values, Jacobi scaling and vectors fit in one CTA's
+// shared memory, the V-cycle from such a level s down runs as one kernel:
+// the level data are copied in once (before the kernel waits on its
+// predecessor: the restriction into level s writes vectors only), level s's
+// x, b, r and d0 after the wait, and the steps follow each other with
+// __syncthreads.  The steps are those of vcycle_level and smooth (the same
+// Chebyshev coefficients, transfers and dense coarsest solve); the row
+// products take one thread per unknown.  Level s's x goes back to global
+// memory at the end.
+constexpr int kTailThreads = 1024;
+constexpr int kTailMaxLevels = 4;
+constexpr int kTailMaxSteps = 33;  // Chebyshev coefficient tables: steps 0 .. max(nu, coarse_steps)
+constexpr size_t kTailSmemMax = 226 * 1024;  // the opt-in limit of one CTA (227 KB) less static shared memory
+
+template <typename T>
+struct TailLevel {
+  Lat lat;
+  int n_brows, nnzb, nu;
+  const int32_t* rp;
+  const int32_t* ci;
+  const T* vals;
+  const T* dinv;
+  const void* lmax;
+  const int32_t* cpos;  // transfer from the finer level (levels after the first)
+  const int32_t* ilo;
+  const double* whi;
+  const double* cinv;  // dense inverse of a coarsest level, or NULL
+  // byte offsets of this level's arrays in shared memory (o_inv: its dense
+  // inverse, or -1 to read it from global memory; o_cheb: its Chebyshev
+  // coefficients, kTailMaxSteps entries; o_cpos, o_ilo, o_whi: the transfer
+  // from the finer level, levels after the first)
+  int o_vals, o_ci, o_rp, o_dinv, o_x, o_b, o_r, o_d0, o_d1, o_inv, o_cheb, o_cpos, o_ilo, o_whi;
+  int n_cpos, n_fine;  // transfer lengths: sum of this level's / the finer level's nodes per direction
+};
+template <typename T>
+struct TailArgs {
+  TailLevel<T> lv[kTailMaxLevels];
+  int nl;  // levels s .. s + nl - 1
+  int nu, coarse_steps;
+  int nsteps;  // Chebyshev coefficients per level: steps 0 .. nsteps-1 (<= kTailMaxSteps)
+  int pre_done;  // the restriction into level s took its first step
+  double ratio;
+  T* x;  // level s in global memory: x (in and out), b, r, d0 (in)
+  const T* b;
+  const T* r;
+  const T* d0;
+};
+
+template <typename T>
+struct TailView {
+  const T* vals;
+  const int32_t* ci;
+  const int32_t* rp;
+  const T* dinv;
+  T *x, *b, *r, *d0, *d1;
+};
+template <typename T>
+__device__ __forceinline__ TailView<T> tail_view(const TailLevel<T>& L, unsigned char* sm) {
+  return TailView<T>{reinterpret_cast<const T*>(sm + L.o_vals), reinterpret_cast<const int32_t*>(sm + L.o_ci),
+                     reinterpret_cast<const int32_t*>(sm + L.o_rp), reinterpret_cast<const T*>(sm + L.o_dinv),
+                     reinterpret_cast<T*>(sm + L.o_x),   reinterpret_cast<T*>(sm + L.o_b),
+                     reinterpret_cast<T*>(sm + L.o_r),   reinterpret_cast<T*>(sm + L.o_d0),
+                     reinterpret_cast<T*>(sm + L.o_d1)};
+}
+
+// q = (A v)_i for every unknown i of a level held in shared memory; epi(i, q).
+// Eight lanes per block row: lane g takes the row's blocks g, g+8, ... for
+// every component, and three xor-shuffles sum the eight partial rows (the
+// loop runs the same number of times in every lane of the block, so the
+// shuffles see full warps).  Pattern indices are clamped to the level's
+// shared-memory arrays: a malformed pattern gives wrong values, never an
+// access outside them.
+constexpr int kTailRowLanes = 8;
+template <int VEC, typename T, class EPI>
+__device__ __forceinline__ void tail_rows(int n_brows, int nnzb, const TailView<T>& V, const T* v, EPI epi) {
+  constexpr int VV = VEC * VEC;
+  const int g = threadIdx.x & (kTailRowLanes - 1);
+  const int rows_per_pass = blockDim.x / kTailRowLanes;
+  for (int base = 0; base < n_brows; base += rows_per_pass) {
+    const int row = base + threadIdx.x / kTailRowLanes;
+    T acc[VEC];
+#pragma unroll
+    for (int c = 0; c < VEC; ++c) acc[c] = T(0);
+    if (row < n_brows) {
+      const int k0 = max(V.rp[row], 0), k1 = min(V.rp[row + 1], nnzb);
+      for (int k = k0 + g; k < k1; k += kTailRowLanes) {
+        const T* blk = V.vals + k * VV;
+        const T* xv = v + min(max(V.ci[k], 0), n_brows - 1) * VEC;
+        T xc[VEC];
+#pragma unroll
+        for (int c = 0; c < VEC; ++c) xc[c] = xv[c];
+#pragma unroll
+        for (int r = 0; r < VEC; ++r)
+#pragma unroll
+          for (int c = 0; c < VEC; ++c) acc[r] = fma(blk[r * VEC + c], xc[c], acc[r]);
+      }
+    }
+#pragma unroll
+    for (int c = 0; c < VEC; ++c)
+#pragma unroll
+      for (int o = kTailRowLanes / 2; o >= 1; o >>= 1) acc[c] += __shfl_xor_sync(0xffffffffu, acc[c], o);
+    if (row < n_brows && g < VEC) {
+      T q = acc[0];
+#pragma unroll
+      for (int c = 1; c < VEC; ++c)
+        if (g == c) q = acc[c];
+      epi(row * VEC + g, q);
+    }
+  }
+}
+
+// smooth() on a level in shared memory, __syncthreads after every step
+template <int VEC, typename T>
+__device__ void tail_smooth(const TailLevel<T>& L, const TailView<T>& V, const ChebCoef* cheb, int m,
+                            bool zero_start, bool want_residual, bool first_done, bool fold) {
+  const int n = L.n_brows * VEC;
+  T* d[2] = {V.d0, V.d1};
+  if (!first_done) {
+    const double inv_theta = cheb[0].inv_theta;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+      const T ri = zero_start ? V.b[i] : V.r[i];
+      if (zero_start) V.r[i] = ri;
+      const T di = T(double(V.dinv[i]) * double(ri) * inv_theta);
+      d[0][i] = di;
+      V.x[i] = zero_start ? di : T(V.x[i] + di);
+    }
+    __syncthreads();
+  }
+  int cur = 0;
+  for (int k = 1; k < m; ++k) {
+    const ChebCoef cf = cheb[k];
+    const T* dold = d[cur];
+    T* dnew = d[cur ^ 1];
+    const bool fk = fold && k == 1;
+    tail_rows<VEC, T>(L.n_brows, L.nnzb, V, dold, [&](int i, T q) {
+      const double rn = double(V.r[i]) - double(q);
+      V.r[i] = T(rn);
+      const T dn = T(cf.a * double(dold[i]) + cf.c * double(V.dinv[i]) * rn);
+      dnew[i] = dn;
+      V.x[i] = fk ? T(T(V.x[i] + dold[i]) + dn) : T(V.x[i] + dn);
+    });
+    __syncthreads();
+    cur ^= 1;
+  }
+  if (want_residual) {
+    const T* dc = d[cur];
+    tail_rows<VEC, T>(L.n_brows, L.nnzb, V, dc, [&](int i, T q) { V.r[i] = T(double(V.r[i]) - double(q)); });
+    __syncthreads();
+  }
+}
+
+// bytes from global to shared memory (dst 16-byte aligned): 16-byte cp.async
+// transfers, all in flight together, when src is 16-byte aligned too, else
+// 4-byte copies (every array here holds 4- or 8-byte values)
+__device__ __forceinline__ void tail_copy(unsigned char* dst, const void* src, int bytes) {
+  const unsigned char* s = static_cast<const unsigned char*>(src);
+  if ((reinterpret_cast<uintptr_t>(s) & 15u) == 0) {
+    const int n16 = bytes >> 4;
+    for (int c = threadIdx.x; c < n16; c += blockDim.x) cp_async16(dst + c * 16, s + c * 16);
+    for (int w = n16 * 4 + threadIdx.x; w < bytes / 4; w += blockDim.x)
+      reinterpret_cast<uint32_t*>(dst)[w] = reinterpret_cast<const uint32_t*>(s)[w];
+  } else {
+    for (int w = threadIdx.x; w < bytes / 4; w += blockDim.x)
+      reinterpret_cast<uint32_t*>(dst)[w] = reinterpret_cast<const uint32_t*>(s)[w];
+  }
+}
+
+template <int VEC, typename T>
+__global__ void __launch_bounds__(kTailThreads, 1) coarse_tail_kernel(const __grid_constant__ TailArgs<T> a) {
+  constexpr int VV = VEC * VEC;
+  extern __shared__ __align__(16) unsigned char tsm[];
+  __shared__ int s_nz[kTailMaxLevels];
+  // Constant level data first (no V-cycle kernel writes it).  The stored
+  // block counts (row_ptr[n]) are read while the fixed-size copies fly.
+  if (threadIdx.x < a.nl) {
+    const TailLevel<T>& L = a.lv[threadIdx.x];
+    s_nz[threadIdx.x] = min(max(L.rp[L.n_brows], 0), L.nnzb);  // within the bound
+  }
+  for (int l = 0; l < a.nl; ++l) {
+    const TailLevel<T>& L = a.lv[l];
+    tail_copy(tsm + L.o_rp, L.rp, (L.n_brows + 1) * 4);
+    tail_copy(tsm + L.o_dinv, L.dinv, L.n_brows * VEC * int(sizeof(T)));
+    if (L.o_inv >= 0) {
+      const int n = L.n_brows * VEC;
+      tail_copy(tsm + L.o_inv, L.cinv, n * n * 8);
+    }
+    if (l > 0) {
+      tail_copy(tsm + L.o_cpos, L.cpos, L.n_cpos * 4);
+      tail_copy(tsm + L.o_ilo, L.ilo, L.n_fine * 4);
+      tail_copy(tsm + L.o_whi, L.whi, L.n_fine * 8);
+    }
+    if ((threadIdx.x >> 5) == l) {  // warp l: level l's Chebyshev coefficients, one step per lane
+      ChebCoef* cheb = reinterpret_cast<ChebCoef*>(tsm + L.o_cheb);
+      for (int k = threadIdx.x & 31; k < a.nsteps; k += 32) cheb[k] = cheb_coef(L.lmax, a.ratio, k);
+    }
+  }
+  __syncthreads();
+  for (int l = 0; l < a.nl; ++l) {
+    const TailLevel<T>& L = a.lv[l];
+    tail_copy(tsm + L.o_vals, L.vals, s_nz[l] * VV * int(sizeof(T)));
+    tail_copy(tsm + L.o_ci, L.ci, s_nz[l] * 4);
+  }
+  cp_async_wait_all();
+  // Level s's vectors after the wait.  The restriction into level s lets this
+  // kernel start early (it calls pdl_trigger after its own wait), so they are
+  // read through L2: an L1 line its CTAs loaded on this SM is not refreshed
+  // by the wait.
+  pdl_wait();
+  {
+    const TailView<T> V = tail_view(a.lv[0], tsm);
+    for (int i = threadIdx.x; i < a.lv[0].n_brows * VEC; i += blockDim.x) {
+      V.x[i] = __ldcg(a.x + i);
+      V.b[i] = __ldcg(a.b + i);
+      V.r[i] = __ldcg(a.r + i);
+      V.d0[i] = __ldcg(a.d0 + i);
+    }
+  }
+  __syncthreads();
+  const int last = a.nl - 1;
+  for (int l = 0; l < last; ++l) {
+    const TailLevel<T>& L = a.lv[l];
+    const TailLevel<T>& C = a.lv[l + 1];
+    const TailView<T> V = tail_view(L, tsm), W = tail_view(C, tsm);
+    const int nul = L.nu > 0 ? L.nu : a.nu;
+    tail_smooth<VEC, T>(L, V, reinterpret_cast<const ChebCoef*>(tsm + L.o_cheb), nul, true, true,
+                        l > 0 || a.pre_done, false);
+    const bool fuse_next = !(l + 1 == last && C.cinv != nullptr);
+    restrict_body<VEC, T>(L.lat, C.lat, reinterpret_cast<const int32_t*>(tsm + C.o_cpos),
+                          reinterpret_cast<const int32_t*>(tsm + C.o_ilo), reinterpret_cast<const double*>(tsm + C.o_whi),
+                          V.r, W.b, fuse_next ? W.dinv : nullptr, W.r, W.d0, W.x,
+                          reinterpret_cast<const ChebCoef*>(tsm + C.o_cheb)[0].inv_theta);
+    __syncthreads();
+  }
+  {
+    const TailLevel<T>& L = a.lv[last];
+    const TailView<T> V = tail_view(L, tsm);
+    if (L.cinv != nullptr) {
+      dense_apply_body<T>(L.n_brows * VEC, L.o_inv >= 0 ? reinterpret_cast<const double*>(tsm + L.o_inv) : L.cinv,
+                          V.b, V.x);
+      __syncthreads();
+    } else {
+      tail_smooth<VEC, T>(L, V, reinterpret_cast<const ChebCoef*>(tsm + L.o_cheb), a.coarse_steps, true, false,
+                          last > 0 || a.pre_done, false);
+    }
+  }
+  for (int l = last - 1; l >= 0; --l) {
+    const TailLevel<T>& L = a.lv[l];
+    const TailLevel<T>& C = a.lv[l + 1];
+    const TailView<T> V = tail_view(L, tsm), W = tail_view(C, tsm);
+    const int nul = L.nu > 0 ? L.nu : a.nu;
+    prolong_add_body<VEC, T>(L.lat, C.lat, reinterpret_cast<const int32_t*>(tsm + C.o_ilo),
+                             reinterpret_cast<const double*>(tsm + C.o_whi), W.x, V.x);
+    __syncthreads();
+    // post-smoothing with two or more steps: the residual forms the first
+    // step's d0 and the second step adds its x += d0 (as vcycle_level)
+    const bool fuse_post = nul >= 2;
+    const ChebCoef* cheb = reinterpret_cast<const ChebCoef*>(tsm + L.o_cheb);
+    const double inv_theta = cheb[0].inv_theta;
+    tail_rows<VEC, T>(L.n_brows, L.nnzb, V, V.x, [&](int i, T q) {
+      const T ri = T(double(V.b[i]) - double(q));
+      V.r[i] = ri;
+      if (fuse_post) V.d0[i] = T(double(V.dinv[i]) * double(ri) * inv_theta);
+    });
+    __syncthreads();
+    tail_smooth<VEC, T>(L, V, cheb, nul, false, false, fuse_post, fuse_post);
+  }
+  const TailView<T> V0 = tail_view(a.lv[0], tsm);
+  for (int i = threadIdx.x; i < a.lv[0].n_brows * VEC; i += blockDim.x) a.x[i] = V0.x[i];
 }
 
 // ---- host side -------------------------------------------------------------------
@@ -614,9 +910,138 @@ int check_levels(int nlevels, const FemMGLevel* L) {
   return FEM_OK;
 }
 
+// The coarse tail (coarse_tail_kernel): FEM_MG_TAIL=0 in the environment
+// turns it off.  A level's blocks are bounded by its lattice stencil,
+// prod_d (3 n_d - 2) (every coarse level is a lattice operator).
+bool mg_tail_enabled() {
+  static int on = -1;
+  if (on < 0) {
+    const char* e = std::getenv("FEM_MG_TAIL");
+    on = (e != nullptr && e[0] == '0') ? 0 : 1;
+  }
+  return on == 1;
+}
+inline size_t al16(size_t x) { return (x + 15) & ~size_t(15); }
+
+// Fills a's levels s .. nlevels-1 with their shared-memory layout; returns
+// the bytes it needs (0 when the levels cannot form a tail).
+template <int VEC, typename T>
+size_t tail_layout(int s, int nlevels, const FemMGLevel* L, TailArgs<T>* a) {
+  const int nl = nlevels - s;
+  if (s < 1 || nl < 2 || nl > kTailMaxLevels) return 0;
+  size_t off = 0;
+  for (int k = 0; k < nl; ++k) {
+    const FemMGLevel& v = L[s + k];
+    if (v.vals_lo != nullptr || v.n_brows * VEC > (int64_t(1) << 20)) return 0;
+    const int64_t nb = (3 * v.nodes[0] - 2) * (3 * v.nodes[1] - 2) * (3 * v.nodes[2] - 2);
+    const size_t n = size_t(v.n_brows) * VEC;
+    TailLevel<T>& t = a->lv[k];
+    t.lat = lat_of(v);
+    t.n_brows = int(v.n_brows);
+    t.nnzb = int(nb);
+    t.nu = v.nu;
+    t.rp = v.row_ptr;
+    t.ci = v.col_idx;
+    t.vals = static_cast<const T*>(v.vals);
+    t.dinv = static_cast<const T*>(v.dinv);
+    t.lmax = v.lmax;
+    t.cpos = v.cpos;
+    t.ilo = v.ilo;
+    t.whi = v.whi;
+    t.cinv = v.cinv;
+    t.o_vals = int(off), off = al16(off + size_t(nb) * VEC * VEC * sizeof(T));
+    t.o_ci = int(off), off = al16(off + size_t(nb) * 4);
+    t.o_rp = int(off), off = al16(off + size_t(v.n_brows + 1) * 4);
+    t.o_dinv = int(off), off = al16(off + n * sizeof(T));
+    t.o_x = int(off), off = al16(off + n * sizeof(T));
+    t.o_b = int(off), off = al16(off + n * sizeof(T));
+    t.o_r = int(off), off = al16(off + n * sizeof(T));
+    t.o_d0 = int(off), off = al16(off + n * sizeof(T));
+    t.o_d1 = int(off), off = al16(off + n * sizeof(T));
+    t.o_cheb = int(off), off = al16(off + kTailMaxSteps * sizeof(ChebCoef));
+    t.o_inv = -1;
+    t.o_cpos = t.o_ilo = t.o_whi = -1;
+    t.n_cpos = t.n_fine = 0;
+    if (k > 0) {
+      const FemMGLevel& f = L[s + k - 1];
+      t.n_cpos = int(v.nodes[0] + v.nodes[1] + v.nodes[2]);
+      t.n_fine = int(f.nodes[0] + f.nodes[1] + f.nodes[2]);
+      t.o_cpos = int(off), off = al16(off + size_t(t.n_cpos) * 4);
+      t.o_ilo = int(off), off = al16(off + size_t(t.n_fine) * 4);
+      t.o_whi = int(off), off = al16(off + size_t(t.n_fine) * 8);
+    }
+    if (off > kTailSmemMax) return 0;
+  }
+  // the dense inverse of the coarsest level too, where it still fits
+  TailLevel<T>& c = a->lv[nl - 1];
+  if (c.cinv != nullptr) {
+    const size_t n = size_t(c.n_brows) * VEC;
+    if (al16(off + n * n * 8) <= kTailSmemMax) {
+      c.o_inv = int(off);
+      off = al16(off + n * n * 8);
+    }
+  }
+  a->nl = nl;
+  return off;
+}
+
+// Chebyshev steps the tail from level s takes on one level, at most (its
+// coefficient tables hold steps 0 .. that)
+inline int tail_steps(int s, int nlevels, const FemMGLevel* L, int nu, int coarse_steps) {
+  int m = 1;
+  for (int l = s; l < nlevels - 1; ++l) m = std::max(m, L[l].nu > 0 ? L[l].nu : nu);
+  if (L[nlevels - 1].cinv == nullptr) m = std::max(m, coarse_steps);
+  return m;
+}
+
+// First level (>= 1) from which the V-cycle runs as one coarse_tail_kernel,
+// or -1.
+template <int VEC, typename T>
+int tail_start(int nlevels, const FemMGLevel* L, int nu, int coarse_steps) {
+  if (!mg_tail_enabled()) return -1;
+  TailArgs<T> a{};
+  for (int s = 1; s <= nlevels - 2; ++s)
+    if (tail_steps(s, nlevels, L, nu, coarse_steps) < kTailMaxSteps && tail_layout<VEC, T>(s, nlevels, L, &a) > 0)
+      return s;
+  return -1;
+}
+
+template <int VEC, typename T>
+int launch_tail(int s, int nlevels, const FemMGLevel* L, int nu, int coarse_steps, double ratio, bool pre_done,
+                cudaStream_t st) {
+  TailArgs<T> a{};
+  const size_t bytes = tail_layout<VEC, T>(s, nlevels, L, &a);
+  FEM_CHECK_ARG(bytes > 0, "coarse tail: levels %d.. do not fit", s);
+  a.nu = nu;
+  a.coarse_steps = coarse_steps;
+  a.nsteps = tail_steps(s, nlevels, L, nu, coarse_steps) + 1;
+  FEM_CHECK_ARG(a.nsteps <= kTailMaxSteps, "coarse tail: %d Chebyshev steps exceed its tables", a.nsteps - 1);
+  a.pre_done = pre_done ? 1 : 0;
+  a.ratio = ratio;
+  a.x = static_cast<T*>(L[s].x);
+  a.b = static_cast<const T*>(L[s].b);
+  a.r = static_cast<const T*>(L[s].r);
+  a.d0 = static_cast<const T*>(L[s].d0);
+  FEM_CUDA_TRY(launch_pdl(coarse_tail_kernel<VEC, T>, 1, kTailThreads, bytes, st, a));
+  FEM_LAUNCH_CHECK();
+  return FEM_OK;
+}
+
 template <int VEC, typename T>
 int ensure_attrs() {
   int rc;
+  {
+    static std::mutex mu;  // per instantiation, once per device
+    static std::set<int> done;
+    int dev = 0;
+    FEM_CUDA_TRY(cudaGetDevice(&dev));
+    std::lock_guard<std::mutex> lock(mu);
+    if (!done.count(dev)) {
+      FEM_CUDA_TRY(cudaFuncSetAttribute(coarse_tail_kernel<VEC, T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        int(kTailSmemMax)));
+      done.insert(dev);
+    }
+  }
   if ((rc = ensure_smem_attr(cheb_step_kernel<VEC, T, T>)) != FEM_OK) return rc;
   if ((rc = ensure_smem_attr(cheb_resid_kernel<VEC, T, T>)) != FEM_OK) return rc;
   if ((rc = ensure_smem_attr(mg_residual_kernel<VEC, T, T>)) != FEM_OK) return rc;
@@ -765,6 +1190,9 @@ template <int VEC, typename T>
 int vcycle_level(int l, int nlevels, const FemMGLevel* L, int nu, int coarse_steps, double ratio, const T* b, T* x,
                  cudaStream_t st, bool pre_done = false) {
   int rc;
+  if (l >= 1 && static_cast<const void*>(b) == L[l].b && static_cast<const void*>(x) == L[l].x &&
+      tail_start<VEC, T>(nlevels, L, nu, coarse_steps) == l)
+    return launch_tail<VEC, T>(l, nlevels, L, nu, coarse_steps, ratio, pre_done, st);
   if (l == nlevels - 1) {
     if (L[l].cinv != nullptr) {
       const int n = int(L[l].n_brows) * VEC;
@@ -786,7 +1214,8 @@ int vcycle_level(int l, int nlevels, const FemMGLevel* L, int nu, int coarse_ste
   FEM_CUDA_TRY(launch_pdl(restrict_kernel<VEC, T>, vgrid(C.n_brows), 256, 0, st, lat_of(L[l]), lat_of(C), C.cpos,
                           C.ilo, C.whi, static_cast<const T*>(L[l].r), bc,
                           fuse_next ? static_cast<const T*>(C.dinv) : static_cast<const T*>(nullptr),
-                          static_cast<T*>(C.r), static_cast<T*>(C.d0), xc, static_cast<const void*>(C.lmax), ratio));
+                          static_cast<T*>(C.r), static_cast<T*>(C.d0), xc, static_cast<const void*>(C.lmax), ratio,
+                          tail_start<VEC, T>(nlevels, L, nu, coarse_steps) == l + 1 ? 1 : 0));
   FEM_LAUNCH_CHECK();
   if ((rc = vcycle_level<VEC, T>(l + 1, nlevels, L, nu, coarse_steps, ratio, bc, xc, st, fuse_next)) != FEM_OK)
     return rc;

@@ -4,6 +4,8 @@
   from the same transfer arrays (1e-12 relative in FP64, 1e-5 in FP32), on a
   graded lattice with an odd cell count;
 - the V-cycle is a symmetric positive operator (r2.V r1 = r1.V r2 to 1e-10);
+- its last levels run as one CTA over shared memory give the per-level
+  launches' z (1e-12 in FP64, 1e-5 in FP32);
 - V-cycle-preconditioned CG solves an eliminated elasticity system to the
   direct solution (1e-8) in far fewer iterations than block-Jacobi CG, with
   the hierarchy in FP64 and in FP32;
@@ -278,6 +280,68 @@ def test_mg_pcg_device_loop_matches_direct_launches(pkg, cuda, fp32, tmp_path):
     its_direct = int(p.stdout.split()[-1])
     assert its == its_direct
     np.testing.assert_array_equal(x.cpu().numpy(), np.load(out))
+
+
+_LEVELS_SCRIPT = r"""
+import sys, numpy as np, torch
+sys.path[:0] = [sys.argv[1], sys.argv[1] + "/tests"]
+from __graft_entry__ import load_package
+import test_gpu_multigrid as t
+pkg = load_package()
+mg, S = t._mods()
+fp32, dense = sys.argv[3] == "1", sys.argv[4] == "1"
+prob, A = t._graded_elastic(pkg, torch.device("cuda", 0), shape=(16, 15, 14))
+A.vals.copy_(torch.from_numpy(np.load(sys.argv[5])))
+M = mg.Multigrid(prob.dev(), prob.mesh.points, prob.mesh.cells, fp32=fp32, dense_coarse=dense)
+M.setup(A)
+r = torch.from_numpy(np.load(sys.argv[6])).cuda()
+z = torch.empty_like(r)
+c0 = pkg._native.launch_count()
+M.vcycle(r, z)
+torch.cuda.synchronize()
+np.save(sys.argv[2], z.cpu().numpy())
+print(pkg._native.launch_count() - c0)
+"""
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("fp32", [False, True])
+@pytest.mark.parametrize("dense", [True, False])
+def test_vcycle_coarse_tail_matches_level_launches(pkg, cuda, fp32, dense, tmp_path):
+    """The last levels of the V-cycle run as one CTA over shared memory
+    (here 5^3 and 3^3 nodes): the same steps as the launches per level and
+    step (FEM_MG_TAIL=0), from fewer launches; z agrees to the rounding of
+    a different summation order, with a dense coarsest inverse and with a
+    smoothed coarsest level."""
+    import os
+    import subprocess
+    import sys
+    mg, _ = _mods()
+    prob, A = _graded_elastic(pkg, cuda, shape=(16, 15, 14))
+    M = mg.Multigrid(prob.dev(), prob.mesh.points, prob.mesh.cells, fp32=fp32, dense_coarse=dense)
+    M.setup(A)
+    assert [n[0] * n[1] * n[2] for n in M.level_nodes[-2:]] == [125, 27] and (M._cinv is not None) == dense
+    dt = torch.float32 if fp32 else torch.float64
+    r = torch.tensor(np.random.default_rng(11).normal(size=A.n_brows * 3), dtype=dt, device=cuda)
+    z = torch.empty_like(r)
+    c0 = pkg._native.launch_count()
+    M.vcycle(r, z)
+    torch.cuda.synchronize()
+    launches = pkg._native.launch_count() - c0
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    out, vals, rhs = tmp_path / "z.npy", tmp_path / "vals.npy", tmp_path / "r.npy"
+    np.save(vals, A.vals.cpu().numpy())
+    np.save(rhs, r.cpu().numpy())
+    env = dict(os.environ, FEM_MG_TAIL="0")
+    p = subprocess.run([sys.executable, "-c", _LEVELS_SCRIPT, root, str(out), "1" if fp32 else "0",
+                        "1" if dense else "0", str(vals), str(rhs)], env=env, capture_output=True, text=True,
+                       timeout=600)
+    assert p.returncode == 0, p.stderr[-2000:]
+    assert launches < int(p.stdout.split()[-1])
+    zl = torch.from_numpy(np.load(out)).double()
+    zt = z.double().cpu()
+    assert torch.isfinite(zt).all()
+    assert float((zt - zl).norm() / zl.norm()) <= (1e-5 if fp32 else 1e-12)
 
 
 @pytest.mark.gpu
