@@ -655,6 +655,8 @@ struct TailArgs {
   const T* d0;
 };
 
+// A level's arrays in shared memory (cpos, ilo, whi: levels after the
+// first; inv: the global copy when the inverse is not staged)
 template <typename T>
 struct TailView {
   const T* vals;
@@ -662,14 +664,30 @@ struct TailView {
   const int32_t* rp;
   const T* dinv;
   T *x, *b, *r, *d0, *d1;
+  const ChebCoef* cheb;
+  const int32_t* cpos;
+  const int32_t* ilo;
+  const double* whi;
+  const double* inv;
 };
 template <typename T>
 __device__ __forceinline__ TailView<T> tail_view(const TailLevel<T>& L, unsigned char* sm) {
-  return TailView<T>{reinterpret_cast<const T*>(sm + L.o_vals), reinterpret_cast<const int32_t*>(sm + L.o_ci),
-                     reinterpret_cast<const int32_t*>(sm + L.o_rp), reinterpret_cast<const T*>(sm + L.o_dinv),
-                     reinterpret_cast<T*>(sm + L.o_x),   reinterpret_cast<T*>(sm + L.o_b),
-                     reinterpret_cast<T*>(sm + L.o_r),   reinterpret_cast<T*>(sm + L.o_d0),
-                     reinterpret_cast<T*>(sm + L.o_d1)};
+  TailView<T> v;
+  v.vals = reinterpret_cast<const T*>(sm + L.o_vals);
+  v.ci = reinterpret_cast<const int32_t*>(sm + L.o_ci);
+  v.rp = reinterpret_cast<const int32_t*>(sm + L.o_rp);
+  v.dinv = reinterpret_cast<const T*>(sm + L.o_dinv);
+  v.x = reinterpret_cast<T*>(sm + L.o_x);
+  v.b = reinterpret_cast<T*>(sm + L.o_b);
+  v.r = reinterpret_cast<T*>(sm + L.o_r);
+  v.d0 = reinterpret_cast<T*>(sm + L.o_d0);
+  v.d1 = reinterpret_cast<T*>(sm + L.o_d1);
+  v.cheb = reinterpret_cast<const ChebCoef*>(sm + L.o_cheb);
+  v.cpos = L.o_cpos >= 0 ? reinterpret_cast<const int32_t*>(sm + L.o_cpos) : nullptr;
+  v.ilo = L.o_ilo >= 0 ? reinterpret_cast<const int32_t*>(sm + L.o_ilo) : nullptr;
+  v.whi = L.o_whi >= 0 ? reinterpret_cast<const double*>(sm + L.o_whi) : nullptr;
+  v.inv = L.o_inv >= 0 ? reinterpret_cast<const double*>(sm + L.o_inv) : L.cinv;
+  return v;
 }
 
 // q = (A v)_i for every unknown i of a level held in shared memory; epi(i, q).
@@ -720,8 +738,9 @@ __device__ __forceinline__ void tail_rows(int n_brows, int nnzb, const TailView<
 
 // smooth() on a level in shared memory, __syncthreads after every step
 template <int VEC, typename T>
-__device__ void tail_smooth(const TailLevel<T>& L, const TailView<T>& V, const ChebCoef* cheb, int m,
-                            bool zero_start, bool want_residual, bool first_done, bool fold) {
+__device__ void tail_smooth(const TailLevel<T>& L, const TailView<T>& V, int m, bool zero_start, bool want_residual,
+                            bool first_done, bool fold) {
+  const ChebCoef* cheb = V.cheb;
   const int n = L.n_brows * VEC;
   T* d[2] = {V.d0, V.d1};
   if (!first_done) {
@@ -831,25 +850,20 @@ __global__ void __launch_bounds__(kTailThreads, 1) coarse_tail_kernel(const __gr
     const TailLevel<T>& C = a.lv[l + 1];
     const TailView<T> V = tail_view(L, tsm), W = tail_view(C, tsm);
     const int nul = L.nu > 0 ? L.nu : a.nu;
-    tail_smooth<VEC, T>(L, V, reinterpret_cast<const ChebCoef*>(tsm + L.o_cheb), nul, true, true,
-                        l > 0 || a.pre_done, false);
+    tail_smooth<VEC, T>(L, V, nul, true, true, l > 0 || a.pre_done, false);
     const bool fuse_next = !(l + 1 == last && C.cinv != nullptr);
-    restrict_body<VEC, T>(L.lat, C.lat, reinterpret_cast<const int32_t*>(tsm + C.o_cpos),
-                          reinterpret_cast<const int32_t*>(tsm + C.o_ilo), reinterpret_cast<const double*>(tsm + C.o_whi),
-                          V.r, W.b, fuse_next ? W.dinv : nullptr, W.r, W.d0, W.x,
-                          reinterpret_cast<const ChebCoef*>(tsm + C.o_cheb)[0].inv_theta);
+    restrict_body<VEC, T>(L.lat, C.lat, W.cpos, W.ilo, W.whi, V.r, W.b, fuse_next ? W.dinv : nullptr, W.r, W.d0, W.x,
+                          W.cheb[0].inv_theta);
     __syncthreads();
   }
   {
     const TailLevel<T>& L = a.lv[last];
     const TailView<T> V = tail_view(L, tsm);
     if (L.cinv != nullptr) {
-      dense_apply_body<T>(L.n_brows * VEC, L.o_inv >= 0 ? reinterpret_cast<const double*>(tsm + L.o_inv) : L.cinv,
-                          V.b, V.x);
+      dense_apply_body<T>(L.n_brows * VEC, V.inv, V.b, V.x);
       __syncthreads();
     } else {
-      tail_smooth<VEC, T>(L, V, reinterpret_cast<const ChebCoef*>(tsm + L.o_cheb), a.coarse_steps, true, false,
-                          last > 0 || a.pre_done, false);
+      tail_smooth<VEC, T>(L, V, a.coarse_steps, true, false, last > 0 || a.pre_done, false);
     }
   }
   for (int l = last - 1; l >= 0; --l) {
@@ -857,21 +871,19 @@ __global__ void __launch_bounds__(kTailThreads, 1) coarse_tail_kernel(const __gr
     const TailLevel<T>& C = a.lv[l + 1];
     const TailView<T> V = tail_view(L, tsm), W = tail_view(C, tsm);
     const int nul = L.nu > 0 ? L.nu : a.nu;
-    prolong_add_body<VEC, T>(L.lat, C.lat, reinterpret_cast<const int32_t*>(tsm + C.o_ilo),
-                             reinterpret_cast<const double*>(tsm + C.o_whi), W.x, V.x);
+    prolong_add_body<VEC, T>(L.lat, C.lat, W.ilo, W.whi, W.x, V.x);
     __syncthreads();
     // post-smoothing with two or more steps: the residual forms the first
     // step's d0 and the second step adds its x += d0 (as vcycle_level)
     const bool fuse_post = nul >= 2;
-    const ChebCoef* cheb = reinterpret_cast<const ChebCoef*>(tsm + L.o_cheb);
-    const double inv_theta = cheb[0].inv_theta;
+    const double inv_theta = V.cheb[0].inv_theta;
     tail_rows<VEC, T>(L.n_brows, L.nnzb, V, V.x, [&](int i, T q) {
       const T ri = T(double(V.b[i]) - double(q));
       V.r[i] = ri;
       if (fuse_post) V.d0[i] = T(double(V.dinv[i]) * double(ri) * inv_theta);
     });
     __syncthreads();
-    tail_smooth<VEC, T>(L, V, cheb, nul, false, false, fuse_post, fuse_post);
+    tail_smooth<VEC, T>(L, V, nul, false, false, fuse_post, fuse_post);
   }
   const TailView<T> V0 = tail_view(a.lv[0], tsm);
   for (int i = threadIdx.x; i < a.lv[0].n_brows * VEC; i += blockDim.x) a.x[i] = V0.x[i];
