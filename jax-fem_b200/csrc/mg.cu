@@ -1266,6 +1266,7 @@ int vcycle_impl(int nlevels, const FemMGLevel* L, int nu, int coarse_steps, doub
 // ---- V-cycle preconditioned CG (FP64) -------------------------------------------
 struct PState {
   double gamma, alpha, beta, rr, tol2, bb, pq;
+  double true_rr;  // ||b - A x||^2 at exit
   int iter, status, maxiter, first;
   int loops;  // bodies run by the device-side loop (its own bound)
 };
@@ -1293,6 +1294,15 @@ __global__ void pcg_init_kernel(int64_t n, const double* r, const double* b, dou
     else if (S->maxiter <= 0) S->status = FEM_ERR_NOT_CONVERGED;
     else S->status = PS_RUNNING;
   }
+}
+
+// ||q||^2 into S->true_rr (the exit check: q = b - A x)
+__global__ void pcg_true_rr_kernel(int64_t n, const double* q, double* partials, unsigned* counter, PState* S) {
+  double v[1] = {0.0};
+  for (int64_t k = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; k < n; k += int64_t(gridDim.x) * blockDim.x)
+    v[0] = fma(q[k], q[k], v[0]);
+  double tot[1];
+  if (last_block_reduce<1>(v, partials, counter, tot)) S->true_rr = tot[0];
 }
 
 // Chronopoulos-Gear form of preconditioned CG: one product and one fused pair
@@ -1564,6 +1574,7 @@ int pcg_impl(int64_t n_brows, const int32_t* rp, const int32_t* ci, const VT* va
     return FEM_OK;
   };
   bool looped = false;
+  int64_t nbody_run = 0;  // kernels per body of the graph launched
   if (mg_graphs_enabled()) {
     // The whole iteration loop as one graph: a WHILE node whose body is one
     // iteration and whose condition the device sets from the state, so the
@@ -1598,9 +1609,8 @@ int pcg_impl(int64_t n_brows, const int32_t* rp, const int32_t* ci, const VT* va
     }
     if (exec != nullptr) {
       FEM_CUDA_TRY(cudaGraphLaunch(exec, st));
-      if ((rc = read_state()) != FEM_OK) return rc;
-      launch_counter().fetch_add(1 + int64_t(hs->loops) * nbody, std::memory_order_relaxed);
       looped = true;
+      nbody_run = nbody;
     }
   }
   if (!looped) {
@@ -1615,19 +1625,21 @@ int pcg_impl(int64_t n_brows, const int32_t* rp, const int32_t* ci, const VT* va
       launched += chunk;
     }
   }
-  const int status = hs->status;
-  const int iters = hs->iter;
-  const double bb = hs->bb;
-  // report the true residual ||b - A x||
+  // the true residual ||b - A x||, queued behind the iterations: one host
+  // wait per solve reads it with the loop's state
   mg_residual_kernel<VEC, VT, double><<<rg, kRowThreads, bsr_rows_smem(), st>>>(
       n_brows, rp, ci, vals, x, b, q, static_cast<const double*>(nullptr), static_cast<double*>(nullptr), nullptr, 0.0,
       static_cast<const double*>(nullptr));
   FEM_LAUNCH_CHECK();
   FEM_CUDA_TRY(cudaMemsetAsync(counter, 0, sizeof(unsigned), st));
-  pcg_init_kernel<VEC><<<vg, 256, 0, st>>>(n, q, b, partials, counter, S, rtol, atol);
+  pcg_true_rr_kernel<<<vg, 256, 0, st>>>(n, q, partials, counter, S);
   FEM_LAUNCH_CHECK();
   if ((rc = read_state()) != FEM_OK) return rc;
-  const double rr = hs->rr;
+  if (looped) launch_counter().fetch_add(1 + int64_t(hs->loops) * nbody_run, std::memory_order_relaxed);
+  const int status = hs->status;
+  const int iters = hs->iter;
+  const double bb = hs->bb;
+  const double rr = hs->true_rr;
   if (h_iters) *h_iters = iters;
   if (h_relres) *h_relres = bb > 0 ? std::sqrt(rr / bb) : std::sqrt(rr);
   if (status == PS_CONVERGED) return FEM_OK;
