@@ -453,6 +453,16 @@ FEM_API int fem_mg_vcycle_f64(int vec, int nlevels, const FemMGLevel* levels, in
                               double ratio, const double* d_rhs, double* d_z, void* stream);
 FEM_API int fem_mg_vcycle_f32(int vec, int nlevels, const FemMGLevel* levels, int nu, int coarse_steps,
                               double ratio, const float* d_rhs, float* d_z, void* stream);
+/* The V-cycle's coarse end (host query, no GPU work): *start = the first
+ * level (>= 1) from which fem_mg_vcycle_* and the multigrid CG run the rest
+ * of each V-cycle as one kernel on one CTA, its data in shared memory, and
+ * *smem_bytes = the shared memory it takes; *start = -1 (and 0 bytes) when
+ * every level runs as launches per step.  It depends on the levels' node
+ * counts, FP16 copies, dense inverse and nu, on the call's nu and
+ * coarse_steps, on fp32 (the hierarchy's type) and on FEM_MG_TAIL=0 in the
+ * environment, which turns it off. */
+FEM_API int fem_mg_tail_plan(int vec, int nlevels, const FemMGLevel* levels, int fp32, int nu, int coarse_steps,
+                             int* start, size_t* smem_bytes);
 /* CG on the FP64 operator (row_ptr, col_idx, vals) preconditioned by one
  * V-cycle per iteration, the linear solve of solver.py:63-92 / 261-284 with
  * a multigrid preconditioner.  levels_fp32 != 0: the hierarchy is FP32 (the

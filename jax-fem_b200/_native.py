@@ -94,6 +94,7 @@ _SIGS = {
     "fem_mg_setup_f32": (I32, [I32, I32, P, P, P, SZ, P]),
     "fem_mg_vcycle_f64": (I32, [I32, I32, P, I32, I32, F64, P, P, P]),
     "fem_mg_vcycle_f32": (I32, [I32, I32, P, I32, I32, F64, P, P, P]),
+    "fem_mg_tail_plan": (I32, [I32, I32, P, I32, I32, I32, IP, _c.POINTER(SZ)]),
     "fem_mg_pcg_workspace_bytes": (SZ, [I32, I64]),
     "fem_mg_pcg_solve": (I32, [I32, I64, P, P, P, P, P, F64, F64, I32, I32, I32, P, I32, I32, I32, F64, P, SZ, IP,
                                DP, P]),

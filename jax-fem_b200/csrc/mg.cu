@@ -1693,6 +1693,30 @@ extern "C" int fem_mg_vcycle_f32(int vec, int nlevels, const FemMGLevel* levels,
                   : vcycle_impl<1, float>(nlevels, levels, nu, coarse_steps, ratio, d_rhs, d_z, as_stream(stream));
 }
 
+extern "C" int fem_mg_tail_plan(int vec, int nlevels, const FemMGLevel* levels, int fp32, int nu, int coarse_steps,
+                                int* start, size_t* smem_bytes) {
+  FEM_CHECK_ARG(vec == 1 || vec == 3, "vec must be 1 or 3");
+  FEM_CHECK_ARG(nlevels >= 1 && nlevels <= 16 && levels != nullptr, "nlevels must be in [1, 16] with levels given");
+  FEM_CHECK_ARG(start != nullptr && smem_bytes != nullptr, "start and smem_bytes must not be NULL");
+  FEM_CHECK_ARG(nu >= 1 && nu <= 16 && coarse_steps >= 1 && coarse_steps <= 512, "nu in [1,16], coarse_steps in [1,512]");
+  int s = -1;
+  size_t bytes = 0;
+  auto plan = [&](auto tag) {
+    using T = decltype(tag);
+    s = vec == 3 ? tail_start<3, T>(nlevels, levels, nu, coarse_steps)
+                 : tail_start<1, T>(nlevels, levels, nu, coarse_steps);
+    if (s >= 0) {
+      TailArgs<T> a{};
+      bytes = vec == 3 ? tail_layout<3, T>(s, nlevels, levels, &a) : tail_layout<1, T>(s, nlevels, levels, &a);
+    }
+  };
+  if (fp32) plan(float{});
+  else plan(double{});
+  *start = s;
+  *smem_bytes = bytes;
+  return FEM_OK;
+}
+
 extern "C" size_t fem_mg_pcg_workspace_bytes(int vec, int64_t n_brows) { return pcg_workspace_bytes(vec, n_brows); }
 
 namespace fem {

@@ -166,6 +166,57 @@ def test_batched_confirmation_by_code(pkg):
     np.testing.assert_allclose(wrong, pts[:, 1] + pts[:, 0], rtol=1e-15)
 
 
+def _hierarchy_levels(nat, nodes, fp32, dense=True, half_level=0):
+    """A FemMGLevel array with the node counts of a lattice hierarchy and
+    stand-in (never dereferenced) pointers, for the host-only tail query."""
+    levels = (nat.FemMGLevel * len(nodes))()
+    for l, n in enumerate(nodes):
+        L = levels[l]
+        L.nodes[0], L.nodes[1], L.nodes[2] = n
+        L.n_brows = n[0] * n[1] * n[2]
+        for f in ("row_ptr", "col_idx", "stencil", "vals", "dinv", "x", "b", "r", "d0", "d1", "lmax"):
+            setattr(L, f, 4096 * (l + 1))
+        if l > 0:
+            L.cpos, L.ilo, L.whi = 4096, 4096, 4096
+    if dense:
+        levels[len(nodes) - 1].cinv = 8192
+    if fp32 and half_level is not None:
+        levels[half_level].vals_lo, levels[half_level].lo_scale = 8192, 8192
+    levels[0].nu = 1
+    return levels
+
+
+def test_mg_tail_plan(pkg):
+    """Where the V-cycle's coarse end runs as one CTA over shared memory, for
+    the 50^3 lattice hierarchy (51^3 ... 3^3 nodes): from the 5^3 level, in
+    the FP32 layout that ran on the B200 (167,632 bytes) and in FP64; not
+    when the smoothed coarsest level needs more Chebyshev steps than the
+    coefficient tables hold, nor through a level with an FP16 copy."""
+    import ctypes
+    nat = pkg._native
+    fn = nat.lib().fem_mg_tail_plan
+    nodes = [(51, 51, 51), (26, 26, 26), (14, 14, 14), (8, 8, 8), (5, 5, 5), (3, 3, 3)]
+
+    def plan(levels, fp32, nu=2, coarse_steps=8):
+        s, b = ctypes.c_int(-2), ctypes.c_size_t(1)
+        nat.check(fn(3, len(nodes), ctypes.byref(levels), int(fp32), nu, coarse_steps, ctypes.byref(s),
+                     ctypes.byref(b)), "tail_plan")
+        return s.value, b.value
+
+    assert plan(_hierarchy_levels(nat, nodes, True), True) == (4, 167632)
+    s64, b64 = plan(_hierarchy_levels(nat, nodes, False), False)
+    assert s64 == 4 and 167632 < b64 <= 226 * 1024 and b64 % 16 == 0
+    # a smoothed coarsest level: its steps must fit the tables (32)
+    assert plan(_hierarchy_levels(nat, nodes, True, dense=False), True, coarse_steps=8)[0] == 4
+    assert plan(_hierarchy_levels(nat, nodes, True, dense=False), True, coarse_steps=40) == (-1, 0)
+    # the dense inverse makes coarse_steps irrelevant
+    assert plan(_hierarchy_levels(nat, nodes, True), True, coarse_steps=40)[0] == 4
+    # a level with an FP16 copy stays with the per-level kernels
+    assert plan(_hierarchy_levels(nat, nodes, True, half_level=4), True) == (-1, 0)
+    with pytest.raises(nat.FEMNativeError):
+        plan(_hierarchy_levels(nat, nodes, True), True, nu=0)
+
+
 _XCUT = 2.0
 
 
