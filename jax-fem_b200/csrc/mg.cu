@@ -607,15 +607,16 @@ __global__ void dense_apply_kernel(int n, const double* __restrict__ inv, const 
 // The last levels of a hierarchy are small (the 50^3 lattice ends with 5^3
 // and 3^3 nodes) and each of their steps as a launch costs its completion
 // and the next launch's dependent loads, 3-5 us, for a few thousand FMAs.
-// When their patterns, values, Jacobi scaling and vectors fit in one CTA's
-// shared memory, the V-cycle from such a level s down runs as one kernel:
-// the level data are copied in once (before the kernel waits on its
-// predecessor: the restriction into level s writes vectors only), level s's
-// x, b, r and d0 after the wait, and the steps follow each other with
-// __syncthreads.  The steps are those of vcycle_level and smooth (the same
-// Chebyshev coefficients, transfers and dense coarsest solve); the row
-// products take one thread per unknown.  Level s's x goes back to global
-// memory at the end.
+// When their patterns, values, Jacobi scaling, vectors, Chebyshev
+// coefficient tables, transfer arrays and (where it fits) the dense coarsest
+// inverse fit in one CTA's shared memory, the V-cycle from such a level s
+// down runs as one kernel.  The restriction into level s releases it early
+// (pdl_trigger after its own wait), so the constant data are copied in while
+// that restriction runs; level s's x, b, r and d0 are read after the wait,
+// through L2.  The steps are those of vcycle_level and smooth (the same
+// coefficients, transfers and dense coarsest solve), separated by
+// __syncthreads; the row products take eight lanes per block row.  Level s's
+// x goes back to global memory at the end.
 constexpr int kTailThreads = 1024;
 constexpr int kTailMaxLevels = 4;
 constexpr int kTailMaxSteps = 33;  // Chebyshev coefficient tables: steps 0 .. max(nu, coarse_steps)
