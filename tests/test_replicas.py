@@ -44,3 +44,20 @@ def test_replica_max_over_ranks_gloo():
         res = dict(out)
     assert res[0][0] == pytest.approx(1.5) and res[1][0] == pytest.approx(1.5)
     assert res[1][1] is None  # the reference arm does no work off rank 0
+
+
+def test_reference_arm_covers_every_load_step():
+    """With fewer timed plus warm-up steps than load steps, the reference
+    arm solves the load steps it has not seen (measured, in the order of the
+    history), so its value is the sum of five measured load-step times."""
+    import math
+    import bench
+
+    class A:
+        n, steps, warmup = 4, 2, 1
+
+    out = bench.run_reference(A, 0, 1)
+    assert math.isfinite(out["value"]) and out["value"] > 0
+    assert out["config"]["load_steps_not_timed_as_steps"] == {1: "warm-up", 4: "after the timed steps",
+                                                              5: "after the timed steps"}
+    assert out["e2e"]["value"] == out["value"] == out["cpu_baseline"]["value"]
