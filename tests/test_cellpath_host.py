@@ -80,6 +80,15 @@ def test_multivariable_problem_layout(pkg):
     masks = [fe.dirichlet_arrays()[0] for fe in p.fes]
     assert masks[0].sum() == 3 * np.isclose(m10.points[:, 0], 0).sum()
     assert masks[1].sum() == np.isclose(m4.points[:, 0], 0).sum()
+    # the compact form the device refresh copies: both variables' constrained
+    # dofs at their global offsets, with the full arrays' values
+    arrays = [fe.dirichlet_arrays() for fe in p.fes]
+    full_mask = np.concatenate([a[0] for a in arrays])
+    full_vals = np.concatenate([a[1] for a in arrays])
+    dofs, vals = p._dirichlet_compact()
+    np.testing.assert_array_equal(dofs, np.flatnonzero(full_mask))
+    np.testing.assert_array_equal(vals, full_vals[dofs])
+    assert dofs.max() >= n_u  # the temperature variable's dofs come after the displacements
 
 
 def test_cell_path_selection(pkg):
