@@ -164,6 +164,13 @@ def test_batched_confirmation_by_code(pkg):
     np.testing.assert_array_equal(again, -2.0 * pts[:, 1])
     wrong = fe_mod._batched_or_pointwise(make(1.0, 1), (pts,), ())
     np.testing.assert_allclose(wrong, pts[:, 1] + pts[:, 0], rtol=1e-15)
+    # only plain numbers in the closure qualify for the two-point check
+    arr = np.array([1.0, 2.0])
+    flag = True
+    assert fe_mod._code_key(lambda p: arr[0] * p[0], ()) is None
+    assert fe_mod._code_key(lambda p: p[0] if flag else p[1], ()) is None
+    assert fe_mod._code_key(np.sin, ()) is None  # no Python code object
+    assert fe_mod._code_key(make(2.0), ()) is not None
 
 
 def _hierarchy_levels(nat, nodes, fp32, dense=True, half_level=0):
